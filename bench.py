@@ -1,0 +1,420 @@
+#!/usr/bin/env python
+"""Benchmark: final-pass vectors/s of the multipass PIV analysis on B200.
+
+Workload (default, `--workload c5`): a synthetic 4096x4096 uint16 (12-bit) particle-image pair
+(0.05 particles/px, diameters 2-4 px, vortex of 10 px plus 0.01/px shear, spurious particle
+clusters in 2 % of the final-pass cells of frame B), four passes 128 -> 64 -> 32 -> 16 px at 75 %
+overlap (1,042,441 vectors in the final pass), FP32 plain path, no preprocessing beyond the
+u16 -> f32 conversion, signal mask off, reference validation defaults.
+
+One step = one frame pair: both frames prepared from device-resident u16 samples, all four
+passes (placement, correlation, validation), final field in device memory. Inputs (2 x 32 MiB
+samples, 2 x 64 MiB prepared images, two alternating pairs) exceed the 126 MB L2 between steps.
+
+Printed JSON line (rank 0): value = whole-job final-pass vectors/s (device-resident inputs);
+e2e = the same through the C ABI with pinned HOST buffers (H2D of both frames and D2H of the
+final field inside the timed region); roofline of the correlation kernels; CPU baseline of the
+oracle port; SM clocks sampled during the timed region.
+
+`--impl reference` times the reference's CPU algorithm (the C++ restatement in oracle/, all host
+threads) on a bounded sample of the same workload; rank 0 only.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "final-pass vectors/sec on 1 B200 at <=0.01 px RMS (plain vs batched TC); p99 latency"
+
+WORKLOADS = {
+    "c5": dict(
+        name="4096x4096 u16 12-bit particle pair, 128->64->32->16 px at 75% overlap, FP32 plain",
+        h=4096, w=4096, bits=12, windows=[128, 64, 32, 16], overlap=0.75, final_iterations=1, ppp=0.05,
+        dmin=2.0, dmax=4.0, vmax=10.0, shear=0.01, outlier_frac=0.02, seed=5),
+    "c2": dict(
+        name="1024x1024 u16 12-bit Lamb-Oseen pair, 64->32->16 px at 50% overlap, FP32 plain",
+        h=1024, w=1024, bits=12, windows=[64, 32, 16], overlap=0.5, final_iterations=1, ppp=0.03,
+        dmin=3.0, dmax=3.0, vmax=8.0, shear=0.0, outlier_frac=0.0, seed=2, core=80.0),
+}
+
+
+def alg_flops(n):
+    """Algorithmic FLOPs per window of side n: three real 2-D FFTs (r2c A, r2c B, c2r) at
+    2.5 n^2 log2(n^2) each, the cross-spectrum multiply 6 n (n/2+1), the peak scan 2 n^2."""
+    return 7.5 * n * n * math.log2(n * n) + 6 * n * (n // 2 + 1) + 2 * n * n
+
+
+def make_inputs(wl, seed_offset=0):
+    from piv_b200 import synthetic as S
+    h, w = wl["h"], wl["w"]
+    field = S.vortex_shear_field(h, w, vmax=wl["vmax"], core=wl.get("core"), shear=wl["shear"])
+    cells = None
+    if wl["outlier_frac"] > 0:
+        import piv_b200 as P
+        g = P.Grid.new(h, w, wl["windows"][-1], wl["overlap"])
+        rng = np.random.default_rng(wl["seed"] + seed_offset)
+        k = rng.choice(len(g), int(round(wl["outlier_frac"] * len(g))), replace=False)
+        cells = np.stack([g.x0 + (k % g.nx) * g.step, g.y0 + (k // g.nx) * g.step], 1)
+    return S.baseline_pair(h, w, wl["seed"] + seed_offset, field, ppp=wl["ppp"], dmin=wl["dmin"], dmax=wl["dmax"],
+                           bits=wl["bits"], outlier_cells=cells, outlier_window=wl["windows"][-1])
+
+
+def piv_config(wl):
+    import piv_b200 as P
+    return P.PivConfig(windows=list(wl["windows"]), overlap=wl["overlap"], final_iterations=wl["final_iterations"])
+
+
+def final_vectors(wl, h=None, w=None):
+    import piv_b200 as P
+    return len(P.Grid.new(h or wl["h"], w or wl["w"], wl["windows"][-1], wl["overlap"]))
+
+
+def pass_windows(wl):
+    return list(wl["windows"]) + [wl["windows"][-1]] * (wl["final_iterations"] - 1)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.gpu_id)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except OSError:
+        return {}
+
+
+def fp32_peak_tflops(dev):
+    """Measured FP32 CUDA-core throughput: a cuBLAS SGEMM (TF32 off), best of 5, 8192^3."""
+    import torch
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        n = 8192
+        a = torch.randn(n, n, device=dev, dtype=torch.float32)
+        b = torch.randn(n, n, device=dev, dtype=torch.float32)
+        for _ in range(2):
+            torch.matmul(a, b)
+        torch.cuda.synchronize()
+        best = 1e30
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch.matmul(a, b)
+            e1.record()
+            e1.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        del a, b
+        return 2 * n ** 3 / (best * 1e-3) / 1e12
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
+
+
+def load_traffic(workload):
+    """Per-launch DRAM traffic of the correlation kernels from a committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", f"correlate_{workload}_traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f)
+    except OSError:
+        return None
+
+
+def cpu_baseline(wl, a, b, budget_s=12.0, crop=1024):
+    """Times the oracle port (reference operation order, OpenMP over windows) on a crop of the
+    workload with the same pass schedule; returns final-pass vectors/s and the sample used."""
+    from oracle import oracle as O
+    ch, cw = min(crop, wl["h"]), min(crop, wl["w"])
+    fa = O.u16_to_f32(np.ascontiguousarray(a[:ch, :cw])) if a.dtype == np.uint16 else O.u8_to_f32(a[:ch, :cw])
+    fb = O.u16_to_f32(np.ascontiguousarray(b[:ch, :cw])) if b.dtype == np.uint16 else O.u8_to_f32(b[:ch, :cw])
+    cfg = O.OracleConfig(tuple(wl["windows"]), wl["overlap"], wl["final_iterations"])
+    nthreads = os.cpu_count() or 1
+    vec = final_vectors(wl, ch, cw)
+    t0 = time.perf_counter()
+    reps = 0
+    while True:
+        O.analyze(cfg, fa, fb, nthreads=nthreads)
+        reps += 1
+        if time.perf_counter() - t0 >= budget_s:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": vec * reps / dt, "unit": "vectors/s", "cores": nthreads, "kind": "port",
+            "sample": f"{reps} x full {len(pass_windows(wl))}-pass analysis of a {ch}x{cw} crop ({vec} final vectors), "
+                      f"oracle/piv_oracle.cpp, {nthreads} OpenMP threads, {dt:.1f} s"}
+
+
+def run_reference(args, wl):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from piv_b200 import synthetic as S  # noqa: F401
+    a, b = make_inputs(wl)
+    for _ in range(args.warmup):
+        pass  # the oracle has no warm-up state; warm-up steps run no work
+    base = None
+    samples = []
+    for _ in range(args.steps):
+        r = cpu_baseline(wl, a, b, budget_s=max(1.0, args.ref_step_s), crop=args.ref_crop)
+        samples.append(r["value"])
+        base = r
+    v = float(np.median(samples))
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "vectors/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * final_vectors(wl) / v,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": wl["name"]},
+            "cpu_baseline": {"value": v, "unit": "vectors/s", "cores": base["cores"], "kind": "port",
+                             "sample": base["sample"]},
+            "e2e": {"value": v, "unit": "vectors/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c5", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-step-s", type=float, default=3.0)
+    ap.add_argument("--ref-crop", type=int, default=1024)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    wl = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        return run_reference(args, wl)
+
+    import torch
+    import torch.distributed as dist
+
+    import piv_b200 as P
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+
+    # ---------------------------------------------------------------- inputs (host, then device)
+    a0, b0 = make_inputs(wl, seed_offset=rank)
+    pairs_host = [(a0, b0), (np.ascontiguousarray(np.roll(a0, (37, 53), (0, 1))),
+                            np.ascontiguousarray(np.roll(b0, (37, 53), (0, 1))))]
+    dtype_code = P.api._dtype_code(a0)
+    h, w = a0.shape
+    # raw u16 samples on the device (held as int16 tensors: same bytes)
+    pairs_dev = [(torch.from_numpy(a.view(np.int16)).to(dev), torch.from_numpy(b.view(np.int16)).to(dev))
+                 for a, b in pairs_host]
+
+    an = P.PivAnalyzer(piv_config(wl), device=local)
+    stream = torch.cuda.Stream(device=dev)
+    an.set_stream(stream.cuda_stream)
+    fa, fb = an.frame(h, w), an.frame(h, w)
+    g = an.output_grid(h, w)
+    nvec = len(g)
+    out_dx = torch.empty(nvec, device=dev, dtype=torch.float32)
+    out_dy = torch.empty_like(out_dx)
+    out_ppr = torch.empty_like(out_dx)
+    out_fl = torch.empty(nvec, device=dev, dtype=torch.uint8)
+    out_sum = torch.empty(8, device=dev, dtype=torch.int64)
+    pre = P.RAW
+
+    def step(i):
+        ta, tb = pairs_dev[i % len(pairs_dev)]
+        fa.prepare_device(ta.data_ptr(), dtype_code, pre)
+        fb.prepare_device(tb.data_ptr(), dtype_code, pre)
+        an.analyze_device(fa, fb, out_dx.data_ptr(), out_dy.data_ptr(), out_ppr.data_ptr(), out_fl.data_ptr(),
+                          out_sum.data_ptr())
+
+    for i in range(args.warmup):
+        step(i)
+    stream.synchronize()
+
+    # ---------------------------------------------------------------- timed: device-resident
+    npass = len(pass_windows(wl))
+    an.set_profiling(True)
+    for p in range(npass):
+        an.profile(p)  # reset
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    gpu_uuid = str(torch.cuda.get_device_properties(local).uuid)
+    sampler = ClockSampler(gpu_uuid if gpu_uuid.startswith("GPU-") else f"GPU-{gpu_uuid}")
+    sampler.start()
+    time.sleep(0.3)
+    l0 = an.launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(args.steps):
+        step(i)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    launches = an.launches() - l0
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    corr = [an.profile(p) for p in range(npass)]
+    an.set_profiling(False)
+    ms_t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    ms_max = float(ms_t.item())
+    value = world * args.steps * nvec / (ms_max * 1e-3)
+
+    # ---------------------------------------------------------------- timed: end to end (host buffers)
+    pin = [(torch.from_numpy(a.view(np.int16)).pin_memory().numpy().view(np.uint16),
+            torch.from_numpy(b.view(np.int16)).pin_memory().numpy().view(np.uint16)) for a, b in pairs_host]
+    hdx = torch.empty(nvec, dtype=torch.float32).pin_memory().numpy().reshape(g.ny, g.nx)
+    hdy = torch.empty(nvec, dtype=torch.float32).pin_memory().numpy().reshape(g.ny, g.nx)
+    hppr = torch.empty(nvec, dtype=torch.float32).pin_memory().numpy().reshape(g.ny, g.nx)
+    hfl = torch.empty(nvec, dtype=torch.uint8).pin_memory().numpy().reshape(g.ny, g.nx)
+    lib = P.load_library()
+    import ctypes
+    summ = P._lib.PivSummaryC()
+    pc = pre._c()
+
+    def e2e_step(i):
+        ha, hb = pin[i % len(pin)]
+        for fr, hx in ((fa, ha), (fb, hb)):
+            P.api._check(lib.piv_frame_prepare(an._h, fr._h, ctypes.c_void_p(hx.ctypes.data), dtype_code,
+                                               ctypes.byref(pc), None))
+        P.api._check(lib.piv_analyze(an._h, fa._h, fb._h, ctypes.c_void_p(hdx.ctypes.data),
+                                     ctypes.c_void_p(hdy.ctypes.data), ctypes.c_void_p(hppr.ctypes.data),
+                                     ctypes.c_void_p(hfl.ctypes.data), ctypes.byref(summ)))
+
+    for i in range(args.warmup):
+        e2e_step(i)
+    e2e_steps = max(3, args.steps // 4)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    t_wall = time.perf_counter()
+    for i in range(e2e_steps):
+        e2e_step(i)
+    e3.record(stream)
+    e3.synchronize()
+    t_wall = time.perf_counter() - t_wall
+    ms2 = e2.elapsed_time(e3)
+    ms2_t = torch.tensor([ms2], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(ms2_t, op=dist.ReduceOp.MAX)
+    e2e_value = world * e2e_steps * nvec / (float(ms2_t.item()) * 1e-3)
+    h2d = sum(x.nbytes for x in pin[0])
+    d2h = hdx.nbytes + hdy.nbytes + hppr.nbytes + hfl.nbytes + 5 * 8
+
+    # ---------------------------------------------------------------- roofline (correlation kernels)
+    pw = pass_windows(wl)
+    flops = 0.0
+    kms = 0.0
+    klaunch = 0
+    per_pass = []
+    for p, n in enumerate(pw):
+        cells = len(an.pass_grid(h, w, p))
+        t_ms, cnt = corr[p]
+        f = cells * alg_flops(n)
+        per_pass.append({"window": n, "cells": cells, "ms_per_launch": t_ms / max(cnt, 1),
+                         "tflops": f / (t_ms / max(cnt, 1) * 1e-3) / 1e12 if cnt else None})
+        flops += f * cnt
+        kms += t_ms
+        klaunch += cnt
+    achieved = flops / (kms * 1e-3) / 1e12 if kms > 0 else 0.0
+    peaks = measured_peaks()
+    sgemm = fp32_peak_tflops(dev) if rank == 0 else None
+    traffic = load_traffic(args.workload)
+    roof = {"bound": "fp32", "achieved": achieved, "peak": sgemm, "unit": "TFLOP/s",
+            "frac": (achieved / sgemm) if sgemm else None,
+            "traffic": (traffic or {}).get("bytes_per_pair"),
+            "kernel": "correlate_kernel (all passes of one pair)",
+            "peak_source": "measured cuBLAS SGEMM (FP32 CUDA cores, TF32 off), 8192^3, in this run",
+            "per_pass": per_pass,
+            "hbm_peak_gbs": peaks.get("hbm_gbs")}
+
+    line = {"metric": METRIC, "value": value, "unit": "vectors/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": wl["name"], "image": f"{h}x{w} u16 ({wl['bits']}-bit)", "windows": pw,
+                       "overlap": wl["overlap"], "final_pass_vectors": nvec, "parallelism": f"replicas x{world}",
+                       "l2": "inputs > L2: 2 alternating pairs, 192 MiB of samples + prepared images per step"},
+            "e2e": {"value": e2e_value, "unit": "vectors/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
+                    "ms_per_step": float(ms2_t.item()) / e2e_steps, "wall_ms_per_step": 1e3 * t_wall / e2e_steps},
+            "gpu_launches": int(launches), "roofline": roof, "clocks": clocks}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(wl, a0, b0)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    an.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,207 @@
+/*
+ * piv_b200 — C ABI of the B200 PIV analysis path (libpivb200.so).
+ *
+ * Drop-in boundary for the reference's per-pair analysis (agoodman/piv, crate piv-core):
+ * plain pointers, sizes and status codes; no CUDA or torch types in any signature. Device
+ * pointers are plain `void*`/`float*` addresses in the current CUDA context; a stream is passed
+ * as `void*` (a cudaStream_t, NULL = the analyzer's own stream).
+ *
+ * Reference interfaces replaced (paths within the reference project):
+ *   PivAnalyzer::new(PivConfig)            rust/crates/piv-core/src/multipass.rs:91-119
+ *   PivAnalyzer::output_grid               rust/crates/piv-core/src/multipass.rs:126-133
+ *   PivAnalyzer::analyze                   rust/crates/piv-core/src/multipass.rs:136-138
+ *   PivAnalyzer::analyze_traced            rust/crates/piv-core/src/multipass.rs:142-150
+ *   PreparedFrame::new                     rust/crates/piv-core/src/preprocess.rs:138-158
+ *   BackgroundEstimator::{add,finish}      rust/crates/piv-core/src/preprocess.rs:47-72
+ *   Grid::new                              rust/crates/piv-core/src/grid.rs:20-44
+ *   validate                               rust/crates/piv-core/src/validate.rs:51-130
+ *   PivError                               rust/crates/piv-core/src/error.rs:4-19
+ *
+ * Output layout: fields are [ny * nx] row-major (ndarray standard layout of VectorField,
+ * field.rs:26-45); flags use the reference's bits (field.rs:6-20).
+ *
+ * Threading: an analyzer (and the frames created from it) is used by one host thread at a
+ * time, as PIVKit pools one analyzer per in-flight pair (swift/Sources/PIVKit/Run.swift:160).
+ */
+#ifndef PIV_B200_H
+#define PIV_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PIV_B200_ABI_VERSION 1
+
+/* Status codes. 1-4 mirror PivError's variants (error.rs:4-19). */
+typedef enum {
+    PIV_OK = 0,
+    PIV_ERR_CONFIG = 1,          /* PivError::Config */
+    PIV_ERR_SHAPE_MISMATCH = 2,  /* PivError::ShapeMismatch */
+    PIV_ERR_IMAGE_TOO_SMALL = 3, /* PivError::ImageTooSmall */
+    PIV_ERR_FRAME_RATE = 4,      /* PivError::FrameRate (not produced by this library) */
+    PIV_ERR_CUDA = 5,            /* a CUDA runtime call failed; see piv_last_error */
+    PIV_ERR_UNSUPPORTED = 6,     /* valid for the reference, not supported by this GPU path */
+    PIV_ERR_ARGUMENT = 7         /* NULL handle or malformed argument */
+} PivStatus;
+
+/* Flag bits (field.rs:6-20). */
+#define PIV_FLAG_NO_SIGNAL 0x01u
+#define PIV_FLAG_LOW_PPR 0x02u
+#define PIV_FLAG_MEDIAN_OUTLIER 0x04u
+#define PIV_FLAG_REPLACED 0x08u
+#define PIV_FLAG_OUT_OF_RANGE 0x10u
+#define PIV_FLAG_INVALID 0x17u
+
+typedef enum { PIV_DTYPE_U8 = 0, PIV_DTYPE_U16 = 1, PIV_DTYPE_F32 = 2 } PivDtype;
+
+/* PivConfig + MaskConfig + ValidationConfig (multipass.rs:22-63, validate.rs:7-37).
+ * Defaults of the reference: windows {96, 64}, overlap 0.5, final_iterations 2, mask 0/0,
+ * ppr 1.3, median threshold 2, median eps 0.1, replace 1. */
+typedef struct {
+    const int32_t* windows; /* window size per pass, largest first; each even and >= 8 */
+    int32_t n_windows;
+    float overlap;          /* in [0, 1) */
+    int32_t final_iterations; /* >= 1 */
+    float min_mean;         /* MaskConfig */
+    float min_std;
+    float ppr_threshold;    /* ValidationConfig */
+    float median_threshold;
+    float median_eps;
+    int32_t replace;
+    int32_t device;         /* CUDA device ordinal; -1 = current device */
+} PivConfigC;
+
+/* PreprocessConfig (preprocess.rs:5-29) plus the percentile clip of integer codes
+ * (clip_percentile in (0, 100]; 0 = off; not in the reference). Reference defaults:
+ * smooth_sigma 1, normalize_radius 4, normalize_eps 0.02. */
+typedef struct {
+    float smooth_sigma;
+    int32_t normalize_radius;
+    float normalize_eps;
+    double clip_percentile;
+} PivPreprocessC;
+
+/* Grid (grid.rs:8-16). */
+typedef struct {
+    int64_t window, step, nx, ny, x0, y0;
+} PivGridC;
+
+/* ValidationSummary (validate.rs:39-46). */
+typedef struct {
+    int64_t no_signal, low_ppr, median_outliers, out_of_range, replaced;
+} PivSummaryC;
+
+typedef struct PivAnalyzer PivAnalyzer;
+typedef struct PivFrame PivFrame;
+
+/* ----------------------------------------------------------------------------- library */
+int32_t piv_abi_version(void);
+/* Message of the last failure on this host thread (also set by creation failures). */
+const char* piv_last_error(void);
+/* Grid::new (grid.rs:20-44) — host arithmetic, no GPU needed. */
+int32_t piv_grid(int64_t height, int64_t width, int64_t window, float overlap, PivGridC* out);
+/* Validates a config exactly as PivAnalyzer::new does (multipass.rs:91-119), then the GPU
+ * restriction (window sizes 8, 12, 16, 24, 32, 48, 64, 96, 128). No GPU needed. */
+int32_t piv_check_config(const PivConfigC* cfg);
+
+/* ----------------------------------------------------------------------------- analyzer */
+/* PivAnalyzer::new (multipass.rs:91-119). */
+int32_t piv_analyzer_create(const PivConfigC* cfg, PivAnalyzer** out);
+void piv_analyzer_destroy(PivAnalyzer* an);
+/* Passes run per pair: windows + (final_iterations - 1) repeats of the last (multipass.rs:166-171). */
+int32_t piv_num_passes(const PivAnalyzer* an);
+/* PivAnalyzer::output_grid (multipass.rs:126-133). */
+int32_t piv_output_grid(const PivAnalyzer* an, int64_t height, int64_t width, PivGridC* out);
+/* Grid of pass `pass` for an image of the given size. */
+int32_t piv_pass_grid(const PivAnalyzer* an, int64_t height, int64_t width, int32_t pass, PivGridC* out);
+/* Use the caller's CUDA stream for all later work of this analyzer (NULL restores its own). */
+int32_t piv_analyzer_set_stream(PivAnalyzer* an, void* stream);
+/* Waits for the analyzer's stream. */
+int32_t piv_analyzer_sync(PivAnalyzer* an);
+/* Kernel launches issued by this analyzer since creation (launch accounting). */
+int64_t piv_analyzer_launches(const PivAnalyzer* an);
+/* Stage timing (no counterpart in the reference, which has only wall-clock splits,
+ * swift/Sources/PIVKit/Run.swift:189-196): when enabled, CUDA events bracket every correlation
+ * kernel; piv_analyzer_profile waits for the stream and returns, for pass `pass`, the summed
+ * kernel milliseconds and the number of launches timed since the last read (then resets). */
+int32_t piv_analyzer_set_profiling(PivAnalyzer* an, int32_t enable);
+int32_t piv_analyzer_profile(PivAnalyzer* an, int32_t pass, double* correlate_ms, int64_t* launches);
+
+/* ----------------------------------------------------------------------------- frames */
+/* Device-resident prepared frame of a fixed size (PreparedFrame, preprocess.rs:127-135). */
+int32_t piv_frame_create(PivAnalyzer* an, int64_t height, int64_t width, PivFrame** out);
+void piv_frame_destroy(PivFrame* f);
+/* PreparedFrame::new (preprocess.rs:138-158) from HOST samples: raw is height*width samples of
+ * `dtype` (u8 -> v/255, u16 -> v/65535 as decode.rs:227-234; f32 as is); background (nullable)
+ * is a host f32 image. Copies to the device and prepares asynchronously on the analyzer stream
+ * (raw and background must stay valid until piv_analyzer_sync or the next blocking call). */
+int32_t piv_frame_prepare(PivAnalyzer* an, PivFrame* f, const void* raw, int32_t dtype, const PivPreprocessC* pre,
+                          const float* background);
+/* Same with DEVICE pointers (raw, background). */
+int32_t piv_frame_prepare_device(PivAnalyzer* an, PivFrame* f, const void* raw_dev, int32_t dtype,
+                                 const PivPreprocessC* pre, const float* background_dev);
+/* Installs an already prepared image (host) and the background-subtracted intensity used by the
+ * signal mask (host; NULL = the image itself), as PIVKit's makeFrame(image:stats:) does. */
+int32_t piv_frame_set_prepared(PivAnalyzer* an, PivFrame* f, const float* image, const float* base);
+/* Copies the prepared image back to the host. */
+int32_t piv_frame_download(PivAnalyzer* an, const PivFrame* f, float* image);
+/* Device address of the prepared image (height*width f32, row-major). */
+const float* piv_frame_image_device(const PivFrame* f);
+
+/* BackgroundEstimator (preprocess.rs:41-72) on DEVICE data: `count` frames of height*width
+ * samples of `dtype`, mode 0 = per-pixel min, 1 = mean; output f32 image (device). */
+int32_t piv_background_device(PivAnalyzer* an, const void* frames_dev, int32_t dtype, int64_t count,
+                              int64_t height, int64_t width, int32_t mode, float* out_dev);
+
+/* ----------------------------------------------------------------------------- analysis */
+/* PivAnalyzer::analyze (multipass.rs:136-138): final field into HOST arrays of
+ * output_grid().nx*ny elements, summary of the final pass. Blocking. */
+int32_t piv_analyze(PivAnalyzer* an, const PivFrame* a, const PivFrame* b, float* dx, float* dy, float* peak_ratio,
+                    uint8_t* flags, PivSummaryC* summary);
+/* Same into DEVICE arrays, asynchronous on the analyzer's stream. summary_dev (nullable) is a
+ * device array of 5 uint64 counts (no_signal, low_ppr, median_outliers, out_of_range, replaced). */
+int32_t piv_analyze_device(PivAnalyzer* an, const PivFrame* a, const PivFrame* b, float* dx, float* dy,
+                           float* peak_ratio, uint8_t* flags, uint64_t* summary_dev);
+
+/* PivAnalyzer::analyze_traced (multipass.rs:142-150, PassTrace :72-81): HOST arrays holding
+ * every pass back to back (pass 0 cells, then pass 1 ...; piv_pass_grid gives each count):
+ * origins 4 floats per cell [ax, ay, bx, by]; raw_* before validation; the rest after.
+ * Any pointer may be NULL. Blocking. */
+typedef struct {
+    float* origins;
+    float* raw_dx;
+    float* raw_dy;
+    float* raw_peak_ratio;
+    uint8_t* raw_flags;
+    float* dx;
+    float* dy;
+    float* peak_ratio;
+    uint8_t* flags;
+} PivTraceC;
+int32_t piv_analyze_traced(PivAnalyzer* an, const PivFrame* a, const PivFrame* b, PivTraceC* trace,
+                           PivSummaryC* summary);
+
+/* ----------------------------------------------------------------------------- stage hooks
+ * Single stages on HOST arrays, for stage-by-stage parity (the reference's own split:
+ * multipass.rs:194-259 pass, validate.rs:51 validate; PIVKit's placeOnGPU/validateOnGPU,
+ * PIVAnalyzer.swift:318-348). Blocking. */
+/* Window origins of one pass from an optional predictor field (NULL = first pass). */
+int32_t piv_place_windows(PivAnalyzer* an, int64_t height, int64_t width, const PivGridC* grid,
+                          const PivGridC* pred_grid, const float* pred_dx, const float* pred_dy, float* origins);
+/* Correlates given origins (4 floats per cell) of frames a, b with window `window`, applying
+ * the analyzer's signal mask: raw dx, dy, peak ratio and flags (0 or NO_SIGNAL). */
+int32_t piv_correlate_origins(PivAnalyzer* an, const PivFrame* a, const PivFrame* b, int64_t window,
+                              const float* origins, int64_t ncells, float* dx, float* dy, float* peak_ratio,
+                              uint8_t* flags);
+/* validate (validate.rs:51-130) of a raw field with the analyzer's thresholds and
+ * max_displacement = windows[0] / 2. Outputs validated dx, dy, flags. */
+int32_t piv_validate_field(PivAnalyzer* an, int64_t ny, int64_t nx, const float* dx, const float* dy,
+                           const float* peak_ratio, const uint8_t* flags, float* out_dx, float* out_dy,
+                           uint8_t* out_flags, PivSummaryC* summary);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PIV_B200_H */

@@ -1,0 +1,122 @@
+"""ctypes binding of libpivb200.so (declarations mirror include/piv_b200.h).
+
+The library is built in-tree (piv_b200/libpivb200.so). There is no fallback: if it is missing or
+fails to load, every entry point raises.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpivb200.so")
+
+PIV_OK, PIV_ERR_CONFIG, PIV_ERR_SHAPE_MISMATCH, PIV_ERR_IMAGE_TOO_SMALL = 0, 1, 2, 3
+PIV_ERR_FRAME_RATE, PIV_ERR_CUDA, PIV_ERR_UNSUPPORTED, PIV_ERR_ARGUMENT = 4, 5, 6, 7
+PIV_DTYPE_U8, PIV_DTYPE_U16, PIV_DTYPE_F32 = 0, 1, 2
+
+# Every symbol include/piv_b200.h declares.
+EXPORTS = [
+    "piv_abi_version", "piv_last_error", "piv_grid", "piv_check_config",
+    "piv_analyzer_create", "piv_analyzer_destroy", "piv_num_passes", "piv_output_grid", "piv_pass_grid",
+    "piv_analyzer_set_stream", "piv_analyzer_sync", "piv_analyzer_launches", "piv_analyzer_set_profiling",
+    "piv_analyzer_profile",
+    "piv_frame_create", "piv_frame_destroy", "piv_frame_prepare", "piv_frame_prepare_device",
+    "piv_frame_set_prepared", "piv_frame_download", "piv_frame_image_device", "piv_background_device",
+    "piv_analyze", "piv_analyze_device", "piv_analyze_traced",
+    "piv_place_windows", "piv_correlate_origins", "piv_validate_field",
+]
+
+
+class PivConfigC(ctypes.Structure):
+    _fields_ = [
+        ("windows", ctypes.POINTER(ctypes.c_int32)),
+        ("n_windows", ctypes.c_int32),
+        ("overlap", ctypes.c_float),
+        ("final_iterations", ctypes.c_int32),
+        ("min_mean", ctypes.c_float),
+        ("min_std", ctypes.c_float),
+        ("ppr_threshold", ctypes.c_float),
+        ("median_threshold", ctypes.c_float),
+        ("median_eps", ctypes.c_float),
+        ("replace", ctypes.c_int32),
+        ("device", ctypes.c_int32),
+    ]
+
+
+class PivPreprocessC(ctypes.Structure):
+    _fields_ = [
+        ("smooth_sigma", ctypes.c_float),
+        ("normalize_radius", ctypes.c_int32),
+        ("normalize_eps", ctypes.c_float),
+        ("clip_percentile", ctypes.c_double),
+    ]
+
+
+class PivGridC(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int64) for n in ("window", "step", "nx", "ny", "x0", "y0")]
+
+
+class PivSummaryC(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int64) for n in ("no_signal", "low_ppr", "median_outliers", "out_of_range", "replaced")]
+
+
+class PivTraceC(ctypes.Structure):
+    _fields_ = [
+        ("origins", ctypes.c_void_p), ("raw_dx", ctypes.c_void_p), ("raw_dy", ctypes.c_void_p),
+        ("raw_peak_ratio", ctypes.c_void_p), ("raw_flags", ctypes.c_void_p), ("dx", ctypes.c_void_p),
+        ("dy", ctypes.c_void_p), ("peak_ratio", ctypes.c_void_p), ("flags", ctypes.c_void_p),
+    ]
+
+
+_lib = None
+
+
+def load():
+    """Loads libpivb200.so (no rebuild, no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"libpivb200.so is not built ({LIB_PATH}); run `python -c 'import __graft_entry__ as g; g.build()'`")
+    L = ctypes.CDLL(LIB_PATH)
+    vp, i32, i64, f32 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_float
+    P = ctypes.POINTER
+    sig = {
+        "piv_abi_version": ([], i32),
+        "piv_last_error": ([], ctypes.c_char_p),
+        "piv_grid": ([i64, i64, i64, f32, P(PivGridC)], i32),
+        "piv_check_config": ([P(PivConfigC)], i32),
+        "piv_analyzer_create": ([P(PivConfigC), P(vp)], i32),
+        "piv_analyzer_destroy": ([vp], None),
+        "piv_num_passes": ([vp], i32),
+        "piv_output_grid": ([vp, i64, i64, P(PivGridC)], i32),
+        "piv_pass_grid": ([vp, i64, i64, i32, P(PivGridC)], i32),
+        "piv_analyzer_set_stream": ([vp, vp], i32),
+        "piv_analyzer_sync": ([vp], i32),
+        "piv_analyzer_launches": ([vp], i64),
+        "piv_analyzer_set_profiling": ([vp, i32], i32),
+        "piv_analyzer_profile": ([vp, i32, P(ctypes.c_double), P(i64)], i32),
+        "piv_frame_create": ([vp, i64, i64, P(vp)], i32),
+        "piv_frame_destroy": ([vp], None),
+        "piv_frame_prepare": ([vp, vp, vp, i32, P(PivPreprocessC), vp], i32),
+        "piv_frame_prepare_device": ([vp, vp, vp, i32, P(PivPreprocessC), vp], i32),
+        "piv_frame_set_prepared": ([vp, vp, vp, vp], i32),
+        "piv_frame_download": ([vp, vp, vp], i32),
+        "piv_frame_image_device": ([vp], vp),
+        "piv_background_device": ([vp, vp, i32, i64, i64, i64, i32, vp], i32),
+        "piv_analyze": ([vp, vp, vp, vp, vp, vp, vp, P(PivSummaryC)], i32),
+        "piv_analyze_device": ([vp, vp, vp, vp, vp, vp, vp, vp], i32),
+        "piv_analyze_traced": ([vp, vp, vp, P(PivTraceC), P(PivSummaryC)], i32),
+        "piv_place_windows": ([vp, i64, i64, P(PivGridC), P(PivGridC), vp, vp, vp], i32),
+        "piv_correlate_origins": ([vp, vp, vp, i64, vp, i64, vp, vp, vp, vp], i32),
+        "piv_validate_field": ([vp, i64, i64, vp, vp, vp, vp, vp, vp, vp, P(PivSummaryC)], i32),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = L
+    return L
+
+
+def last_error():
+    return load().piv_last_error().decode(errors="replace")

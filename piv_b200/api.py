@@ -1,0 +1,453 @@
+"""Host-side mirror of the reference's `piv-core` interface over the CUDA path.
+
+Names, argument meaning, defaults and errors follow the reference:
+  PivConfig / MaskConfig        rust/crates/piv-core/src/multipass.rs:20-63
+  ValidationConfig              rust/crates/piv-core/src/validate.rs:7-37
+  PreprocessConfig              rust/crates/piv-core/src/preprocess.rs:5-29
+  Grid                          rust/crates/piv-core/src/grid.rs:5-75
+  VectorField, flags            rust/crates/piv-core/src/field.rs:5-95
+  PivError                      rust/crates/piv-core/src/error.rs:4-19
+  PivAnalyzer::{new, output_grid, analyze, analyze_traced}  multipass.rs:91-150
+  PreparedFrame::new            preprocess.rs:138-158
+
+Every computation runs in libpivb200.so on the GPU; this module only marshals arguments.
+"""
+import ctypes
+from dataclasses import dataclass, field as dc_field
+from typing import List, Optional, Tuple
+
+import numpy as np
+
+from . import _lib
+
+
+# --------------------------------------------------------------------------------- errors
+class PivError(Exception):
+    """PivError (error.rs:4-19)."""
+
+
+class ConfigError(PivError):
+    pass
+
+
+class ShapeMismatchError(PivError):
+    pass
+
+
+class ImageTooSmallError(PivError):
+    pass
+
+
+class CudaError(PivError):
+    pass
+
+
+class UnsupportedError(PivError):
+    pass
+
+
+def _check(status):
+    if status == _lib.PIV_OK:
+        return
+    msg = _lib.last_error()
+    cls = {
+        _lib.PIV_ERR_CONFIG: ConfigError,
+        _lib.PIV_ERR_SHAPE_MISMATCH: ShapeMismatchError,
+        _lib.PIV_ERR_IMAGE_TOO_SMALL: ImageTooSmallError,
+        _lib.PIV_ERR_CUDA: CudaError,
+        _lib.PIV_ERR_UNSUPPORTED: UnsupportedError,
+    }.get(status, PivError)
+    raise cls(msg)
+
+
+# --------------------------------------------------------------------------------- flags
+class flags:  # noqa: N801 - mirrors the reference's `flags` module (field.rs:6-20)
+    NO_SIGNAL = 1 << 0
+    LOW_PPR = 1 << 1
+    MEDIAN_OUTLIER = 1 << 2
+    REPLACED = 1 << 3
+    OUT_OF_RANGE = 1 << 4
+    INVALID = NO_SIGNAL | LOW_PPR | MEDIAN_OUTLIER | OUT_OF_RANGE
+
+
+# --------------------------------------------------------------------------------- configs
+@dataclass
+class MaskConfig:
+    min_mean: float = 0.0
+    min_std: float = 0.0
+
+
+@dataclass
+class ValidationConfig:
+    ppr_threshold: float = 1.3
+    median_threshold: float = 2.0
+    median_eps: float = 0.1
+    replace: bool = True
+
+
+@dataclass
+class PivConfig:
+    windows: List[int] = dc_field(default_factory=lambda: [96, 64])
+    overlap: float = 0.5
+    final_iterations: int = 2
+    mask: MaskConfig = dc_field(default_factory=MaskConfig)
+    validation: ValidationConfig = dc_field(default_factory=ValidationConfig)
+
+    def passes(self):
+        return list(self.windows) + [self.windows[-1]] * (self.final_iterations - 1)
+
+    def _c(self, device=-1):
+        w = (ctypes.c_int32 * max(len(self.windows), 1))(*[int(x) for x in self.windows])
+        c = _lib.PivConfigC(w, len(self.windows), float(self.overlap), int(self.final_iterations),
+                            float(self.mask.min_mean), float(self.mask.min_std),
+                            float(self.validation.ppr_threshold), float(self.validation.median_threshold),
+                            float(self.validation.median_eps), int(bool(self.validation.replace)), int(device))
+        c._keep = w
+        return c
+
+
+@dataclass
+class PreprocessConfig:
+    """PreprocessConfig (preprocess.rs:5-29) plus `clip_percentile` (0 = off; an addition)."""
+    smooth_sigma: float = 1.0
+    normalize_radius: int = 4
+    normalize_eps: float = 0.02
+    clip_percentile: float = 0.0
+
+    def _c(self):
+        return _lib.PivPreprocessC(float(self.smooth_sigma), int(self.normalize_radius), float(self.normalize_eps),
+                                   float(self.clip_percentile))
+
+
+RAW = PreprocessConfig(smooth_sigma=0.0, normalize_radius=0, normalize_eps=0.0)
+
+
+# --------------------------------------------------------------------------------- grid / field
+@dataclass(frozen=True)
+class Grid:
+    window: int
+    step: int
+    nx: int
+    ny: int
+    x0: int
+    y0: int
+
+    @staticmethod
+    def new(height, width, window, overlap) -> "Grid":
+        g = _lib.PivGridC()
+        _check(_lib.load().piv_grid(int(height), int(width), int(window), float(overlap), ctypes.byref(g)))
+        return Grid._from_c(g)
+
+    @staticmethod
+    def _from_c(g):
+        return Grid(g.window, g.step, g.nx, g.ny, g.x0, g.y0)
+
+    def _c(self):
+        return _lib.PivGridC(self.window, self.step, self.nx, self.ny, self.x0, self.y0)
+
+    def __len__(self):
+        return self.nx * self.ny
+
+    def window_origin(self, ix, iy):
+        return self.x0 + ix * self.step, self.y0 + iy * self.step
+
+    def center_x(self, ix):
+        return np.float32(self.x0 + ix * self.step) + (np.float32(self.window) - np.float32(1)) / np.float32(2)
+
+    def center_y(self, iy):
+        return np.float32(self.y0 + iy * self.step) + (np.float32(self.window) - np.float32(1)) / np.float32(2)
+
+    def xs(self):
+        return np.array([self.center_x(i) for i in range(self.nx)], np.float32)
+
+    def ys(self):
+        return np.array([self.center_y(i) for i in range(self.ny)], np.float32)
+
+
+@dataclass
+class VectorField:
+    """VectorField (field.rs:26-45): [ny, nx] arrays, NaN where NO_SIGNAL."""
+    grid: Grid
+    dx: np.ndarray
+    dy: np.ndarray
+    peak_ratio: np.ndarray
+    flags: np.ndarray
+
+    def valid_count(self):
+        return int(np.count_nonzero((self.flags & flags.INVALID) == 0))
+
+
+@dataclass
+class ValidationSummary:
+    no_signal: int = 0
+    low_ppr: int = 0
+    median_outliers: int = 0
+    out_of_range: int = 0
+    replaced: int = 0
+
+    @staticmethod
+    def _from_c(s):
+        return ValidationSummary(s.no_signal, s.low_ppr, s.median_outliers, s.out_of_range, s.replaced)
+
+    def as_dict(self):
+        return dict(no_signal=self.no_signal, low_ppr=self.low_ppr, median_outliers=self.median_outliers,
+                    out_of_range=self.out_of_range, replaced=self.replaced)
+
+
+@dataclass
+class PairResult:
+    field: VectorField
+    summary: ValidationSummary
+
+
+@dataclass
+class PassTrace:
+    """PassTrace (multipass.rs:72-81)."""
+    origins: np.ndarray
+    raw: VectorField
+    validated: VectorField
+
+
+def _ptr(a):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+def _dtype_code(a):
+    if a.dtype == np.uint8:
+        return _lib.PIV_DTYPE_U8
+    if a.dtype == np.uint16:
+        return _lib.PIV_DTYPE_U16
+    if a.dtype == np.float32:
+        return _lib.PIV_DTYPE_F32
+    raise PivError(f"unsupported sample type {a.dtype}")
+
+
+# --------------------------------------------------------------------------------- frames
+class PreparedFrame:
+    """A device-resident prepared frame (PreparedFrame, preprocess.rs:127-158)."""
+
+    def __init__(self, analyzer: "PivAnalyzer", height: int, width: int):
+        self.analyzer = analyzer
+        self.height, self.width = int(height), int(width)
+        h = ctypes.c_void_p()
+        _check(_lib.load().piv_frame_create(analyzer._h, self.height, self.width, ctypes.byref(h)))
+        self._h = h
+        self._keep = None
+
+    @staticmethod
+    def new(raw, cfg: PreprocessConfig = None, background=None, analyzer: "PivAnalyzer" = None) -> "PreparedFrame":
+        """PreparedFrame::new(raw, cfg, background) from host samples (u8, u16 or f32 in 0..1)."""
+        if analyzer is None:
+            raise PivError("a PreparedFrame lives on an analyzer's device: pass analyzer=")
+        raw = np.ascontiguousarray(raw)
+        f = PreparedFrame(analyzer, raw.shape[0], raw.shape[1])
+        f.prepare(raw, cfg, background)
+        return f
+
+    def prepare(self, raw, cfg: PreprocessConfig = None, background=None):
+        cfg = PreprocessConfig() if cfg is None else cfg
+        raw = np.ascontiguousarray(raw)
+        if raw.shape != (self.height, self.width):
+            raise ShapeMismatchError(f"frame shape {raw.shape} vs {(self.height, self.width)}")
+        bg = None if background is None else np.ascontiguousarray(background, dtype=np.float32)
+        pc = cfg._c()
+        _check(_lib.load().piv_frame_prepare(self.analyzer._h, self._h, _ptr(raw), _dtype_code(raw), ctypes.byref(pc),
+                                             _ptr(bg)))
+        self._keep = (raw, bg)  # host buffers stay alive until the next blocking call
+        self.analyzer.sync()
+        self._keep = None
+        return self
+
+    def prepare_device(self, raw_ptr: int, dtype: int, cfg: PreprocessConfig = None, background_ptr: Optional[int] = None):
+        """Asynchronous preparation from device memory (e.g. a torch CUDA tensor's data_ptr())."""
+        cfg = PreprocessConfig() if cfg is None else cfg
+        pc = cfg._c()
+        _check(_lib.load().piv_frame_prepare_device(self.analyzer._h, self._h, ctypes.c_void_p(raw_ptr), int(dtype),
+                                                    ctypes.byref(pc),
+                                                    None if background_ptr is None else ctypes.c_void_p(background_ptr)))
+        return self
+
+    def set_prepared(self, image, base=None):
+        image = np.ascontiguousarray(image, dtype=np.float32)
+        base = None if base is None else np.ascontiguousarray(base, dtype=np.float32)
+        _check(_lib.load().piv_frame_set_prepared(self.analyzer._h, self._h, _ptr(image), _ptr(base)))
+        return self
+
+    @property
+    def image(self) -> np.ndarray:
+        out = np.empty((self.height, self.width), np.float32)
+        _check(_lib.load().piv_frame_download(self.analyzer._h, self._h, _ptr(out)))
+        return out
+
+    def dim(self):
+        return self.height, self.width
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.load().piv_frame_destroy(self._h)
+            self._h = None
+        self.analyzer = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# --------------------------------------------------------------------------------- analyzer
+class PivAnalyzer:
+    """PivAnalyzer (multipass.rs:83-150) running every stage on one GPU."""
+
+    def __init__(self, cfg: PivConfig = None, device: int = -1):
+        self.cfg = PivConfig() if cfg is None else cfg
+        c = self.cfg._c(device)
+        h = ctypes.c_void_p()
+        _check(_lib.load().piv_analyzer_create(ctypes.byref(c), ctypes.byref(h)))
+        self._h = h
+
+    @staticmethod
+    def new(cfg: PivConfig) -> "PivAnalyzer":
+        return PivAnalyzer(cfg)
+
+    @staticmethod
+    def check_config(cfg: PivConfig):
+        c = cfg._c()
+        _check(_lib.load().piv_check_config(ctypes.byref(c)))
+
+    def config(self):
+        return self.cfg
+
+    def num_passes(self):
+        return _lib.load().piv_num_passes(self._h)
+
+    def output_grid(self, height, width) -> Grid:
+        g = _lib.PivGridC()
+        _check(_lib.load().piv_output_grid(self._h, int(height), int(width), ctypes.byref(g)))
+        return Grid._from_c(g)
+
+    def pass_grid(self, height, width, p) -> Grid:
+        g = _lib.PivGridC()
+        _check(_lib.load().piv_pass_grid(self._h, int(height), int(width), int(p), ctypes.byref(g)))
+        return Grid._from_c(g)
+
+    def sync(self):
+        _check(_lib.load().piv_analyzer_sync(self._h))
+
+    def set_stream(self, stream_ptr: Optional[int]):
+        _check(_lib.load().piv_analyzer_set_stream(self._h, None if not stream_ptr else ctypes.c_void_p(stream_ptr)))
+
+    def launches(self) -> int:
+        return int(_lib.load().piv_analyzer_launches(self._h))
+
+    def prepare(self, raw, cfg: PreprocessConfig = None, background=None) -> PreparedFrame:
+        return PreparedFrame.new(raw, cfg, background, analyzer=self)
+
+    def frame(self, height, width) -> PreparedFrame:
+        return PreparedFrame(self, height, width)
+
+    def analyze(self, a: PreparedFrame, b: PreparedFrame) -> PairResult:
+        """Displacement field from frame `a` to frame `b`, in pixels (multipass.rs:136-138)."""
+        g = self.output_grid(a.height, a.width) if a.dim() == b.dim() else None
+        if g is None:
+            raise ShapeMismatchError(f"frames have different shapes: {a.dim()} vs {b.dim()}")
+        dx, dy, ppr = (np.empty((g.ny, g.nx), np.float32) for _ in range(3))
+        fl = np.empty((g.ny, g.nx), np.uint8)
+        s = _lib.PivSummaryC()
+        _check(_lib.load().piv_analyze(self._h, a._h, b._h, _ptr(dx), _ptr(dy), _ptr(ppr), _ptr(fl), ctypes.byref(s)))
+        return PairResult(VectorField(g, dx, dy, ppr, fl), ValidationSummary._from_c(s))
+
+    def analyze_device(self, a: PreparedFrame, b: PreparedFrame, dx_ptr, dy_ptr, ppr_ptr, flags_ptr, summary_ptr=None):
+        """Final field into device buffers (addresses), asynchronous on the analyzer's stream."""
+        vp = ctypes.c_void_p
+        _check(_lib.load().piv_analyze_device(self._h, a._h, b._h, vp(dx_ptr), vp(dy_ptr), vp(ppr_ptr), vp(flags_ptr),
+                                              None if summary_ptr is None else vp(summary_ptr)))
+
+    def analyze_traced(self, a: PreparedFrame, b: PreparedFrame) -> Tuple[PairResult, List[PassTrace]]:
+        """Like analyze, but also returns what each pass did (multipass.rs:142-150)."""
+        if a.dim() != b.dim():
+            raise ShapeMismatchError(f"frames have different shapes: {a.dim()} vs {b.dim()}")
+        grids = [self.pass_grid(a.height, a.width, p) for p in range(self.num_passes())]
+        tot = sum(len(g) for g in grids)
+        arr = dict(origins=np.empty((tot, 4), np.float32), raw_dx=np.empty(tot, np.float32),
+                   raw_dy=np.empty(tot, np.float32), raw_peak_ratio=np.empty(tot, np.float32),
+                   raw_flags=np.empty(tot, np.uint8), dx=np.empty(tot, np.float32), dy=np.empty(tot, np.float32),
+                   peak_ratio=np.empty(tot, np.float32), flags=np.empty(tot, np.uint8))
+        tr = _lib.PivTraceC(*[arr[k].ctypes.data for k in ("origins", "raw_dx", "raw_dy", "raw_peak_ratio", "raw_flags",
+                                                           "dx", "dy", "peak_ratio", "flags")])
+        s = _lib.PivSummaryC()
+        _check(_lib.load().piv_analyze_traced(self._h, a._h, b._h, ctypes.byref(tr), ctypes.byref(s)))
+        traces, off = [], 0
+        for g in grids:
+            c = len(g)
+            sl, sh = slice(off, off + c), (g.ny, g.nx)
+            raw = VectorField(g, arr["raw_dx"][sl].reshape(sh), arr["raw_dy"][sl].reshape(sh),
+                              arr["raw_peak_ratio"][sl].reshape(sh), arr["raw_flags"][sl].reshape(sh))
+            val = VectorField(g, arr["dx"][sl].reshape(sh), arr["dy"][sl].reshape(sh),
+                              arr["peak_ratio"][sl].reshape(sh), arr["flags"][sl].reshape(sh))
+            traces.append(PassTrace(arr["origins"][sl], raw, val))
+            off += c
+        return PairResult(traces[-1].validated, ValidationSummary._from_c(s)), traces
+
+    # ------------------------------------------------------------------ stage hooks
+    def place_windows(self, height, width, grid: Grid, predictor: Optional[VectorField] = None) -> np.ndarray:
+        out = np.empty((len(grid), 4), np.float32)
+        gc = grid._c()
+        if predictor is None:
+            _check(_lib.load().piv_place_windows(self._h, int(height), int(width), ctypes.byref(gc), None, None, None,
+                                                 _ptr(out)))
+        else:
+            pg = predictor.grid._c()
+            pdx = np.ascontiguousarray(predictor.dx, np.float32)
+            pdy = np.ascontiguousarray(predictor.dy, np.float32)
+            _check(_lib.load().piv_place_windows(self._h, int(height), int(width), ctypes.byref(gc), ctypes.byref(pg),
+                                                 _ptr(pdx), _ptr(pdy), _ptr(out)))
+        return out
+
+    def correlate_origins(self, a: PreparedFrame, b: PreparedFrame, window: int, origins):
+        origins = np.ascontiguousarray(origins, np.float32).reshape(-1, 4)
+        c = origins.shape[0]
+        dx, dy, ppr = (np.empty(c, np.float32) for _ in range(3))
+        fl = np.empty(c, np.uint8)
+        _check(_lib.load().piv_correlate_origins(self._h, a._h, b._h, int(window), _ptr(origins), c, _ptr(dx), _ptr(dy),
+                                                 _ptr(ppr), _ptr(fl)))
+        return dx, dy, ppr, fl
+
+    def validate_field(self, dx, dy, peak_ratio, fl):
+        dx, dy, ppr = (np.ascontiguousarray(x, np.float32) for x in (dx, dy, peak_ratio))
+        fl = np.ascontiguousarray(fl, np.uint8)
+        ny, nx = dx.shape
+        ox, oy = np.empty_like(dx), np.empty_like(dy)
+        of = np.empty_like(fl)
+        s = _lib.PivSummaryC()
+        _check(_lib.load().piv_validate_field(self._h, ny, nx, _ptr(dx), _ptr(dy), _ptr(ppr), _ptr(fl), _ptr(ox),
+                                              _ptr(oy), _ptr(of), ctypes.byref(s)))
+        return ox, oy, of, ValidationSummary._from_c(s)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.load().piv_analyzer_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _profile_methods():
+    def set_profiling(self, enable=True):
+        _check(_lib.load().piv_analyzer_set_profiling(self._h, int(bool(enable))))
+
+    def profile(self, p):
+        """(summed correlation-kernel ms, launches) of pass `p` since the last read."""
+        ms, n = ctypes.c_double(), ctypes.c_int64()
+        _check(_lib.load().piv_analyzer_profile(self._h, int(p), ctypes.byref(ms), ctypes.byref(n)))
+        return ms.value, n.value
+
+    PivAnalyzer.set_profiling = set_profiling
+    PivAnalyzer.profile = profile
+
+
+_profile_methods()

@@ -1,0 +1,850 @@
+// C ABI of libpivb200.so: analyzer and frame handles, the multipass driver (multipass.rs:152-259)
+// on one CUDA stream with no host synchronisation between passes, and the stage hooks.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/piv_b200.h"
+#include "common.cuh"
+#include "kernels.h"
+
+using namespace pivb200;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+#define CUDA_TRY(expr)                                                                          \
+    do {                                                                                        \
+        cudaError_t _e = (expr);                                                                \
+        if (_e != cudaSuccess) return fail(PIV_ERR_CUDA, "%s: %s (%s:%d)", #expr, cudaGetErrorString(_e), __FILE__, __LINE__); \
+    } while (0)
+
+// Grid::new (grid.rs:20-44), f32 step arithmetic as the reference.
+int make_grid(int64_t h, int64_t w, int64_t window, float overlap, PivGridC* g) {
+    if (!(overlap >= 0.0f && overlap < 1.0f)) return fail(PIV_ERR_CONFIG, "overlap %g must be in [0, 1)", overlap);
+    if (window <= 0 || window > w || window > h)
+        return fail(PIV_ERR_IMAGE_TOO_SMALL, "image (%lldx%lld) is smaller than the %lld px interrogation window",
+                    (long long)h, (long long)w, (long long)window);
+    const float st = std::round((float)window * (1.0f - overlap));
+    int64_t step = st > 0.0f ? (int64_t)st : 0;
+    if (step < 1) step = 1;
+    g->window = window;
+    g->step = step;
+    g->nx = (w - window) / step + 1;
+    g->ny = (h - window) / step + 1;
+    g->x0 = (w - window - (g->nx - 1) * step) / 2;
+    g->y0 = (h - window - (g->ny - 1) * step) / 2;
+    return PIV_OK;
+}
+
+GridP to_gp(const PivGridC& g) {
+    return GridP{(int32_t)g.window, (int32_t)g.step, (int32_t)g.nx, (int32_t)g.ny, (int32_t)g.x0, (int32_t)g.y0};
+}
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+struct PassBuf {
+    PivGridC grid;
+    int64_t cells;
+    float4* origins;
+    uint8_t* status;
+    float* raw_dx;
+    float* raw_dy;
+    float* raw_ppr;
+    uint8_t* raw_flags;
+    uint8_t* f1;
+    uint8_t* f2;
+    float* dx;
+    float* dy;
+    uint8_t* flags;
+};
+
+std::mutex g_init_mu;
+std::vector<int> g_inited_devices;
+
+int ensure_device_init(int dev) {
+    std::lock_guard<std::mutex> lk(g_init_mu);
+    for (int d : g_inited_devices)
+        if (d == dev) return PIV_OK;
+    CUDA_TRY(corr_init_device());
+    g_inited_devices.push_back(dev);
+    return PIV_OK;
+}
+
+}  // namespace
+
+struct PivAnalyzer {
+    std::vector<int32_t> windows;
+    float overlap = 0.5f;
+    int32_t final_iterations = 2;
+    float min_mean = 0.0f, min_std = 0.0f;
+    float ppr_threshold = 1.3f, median_threshold = 2.0f, median_eps = 0.1f;
+    int32_t replace = 1;
+    int device = 0;
+    cudaStream_t own = nullptr;
+    cudaStream_t cur = nullptr;
+    // per-pair workspace, sized for (H, W)
+    int64_t H = 0, W = 0;
+    std::vector<PassBuf> passes;
+    void* arena = nullptr;
+    unsigned long long* d_counts = nullptr;
+    long long launches = 0;
+    // stage timing: per pass, pending (start, end) event pairs and the events to reuse
+    bool profiling = false;
+    std::vector<std::vector<std::pair<cudaEvent_t, cudaEvent_t>>> pending;
+    std::vector<cudaEvent_t> spare;
+
+    bool mask_trivial() const { return min_mean <= 0.0f && min_std <= 0.0f; }
+    std::vector<int32_t> pass_windows() const {
+        std::vector<int32_t> v = windows;
+        for (int i = 1; i < final_iterations; ++i) v.push_back(windows.back());
+        return v;
+    }
+};
+
+struct PivFrame {
+    PivAnalyzer* an = nullptr;
+    int device = 0;
+    int64_t H = 0, W = 0;
+    float* image = nullptr;
+    float* base = nullptr;  // background-subtracted intensity; aliases image when no blur/normalize
+    float* base_store = nullptr;
+    float* tmp = nullptr;
+    long long* sum = nullptr;
+    long long* sumsq = nullptr;
+    int* scales = nullptr;
+    unsigned int* words = nullptr;  // maxbits[2] + histogram scratch
+    bool stats_valid = false;
+    bool nonneg = false;
+    void* d_raw = nullptr;
+    size_t d_raw_bytes = 0;
+    float* d_bg = nullptr;
+};
+
+namespace {
+
+int check_cfg(const PivConfigC* c) {
+    // multipass.rs:91-119
+    if (!c) return fail(PIV_ERR_ARGUMENT, "null config");
+    if (c->n_windows <= 0 || !c->windows) return fail(PIV_ERR_CONFIG, "at least one window size is required");
+    for (int i = 0; i < c->n_windows; ++i)
+        if (c->windows[i] < 8 || c->windows[i] % 2 != 0)
+            return fail(PIV_ERR_CONFIG, "window size %d must be even and >= 8", c->windows[i]);
+    if (!(c->overlap >= 0.0f && c->overlap < 1.0f)) return fail(PIV_ERR_CONFIG, "overlap %g must be in [0, 1)", c->overlap);
+    if (c->final_iterations < 1) return fail(PIV_ERR_CONFIG, "final_iterations must be at least 1");
+    for (int i = 0; i < c->n_windows; ++i)
+        if (!corr_supported(c->windows[i]))
+            return fail(PIV_ERR_UNSUPPORTED, "window size %d is not supported on the GPU (8, 12, 16, 24, 32, 48, 64, 96, 128)",
+                        c->windows[i]);
+    return PIV_OK;
+}
+
+int use_device(PivAnalyzer* an) {
+    CUDA_TRY(cudaSetDevice(an->device));
+    return PIV_OK;
+}
+
+int ensure_workspace(PivAnalyzer* an, int64_t H, int64_t W) {
+    if (an->arena && an->H == H && an->W == W) return PIV_OK;
+    if (an->arena) {
+        CUDA_TRY(cudaStreamSynchronize(an->cur));
+        CUDA_TRY(cudaFree(an->arena));
+        an->arena = nullptr;
+    }
+    an->passes.clear();
+    const auto wins = an->pass_windows();
+    size_t total = align256(sizeof(unsigned long long) * 8);
+    for (int32_t n : wins) {
+        PassBuf pb{};
+        int st = make_grid(H, W, n, an->overlap, &pb.grid);
+        if (st) return st;
+        pb.cells = pb.grid.nx * pb.grid.ny;
+        if (pb.cells > (int64_t)1 << 30) return fail(PIV_ERR_UNSUPPORTED, "too many windows in one pass");
+        const size_t c = (size_t)pb.cells;
+        total += align256(16 * c) + align256(c) + 3 * align256(4 * c) + 3 * align256(c) + 2 * align256(4 * c) + align256(c);
+        an->passes.push_back(pb);
+    }
+    CUDA_TRY(cudaMalloc(&an->arena, total));
+    char* p = (char*)an->arena;
+    auto take = [&](size_t bytes) {
+        void* r = p;
+        p += align256(bytes);
+        return r;
+    };
+    an->d_counts = (unsigned long long*)take(sizeof(unsigned long long) * 8);
+    for (auto& pb : an->passes) {
+        const size_t c = (size_t)pb.cells;
+        pb.origins = (float4*)take(16 * c);
+        pb.status = (uint8_t*)take(c);
+        pb.raw_dx = (float*)take(4 * c);
+        pb.raw_dy = (float*)take(4 * c);
+        pb.raw_ppr = (float*)take(4 * c);
+        pb.raw_flags = (uint8_t*)take(c);
+        pb.f1 = (uint8_t*)take(c);
+        pb.f2 = (uint8_t*)take(c);
+        pb.dx = (float*)take(4 * c);
+        pb.dy = (float*)take(4 * c);
+        pb.flags = (uint8_t*)take(c);
+    }
+    an->H = H;
+    an->W = W;
+    return PIV_OK;
+}
+
+StatsView stats_of(const PivFrame* f) { return StatsView{f->sum, f->sumsq, f->scales, (int)f->H, (int)f->W}; }
+
+bool needs_stats(const PivAnalyzer* an, const PivFrame* f) { return !an->mask_trivial() || !f->nonneg; }
+
+int alloc_stats(PivFrame* f) {
+    if (f->sum) return PIV_OK;
+    const size_t cells = (size_t)(f->H + 1) * (size_t)(f->W + 1);
+    CUDA_TRY(cudaMalloc(&f->sum, sizeof(long long) * cells));
+    CUDA_TRY(cudaMalloc(&f->sumsq, sizeof(long long) * cells));
+    return PIV_OK;
+}
+
+// The multipass loop (multipass.rs:152-192): every pass is placement -> correlation ->
+// validation on the analyzer's stream; the predictor is the previous pass's validated field.
+int run_passes(PivAnalyzer* an, const PivFrame* a, const PivFrame* b) {
+    if (!a || !b) return fail(PIV_ERR_ARGUMENT, "null frame");
+    if (a->H != b->H || a->W != b->W)
+        return fail(PIV_ERR_SHAPE_MISMATCH, "frames have different shapes: (%lld, %lld) vs (%lld, %lld)", (long long)a->H,
+                    (long long)a->W, (long long)b->H, (long long)b->W);
+    int st = use_device(an);
+    if (st) return st;
+    st = ensure_workspace(an, a->H, a->W);
+    if (st) return st;
+    const bool use_stats = needs_stats(an, a) || needs_stats(an, b);
+    if (use_stats && !(a->stats_valid && b->stats_valid))
+        return fail(PIV_ERR_ARGUMENT, "frame statistics missing for the signal mask");
+    for (size_t i = 0; i < an->passes.size(); ++i) {
+        PassBuf& pb = an->passes[i];
+        PlaceParams pp{};
+        pp.grid = to_gp(pb.grid);
+        pp.H = (int)a->H;
+        pp.W = (int)a->W;
+        pp.has_pred = i > 0;
+        if (i > 0) {
+            pp.pgrid = to_gp(an->passes[i - 1].grid);
+            pp.pdx = an->passes[i - 1].dx;
+            pp.pdy = an->passes[i - 1].dy;
+        }
+        pp.origins = pb.origins;
+        pp.status = pb.status;
+        pp.use_stats = use_stats;
+        if (use_stats) {
+            pp.sa = stats_of(a);
+            pp.sb = stats_of(b);
+        }
+        pp.min_mean = an->min_mean;
+        pp.min_std = an->min_std;
+        CUDA_TRY(launch_place(pp, an->cur));
+        CorrParams cp{a->image, b->image, (int)a->H, (int)a->W, pb.origins, pb.status, (int)pb.cells,
+                      pb.raw_dx, pb.raw_dy, pb.raw_ppr, pb.raw_flags};
+        cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+        if (an->profiling) {
+            for (cudaEvent_t* ev : {&ev0, &ev1}) {
+                if (!an->spare.empty()) {
+                    *ev = an->spare.back();
+                    an->spare.pop_back();
+                } else {
+                    CUDA_TRY(cudaEventCreate(ev));
+                }
+            }
+            CUDA_TRY(cudaEventRecord(ev0, an->cur));
+        }
+        CUDA_TRY(launch_correlate((int)pb.grid.window, cp, an->cur));
+        if (an->profiling) {
+            CUDA_TRY(cudaEventRecord(ev1, an->cur));
+            if (an->pending.size() < an->passes.size()) an->pending.resize(an->passes.size());
+            an->pending[i].push_back({ev0, ev1});
+        }
+        ValidateParams vp{(int)pb.grid.nx, (int)pb.grid.ny, pb.raw_dx, pb.raw_dy, pb.raw_ppr, pb.raw_flags, pb.f1, pb.f2,
+                          pb.dx, pb.dy, pb.flags, (float)an->windows[0] / 2.0f, an->ppr_threshold,
+                          an->median_threshold, an->median_eps, an->replace};
+        CUDA_TRY(launch_validate(vp, an->cur));
+        an->launches += 1 + kCorrLaunches + kValidateLaunches;
+    }
+    const PassBuf& last = an->passes.back();
+    CUDA_TRY(launch_summary(last.flags, (int)last.cells, an->d_counts, an->cur));
+    an->launches += kSummaryLaunches;
+    return PIV_OK;
+}
+
+int copy_summary(PivAnalyzer* an, PivSummaryC* s) {
+    if (!s) return PIV_OK;
+    unsigned long long c[5];
+    CUDA_TRY(cudaMemcpyAsync(c, an->d_counts, sizeof(c), cudaMemcpyDeviceToHost, an->cur));
+    CUDA_TRY(cudaStreamSynchronize(an->cur));
+    s->no_signal = (int64_t)c[0];
+    s->low_ppr = (int64_t)c[1];
+    s->median_outliers = (int64_t)c[2];
+    s->out_of_range = (int64_t)c[3];
+    s->replaced = (int64_t)c[4];
+    return PIV_OK;
+}
+
+size_t dtype_size(int32_t dtype) {
+    switch (dtype) {
+        case PIV_DTYPE_U8: return 1;
+        case PIV_DTYPE_U16: return 2;
+        case PIV_DTYPE_F32: return 4;
+        default: return 0;
+    }
+}
+
+int prepare_common(PivAnalyzer* an, PivFrame* f, const void* raw_dev, int32_t dtype, const PivPreprocessC* pre,
+                   const float* bg_dev) {
+    PivPreprocessC dflt{1.0f, 4, 0.02f, 0.0};
+    if (!pre) pre = &dflt;
+    if (pre->clip_percentile > 0.0 && dtype == PIV_DTYPE_F32)
+        return fail(PIV_ERR_UNSUPPORTED, "percentile clipping needs integer (u8/u16) samples");
+    if (pre->normalize_radius > 16) return fail(PIV_ERR_UNSUPPORTED, "normalize_radius > 16 is not supported");
+    if (pre->smooth_sigma > 0.0f && std::ceil(3.0f * pre->smooth_sigma) > 32.0f)
+        return fail(PIV_ERR_UNSUPPORTED, "smooth_sigma > 32/3 is not supported");
+    const bool chain = pre->smooth_sigma > 0.0f || pre->normalize_radius > 0;
+    f->nonneg = dtype != PIV_DTYPE_F32 || bg_dev != nullptr;
+    const size_t n = (size_t)f->H * (size_t)f->W;
+    if (chain && !f->base_store) CUDA_TRY(cudaMalloc(&f->base_store, sizeof(float) * n));
+    if (pre->smooth_sigma > 0.0f && pre->normalize_radius > 0 && !f->tmp) CUDA_TRY(cudaMalloc(&f->tmp, sizeof(float) * n));
+    f->base = chain ? f->base_store : f->image;
+    const bool stats = needs_stats(an, f);
+    if (stats) {
+        int st = alloc_stats(f);
+        if (st) return st;
+    }
+    PrepParams pp{};
+    pp.H = (int)f->H;
+    pp.W = (int)f->W;
+    pp.raw = raw_dev;
+    pp.raw_type = dtype == PIV_DTYPE_U8 ? RAW_U8 : (dtype == PIV_DTYPE_U16 ? RAW_U16 : RAW_F32);
+    pp.background = bg_dev;
+    pp.clip_percentile_on = pre->clip_percentile > 0.0;
+    pp.clip_percentile = pre->clip_percentile;
+    pp.hist = f->words + 4;
+    pp.base = f->base;
+    pp.image = f->image;
+    pp.tmp = f->tmp;
+    pp.smooth_sigma = pre->smooth_sigma;
+    pp.normalize_radius = pre->normalize_radius;
+    pp.normalize_eps = pre->normalize_eps;
+    pp.build_stats = stats;
+    pp.sum = f->sum;
+    pp.sumsq = f->sumsq;
+    pp.scales = f->scales;
+    pp.maxbits = f->words;
+    int nl = 0;
+    CUDA_TRY(launch_prepare(pp, an->cur, &nl));
+    an->launches += nl;
+    f->stats_valid = stats;
+    return PIV_OK;
+}
+
+int stage_raw(PivFrame* f, size_t bytes) {
+    if (f->d_raw_bytes >= bytes) return PIV_OK;
+    if (f->d_raw) CUDA_TRY(cudaFree(f->d_raw));
+    f->d_raw = nullptr;
+    f->d_raw_bytes = 0;
+    CUDA_TRY(cudaMalloc(&f->d_raw, bytes));
+    f->d_raw_bytes = bytes;
+    return PIV_OK;
+}
+
+__global__ void background_kernel(const void* frames, int dtype, long long count, long long npix, int mode, float* out) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < npix; i += (long long)gridDim.x * blockDim.x) {
+        float acc = 0.0f;
+        for (long long k = 0; k < count; ++k) {
+            float v;
+            if (dtype == PIV_DTYPE_U8)
+                v = __fdiv_rn((float)((const uint8_t*)frames)[k * npix + i], 255.0f);
+            else if (dtype == PIV_DTYPE_U16)
+                v = __fdiv_rn((float)((const uint16_t*)frames)[k * npix + i], 65535.0f);
+            else
+                v = ((const float*)frames)[k * npix + i];
+            if (k == 0)
+                acc = v;
+            else if (mode == 0)
+                acc = fminf(acc, v);
+            else
+                acc = __fadd_rn(acc, v);
+        }
+        if (mode == 1) acc = __fdiv_rn(acc, (float)count);
+        out[i] = acc;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t piv_abi_version(void) { return PIV_B200_ABI_VERSION; }
+
+const char* piv_last_error(void) { return g_last_error.c_str(); }
+
+int32_t piv_grid(int64_t height, int64_t width, int64_t window, float overlap, PivGridC* out) {
+    if (!out) return fail(PIV_ERR_ARGUMENT, "null output");
+    return make_grid(height, width, window, overlap, out);
+}
+
+int32_t piv_check_config(const PivConfigC* cfg) { return check_cfg(cfg); }
+
+int32_t piv_analyzer_create(const PivConfigC* cfg, PivAnalyzer** out) {
+    if (!out) return fail(PIV_ERR_ARGUMENT, "null output");
+    *out = nullptr;
+    int st = check_cfg(cfg);
+    if (st) return st;
+    int dev = cfg->device;
+    if (dev < 0) CUDA_TRY(cudaGetDevice(&dev));
+    CUDA_TRY(cudaSetDevice(dev));
+    st = ensure_device_init(dev);
+    if (st) return st;
+    PivAnalyzer* an = new PivAnalyzer();
+    an->windows.assign(cfg->windows, cfg->windows + cfg->n_windows);
+    an->overlap = cfg->overlap;
+    an->final_iterations = cfg->final_iterations;
+    an->min_mean = cfg->min_mean;
+    an->min_std = cfg->min_std;
+    an->ppr_threshold = cfg->ppr_threshold;
+    an->median_threshold = cfg->median_threshold;
+    an->median_eps = cfg->median_eps;
+    an->replace = cfg->replace;
+    an->device = dev;
+    cudaError_t e = cudaStreamCreateWithFlags(&an->own, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete an;
+        return fail(PIV_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
+    }
+    an->cur = an->own;
+    *out = an;
+    return PIV_OK;
+}
+
+void piv_analyzer_destroy(PivAnalyzer* an) {
+    if (!an) return;
+    cudaSetDevice(an->device);
+    // Only the analyzer's own stream is known to be alive here; cudaFree waits for the device.
+    if (an->own) cudaStreamSynchronize(an->own);
+    for (auto& v : an->pending)
+        for (auto& pr : v) {
+            cudaEventDestroy(pr.first);
+            cudaEventDestroy(pr.second);
+        }
+    for (cudaEvent_t e : an->spare) cudaEventDestroy(e);
+    if (an->arena) cudaFree(an->arena);
+    if (an->own) cudaStreamDestroy(an->own);
+    delete an;
+}
+
+int32_t piv_num_passes(const PivAnalyzer* an) {
+    if (!an) return fail(PIV_ERR_ARGUMENT, "null analyzer");
+    return (int32_t)an->pass_windows().size();
+}
+
+int32_t piv_output_grid(const PivAnalyzer* an, int64_t height, int64_t width, PivGridC* out) {
+    if (!an || !out) return fail(PIV_ERR_ARGUMENT, "null argument");
+    return make_grid(height, width, an->windows.back(), an->overlap, out);
+}
+
+int32_t piv_pass_grid(const PivAnalyzer* an, int64_t height, int64_t width, int32_t pass, PivGridC* out) {
+    if (!an || !out) return fail(PIV_ERR_ARGUMENT, "null argument");
+    const auto w = an->pass_windows();
+    if (pass < 0 || pass >= (int32_t)w.size()) return fail(PIV_ERR_ARGUMENT, "pass %d out of range", pass);
+    return make_grid(height, width, w[pass], an->overlap, out);
+}
+
+int32_t piv_analyzer_set_stream(PivAnalyzer* an, void* stream) {
+    if (!an) return fail(PIV_ERR_ARGUMENT, "null analyzer");
+    an->cur = stream ? (cudaStream_t)stream : an->own;
+    return PIV_OK;
+}
+
+int32_t piv_analyzer_sync(PivAnalyzer* an) {
+    if (!an) return fail(PIV_ERR_ARGUMENT, "null analyzer");
+    int st = use_device(an);
+    if (st) return st;
+    CUDA_TRY(cudaStreamSynchronize(an->cur));
+    return PIV_OK;
+}
+
+int64_t piv_analyzer_launches(const PivAnalyzer* an) { return an ? an->launches : 0; }
+
+int32_t piv_analyzer_set_profiling(PivAnalyzer* an, int32_t enable) {
+    if (!an) return fail(PIV_ERR_ARGUMENT, "null analyzer");
+    an->profiling = enable != 0;
+    return PIV_OK;
+}
+
+int32_t piv_analyzer_profile(PivAnalyzer* an, int32_t pass, double* correlate_ms, int64_t* launches) {
+    if (!an) return fail(PIV_ERR_ARGUMENT, "null analyzer");
+    int st = use_device(an);
+    if (st) return st;
+    double ms = 0.0;
+    int64_t n = 0;
+    if (pass >= 0 && pass < (int32_t)an->pending.size()) {
+        CUDA_TRY(cudaStreamSynchronize(an->cur));
+        for (auto& pr : an->pending[pass]) {
+            float t = 0.0f;
+            CUDA_TRY(cudaEventElapsedTime(&t, pr.first, pr.second));
+            ms += t;
+            ++n;
+            an->spare.push_back(pr.first);
+            an->spare.push_back(pr.second);
+        }
+        an->pending[pass].clear();
+    }
+    if (correlate_ms) *correlate_ms = ms;
+    if (launches) *launches = n;
+    return PIV_OK;
+}
+
+int32_t piv_frame_create(PivAnalyzer* an, int64_t height, int64_t width, PivFrame** out) {
+    if (!an || !out) return fail(PIV_ERR_ARGUMENT, "null argument");
+    *out = nullptr;
+    if (height <= 0 || width <= 0 || height > (1 << 16) || width > (1 << 16))
+        return fail(PIV_ERR_ARGUMENT, "frame size %lldx%lld out of range", (long long)height, (long long)width);
+    int st = use_device(an);
+    if (st) return st;
+    PivFrame* f = new PivFrame();
+    f->an = an;
+    f->device = an->device;
+    f->H = height;
+    f->W = width;
+    const size_t n = (size_t)height * (size_t)width;
+    cudaError_t e = cudaMalloc(&f->image, sizeof(float) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&f->words, sizeof(unsigned int) * (4 + 512 + 4));
+    if (e == cudaSuccess) e = cudaMalloc(&f->scales, sizeof(int) * 2);
+    if (e != cudaSuccess) {
+        piv_frame_destroy(f);
+        return fail(PIV_ERR_CUDA, "frame allocation: %s", cudaGetErrorString(e));
+    }
+    f->base = f->image;
+    *out = f;
+    return PIV_OK;
+}
+
+void piv_frame_destroy(PivFrame* f) {
+    if (!f) return;
+    // A frame may outlive its analyzer: touch nothing of it. cudaFree synchronises the device.
+    cudaSetDevice(f->device);
+    cudaFree(f->image);
+    cudaFree(f->base_store);
+    cudaFree(f->tmp);
+    cudaFree(f->sum);
+    cudaFree(f->sumsq);
+    cudaFree(f->scales);
+    cudaFree(f->words);
+    cudaFree(f->d_raw);
+    cudaFree(f->d_bg);
+    delete f;
+}
+
+int32_t piv_frame_prepare_device(PivAnalyzer* an, PivFrame* f, const void* raw_dev, int32_t dtype,
+                                 const PivPreprocessC* pre, const float* background_dev) {
+    if (!an || !f || !raw_dev) return fail(PIV_ERR_ARGUMENT, "null argument");
+    if (!dtype_size(dtype)) return fail(PIV_ERR_ARGUMENT, "unknown dtype %d", dtype);
+    int st = use_device(an);
+    if (st) return st;
+    return prepare_common(an, f, raw_dev, dtype, pre, background_dev);
+}
+
+int32_t piv_frame_prepare(PivAnalyzer* an, PivFrame* f, const void* raw, int32_t dtype, const PivPreprocessC* pre,
+                          const float* background) {
+    if (!an || !f || !raw) return fail(PIV_ERR_ARGUMENT, "null argument");
+    const size_t es = dtype_size(dtype);
+    if (!es) return fail(PIV_ERR_ARGUMENT, "unknown dtype %d", dtype);
+    int st = use_device(an);
+    if (st) return st;
+    const size_t n = (size_t)f->H * (size_t)f->W;
+    st = stage_raw(f, es * n);
+    if (st) return st;
+    CUDA_TRY(cudaMemcpyAsync(f->d_raw, raw, es * n, cudaMemcpyHostToDevice, an->cur));
+    const float* bg = nullptr;
+    if (background) {
+        if (!f->d_bg) CUDA_TRY(cudaMalloc(&f->d_bg, sizeof(float) * n));
+        CUDA_TRY(cudaMemcpyAsync(f->d_bg, background, sizeof(float) * n, cudaMemcpyHostToDevice, an->cur));
+        bg = f->d_bg;
+    }
+    return prepare_common(an, f, f->d_raw, dtype, pre, bg);
+}
+
+int32_t piv_frame_set_prepared(PivAnalyzer* an, PivFrame* f, const float* image, const float* base) {
+    if (!an || !f || !image) return fail(PIV_ERR_ARGUMENT, "null argument");
+    int st = use_device(an);
+    if (st) return st;
+    const size_t n = (size_t)f->H * (size_t)f->W;
+    CUDA_TRY(cudaMemcpyAsync(f->image, image, sizeof(float) * n, cudaMemcpyHostToDevice, an->cur));
+    f->nonneg = false;  // unknown: statistics are always built
+    st = alloc_stats(f);
+    if (st) return st;
+    const float* bsrc = f->image;
+    if (base) {
+        if (!f->base_store) CUDA_TRY(cudaMalloc(&f->base_store, sizeof(float) * n));
+        CUDA_TRY(cudaMemcpyAsync(f->base_store, base, sizeof(float) * n, cudaMemcpyHostToDevice, an->cur));
+        bsrc = f->base_store;
+    }
+    f->base = const_cast<float*>(bsrc);
+    int nl = 0;
+    CUDA_TRY(launch_stats(bsrc, (int)f->H, (int)f->W, f->sum, f->sumsq, f->scales, f->words, an->cur, &nl));
+    an->launches += nl;
+    f->stats_valid = true;
+    CUDA_TRY(cudaStreamSynchronize(an->cur));
+    return PIV_OK;
+}
+
+int32_t piv_frame_download(PivAnalyzer* an, const PivFrame* f, float* image) {
+    if (!an || !f || !image) return fail(PIV_ERR_ARGUMENT, "null argument");
+    int st = use_device(an);
+    if (st) return st;
+    CUDA_TRY(cudaMemcpyAsync(image, f->image, sizeof(float) * f->H * f->W, cudaMemcpyDeviceToHost, an->cur));
+    CUDA_TRY(cudaStreamSynchronize(an->cur));
+    return PIV_OK;
+}
+
+const float* piv_frame_image_device(const PivFrame* f) { return f ? f->image : nullptr; }
+
+int32_t piv_background_device(PivAnalyzer* an, const void* frames_dev, int32_t dtype, int64_t count, int64_t height,
+                              int64_t width, int32_t mode, float* out_dev) {
+    if (!an || !frames_dev || !out_dev || count <= 0) return fail(PIV_ERR_ARGUMENT, "bad argument");
+    if (!dtype_size(dtype)) return fail(PIV_ERR_ARGUMENT, "unknown dtype %d", dtype);
+    int st = use_device(an);
+    if (st) return st;
+    const long long npix = (long long)height * width;
+    background_kernel<<<(int)std::min<long long>((npix + 255) / 256, 148 * 16), 256, 0, an->cur>>>(
+        frames_dev, dtype, count, npix, mode, out_dev);
+    CUDA_TRY(cudaGetLastError());
+    an->launches += 1;
+    return PIV_OK;
+}
+
+int32_t piv_analyze_device(PivAnalyzer* an, const PivFrame* a, const PivFrame* b, float* dx, float* dy,
+                           float* peak_ratio, uint8_t* flags, uint64_t* summary_dev) {
+    if (!an) return fail(PIV_ERR_ARGUMENT, "null analyzer");
+    int st = run_passes(an, a, b);
+    if (st) return st;
+    const PassBuf& last = an->passes.back();
+    const size_t c = (size_t)last.cells;
+    if (dx) CUDA_TRY(cudaMemcpyAsync(dx, last.dx, 4 * c, cudaMemcpyDeviceToDevice, an->cur));
+    if (dy) CUDA_TRY(cudaMemcpyAsync(dy, last.dy, 4 * c, cudaMemcpyDeviceToDevice, an->cur));
+    if (peak_ratio) CUDA_TRY(cudaMemcpyAsync(peak_ratio, last.raw_ppr, 4 * c, cudaMemcpyDeviceToDevice, an->cur));
+    if (flags) CUDA_TRY(cudaMemcpyAsync(flags, last.flags, c, cudaMemcpyDeviceToDevice, an->cur));
+    if (summary_dev)
+        CUDA_TRY(cudaMemcpyAsync(summary_dev, an->d_counts, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToDevice, an->cur));
+    return PIV_OK;
+}
+
+int32_t piv_analyze(PivAnalyzer* an, const PivFrame* a, const PivFrame* b, float* dx, float* dy, float* peak_ratio,
+                    uint8_t* flags, PivSummaryC* summary) {
+    if (!an) return fail(PIV_ERR_ARGUMENT, "null analyzer");
+    int st = run_passes(an, a, b);
+    if (st) return st;
+    const PassBuf& last = an->passes.back();
+    const size_t c = (size_t)last.cells;
+    if (dx) CUDA_TRY(cudaMemcpyAsync(dx, last.dx, 4 * c, cudaMemcpyDeviceToHost, an->cur));
+    if (dy) CUDA_TRY(cudaMemcpyAsync(dy, last.dy, 4 * c, cudaMemcpyDeviceToHost, an->cur));
+    if (peak_ratio) CUDA_TRY(cudaMemcpyAsync(peak_ratio, last.raw_ppr, 4 * c, cudaMemcpyDeviceToHost, an->cur));
+    if (flags) CUDA_TRY(cudaMemcpyAsync(flags, last.flags, c, cudaMemcpyDeviceToHost, an->cur));
+    st = copy_summary(an, summary);
+    if (st) return st;
+    CUDA_TRY(cudaStreamSynchronize(an->cur));
+    return PIV_OK;
+}
+
+int32_t piv_analyze_traced(PivAnalyzer* an, const PivFrame* a, const PivFrame* b, PivTraceC* tr, PivSummaryC* summary) {
+    if (!an || !tr) return fail(PIV_ERR_ARGUMENT, "null argument");
+    int st = run_passes(an, a, b);
+    if (st) return st;
+    size_t off = 0;
+    for (const PassBuf& pb : an->passes) {
+        const size_t c = (size_t)pb.cells;
+        auto d2h = [&](void* dst, const void* src, size_t es) -> cudaError_t {
+            if (!dst) return cudaSuccess;
+            return cudaMemcpyAsync((char*)dst + off * es, src, es * c, cudaMemcpyDeviceToHost, an->cur);
+        };
+        if (tr->origins) CUDA_TRY(cudaMemcpyAsync(tr->origins + 4 * off, pb.origins, 16 * c, cudaMemcpyDeviceToHost, an->cur));
+        CUDA_TRY(d2h(tr->raw_dx, pb.raw_dx, 4));
+        CUDA_TRY(d2h(tr->raw_dy, pb.raw_dy, 4));
+        CUDA_TRY(d2h(tr->raw_peak_ratio, pb.raw_ppr, 4));
+        CUDA_TRY(d2h(tr->raw_flags, pb.raw_flags, 1));
+        CUDA_TRY(d2h(tr->dx, pb.dx, 4));
+        CUDA_TRY(d2h(tr->dy, pb.dy, 4));
+        CUDA_TRY(d2h(tr->peak_ratio, pb.raw_ppr, 4));
+        CUDA_TRY(d2h(tr->flags, pb.flags, 1));
+        off += c;
+    }
+    st = copy_summary(an, summary);
+    if (st) return st;
+    CUDA_TRY(cudaStreamSynchronize(an->cur));
+    return PIV_OK;
+}
+
+int32_t piv_place_windows(PivAnalyzer* an, int64_t height, int64_t width, const PivGridC* grid,
+                          const PivGridC* pred_grid, const float* pred_dx, const float* pred_dy, float* origins) {
+    if (!an || !grid || !origins) return fail(PIV_ERR_ARGUMENT, "null argument");
+    int st = use_device(an);
+    if (st) return st;
+    const size_t c = (size_t)(grid->nx * grid->ny);
+    const size_t pc = pred_grid ? (size_t)(pred_grid->nx * pred_grid->ny) : 0;
+    void* buf = nullptr;
+    CUDA_TRY(cudaMalloc(&buf, align256(16 * c) + align256(c) + 2 * align256(4 * pc + 4)));
+    char* p = (char*)buf;
+    float4* d_org = (float4*)p;
+    p += align256(16 * c);
+    uint8_t* d_st = (uint8_t*)p;
+    p += align256(c);
+    float* d_pdx = (float*)p;
+    p += align256(4 * pc + 4);
+    float* d_pdy = (float*)p;
+    PlaceParams pp{};
+    pp.grid = to_gp(*grid);
+    pp.H = (int)height;
+    pp.W = (int)width;
+    pp.has_pred = pred_grid && pred_dx && pred_dy;
+    cudaError_t e = cudaSuccess;
+    if (pp.has_pred) {
+        pp.pgrid = to_gp(*pred_grid);
+        e = cudaMemcpyAsync(d_pdx, pred_dx, 4 * pc, cudaMemcpyHostToDevice, an->cur);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(d_pdy, pred_dy, 4 * pc, cudaMemcpyHostToDevice, an->cur);
+        pp.pdx = d_pdx;
+        pp.pdy = d_pdy;
+    }
+    pp.origins = d_org;
+    pp.status = d_st;
+    pp.use_stats = 0;
+    if (e == cudaSuccess) e = launch_place(pp, an->cur);
+    an->launches += 1;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(origins, d_org, 16 * c, cudaMemcpyDeviceToHost, an->cur);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(an->cur);
+    cudaFree(buf);
+    if (e != cudaSuccess) return fail(PIV_ERR_CUDA, "place: %s", cudaGetErrorString(e));
+    return PIV_OK;
+}
+
+int32_t piv_correlate_origins(PivAnalyzer* an, const PivFrame* a, const PivFrame* b, int64_t window,
+                              const float* origins, int64_t ncells, float* dx, float* dy, float* peak_ratio,
+                              uint8_t* flags) {
+    if (!an || !a || !b || !origins || ncells < 0) return fail(PIV_ERR_ARGUMENT, "bad argument");
+    if (a->H != b->H || a->W != b->W) return fail(PIV_ERR_SHAPE_MISMATCH, "frames have different shapes");
+    if (!corr_supported((int)window)) return fail(PIV_ERR_UNSUPPORTED, "window size %lld", (long long)window);
+    if (window > a->W || window > a->H) return fail(PIV_ERR_IMAGE_TOO_SMALL, "window larger than image");
+    // Host-side bounds check of the origins (the kernel also clamps every index).
+    for (int64_t k = 0; k < ncells; ++k)
+        for (int j = 0; j < 4; ++j) {
+            const float v = origins[4 * k + j];
+            const float lim = (float)((j % 2 == 0 ? a->W : a->H) - window);
+            if (!(v >= 0.0f && v <= lim)) return fail(PIV_ERR_ARGUMENT, "origin %lld out of the image", (long long)k);
+        }
+    int st = use_device(an);
+    if (st) return st;
+    const bool use_stats = needs_stats(an, a) || needs_stats(an, b);
+    if (use_stats && !(a->stats_valid && b->stats_valid)) return fail(PIV_ERR_ARGUMENT, "frame statistics missing");
+    const size_t c = (size_t)ncells;
+    void* buf = nullptr;
+    CUDA_TRY(cudaMalloc(&buf, align256(16 * c) + align256(c) + 3 * align256(4 * c) + align256(c) + 256));
+    char* p = (char*)buf;
+    float4* d_org = (float4*)p;
+    p += align256(16 * c);
+    uint8_t* d_st = (uint8_t*)p;
+    p += align256(c);
+    float* d_dx = (float*)p;
+    p += align256(4 * c);
+    float* d_dy = (float*)p;
+    p += align256(4 * c);
+    float* d_ppr = (float*)p;
+    p += align256(4 * c);
+    uint8_t* d_fl = (uint8_t*)p;
+    cudaError_t e = cudaMemcpyAsync(d_org, origins, 16 * c, cudaMemcpyHostToDevice, an->cur);
+    PlaceParams pp{};
+    pp.grid.window = (int)window;
+    pp.H = (int)a->H;
+    pp.W = (int)a->W;
+    pp.status = d_st;
+    pp.use_stats = use_stats;
+    if (use_stats) {
+        pp.sa = stats_of(a);
+        pp.sb = stats_of(b);
+    }
+    pp.min_mean = an->min_mean;
+    pp.min_std = an->min_std;
+    if (e == cudaSuccess) e = launch_mask(pp, d_org, (int)ncells, an->cur);
+    CorrParams cp{a->image, b->image, (int)a->H, (int)a->W, d_org, d_st, (int)ncells, d_dx, d_dy, d_ppr, d_fl};
+    if (e == cudaSuccess) e = launch_correlate((int)window, cp, an->cur);
+    an->launches += 2;
+    if (e == cudaSuccess && dx) e = cudaMemcpyAsync(dx, d_dx, 4 * c, cudaMemcpyDeviceToHost, an->cur);
+    if (e == cudaSuccess && dy) e = cudaMemcpyAsync(dy, d_dy, 4 * c, cudaMemcpyDeviceToHost, an->cur);
+    if (e == cudaSuccess && peak_ratio) e = cudaMemcpyAsync(peak_ratio, d_ppr, 4 * c, cudaMemcpyDeviceToHost, an->cur);
+    if (e == cudaSuccess && flags) e = cudaMemcpyAsync(flags, d_fl, c, cudaMemcpyDeviceToHost, an->cur);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(an->cur);
+    cudaFree(buf);
+    if (e != cudaSuccess) return fail(PIV_ERR_CUDA, "correlate: %s", cudaGetErrorString(e));
+    return PIV_OK;
+}
+
+int32_t piv_validate_field(PivAnalyzer* an, int64_t ny, int64_t nx, const float* dx, const float* dy,
+                           const float* peak_ratio, const uint8_t* flags, float* out_dx, float* out_dy,
+                           uint8_t* out_flags, PivSummaryC* summary) {
+    if (!an || !dx || !dy || !peak_ratio || !flags) return fail(PIV_ERR_ARGUMENT, "null argument");
+    if (ny <= 0 || nx <= 0) return fail(PIV_ERR_ARGUMENT, "empty field");
+    int st = use_device(an);
+    if (st) return st;
+    const size_t c = (size_t)(ny * nx);
+    void* buf = nullptr;
+    CUDA_TRY(cudaMalloc(&buf, 5 * align256(4 * c) + 4 * align256(c) + 256));
+    char* p = (char*)buf;
+    auto take = [&](size_t bytes) {
+        void* r = p;
+        p += align256(bytes);
+        return r;
+    };
+    float* d_dx = (float*)take(4 * c);
+    float* d_dy = (float*)take(4 * c);
+    float* d_ppr = (float*)take(4 * c);
+    float* o_dx = (float*)take(4 * c);
+    float* o_dy = (float*)take(4 * c);
+    uint8_t* f0 = (uint8_t*)take(c);
+    uint8_t* f1 = (uint8_t*)take(c);
+    uint8_t* f2 = (uint8_t*)take(c);
+    uint8_t* fo = (uint8_t*)take(c);
+    unsigned long long* cnt = (unsigned long long*)take(64);
+    cudaError_t e = cudaMemcpyAsync(d_dx, dx, 4 * c, cudaMemcpyHostToDevice, an->cur);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_dy, dy, 4 * c, cudaMemcpyHostToDevice, an->cur);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_ppr, peak_ratio, 4 * c, cudaMemcpyHostToDevice, an->cur);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(f0, flags, c, cudaMemcpyHostToDevice, an->cur);
+    ValidateParams vp{(int)nx, (int)ny, d_dx, d_dy, d_ppr, f0, f1, f2, o_dx, o_dy, fo, (float)an->windows[0] / 2.0f,
+                      an->ppr_threshold, an->median_threshold, an->median_eps, an->replace};
+    if (e == cudaSuccess) e = launch_validate(vp, an->cur);
+    if (e == cudaSuccess) e = launch_summary(fo, (int)c, cnt, an->cur);
+    an->launches += kValidateLaunches + kSummaryLaunches;
+    unsigned long long hc[5] = {0, 0, 0, 0, 0};
+    if (e == cudaSuccess && out_dx) e = cudaMemcpyAsync(out_dx, o_dx, 4 * c, cudaMemcpyDeviceToHost, an->cur);
+    if (e == cudaSuccess && out_dy) e = cudaMemcpyAsync(out_dy, o_dy, 4 * c, cudaMemcpyDeviceToHost, an->cur);
+    if (e == cudaSuccess && out_flags) e = cudaMemcpyAsync(out_flags, fo, c, cudaMemcpyDeviceToHost, an->cur);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, an->cur);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(an->cur);
+    cudaFree(buf);
+    if (e != cudaSuccess) return fail(PIV_ERR_CUDA, "validate: %s", cudaGetErrorString(e));
+    if (summary) {
+        summary->no_signal = (int64_t)hc[0];
+        summary->low_ppr = (int64_t)hc[1];
+        summary->median_outliers = (int64_t)hc[2];
+        summary->out_of_range = (int64_t)hc[3];
+        summary->replaced = (int64_t)hc[4];
+    }
+    return PIV_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,114 @@
+// Host-side launchers of the B200 PIV kernels (internal to libpivb200.so).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace pivb200 {
+
+// ----------------------------------------------------------------------------- correlation
+struct CorrParams {
+    const float* img_a;
+    const float* img_b;
+    int H, W;
+    const float4* origins;   // [ax, ay, bx, by] per cell
+    const uint8_t* status;   // 1 = window pair has signal, 0 = masked (NO_SIGNAL)
+    int ncells;
+    float* raw_dx;
+    float* raw_dy;
+    float* raw_ppr;
+    uint8_t* raw_flags;      // 0 or NO_SIGNAL
+};
+
+bool corr_supported(int n);
+cudaError_t corr_init_device();  // uploads the root-of-unity table to the current device
+cudaError_t launch_correlate(int n, const CorrParams& p, cudaStream_t s);
+// Number of kernel launches launch_correlate issues (for launch accounting).
+constexpr int kCorrLaunches = 1;
+
+// ----------------------------------------------------------------------------- field stages
+// Exact window statistics of a frame's background-subtracted intensity (preprocess.rs:76-125):
+// int64 fixed-point integral tables plus the fixed-point scales.
+struct StatsView {
+    const long long* sum;    // (H+1) x (W+1)
+    const long long* sumsq;  // (H+1) x (W+1)
+    const int* scales;       // [s1, s2]
+    int H, W;
+};
+
+struct PlaceParams {
+    GridP grid;
+    int H, W;
+    GridP pgrid;
+    int has_pred;
+    const float* pdx;  // predictor = previous pass's validated field
+    const float* pdy;
+    float4* origins;
+    uint8_t* status;
+    // signal mask (multipass.rs:233-241); use_stats = 0 means every window has signal
+    int use_stats;
+    StatsView sa, sb;
+    float min_mean, min_std;
+};
+
+cudaError_t launch_place(const PlaceParams& p, cudaStream_t s);
+// Mask only (origins given): fills status from origins.
+cudaError_t launch_mask(const PlaceParams& p, const float4* origins, int ncells, cudaStream_t s);
+
+struct ValidateParams {
+    int nx, ny;
+    const float* dx;      // raw field
+    const float* dy;
+    const float* ppr;
+    const uint8_t* flags0;  // raw flags (0 / NO_SIGNAL)
+    uint8_t* flags1;        // scratch: after per-vector tests
+    uint8_t* flags2;        // scratch: after the median test
+    float* out_dx;
+    float* out_dy;
+    uint8_t* out_flags;
+    float max_displacement, ppr_threshold, median_threshold, median_eps;
+    int replace;
+};
+
+cudaError_t launch_validate(const ValidateParams& p, cudaStream_t s);
+constexpr int kValidateLaunches = 3;
+
+// Summary counts from a validated flag field (validate.rs:40-46): no_signal, low_ppr,
+// median_outliers, out_of_range, replaced.
+cudaError_t launch_summary(const uint8_t* flags, int n, unsigned long long* counts5, cudaStream_t s);
+constexpr int kSummaryLaunches = 2;
+
+// ----------------------------------------------------------------------------- preprocessing
+enum RawType { RAW_U8 = 0, RAW_U16 = 1, RAW_F32 = 2 };
+
+struct PrepParams {
+    int H, W;
+    const void* raw;
+    int raw_type;
+    const float* background;  // nullable
+    int clip_percentile_on;
+    double clip_percentile;
+    unsigned int* hist;       // scratch: 256 + 256 + 4 words when clipping
+    float* base;              // background-subtracted intensity (output, H x W)
+    float* image;             // prepared image (output, H x W)
+    float* tmp;               // scratch H x W (blur intermediate)
+    float smooth_sigma;
+    int normalize_radius;
+    float normalize_eps;
+    // integral tables of `base` (built when build_stats)
+    int build_stats;
+    long long* sum;
+    long long* sumsq;
+    int* scales;
+    unsigned int* maxbits;    // scratch word
+};
+
+// Runs the whole PreparedFrame::new chain; returns the number of kernels launched in *launches.
+cudaError_t launch_prepare(const PrepParams& p, cudaStream_t s, int* launches);
+// Integral tables only (used when the prepared image is supplied directly).
+cudaError_t launch_stats(const float* base, int H, int W, long long* sum, long long* sumsq, int* scales,
+                         unsigned int* maxbits, cudaStream_t s, int* launches);
+
+}  // namespace pivb200

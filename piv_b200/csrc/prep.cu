@@ -1,0 +1,437 @@
+// Frame preparation: PreparedFrame::new (preprocess.rs:138-158) on the device.
+//
+//   raw u8/u16 -> f32 as v/255 or v/65535 (decode.rs:227-234); f32 frames pass through
+//   optional percentile clip of the integer codes (not in the reference; see below)
+//   base = max(raw - background, 0)                     preprocess.rs:140-142
+//   integral tables of base for the signal mask          preprocess.rs:76-125 (exact int64 here)
+//   separable Gaussian blur, radius ceil(3 sigma), clamped edges, f32 sums in kernel order
+//                                                        preprocess.rs:161-195
+//   local mean/std normalization over the clipped (2r+1)^2 box    preprocess.rs:199-216
+//
+// The blur repeats the reference's f32 operations in order (no FMA), so it is bit-exact given
+// the same kernel weights. The normalization's box statistics are exact integer sums turned into
+// f32 mean/std through double-float arithmetic (see common.cuh), matching the reference's f64
+// integral image to within a rounding-boundary case.
+//
+// Percentile clip (an addition, parity unpinned against the reference, pinned against the
+// oracle): the clip code is the smallest code c with #(codes <= c) >= ceil(p/100 * H*W); codes
+// above it are set to it before conversion. Found with two 256-bin histogram passes.
+#include <cmath>
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace pivb200 {
+
+constexpr int kMaxBlurTaps = 65;  // radius <= 32
+constexpr int kMaxNormRadius = 16;
+
+struct BlurKernel {
+    float w[kMaxBlurTaps];
+    int radius;
+};
+
+// ------------------------------------------------------------------------------- percentile
+template <typename CodeT>
+__global__ void hist_kernel(const CodeT* __restrict__ raw, long long n, unsigned int* hist, int level,
+                            const unsigned int* sel) {
+    __shared__ unsigned int h[256];
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) h[i] = 0;
+    __syncthreads();
+    const unsigned int coarse = level ? sel[0] : 0u;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const unsigned int c = raw[i];
+        if (level == 0)
+            atomicAdd(&h[c >> 8], 1u);
+        else if ((c >> 8) == coarse)
+            atomicAdd(&h[c & 255u], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 256; i += blockDim.x)
+        if (h[i]) atomicAdd(&hist[i], h[i]);
+}
+
+// sel[0] = coarse bin, sel[1] = remaining rank inside it; level 1 writes sel[2] = clip code.
+__global__ void select_kernel(const unsigned int* hist, unsigned int* sel, unsigned long long target, int level) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    unsigned long long acc = 0, want = level == 0 ? target : sel[1];
+    for (int b = 0; b < 256; ++b) {
+        if (acc + hist[b] >= want) {
+            if (level == 0) {
+                sel[0] = b;
+                sel[1] = (unsigned int)(want - acc);
+            } else {
+                sel[2] = (sel[0] << 8) | (unsigned int)b;
+            }
+            return;
+        }
+        acc += hist[b];
+    }
+    if (level == 0) {
+        sel[0] = 255;
+        sel[1] = 0;
+    } else {
+        sel[2] = (sel[0] << 8) | 255u;
+    }
+}
+
+// ------------------------------------------------------------------------------- conversion
+template <typename CodeT>
+__device__ __forceinline__ float to_f32(CodeT c);
+template <>
+__device__ __forceinline__ float to_f32<uint8_t>(uint8_t c) { return __fdiv_rn((float)c, 255.0f); }
+template <>
+__device__ __forceinline__ float to_f32<uint16_t>(uint16_t c) { return __fdiv_rn((float)c, 65535.0f); }
+
+template <typename CodeT>
+__global__ void convert_kernel(const CodeT* __restrict__ raw, long long n, const float* __restrict__ bg,
+                               const unsigned int* clip, float* __restrict__ out) {
+    const unsigned int cl = clip ? clip[2] : 0xffffffffu;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        unsigned int c = raw[i];
+        if (c > cl) c = cl;
+        float v = to_f32<CodeT>((CodeT)c);
+        if (bg) v = fmaxf(__fsub_rn(v, bg[i]), 0.0f);
+        out[i] = v;
+    }
+}
+
+__global__ void convert_f32_kernel(const float* __restrict__ raw, long long n, const float* __restrict__ bg,
+                                   float* __restrict__ out) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        float v = raw[i];
+        if (bg) v = fmaxf(__fsub_rn(v, bg[i]), 0.0f);
+        out[i] = v;
+    }
+}
+
+// ------------------------------------------------------------------------------- max |v|
+__global__ void maxabs_kernel(const float* __restrict__ v, long long n, unsigned int* out) {
+    float m = 0.0f;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        m = fmaxf(m, fabsf(v[i]));
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));  // non-negative floats order as uints
+}
+
+// ------------------------------------------------------------------------------- integral tables
+// Row pass: T[y+1][x+1] = sum_{x' <= x} q(v[y][x']) for both tables; T[y+1][0] = 0.
+__global__ void integral_rows_kernel(const float* __restrict__ v, int H, int W, long long* sum, long long* sumsq,
+                                     const unsigned int* maxbits, int* scales) {
+    const int y = blockIdx.x;
+    const FixScale fs = fix_scale(__uint_as_float(*maxbits), (long long)H * W);
+    if (y == 0 && threadIdx.x == 0) {
+        scales[0] = fs.s1;
+        scales[1] = fs.s2;
+    }
+    const int stride = W + 1;
+    long long* r1 = sum + (size_t)(y + 1) * stride;
+    long long* r2 = sumsq + (size_t)(y + 1) * stride;
+    const float* row = v + (size_t)y * W;
+    __shared__ long long c1[32], c2[32];
+    __shared__ long long carry1, carry2;
+    if (threadIdx.x == 0) {
+        r1[0] = 0;
+        r2[0] = 0;
+        carry1 = 0;
+        carry2 = 0;
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int base = 0; base < W; base += blockDim.x) {
+        const int x = base + threadIdx.x;
+        long long a = 0, b = 0;
+        if (x < W) {
+            const float f = row[x];
+            a = fix_q1(f, fs);
+            b = fix_q2(f, fs);
+        }
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long ua = __shfl_up_sync(0xffffffffu, a, o), ub = __shfl_up_sync(0xffffffffu, b, o);
+            if (lane >= o) {
+                a += ua;
+                b += ub;
+            }
+        }
+        if (lane == 31) {
+            c1[warp] = a;
+            c2[warp] = b;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            long long wa = lane < nw ? c1[lane] : 0, wb = lane < nw ? c2[lane] : 0;
+            for (int o = 1; o < 32; o <<= 1) {
+                const long long ua = __shfl_up_sync(0xffffffffu, wa, o), ub = __shfl_up_sync(0xffffffffu, wb, o);
+                if (lane >= o) {
+                    wa += ua;
+                    wb += ub;
+                }
+            }
+            if (lane < nw) {
+                c1[lane] = wa;
+                c2[lane] = wb;
+            }
+        }
+        __syncthreads();
+        const long long off1 = carry1 + (warp > 0 ? c1[warp - 1] : 0);
+        const long long off2 = carry2 + (warp > 0 ? c2[warp - 1] : 0);
+        if (x < W) {
+            r1[x + 1] = a + off1;
+            r2[x + 1] = b + off2;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            carry1 += c1[nw - 1];
+            carry2 += c2[nw - 1];
+        }
+        __syncthreads();
+    }
+}
+
+// Column pass: cumulative sums down each column of both tables (rows 1..H). Row 0 is zero.
+__global__ void integral_cols_kernel(int H, int W, long long* sum, long long* sumsq) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int stride = W + 1;
+    if (x > W) return;
+    sum[x] = 0;
+    sumsq[x] = 0;
+    long long a = 0, b = 0;
+    int y = 1;
+    for (; y + 4 <= H + 1; y += 4) {
+        long long va[4], vb[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            va[i] = sum[(size_t)(y + i) * stride + x];
+            vb[i] = sumsq[(size_t)(y + i) * stride + x];
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            a += va[i];
+            b += vb[i];
+            sum[(size_t)(y + i) * stride + x] = a;
+            sumsq[(size_t)(y + i) * stride + x] = b;
+        }
+    }
+    for (; y <= H; ++y) {
+        a += sum[(size_t)y * stride + x];
+        b += sumsq[(size_t)y * stride + x];
+        sum[(size_t)y * stride + x] = a;
+        sumsq[(size_t)y * stride + x] = b;
+    }
+}
+
+// ------------------------------------------------------------------------------- blur
+constexpr int BT_X = 32, BT_Y = 16;
+
+__global__ void blur_kernel(const float* __restrict__ src, int H, int W, const BlurKernel k, float* __restrict__ out) {
+    extern __shared__ float sm[];
+    const int R = k.radius;
+    const int TW = BT_X + 2 * R, TH = BT_Y + 2 * R;
+    float* tin = sm;             // TH x TW
+    float* trow = sm + TH * TW;  // TH x BT_X
+    const int gx0 = blockIdx.x * BT_X, gy0 = blockIdx.y * BT_Y;
+    for (int i = threadIdx.x; i < TH * TW; i += blockDim.x) {
+        const int ty = i / TW, tx = i % TW;
+        const int gy = min(max(gy0 + ty - R, 0), H - 1);
+        const int gx = min(max(gx0 + tx - R, 0), W - 1);
+        tin[i] = src[(size_t)gy * W + gx];
+    }
+    __syncthreads();
+    // Row pass over every tile row (vertical halo included): sum in kernel order from -0.0.
+    for (int i = threadIdx.x; i < TH * BT_X; i += blockDim.x) {
+        const int ty = i / BT_X, tx = i % BT_X;
+        float s = -0.0f;
+        for (int j = 0; j <= 2 * R; ++j) s = __fadd_rn(s, __fmul_rn(k.w[j], tin[ty * TW + tx + j]));
+        trow[i] = s;
+    }
+    __syncthreads();
+    // Column pass: out starts at 0.0 and accumulates kernel terms in order (preprocess.rs:186-193).
+    for (int i = threadIdx.x; i < BT_X * BT_Y; i += blockDim.x) {
+        const int ty = i / BT_X, tx = i % BT_X;
+        const int gx = gx0 + tx, gy = gy0 + ty;
+        if (gx >= W || gy >= H) continue;
+        float o = 0.0f;
+        for (int j = 0; j <= 2 * R; ++j) o = __fadd_rn(o, __fmul_rn(k.w[j], trow[(ty + j) * BT_X + tx]));
+        out[(size_t)gy * W + gx] = o;
+    }
+}
+
+// ------------------------------------------------------------------------------- normalize
+constexpr int NT_X = 32, NT_Y = 8;
+
+__global__ void normalize_kernel(const float* __restrict__ src, int H, int W, int r, float eps,
+                                 const unsigned int* maxbits, float* __restrict__ out) {
+    extern __shared__ long long smq[];
+    const int TW = NT_X + 2 * r, TH = NT_Y + 2 * r;
+    long long* q1 = smq;                 // TH x TW
+    long long* q2 = q1 + TH * TW;        // TH x TW
+    long long* h1 = q2 + TH * TW;        // TH x NT_X
+    long long* h2 = h1 + TH * NT_X;      // TH x NT_X
+    const FixScale fs = fix_scale(__uint_as_float(*maxbits), (long long)(2 * r + 1) * (2 * r + 1));
+    const int gx0 = blockIdx.x * NT_X, gy0 = blockIdx.y * NT_Y;
+    for (int i = threadIdx.x; i < TH * TW; i += blockDim.x) {
+        const int ty = i / TW, tx = i % TW;
+        const int gy = gy0 + ty - r, gx = gx0 + tx - r;
+        long long a = 0, b = 0;
+        if (gy >= 0 && gy < H && gx >= 0 && gx < W) {
+            const float f = src[(size_t)gy * W + gx];
+            a = fix_q1(f, fs);
+            b = fix_q2(f, fs);
+        }
+        q1[i] = a;
+        q2[i] = b;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < TH * NT_X; i += blockDim.x) {
+        const int ty = i / NT_X, tx = i % NT_X;
+        long long a = 0, b = 0;
+        for (int j = 0; j <= 2 * r; ++j) {
+            a += q1[ty * TW + tx + j];
+            b += q2[ty * TW + tx + j];
+        }
+        h1[i] = a;
+        h2[i] = b;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < NT_X * NT_Y; i += blockDim.x) {
+        const int ty = i / NT_X, tx = i % NT_X;
+        const int gx = gx0 + tx, gy = gy0 + ty;
+        if (gx >= W || gy >= H) continue;
+        long long a = 0, b = 0;
+        for (int j = 0; j <= 2 * r; ++j) {
+            a += h1[(ty + j) * NT_X + tx];
+            b += h2[(ty + j) * NT_X + tx];
+        }
+        const int x0 = max(gx - r, 0), x1 = min(gx + r + 1, W);
+        const int y0 = max(gy - r, 0), y1 = min(gy + r + 1, H);
+        float mean, sd;
+        fix_stats(a, b, fs, (float)((x1 - x0) * (y1 - y0)), &mean, &sd);
+        const float v = src[(size_t)gy * W + gx];
+        out[(size_t)gy * W + gx] = __fdiv_rn(__fsub_rn(v, mean), __fadd_rn(sd, eps));
+    }
+}
+
+// ------------------------------------------------------------------------------- drivers
+static int grid_for(long long n) {
+    long long b = (n + 255) / 256;
+    if (b > 148 * 16) b = 148 * 16;
+    if (b < 1) b = 1;
+    return (int)b;
+}
+
+cudaError_t launch_stats(const float* base, int H, int W, long long* sum, long long* sumsq, int* scales,
+                         unsigned int* maxbits, cudaStream_t s, int* launches) {
+    const long long n = (long long)H * W;
+    cudaError_t e = cudaMemsetAsync(maxbits, 0, sizeof(unsigned int), s);
+    if (e != cudaSuccess) return e;
+    maxabs_kernel<<<grid_for(n), 256, 0, s>>>(base, n, maxbits);
+    integral_rows_kernel<<<H, 256, 0, s>>>(base, H, W, sum, sumsq, maxbits, scales);
+    integral_cols_kernel<<<(W + 1 + 127) / 128, 128, 0, s>>>(H, W, sum, sumsq);
+    if (launches) *launches += 3;
+    return cudaGetLastError();
+}
+
+// Blur weights exactly as preprocess.rs:162-168 computes them (f32 exp of an f32 argument,
+// normalised by their f32 sum in order).
+static BlurKernel make_blur(float sigma) {
+    BlurKernel k{};
+    const int radius = (int)std::max(std::ceil(3.0f * sigma), 1.0f);
+    k.radius = radius;
+    float total = 0.0f;
+    for (int i = -radius; i <= radius; ++i) {
+        const float v = std::exp(-(float)(i * i) / (2.0f * sigma * sigma));
+        k.w[i + radius] = v;
+    }
+    for (int j = 0; j <= 2 * radius; ++j) total += k.w[j];
+    for (int j = 0; j <= 2 * radius; ++j) k.w[j] /= total;
+    return k;
+}
+
+cudaError_t launch_prepare(const PrepParams& p, cudaStream_t s, int* launches) {
+    const long long n = (long long)p.H * p.W;
+    cudaError_t e;
+    int nl = 0;
+    const unsigned int* clip = nullptr;
+    if (p.clip_percentile_on && (p.raw_type == RAW_U8 || p.raw_type == RAW_U16)) {
+        e = cudaMemsetAsync(p.hist, 0, sizeof(unsigned int) * (512 + 4), s);
+        if (e != cudaSuccess) return e;
+        double pc = std::min(std::max(p.clip_percentile, 0.0), 100.0);
+        unsigned long long target = (unsigned long long)std::ceil(pc / 100.0 * (double)n);
+        if (target < 1) target = 1;
+        unsigned int* h0 = p.hist;
+        unsigned int* h1 = p.hist + 256;
+        unsigned int* sel = p.hist + 512;
+        if (p.raw_type == RAW_U16) {
+            hist_kernel<uint16_t><<<grid_for(n), 256, 0, s>>>((const uint16_t*)p.raw, n, h0, 0, sel);
+            select_kernel<<<1, 32, 0, s>>>(h0, sel, target, 0);
+            hist_kernel<uint16_t><<<grid_for(n), 256, 0, s>>>((const uint16_t*)p.raw, n, h1, 1, sel);
+        } else {
+            hist_kernel<uint8_t><<<grid_for(n), 256, 0, s>>>((const uint8_t*)p.raw, n, h0, 0, sel);
+            select_kernel<<<1, 32, 0, s>>>(h0, sel, target, 0);
+            hist_kernel<uint8_t><<<grid_for(n), 256, 0, s>>>((const uint8_t*)p.raw, n, h1, 1, sel);
+        }
+        select_kernel<<<1, 32, 0, s>>>(h1, sel, target, 1);
+        nl += 4;
+        clip = sel;
+    }
+    const bool blur = p.smooth_sigma > 0.0f;
+    const bool norm = p.normalize_radius > 0;
+    // base goes straight to `image` when no further stage follows.
+    float* base = p.base;
+    switch (p.raw_type) {
+        case RAW_U8:
+            convert_kernel<uint8_t><<<grid_for(n), 256, 0, s>>>((const uint8_t*)p.raw, n, p.background, clip, base);
+            break;
+        case RAW_U16:
+            convert_kernel<uint16_t><<<grid_for(n), 256, 0, s>>>((const uint16_t*)p.raw, n, p.background, clip, base);
+            break;
+        default:
+            convert_f32_kernel<<<grid_for(n), 256, 0, s>>>((const float*)p.raw, n, p.background, base);
+            break;
+    }
+    nl += 1;
+    if (p.build_stats) {
+        e = launch_stats(base, p.H, p.W, p.sum, p.sumsq, p.scales, p.maxbits, s, &nl);
+        if (e != cudaSuccess) return e;
+    }
+    const float* cur = base;
+    if (blur) {
+        const BlurKernel k = make_blur(p.smooth_sigma);
+        if (k.radius > (kMaxBlurTaps - 1) / 2) return cudaErrorInvalidValue;
+        const int R = k.radius;
+        const size_t sm = sizeof(float) * ((size_t)(BT_Y + 2 * R) * (BT_X + 2 * R) + (size_t)(BT_Y + 2 * R) * BT_X);
+        if (sm > 48 * 1024) {
+            e = cudaFuncSetAttribute(blur_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+            if (e != cudaSuccess) return e;
+        }
+        float* dst = norm ? p.tmp : p.image;
+        dim3 grid((p.W + BT_X - 1) / BT_X, (p.H + BT_Y - 1) / BT_Y);
+        blur_kernel<<<grid, 256, sm, s>>>(cur, p.H, p.W, k, dst);
+        nl += 1;
+        cur = dst;
+    }
+    if (norm) {
+        const int r = p.normalize_radius;
+        if (r > kMaxNormRadius) return cudaErrorInvalidValue;
+        e = cudaMemsetAsync(p.maxbits + 1, 0, sizeof(unsigned int), s);
+        if (e != cudaSuccess) return e;
+        maxabs_kernel<<<grid_for(n), 256, 0, s>>>(cur, n, p.maxbits + 1);
+        const size_t sm = sizeof(long long) * (2 * (size_t)(NT_Y + 2 * r) * (NT_X + 2 * r) + 2 * (size_t)(NT_Y + 2 * r) * NT_X);
+        if (sm > 48 * 1024) {
+            e = cudaFuncSetAttribute(normalize_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+            if (e != cudaSuccess) return e;
+        }
+        dim3 grid((p.W + NT_X - 1) / NT_X, (p.H + NT_Y - 1) / NT_Y);
+        normalize_kernel<<<grid, 256, sm, s>>>(cur, p.H, p.W, r, p.normalize_eps, p.maxbits + 1, p.image);
+        nl += 2;
+        cur = p.image;
+    }
+    if (cur != p.image) {
+        e = cudaMemcpyAsync(p.image, cur, sizeof(float) * n, cudaMemcpyDeviceToDevice, s);
+        if (e != cudaSuccess) return e;
+    }
+    if (launches) *launches += nl;
+    return cudaGetLastError();
+}
+
+}  // namespace pivb200
