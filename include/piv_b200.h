@@ -201,6 +201,22 @@ int32_t piv_validate_field(PivAnalyzer* an, int64_t ny, int64_t nx, const float*
                            const float* peak_ratio, const uint8_t* flags, float* out_dx, float* out_dy,
                            uint8_t* out_flags, PivSummaryC* summary);
 
+/* ----------------------------------------------------------------------------- no allocation
+ * No counterpart in the reference. Validation of a raw field (the same rules as
+ * piv_validate_field, with the thresholds and max_displacement passed in) that allocates no
+ * device memory, for callers that cannot call cudaMalloc once running: deadline-bound
+ * acquisition loops (cudaFree waits for the whole device) and processes whose device memory is
+ * already reserved by another allocator. All pointers are DEVICE pointers owned by the caller;
+ * work is queued on `stream` (NULL = the default stream) and the call returns without waiting.
+ * Scratch lives in a fixed device array inside the library of 2 x 2,097,152 bytes, held by every
+ * GPU that loads the library until exit; fields above 2,097,152 cells are rejected
+ * (PIV_ERR_UNSUPPORTED). The first call on a device looks up that array's address, so make it
+ * before any stream capture. All calls share the array: calls whose work overlaps on the GPU race. */
+int32_t piv_validate_field_noalloc(int64_t ny, int64_t nx, const float* dx, const float* dy, const float* peak_ratio,
+                                   const uint8_t* flags, float max_displacement, float ppr_threshold,
+                                   float median_threshold, float median_eps, int32_t replace, float* out_dx,
+                                   float* out_dy, uint8_t* out_flags, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -22,7 +22,7 @@ EXPORTS = [
     "piv_frame_create", "piv_frame_destroy", "piv_frame_prepare", "piv_frame_prepare_device",
     "piv_frame_set_prepared", "piv_frame_download", "piv_frame_image_device", "piv_background_device",
     "piv_analyze", "piv_analyze_device", "piv_analyze_traced",
-    "piv_place_windows", "piv_correlate_origins", "piv_validate_field",
+    "piv_place_windows", "piv_correlate_origins", "piv_validate_field", "piv_validate_field_noalloc",
 ]
 
 
@@ -109,6 +109,7 @@ def load():
         "piv_place_windows": ([vp, i64, i64, P(PivGridC), P(PivGridC), vp, vp, vp], i32),
         "piv_correlate_origins": ([vp, vp, vp, i64, vp, i64, vp, vp, vp, vp], i32),
         "piv_validate_field": ([vp, i64, i64, vp, vp, vp, vp, vp, vp, vp, P(PivSummaryC)], i32),
+        "piv_validate_field_noalloc": ([i64, i64, vp, vp, vp, vp, f32, f32, f32, f32, i32, vp, vp, vp, vp], i32),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)

@@ -22,6 +22,7 @@ UNITS = {
     "field.cu": ["--fmad=false"],
     "prep.cu": ["--fmad=false"],
     "api.cu": ["--fmad=false"],
+    "noalloc.cu": ["--fmad=false"],
 }
 HEADERS = ["common.cuh", "fft.cuh", "kernels.h"]
 

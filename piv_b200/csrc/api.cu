@@ -18,6 +18,12 @@ namespace {
 
 thread_local std::string g_last_error;
 
+}  // namespace
+
+void pivb200::set_last_error(const char* msg) { g_last_error = msg; }
+
+namespace {
+
 int fail(int code, const char* fmt, ...) {
     char buf[512];
     va_list ap;

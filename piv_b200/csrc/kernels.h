@@ -8,6 +8,9 @@
 
 namespace pivb200 {
 
+// Sets the message piv_last_error returns on this host thread.
+void set_last_error(const char* msg);
+
 // ----------------------------------------------------------------------------- correlation
 struct CorrParams {
     const float* img_a;
