@@ -236,6 +236,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c5", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--ref-step-s", type=float, default=3.0)
     ap.add_argument("--ref-crop", type=int, default=1024)
     args = ap.parse_args()
@@ -288,6 +289,10 @@ def main():
         an.analyze_device(fa, fb, out_dx.data_ptr(), out_dy.data_ptr(), out_ppr.data_ptr(), out_fl.data_ptr(),
                           out_sum.data_ptr())
 
+    # launch-geometry autotuning on the first pair (results are identical across variants)
+    fa.prepare_device(pairs_dev[0][0].data_ptr(), dtype_code, pre)
+    fb.prepare_device(pairs_dev[0][1].data_ptr(), dtype_code, pre)
+    tuned = an.autotune(fa, fb) if not args.no_autotune else {}
     for i in range(args.warmup):
         step(i)
     stream.synchronize()
@@ -404,7 +409,7 @@ def main():
             "e2e": {"value": e2e_value, "unit": "vectors/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
                     "ms_per_step": float(ms2_t.item()) / e2e_steps, "wall_ms_per_step": 1e3 * t_wall / e2e_steps},
-            "gpu_launches": int(launches), "roofline": roof, "clocks": clocks}
+            "gpu_launches": int(launches), "roofline": roof, "clocks": clocks, "autotuned_variants": tuned}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(wl, a0, b0)
     if rank == 0:

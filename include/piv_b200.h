@@ -122,6 +122,14 @@ int32_t piv_analyzer_set_stream(PivAnalyzer* an, void* stream);
 int32_t piv_analyzer_sync(PivAnalyzer* an);
 /* Kernel launches issued by this analyzer since creation (launch accounting). */
 int64_t piv_analyzer_launches(const PivAnalyzer* an);
+/* Launch-geometry autotuning (no counterpart in the reference; the batching form of this
+ * project): analyses the pair once while timing, for every pass, each launch variant of the
+ * correlation kernel of that window size on the live data, and keeps the fastest per window
+ * size for this analyzer. Variants of one size differ only in threads per block, register cap
+ * and sampler, never in arithmetic: results are bit-identical whichever is chosen. Blocking. */
+int32_t piv_analyzer_autotune(PivAnalyzer* an, const PivFrame* a, const PivFrame* b);
+/* Name of the variant in use for `window` ("<n>/T<lanes per line>/G<groups>/B<min blocks>/<sampler>"). */
+int32_t piv_analyzer_variant(const PivAnalyzer* an, int32_t window, char* name, int32_t capacity);
 /* Stage timing (no counterpart in the reference, which has only wall-clock splits,
  * swift/Sources/PIVKit/Run.swift:189-196): when enabled, CUDA events bracket every correlation
  * kernel; piv_analyzer_profile waits for the stream and returns, for pass `pass`, the summed

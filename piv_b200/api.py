@@ -446,8 +446,21 @@ def _profile_methods():
         _check(_lib.load().piv_analyzer_profile(self._h, int(p), ctypes.byref(ms), ctypes.byref(n)))
         return ms.value, n.value
 
+    def autotune(self, a, b):
+        """Times every launch variant of each pass's window size on this pair and keeps the
+        fastest (results are identical across variants)."""
+        _check(_lib.load().piv_analyzer_autotune(self._h, a._h, b._h))
+        return {n: self.variant(n) for n in sorted(set(self.cfg.passes()))}
+
+    def variant(self, window):
+        buf = ctypes.create_string_buffer(64)
+        _check(_lib.load().piv_analyzer_variant(self._h, int(window), buf, 64))
+        return buf.value.decode()
+
     PivAnalyzer.set_profiling = set_profiling
     PivAnalyzer.profile = profile
+    PivAnalyzer.autotune = autotune
+    PivAnalyzer.variant = variant
 
 
 _profile_methods()

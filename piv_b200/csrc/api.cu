@@ -115,6 +115,9 @@ struct PivAnalyzer {
     std::vector<std::vector<std::pair<cudaEvent_t, cudaEvent_t>>> pending;
     std::vector<cudaEvent_t> spare;
 
+    // correlation launch variant chosen per window size (0 until autotuned)
+    int variant[129] = {};
+
     bool mask_trivial() const { return min_mean <= 0.0f && min_std <= 0.0f; }
     std::vector<int32_t> pass_windows() const {
         std::vector<int32_t> v = windows;
@@ -226,7 +229,7 @@ int alloc_stats(PivFrame* f) {
 
 // The multipass loop (multipass.rs:152-192): every pass is placement -> correlation ->
 // validation on the analyzer's stream; the predictor is the previous pass's validated field.
-int run_passes(PivAnalyzer* an, const PivFrame* a, const PivFrame* b) {
+int run_passes(PivAnalyzer* an, const PivFrame* a, const PivFrame* b, bool tune = false) {
     if (!a || !b) return fail(PIV_ERR_ARGUMENT, "null frame");
     if (a->H != b->H || a->W != b->W)
         return fail(PIV_ERR_SHAPE_MISMATCH, "frames have different shapes: (%lld, %lld) vs (%lld, %lld)", (long long)a->H,
@@ -274,7 +277,34 @@ int run_passes(PivAnalyzer* an, const PivFrame* a, const PivFrame* b) {
             }
             CUDA_TRY(cudaEventRecord(ev0, an->cur));
         }
-        CUDA_TRY(launch_correlate((int)pb.grid.window, cp, an->cur));
+        const int nwin = (int)pb.grid.window;
+        if (tune) {
+            // Time every launch variant of this window size on this pass's data (all compute the
+            // same results) and keep the fastest for later calls.
+            cudaEvent_t t0, t1;
+            CUDA_TRY(cudaEventCreate(&t0));
+            CUDA_TRY(cudaEventCreate(&t1));
+            float best = 1e30f;
+            int best_v = 0;
+            for (int v = 0; v < corr_num_variants(nwin); ++v) {
+                CUDA_TRY(launch_correlate_variant(nwin, v, cp, an->cur));
+                CUDA_TRY(cudaEventRecord(t0, an->cur));
+                for (int r = 0; r < 3; ++r) CUDA_TRY(launch_correlate_variant(nwin, v, cp, an->cur));
+                CUDA_TRY(cudaEventRecord(t1, an->cur));
+                CUDA_TRY(cudaEventSynchronize(t1));
+                float ms = 0.0f;
+                CUDA_TRY(cudaEventElapsedTime(&ms, t0, t1));
+                an->launches += 4;
+                if (ms < best) {
+                    best = ms;
+                    best_v = v;
+                }
+            }
+            cudaEventDestroy(t0);
+            cudaEventDestroy(t1);
+            an->variant[nwin] = best_v;
+        }
+        CUDA_TRY(launch_correlate_variant(nwin, an->variant[nwin], cp, an->cur));
         if (an->profiling) {
             CUDA_TRY(cudaEventRecord(ev1, an->cur));
             if (an->pending.size() < an->passes.size()) an->pending.resize(an->passes.size());
@@ -488,6 +518,21 @@ int32_t piv_analyzer_sync(PivAnalyzer* an) {
 }
 
 int64_t piv_analyzer_launches(const PivAnalyzer* an) { return an ? an->launches : 0; }
+
+int32_t piv_analyzer_autotune(PivAnalyzer* an, const PivFrame* a, const PivFrame* b) {
+    if (!an) return fail(PIV_ERR_ARGUMENT, "null analyzer");
+    int st = run_passes(an, a, b, true);
+    if (st) return st;
+    CUDA_TRY(cudaStreamSynchronize(an->cur));
+    return PIV_OK;
+}
+
+int32_t piv_analyzer_variant(const PivAnalyzer* an, int32_t window, char* name, int32_t capacity) {
+    if (!an || !name || capacity <= 0) return fail(PIV_ERR_ARGUMENT, "bad argument");
+    if (!corr_supported(window)) return fail(PIV_ERR_UNSUPPORTED, "window size %d", window);
+    snprintf(name, (size_t)capacity, "%s", corr_variant_name(window, an->variant[window]));
+    return PIV_OK;
+}
 
 int32_t piv_analyzer_set_profiling(PivAnalyzer* an, int32_t enable) {
     if (!an) return fail(PIV_ERR_ARGUMENT, "null analyzer");

@@ -4,21 +4,22 @@
 // (correlate.rs:182-210), find_peak (correlate.rs:215-303) and the pair assembly of
 // PivAnalyzer::pass (multipass.rs:242-259).
 //
-// Work decomposition (one thread group = N*T threads, one window PAIR per group):
-//   1. window A and window B of a pair are sampled (bilinear, same f32 operation order as the
-//      reference, no FMA) straight into registers as one complex plane z = a + i*b; lane (x, t)
-//      holds column x at rows t + T*p, so every load instruction reads contiguous image rows;
-//   2. mean removal and energy (group reductions), 2-D FFT of z (columns in registers, transpose
-//      through shared memory, rows in registers);
-//   3. the two real spectra are separated with the Hermitian partner Z[-k] (one shared-memory
-//      exchange) and the cross spectrum conj(FA)*FB formed in registers;
-//   4. the second window of the pair repeats 1-3; both cross spectra are Hermitian, so their
-//      inverse transforms are packed into ONE complex inverse 2-D FFT (real part = first
-//      correlation plane, imaginary part = second);
+// Work decomposition (one thread group = N*T threads, one PAIR of windows per group):
+//   1. both windows of the pair are sampled (bilinear, the reference's f32 operation order, no
+//      FMA) straight into registers, each as one complex plane z = a + i*b (frame A's window in
+//      the real part, frame B's in the imaginary part); lane (x, t) holds column x at rows
+//      t + T*p, so each load instruction reads contiguous image rows;
+//   2. mean removal and energies (one group reduction of 4 sums for both windows), 2-D FFT of
+//      both planes at once: columns in registers, transpose through shared memory, rows in
+//      registers;
+//   3. each plane's two real spectra are separated with the Hermitian partner Z[-k] (one
+//      shared-memory exchange) and the cross spectrum conj(FA)*FB formed in registers;
+//   4. both cross spectra are Hermitian, so their inverse transforms are packed into ONE complex
+//      inverse 2-D FFT (real part = first correlation plane, imaginary part = second);
 //   5. the scaled planes go to shared memory; argmax (lowest row-major index on ties), the
-//      half-width footprint, the second local maximum and the 3-point Gaussian fit run on them.
-// The 128 px window has no room for the pair stash in registers and runs one window per group
-// with a full complex inverse.
+//      half-width footprint, the second local maximum (a vectorised 3x3 maximum) and the 3-point
+//      Gaussian fit follow.
+// The 128 px window runs one window per group with a full complex inverse (registers).
 #include <cfloat>
 #include <cmath>
 #include <cstdio>
@@ -29,8 +30,14 @@
 
 namespace pivb200 {
 
-template <int N, int T, bool PAIR, int G>
+// Compile-time shape of one correlation kernel: window N, lanes per line T, window pairs or
+// single windows, groups per CTA G, minimum resident CTAs per SM (register cap), sampler.
+// G and MINB only change the launch geometry, never the arithmetic; N, T and PAIR fix the FFT
+// decomposition and therefore the rounding of the results.
+template <int N_, int T_, bool PAIR_, int G_, int MINB_, bool SHFL_ = false>
 struct CorrCfg {
+    static constexpr int N = N_, T = T_, G = G_, MINB = MINB_;
+    static constexpr bool PAIR = PAIR_, SHFL_SAMPLE = SHFL_;
     static constexpr int P = N / T;
     static constexpr int NT = N * T;
     static constexpr int THREADS = G * NT;
@@ -39,7 +46,10 @@ struct CorrCfg {
     // Shuffle segment: largest power of two dividing NT, at most a warp.
     static constexpr int SW = (NT % 32 == 0) ? 32 : (NT % 16 == 0) ? 16 : (NT % 8 == 0) ? 8 : (NT % 4 == 0) ? 4 : (NT % 2 == 0) ? 2 : 1;
     static constexpr int NSEG = NT / SW;
-    static constexpr size_t SMEM = sizeof(float2) * (size_t)(G * N * LD + N) + sizeof(float) * (size_t)(G * NSEG * 4) + 64;
+    // plane0: float2 N x LD; plane1: float2 (PAIR) or float (single) N x LD.
+    static constexpr size_t PLANE0 = sizeof(float2) * (size_t)N * LD;
+    static constexpr size_t PLANE1 = (PAIR ? sizeof(float2) : sizeof(float)) * (size_t)N * LD;
+    static constexpr size_t SMEM = (size_t)G * (PLANE0 + PLANE1) + sizeof(float2) * N + sizeof(float) * (size_t)G * NSEG * 4 + 64;
 };
 
 // ---------------------------------------------------------------------------------------------
@@ -47,27 +57,29 @@ struct CorrCfg {
 // Every thread of the group returns the same value; the combination order is fixed.
 // ---------------------------------------------------------------------------------------------
 template <class C>
-__device__ __forceinline__ float2 group_sum2(float2 v, float* s_red, int g, int gt) {
+__device__ __forceinline__ float4 group_sum4(float4 v, float* s_red, int g, int gt) {
     constexpr int SW = C::SW, NSEG = C::NSEG;
 #pragma unroll
     for (int o = SW / 2; o > 0; o >>= 1) {
         v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
         v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+        v.z += __shfl_xor_sync(0xffffffffu, v.z, o);
+        v.w += __shfl_xor_sync(0xffffffffu, v.w, o);
     }
     if constexpr (NSEG == 1) {
         return v;
     } else {
-        float* r = s_red + g * NSEG * 4;
-        if (gt % SW == 0) {
-            r[(gt / SW) * 2 + 0] = v.x;
-            r[(gt / SW) * 2 + 1] = v.y;
-        }
+        float4* r = reinterpret_cast<float4*>(s_red) + g * NSEG;
+        if (gt % SW == 0) r[gt / SW] = v;
         __syncthreads();
-        float2 s = make_float2(0.f, 0.f);
+        float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
         for (int i = 0; i < NSEG; ++i) {
-            s.x += r[i * 2 + 0];
-            s.y += r[i * 2 + 1];
+            const float4 q = r[i];
+            s.x += q.x;
+            s.y += q.y;
+            s.z += q.z;
+            s.w += q.w;
         }
         __syncthreads();
         return s;
@@ -75,19 +87,25 @@ __device__ __forceinline__ float2 group_sum2(float2 v, float* s_red, int g, int 
 }
 
 template <class C>
-__device__ __forceinline__ float group_max(float v, float* s_red, int g, int gt) {
+__device__ __forceinline__ float2 group_max2(float2 v, float* s_red, int g, int gt) {
     constexpr int SW = C::SW, NSEG = C::NSEG;
 #pragma unroll
-    for (int o = SW / 2; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    for (int o = SW / 2; o > 0; o >>= 1) {
+        v.x = fmaxf(v.x, __shfl_xor_sync(0xffffffffu, v.x, o));
+        v.y = fmaxf(v.y, __shfl_xor_sync(0xffffffffu, v.y, o));
+    }
     if constexpr (NSEG == 1) {
         return v;
     } else {
-        float* r = s_red + g * NSEG * 4;
+        float2* r = reinterpret_cast<float2*>(s_red) + g * NSEG * 2;
         if (gt % SW == 0) r[gt / SW] = v;
         __syncthreads();
-        float s = -INFINITY;
+        float2 s = make_float2(-INFINITY, -INFINITY);
 #pragma unroll
-        for (int i = 0; i < NSEG; ++i) s = fmaxf(s, r[i]);
+        for (int i = 0; i < NSEG; ++i) {
+            s.x = fmaxf(s.x, r[i].x);
+            s.y = fmaxf(s.y, r[i].y);
+        }
         __syncthreads();
         return s;
     }
@@ -106,21 +124,18 @@ __device__ __forceinline__ void group_argmax(float& v, int& idx, float* s_red, i
     constexpr int SW = C::SW, NSEG = C::NSEG;
 #pragma unroll
     for (int o = SW / 2; o > 0; o >>= 1) {
-        float ov = __shfl_xor_sync(0xffffffffu, v, o);
-        int oi = __shfl_xor_sync(0xffffffffu, idx, o);
+        const float ov = __shfl_xor_sync(0xffffffffu, v, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, idx, o);
         amax_combine(v, idx, ov, oi);
     }
     if constexpr (NSEG > 1) {
-        float* r = s_red + g * NSEG * 4;
-        if (gt % SW == 0) {
-            r[(gt / SW) * 2 + 0] = v;
-            r[(gt / SW) * 2 + 1] = __int_as_float(idx);
-        }
+        float2* r = reinterpret_cast<float2*>(s_red) + g * NSEG * 2;
+        if (gt % SW == 0) r[gt / SW] = make_float2(v, __int_as_float(idx));
         __syncthreads();
         float bv = -INFINITY;
         int bi = 0x7fffffff;
 #pragma unroll
-        for (int i = 0; i < NSEG; ++i) amax_combine(bv, bi, r[i * 2 + 0], __float_as_int(r[i * 2 + 1]));
+        for (int i = 0; i < NSEG; ++i) amax_combine(bv, bi, r[i].x, __float_as_int(r[i].y));
         __syncthreads();
         v = bv;
         idx = bi;
@@ -132,9 +147,14 @@ __device__ __forceinline__ void group_argmax(float& v, int& idx, float* s_red, i
 // otherwise bilinear with weights (1-tx)(1-ty), tx(1-ty), (1-tx)ty, tx*ty summed left to right.
 // Indices are clamped into the image so that no access can leave it whatever the origin.
 // ---------------------------------------------------------------------------------------------
-template <int N, int T>
-__device__ __forceinline__ void sample_column(const float* __restrict__ img, int H, int W, float ox, float oy,
-                                              int x, int t, float (&v)[N / T]) {
+//
+// Two samplers with identical results. sample_column_direct loads the four bilinear taps of
+// every pixel itself (fewest live registers). sample_column loads each pixel of the patch once
+// and trades the other taps through shuffles (fewest load instructions); it suits the window
+// sizes whose register budget allows it.
+template <int N, int T, bool IMAG>
+__device__ __forceinline__ void sample_column_direct(const float* __restrict__ img, int H, int W, float ox, float oy,
+                                                     int x, int t, float2 (&z)[N / T]) {
     constexpr int P = N / T;
     const float fx0 = floorf(ox), fy0 = floorf(oy);
     const int x0 = min(max((int)fx0, 0), W - 1), y0 = min(max((int)fy0, 0), H - 1);
@@ -143,23 +163,83 @@ __device__ __forceinline__ void sample_column(const float* __restrict__ img, int
     if (tx < 1e-4f && ty < 1e-4f) {
 #pragma unroll
         for (int p = 0; p < P; ++p) {
-            const int r = min(y0 + t + T * p, H - 1);
-            v[p] = __ldg(img + (size_t)r * W + c0);
+            const float v = __ldg(img + (size_t)min(y0 + t + T * p, H - 1) * W + c0);
+            if (IMAG) z[p].y = v; else z[p].x = v;
         }
     } else {
         const float ux = __fsub_rn(1.0f, tx), uy = __fsub_rn(1.0f, ty);
         const float w00 = __fmul_rn(ux, uy), w01 = __fmul_rn(tx, uy), w10 = __fmul_rn(ux, ty), w11 = __fmul_rn(tx, ty);
 #pragma unroll
         for (int p = 0; p < P; ++p) {
-            const int r0 = min(y0 + t + T * p, H - 1), r1 = min(y0 + t + T * p + 1, H - 1);
-            const float* top = img + (size_t)r0 * W;
-            const float* bot = img + (size_t)r1 * W;
+            const float* top = img + (size_t)min(y0 + t + T * p, H - 1) * W;
+            const float* bot = img + (size_t)min(y0 + t + T * p + 1, H - 1) * W;
             float s = __fmul_rn(w00, __ldg(top + c0));
             s = __fadd_rn(s, __fmul_rn(w01, __ldg(top + c1)));
             s = __fadd_rn(s, __fmul_rn(w10, __ldg(bot + c0)));
             s = __fadd_rn(s, __fmul_rn(w11, __ldg(bot + c1)));
-            v[p] = s;
+            if (IMAG) z[p].y = s; else z[p].x = s;
         }
+    }
+}
+
+// Each pixel of the (N+1) x (N+1) source patch is loaded once: a lane loads its own column at
+// its own rows; the right-hand column comes from the lane of the next line (T lanes further) by
+// a shuffle, and the row below from the lane holding that row (the next register for T = 1, the
+// next lane of the line otherwise). Lanes whose neighbour is outside their warp or beyond the
+// window load the missing value themselves.
+template <int N, int T, bool IMAG>
+__device__ __forceinline__ void sample_column(const float* __restrict__ img, int H, int W, float ox, float oy, int x,
+                                              int t, float2 (&z)[N / T]) {
+    constexpr int P = N / T;
+    const int lane = threadIdx.x & 31;
+    const float fx0 = floorf(ox), fy0 = floorf(oy);
+    const int x0 = min(max((int)fx0, 0), W - 1), y0 = min(max((int)fy0, 0), H - 1);
+    const float tx = __fsub_rn(ox, fx0), ty = __fsub_rn(oy, fy0);
+    const int c0 = min(x0 + x, W - 1), c1 = min(x0 + x + 1, W - 1);
+    const bool integer = tx < 1e-4f && ty < 1e-4f;
+    float top[P];
+#pragma unroll
+    for (int p = 0; p < P; ++p) top[p] = __ldg(img + (size_t)min(y0 + t + T * p, H - 1) * W + c0);
+    // Every lane runs the shuffles below (a warp may hold windows of both kinds); an integer
+    // window then keeps its copied values.
+    // Row N of the patch (below the window), held by the last lane of each line.
+    const int rN = min(y0 + N, H - 1);
+    const float extra = __ldg(img + (size_t)rN * W + c0);
+    const bool edge = lane + T >= 32 || x == N - 1;  // right neighbour not reachable by a shuffle
+    float right[P];
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+        right[p] = __shfl_down_sync(0xffffffffu, top[p], T);
+        if (edge) right[p] = __ldg(img + (size_t)min(y0 + t + T * p, H - 1) * W + c1);
+    }
+    float extra_r = __shfl_down_sync(0xffffffffu, extra, T);
+    if (edge) extra_r = __ldg(img + (size_t)rN * W + c1);
+    const float ux = __fsub_rn(1.0f, tx), uy = __fsub_rn(1.0f, ty);
+    const float w00 = __fmul_rn(ux, uy), w01 = __fmul_rn(tx, uy), w10 = __fmul_rn(ux, ty), w11 = __fmul_rn(tx, ty);
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+        float b0, b1;  // row y + 1 at columns x and x + 1
+        if constexpr (T == 1) {
+            b0 = p + 1 < P ? top[p + 1] : extra;
+            b1 = p + 1 < P ? right[p + 1] : extra_r;
+        } else {
+            // Row y + 1 of lane t < T-1 is the next lane's element p; of lane T-1 it is lane 0's
+            // element p + 1. The source lane chooses what it sends: lane 0 sends element p + 1,
+            // every other lane element p.
+            const int q = p + 1 < P ? p + 1 : p;
+            const int src = t < T - 1 ? lane + 1 : lane - (T - 1);
+            const float n0 = __shfl_sync(0xffffffffu, t == 0 ? top[q] : top[p], src);
+            const float n1 = __shfl_sync(0xffffffffu, t == 0 ? right[q] : right[p], src);
+            const bool last = (t == T - 1) && (p == P - 1);
+            b0 = last ? extra : n0;
+            b1 = last ? extra_r : n1;
+        }
+        float s = __fmul_rn(w00, top[p]);
+        s = __fadd_rn(s, __fmul_rn(w01, right[p]));
+        s = __fadd_rn(s, __fmul_rn(w10, b0));
+        s = __fadd_rn(s, __fmul_rn(w11, b1));
+        if (integer) s = top[p];
+        if (IMAG) z[p].y = s; else z[p].x = s;
     }
 }
 
@@ -176,213 +256,300 @@ __device__ __forceinline__ float subpixel(float m, float c, float p) {
     return 0.0f;
 }
 
-template <int N, int T, bool PAIR, int G>
-__global__ void __launch_bounds__(G * N * T) correlate_kernel(const CorrParams prm) {
-    using C = CorrCfg<N, T, PAIR, G>;
-    constexpr int P = C::P, NT = C::NT, LD = C::LD, WPG = C::WPG;
-    extern __shared__ float4 smem_f4[];
-    float2* planes = reinterpret_cast<float2*>(smem_f4);
-    float2* s_roots = planes + G * N * LD;
-    float* s_red = reinterpret_cast<float*>(s_roots + N);
-    __shared__ int s_hw[G][8];
+// Separates Z and its Hermitian partner M = Z[-k] into the cross spectrum (times 4):
+//   2FA = Z + conj(M), 2FB = -i (Z - conj(M)), C = conj(2FA) * 2FB.
+__device__ __forceinline__ float2 cross4(float2 z, float2 m) {
+    const float far = z.x + m.x, fai = z.y - m.y;
+    const float fbr = z.y + m.y, fbi = m.x - z.x;
+    return make_float2(far * fbr + fai * fbi, far * fbi - fai * fbr);
+}
 
+template <class C>
+__global__ void __launch_bounds__(C::THREADS, C::MINB) correlate_kernel(const CorrParams prm) {
+    constexpr int N = C::N, T = C::T, G = C::G, P = C::P, NT = C::NT, LD = C::LD, WPG = C::WPG;
+    constexpr bool PAIR = C::PAIR;
+    extern __shared__ float4 smem_f4[];
+    char* sbase = reinterpret_cast<char*>(smem_f4);
     const int tid = threadIdx.x;
     const int g = tid / NT;
     const int gt = tid - g * NT;
     const int line = gt / T;
     const int t = gt - line * T;
     const int rt = bitrev<T>(t);
-    float2* plane = planes + g * N * LD;
+    float2* plane0 = reinterpret_cast<float2*>(sbase + (size_t)g * (C::PLANE0 + C::PLANE1));
+    char* plane1_raw = sbase + (size_t)g * (C::PLANE0 + C::PLANE1) + C::PLANE0;
+    float2* s_roots = reinterpret_cast<float2*>(sbase + (size_t)G * (C::PLANE0 + C::PLANE1));
+    float* s_red = reinterpret_cast<float*>(s_roots + N);
+    __shared__ int s_hw[G][8];
 
     for (int i = tid; i < N; i += C::THREADS) s_roots[i] = c_roots[root_off(N) + i];
     __syncthreads();
 
     const long long base_cell = ((long long)blockIdx.x * G + g) * WPG;
-
-    float2 stash[PAIR ? P : 1];
-    float2 z[P];
-    float scale[WPG];
-    bool ok[WPG];
     float4 org[WPG];
+    bool ok[WPG];
+    float scale[WPG];
+    float2 z0[P];
+    float2 z1[PAIR ? P : 1];
 
+    // ------------------------------------------------------------------ sampling and moments
 #pragma unroll
     for (int wi = 0; wi < WPG; ++wi) {
         const long long cell = base_cell + wi;
         const bool active = cell < prm.ncells;
-        const float4 o = active ? prm.origins[cell] : make_float4(0.f, 0.f, 0.f, 0.f);
-        const bool sig = active && prm.status[cell] != 0;
-        org[wi] = o;
-        {
-            float va[P], vb[P];
-            sample_column<N, T>(prm.img_a, prm.H, prm.W, o.x, o.y, line, t, va);
-            sample_column<N, T>(prm.img_b, prm.H, prm.W, o.z, o.w, line, t, vb);
-            float2 s = make_float2(0.f, 0.f);
-#pragma unroll
-            for (int p = 0; p < P; ++p) {
-                s.x += va[p];
-                s.y += vb[p];
-            }
-            s = group_sum2<C>(s, s_red, g, gt);
-            const float inv = 1.0f / (float)(N * N);
-            const float ma = s.x * inv, mb = s.y * inv;
-            float2 e = make_float2(0.f, 0.f);
-#pragma unroll
-            for (int p = 0; p < P; ++p) {
-                const float a = __fsub_rn(va[p], ma), b = __fsub_rn(vb[p], mb);
-                z[p] = make_float2(a, b);
-                e.x += a * a;
-                e.y += b * b;
-            }
-            e = group_sum2<C>(e, s_red, g, gt);
-            ok[wi] = sig && e.x > 1e-12f && e.y > 1e-12f;
-            // correlate.rs:136: 1 / (n^2 * sqrt(Ea*Eb)); the factor 1/4 undoes the 2x folded
-            // into each separated spectrum below (exact power-of-two scaling).
-            scale[wi] = 0.25f / ((float)(N * N) * (sqrtf(e.x) * sqrtf(e.y)));
-        }
-        // Forward 2-D FFT: columns (lane = column, interleaved rows) ...
-        fft_line_interleaved<N, T, 1>(z, t, s_roots);
-#pragma unroll
-        for (int k = 0; k < P; ++k) plane[(k + P * rt) * LD + line] = z[k];
-        __syncthreads();
-        // ... then rows (lane = row ky, interleaved columns).
-#pragma unroll
-        for (int q = 0; q < P; ++q) z[q] = plane[line * LD + t + T * q];
-        __syncthreads();
-        fft_line_interleaved<N, T, 1>(z, t, s_roots);
-        // Cross spectrum from Z[k] and its Hermitian partner Z[-k]:
-        //   2FA = Z + conj(Z[-k]), 2FB = -i (Z - conj(Z[-k])), C = conj(2FA) * 2FB.
-#pragma unroll
-        for (int k = 0; k < P; ++k) plane[line * LD + k + P * rt] = z[k];
-        __syncthreads();
-        {
-            const int my = (N - line) % N;
-#pragma unroll
-            for (int k = 0; k < P; ++k) {
-                const int kx = k + P * rt;
-                const float2 m = plane[my * LD + (N - kx) % N];
-                const float far = z[k].x + m.x, fai = z[k].y - m.y;
-                const float fbr = z[k].y + m.y, fbi = m.x - z[k].x;
-                z[k] = make_float2(far * fbr + fai * fbi, far * fbi - fai * fbr);
-            }
-        }
-        __syncthreads();
+        org[wi] = active ? prm.origins[cell] : make_float4(0.f, 0.f, 0.f, 0.f);
+        ok[wi] = active && prm.status[cell] != 0;
+    }
+    if constexpr (C::SHFL_SAMPLE) {
+        sample_column<N, T, false>(prm.img_a, prm.H, prm.W, org[0].x, org[0].y, line, t, z0);
+        sample_column<N, T, true>(prm.img_b, prm.H, prm.W, org[0].z, org[0].w, line, t, z0);
         if constexpr (PAIR) {
-            if (wi == 0) {
+            sample_column<N, T, false>(prm.img_a, prm.H, prm.W, org[1].x, org[1].y, line, t, z1);
+            sample_column<N, T, true>(prm.img_b, prm.H, prm.W, org[1].z, org[1].w, line, t, z1);
+        }
+    } else {
+        sample_column_direct<N, T, false>(prm.img_a, prm.H, prm.W, org[0].x, org[0].y, line, t, z0);
+        sample_column_direct<N, T, true>(prm.img_b, prm.H, prm.W, org[0].z, org[0].w, line, t, z0);
+        if constexpr (PAIR) {
+            sample_column_direct<N, T, false>(prm.img_a, prm.H, prm.W, org[1].x, org[1].y, line, t, z1);
+            sample_column_direct<N, T, true>(prm.img_b, prm.H, prm.W, org[1].z, org[1].w, line, t, z1);
+        }
+    }
+    {
+        float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-                for (int k = 0; k < P; ++k) stash[k] = z[k];
+        for (int p = 0; p < P; ++p) {
+            s.x += z0[p].x;
+            s.y += z0[p].y;
+            if constexpr (PAIR) {
+                s.z += z1[p].x;
+                s.w += z1[p].y;
             }
+        }
+        s = group_sum4<C>(s, s_red, g, gt);
+        constexpr float inv = 1.0f / (float)(N * N);
+        const float m0a = s.x * inv, m0b = s.y * inv, m1a = s.z * inv, m1b = s.w * inv;
+        float4 e = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+            z0[p].x = __fsub_rn(z0[p].x, m0a);
+            z0[p].y = __fsub_rn(z0[p].y, m0b);
+            e.x += z0[p].x * z0[p].x;
+            e.y += z0[p].y * z0[p].y;
+            if constexpr (PAIR) {
+                z1[p].x = __fsub_rn(z1[p].x, m1a);
+                z1[p].y = __fsub_rn(z1[p].y, m1b);
+                e.z += z1[p].x * z1[p].x;
+                e.w += z1[p].y * z1[p].y;
+            }
+        }
+        e = group_sum4<C>(e, s_red, g, gt);
+        // correlate.rs:110 (flat window) and :136 (scale 1 / (n^2 sqrt(Ea Eb))); the factor 1/4
+        // undoes the 2x folded into each separated spectrum (exact power-of-two scaling).
+        ok[0] = ok[0] && e.x > 1e-12f && e.y > 1e-12f;
+        scale[0] = 0.25f / ((float)(N * N) * (sqrtf(e.x) * sqrtf(e.y)));
+        if constexpr (PAIR) {
+            ok[1] = ok[1] && e.z > 1e-12f && e.w > 1e-12f;
+            scale[1] = 0.25f / ((float)(N * N) * (sqrtf(e.z) * sqrtf(e.w)));
         }
     }
 
-    if constexpr (PAIR) {
-        // D = C0 + i*C1: both inverse transforms in one complex transform.
+    // ------------------------------------------------------------------ forward 2-D FFTs
+    float2* plane1 = reinterpret_cast<float2*>(plane1_raw);
+    fft_line_interleaved<N, T, 1>(z0, t, s_roots);
+    if constexpr (PAIR) fft_line_interleaved<N, T, 1>(z1, t, s_roots);
 #pragma unroll
-        for (int k = 0; k < P; ++k) z[k] = make_float2(stash[k].x - z[k].y, stash[k].y + z[k].x);
+    for (int k = 0; k < P; ++k) {
+        plane0[(k + P * rt) * LD + line] = z0[k];
+        if constexpr (PAIR) plane1[(k + P * rt) * LD + line] = z1[k];
     }
-    // Inverse 2-D FFT: rows first (block layout from the forward pass) ...
-    fft_line_blocked<N, T, -1>(z, t, s_roots);
-#pragma unroll
-    for (int k = 0; k < P; ++k) plane[line * LD + t + T * k] = z[k];
     __syncthreads();
-    // ... then columns.
 #pragma unroll
-    for (int q = 0; q < P; ++q) z[q] = plane[(t + T * q) * LD + line];
+    for (int q = 0; q < P; ++q) {
+        z0[q] = plane0[line * LD + t + T * q];
+        if constexpr (PAIR) z1[q] = plane1[line * LD + t + T * q];
+    }
     __syncthreads();
-    fft_line_interleaved<N, T, -1>(z, t, s_roots);
+    fft_line_interleaved<N, T, 1>(z0, t, s_roots);
+    if constexpr (PAIR) fft_line_interleaved<N, T, 1>(z1, t, s_roots);
+    // ------------------------------------------------------------------ cross spectra
+#pragma unroll
+    for (int k = 0; k < P; ++k) {
+        plane0[line * LD + k + P * rt] = z0[k];
+        if constexpr (PAIR) plane1[line * LD + k + P * rt] = z1[k];
+    }
+    __syncthreads();
+    {
+        const int my = (N - line) % N;
+#pragma unroll
+        for (int k = 0; k < P; ++k) {
+            const int kx = (N - (k + P * rt)) % N;
+            const float2 c0 = cross4(z0[k], plane0[my * LD + kx]);
+            if constexpr (PAIR) {
+                const float2 c1 = cross4(z1[k], plane1[my * LD + kx]);
+                z0[k] = make_float2(c0.x - c1.y, c0.y + c1.x);  // D = C0 + i*C1
+            } else {
+                z0[k] = c0;
+            }
+        }
+    }
+    __syncthreads();
+
+    // ------------------------------------------------------------------ inverse 2-D FFT
+    fft_line_blocked<N, T, -1>(z0, t, s_roots);
+#pragma unroll
+    for (int k = 0; k < P; ++k) plane0[line * LD + t + T * k] = z0[k];
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < P; ++q) z0[q] = plane0[(t + T * q) * LD + line];
+    __syncthreads();
+    fft_line_interleaved<N, T, -1>(z0, t, s_roots);
     // Lane now holds corr[y = k + P*rt][x = line]; scale as the reference does (c *= scale).
 #pragma unroll
     for (int k = 0; k < P; ++k) {
-        z[k].x = z[k].x * scale[0];
-        z[k].y = PAIR ? z[k].y * scale[WPG - 1] : 0.0f;
-        plane[(k + P * rt) * LD + line] = z[k];
+        z0[k].x = z0[k].x * scale[0];
+        z0[k].y = PAIR ? z0[k].y * scale[WPG - 1] : 0.0f;
+        plane0[(k + P * rt) * LD + line] = z0[k];
+    }
+
+    // ------------------------------------------------------------------ find_peak
+    // Argmax of both planes (lowest row-major index among equal maxima).
+    float2 best = make_float2(-INFINITY, -INFINITY);
+    int bi0 = 0x7fffffff, bi1 = 0x7fffffff;
+#pragma unroll
+    for (int k = 0; k < P; ++k) {
+        const int idx = (k + P * rt) * N + line;
+        if (z0[k].x > -INFINITY) amax_combine(best.x, bi0, z0[k].x, idx);
+        if (PAIR && z0[k].y > -INFINITY) amax_combine(best.y, bi1, z0[k].y, idx);
+    }
+    group_argmax<C>(best.x, bi0, s_red, g, gt);
+    if constexpr (PAIR) group_argmax<C>(best.y, bi1, s_red, g, gt);
+    if (!(best.x > -INFINITY)) bi0 = 0;
+    if (!(best.y > -INFINITY)) bi1 = 0;
+    __syncthreads();  // the scaled planes are complete in shared memory
+    auto at = [&](int ch, int y, int x) -> float {
+        const float2 v = plane0[(y % N) * LD + (x % N)];
+        return ch == 0 ? v.x : v.y;
+    };
+    // Footprint of the primary peak (correlate.rs:242-254): half-width along +-y, +-x.
+    if (gt < 4 * WPG) {
+        const int ch = gt >> 2, dir = gt & 3;
+        const int bidx = ch == 0 ? bi0 : bi1;
+        const int by = bidx / N, bx = bidx % N;
+        const int sy = dir == 0 ? 1 : (dir == 1 ? N - 1 : 0);
+        const int sx = dir == 2 ? 1 : (dir == 3 ? N - 1 : 0);
+        const float half = 0.5f * (ch == 0 ? best.x : best.y);
+        int k = 0;
+        while (k < N / 2 && at(ch, by + k * sy, bx + k * sx) > half) ++k;
+        s_hw[g][gt] = k;
+    }
+    // Vertical 3-maximum of each column, for the local-maximum test.
+    float* vm = reinterpret_cast<float*>(plane1_raw);  // float2 (PAIR) or float (single) per cell
+    {
+        float2 up, dn;  // neighbours across this lane's block boundary (rows k = -1 and P)
+        if constexpr (T == 1) {
+            up = z0[P - 1];
+            dn = z0[0];
+        } else {
+            const int lane = threadIdx.x & 31;
+            const int base = lane - t;  // first lane of this line
+            const int src_up = base + bitrev<T>((rt + T - 1) % T);
+            const int src_dn = base + bitrev<T>((rt + 1) % T);
+            up.x = __shfl_sync(0xffffffffu, z0[P - 1].x, src_up);
+            up.y = __shfl_sync(0xffffffffu, z0[P - 1].y, src_up);
+            dn.x = __shfl_sync(0xffffffffu, z0[0].x, src_dn);
+            dn.y = __shfl_sync(0xffffffffu, z0[0].y, src_dn);
+        }
+#pragma unroll
+        for (int k = 0; k < P; ++k) {
+            const float2 a = k == 0 ? up : z0[k - 1];
+            const float2 b = k == P - 1 ? dn : z0[k + 1];
+            const float m0 = fmaxf(fmaxf(a.x, b.x), z0[k].x);
+            const int o = (k + P * rt) * LD + line;
+            if constexpr (PAIR) {
+                reinterpret_cast<float2*>(vm)[o] = make_float2(m0, fmaxf(fmaxf(a.y, b.y), z0[k].y));
+            } else {
+                vm[o] = m0;
+            }
+        }
     }
     __syncthreads();
-
-    // --------------------------------------------------------------------------- find_peak
-#pragma unroll
-    for (int wi = 0; wi < WPG; ++wi) {
-        auto at = [&](int y, int x) -> float {
-            const float2 v = plane[(y % N) * LD + (x % N)];
-            return wi == 0 ? v.x : v.y;
+    const int hw0 = max(max(s_hw[g][0], s_hw[g][1]), max(s_hw[g][2], s_hw[g][3]));
+    const int ex0 = max((int)ceilf(1.5f * (float)hw0), 2);
+    int ex1 = 0;
+    if constexpr (PAIR) {
+        const int hw1 = max(max(s_hw[g][4], s_hw[g][5]), max(s_hw[g][6], s_hw[g][7]));
+        ex1 = max((int)ceilf(1.5f * (float)hw1), 2);
+    }
+    // Highest local maximum outside the footprint (correlate.rs:255-267): v is a local maximum
+    // when it equals the maximum of its circular 3x3 neighbourhood.
+    float2 second = make_float2(-INFINITY, -INFINITY);
+    {
+        const int xl = (line + N - 1) % N, xr = (line + 1) % N;
+        const int by0 = bi0 / N, bx0 = bi0 % N, by1 = bi1 / N, bx1 = bi1 % N;
+        auto circ = [](int a, int b) {
+            const int d = abs(a - b);
+            return min(d, N - d);
         };
-        float best = -INFINITY;
-        int bidx = 0x7fffffff;
+        const int cx0 = circ(line, bx0), cx1 = circ(line, bx1);
 #pragma unroll
         for (int k = 0; k < P; ++k) {
-            const float v = wi == 0 ? z[k].x : z[k].y;
-            const int idx = (k + P * rt) * N + line;
-            if (v > -INFINITY) amax_combine(best, bidx, v, idx);
-        }
-        group_argmax<C>(best, bidx, s_red, g, gt);
-        if (!(best > -INFINITY)) bidx = 0;
-        const int by = bidx / N, bx = bidx % N;
-        // Footprint of the primary peak (correlate.rs:242-254): half-width along +-x, +-y.
-        if (gt < 4) {
-            const int sy = gt == 0 ? 1 : (gt == 1 ? N - 1 : 0);
-            const int sx = gt == 2 ? 1 : (gt == 3 ? N - 1 : 0);
-            const float half = 0.5f * best;
-            int k = 0;
-            while (k < N / 2 && at(by + k * sy, bx + k * sx) > half) ++k;
-            s_hw[g][gt] = k;
-        }
-        __syncthreads();
-        const int hw = max(max(s_hw[g][0], s_hw[g][1]), max(s_hw[g][2], s_hw[g][3]));
-        const int exclude = max((int)ceilf(1.5f * (float)hw), 2);
-        // Highest local maximum outside the footprint (correlate.rs:255-267).
-        float second = -INFINITY;
-#pragma unroll
-        for (int k = 0; k < P; ++k) {
-            const float v = wi == 0 ? z[k].x : z[k].y;
-            const int y = k + P * rt, x = line;
-            if (v > second) {
-                const int dy = abs(y - by), dx = abs(x - bx);
-                const int cy = min(dy, N - dy), cx = min(dx, N - dx);
-                if (max(cy, cx) > exclude) {
-                    const bool lm = at(y + N - 1, x + N - 1) <= v && at(y + N - 1, x) <= v && at(y + N - 1, x + 1) <= v &&
-                                    at(y, x + N - 1) <= v && at(y, x + 1) <= v && at(y + 1, x + N - 1) <= v &&
-                                    at(y + 1, x) <= v && at(y + 1, x + 1) <= v;
-                    if (lm) second = v;
-                }
+            const int y = k + P * rt;
+            if constexpr (PAIR) {
+                const float2* v2 = reinterpret_cast<const float2*>(vm);
+                const float2 l = v2[y * LD + xl], c = v2[y * LD + line], r = v2[y * LD + xr];
+                const float h0 = fmaxf(fmaxf(l.x, r.x), c.x), h1 = fmaxf(fmaxf(l.y, r.y), c.y);
+                if (z0[k].x == h0 && max(circ(y, by0), cx0) > ex0) second.x = fmaxf(second.x, z0[k].x);
+                if (z0[k].y == h1 && max(circ(y, by1), cx1) > ex1) second.y = fmaxf(second.y, z0[k].y);
+            } else {
+                const float h0 = fmaxf(fmaxf(vm[y * LD + xl], vm[y * LD + xr]), vm[y * LD + line]);
+                if (z0[k].x == h0 && max(circ(y, by0), cx0) > ex0) second.x = fmaxf(second.x, z0[k].x);
             }
         }
-        second = group_max<C>(second, s_red, g, gt);
-        if (gt == 0) {
-            const long long cell = base_cell + wi;
-            if (cell < prm.ncells) {
-                if (ok[wi]) {
-                    const float sx = subpixel(at(by, bx + N - 1), best, at(by, bx + 1));
-                    const float sy = subpixel(at(by + N - 1, bx), best, at(by + 1, bx));
-                    const float wx = bx >= N / 2 ? (float)bx - (float)N : (float)bx;
-                    const float wy = by >= N / 2 ? (float)by - (float)N : (float)by;
-                    const float pdx = __fadd_rn(wx, sx), pdy = __fadd_rn(wy, sy);
-                    const float ppr = second > 0.0f ? fminf(__fdiv_rn(best, second), MAX_PPR) : MAX_PPR;
-                    const float4 o = org[wi];
-                    prm.raw_dx[cell] = __fadd_rn(__fsub_rn(o.z, o.x), pdx);
-                    prm.raw_dy[cell] = __fadd_rn(__fsub_rn(o.w, o.y), pdy);
-                    prm.raw_ppr[cell] = ppr;
-                    prm.raw_flags[cell] = 0;
-                } else {
-                    prm.raw_dx[cell] = NAN;
-                    prm.raw_dy[cell] = NAN;
-                    prm.raw_ppr[cell] = 0.0f;
-                    prm.raw_flags[cell] = F_NO_SIGNAL;
-                }
+    }
+    second = group_max2<C>(second, s_red, g, gt);
+
+    // ------------------------------------------------------------------ sub-pixel fit, output
+    if (gt < WPG) {
+        const int ch = gt;
+        const long long cell = base_cell + ch;
+        const bool okc = (ch == 0) ? ok[0] : ok[WPG - 1];
+        const float4 o = (ch == 0) ? org[0] : org[WPG - 1];
+        if (cell < prm.ncells) {
+            if (okc) {
+                const int bidx = ch == 0 ? bi0 : bi1;
+                const int by = bidx / N, bx = bidx % N;
+                const float bv = ch == 0 ? best.x : best.y;
+                const float sv = ch == 0 ? second.x : second.y;
+                const float sx = subpixel(at(ch, by, bx + N - 1), bv, at(ch, by, bx + 1));
+                const float sy = subpixel(at(ch, by + N - 1, bx), bv, at(ch, by + 1, bx));
+                const float wx = bx >= N / 2 ? (float)bx - (float)N : (float)bx;
+                const float wy = by >= N / 2 ? (float)by - (float)N : (float)by;
+                const float pdx = __fadd_rn(wx, sx), pdy = __fadd_rn(wy, sy);
+                const float ppr = sv > 0.0f ? fminf(__fdiv_rn(bv, sv), MAX_PPR) : MAX_PPR;
+                prm.raw_dx[cell] = __fadd_rn(__fsub_rn(o.z, o.x), pdx);
+                prm.raw_dy[cell] = __fadd_rn(__fsub_rn(o.w, o.y), pdy);
+                prm.raw_ppr[cell] = ppr;
+                prm.raw_flags[cell] = 0;
+            } else {
+                prm.raw_dx[cell] = NAN;
+                prm.raw_dy[cell] = NAN;
+                prm.raw_ppr[cell] = 0.0f;
+                prm.raw_flags[cell] = F_NO_SIGNAL;
             }
         }
-        __syncthreads();
     }
 }
 
-template <int N, int T, bool PAIR, int G>
+template <class C>
 static cudaError_t launch_t(const CorrParams& p, cudaStream_t s) {
-    using C = CorrCfg<N, T, PAIR, G>;
     static_assert(C::SMEM <= 227 * 1024, "shared memory");
     if (p.ncells <= 0) return cudaSuccess;
-    auto kern = correlate_kernel<N, T, PAIR, G>;
+    auto kern = correlate_kernel<C>;
     // Attribute setting is idempotent and per device; done on every launch for simplicity.
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
     if (e != cudaSuccess) return e;
-    const long long per_block = (long long)G * C::WPG;
+    const long long per_block = (long long)C::G * C::WPG;
     const long long blocks = (p.ncells + per_block - 1) / per_block;
     kern<<<(unsigned)blocks, C::THREADS, C::SMEM, s>>>(p);
     return cudaGetLastError();
@@ -395,20 +562,78 @@ bool corr_supported(int n) {
     }
 }
 
-cudaError_t launch_correlate(int n, const CorrParams& p, cudaStream_t s) {
+// ---------------------------------------------------------------------------------------------
+// Launch variants per window size. Within one size every variant has the same N, T and PAIR,
+// so all of them compute bit-identical results; they differ in groups per CTA, register cap and
+// sampler. Variant 0 is the default; the autotuner (api.cu) times the others on live data.
+// ---------------------------------------------------------------------------------------------
+struct CorrVariant {
+    const char* name;
+    cudaError_t (*launch)(const CorrParams&, cudaStream_t);
+};
+
+#define PIV_V(N, T, PR, G, MB, SH) {#N "/T" #T "/G" #G "/B" #MB "/" #SH, &launch_t<CorrCfg<N, T, PR, G, MB, SH>>}
+static const CorrVariant kV8[] = {PIV_V(8, 1, true, 32, 1, false), PIV_V(8, 1, true, 16, 2, false),
+                                  PIV_V(8, 1, true, 32, 2, true)};
+static const CorrVariant kV12[] = {PIV_V(12, 1, true, 16, 1, false), PIV_V(12, 1, true, 8, 3, false),
+                                   PIV_V(12, 1, true, 16, 2, true)};
+static const CorrVariant kV16[] = {PIV_V(16, 1, true, 16, 2, false), PIV_V(16, 1, true, 8, 4, false),
+                                   PIV_V(16, 1, true, 8, 3, false), PIV_V(16, 1, true, 16, 2, true),
+                                   PIV_V(16, 1, true, 8, 4, true)};
+static const CorrVariant kV24[] = {PIV_V(24, 2, true, 4, 2, true), PIV_V(24, 2, true, 4, 2, false),
+                                   PIV_V(24, 2, true, 2, 4, true)};
+static const CorrVariant kV32[] = {PIV_V(32, 2, true, 4, 2, true), PIV_V(32, 2, true, 4, 2, false),
+                                   PIV_V(32, 2, true, 2, 4, true), PIV_V(32, 2, true, 2, 3, true)};
+static const CorrVariant kV48[] = {PIV_V(48, 4, true, 1, 2, true), PIV_V(48, 4, true, 1, 2, false),
+                                   PIV_V(48, 4, true, 1, 1, true)};
+static const CorrVariant kV64[] = {PIV_V(64, 4, true, 1, 2, true), PIV_V(64, 4, true, 1, 2, false),
+                                   PIV_V(64, 4, true, 1, 1, true)};
+static const CorrVariant kV96[] = {PIV_V(96, 4, true, 1, 1, true), PIV_V(96, 4, true, 1, 1, false)};
+static const CorrVariant kV128[] = {PIV_V(128, 4, false, 1, 1, false), PIV_V(128, 4, false, 1, 1, true)};
+#undef PIV_V
+
+static const CorrVariant* variants(int n, int* count) {
+#define PIV_CASE(N, A)                          \
+    case N:                                     \
+        *count = (int)(sizeof(A) / sizeof(A[0])); \
+        return A;
     switch (n) {
-        case 8: return launch_t<8, 1, true, 32>(p, s);
-        case 12: return launch_t<12, 1, true, 16>(p, s);
-        case 16: return launch_t<16, 1, true, 16>(p, s);
-        case 24: return launch_t<24, 2, true, 4>(p, s);
-        case 32: return launch_t<32, 2, true, 4>(p, s);
-        case 48: return launch_t<48, 4, true, 1>(p, s);
-        case 64: return launch_t<64, 4, true, 1>(p, s);
-        case 96: return launch_t<96, 4, true, 1>(p, s);
-        case 128: return launch_t<128, 4, false, 1>(p, s);
-        default: return cudaErrorInvalidValue;
+        PIV_CASE(8, kV8)
+        PIV_CASE(12, kV12)
+        PIV_CASE(16, kV16)
+        PIV_CASE(24, kV24)
+        PIV_CASE(32, kV32)
+        PIV_CASE(48, kV48)
+        PIV_CASE(64, kV64)
+        PIV_CASE(96, kV96)
+        PIV_CASE(128, kV128)
+        default:
+            *count = 0;
+            return nullptr;
     }
+#undef PIV_CASE
 }
+
+int corr_num_variants(int n) {
+    int c = 0;
+    variants(n, &c);
+    return c;
+}
+
+const char* corr_variant_name(int n, int v) {
+    int c = 0;
+    const CorrVariant* vs = variants(n, &c);
+    return (vs && v >= 0 && v < c) ? vs[v].name : "";
+}
+
+cudaError_t launch_correlate_variant(int n, int v, const CorrParams& p, cudaStream_t s) {
+    int c = 0;
+    const CorrVariant* vs = variants(n, &c);
+    if (!vs || v < 0 || v >= c) return cudaErrorInvalidValue;
+    return vs[v].launch(p, s);
+}
+
+cudaError_t launch_correlate(int n, const CorrParams& p, cudaStream_t s) { return launch_correlate_variant(n, 0, p, s); }
 
 cudaError_t corr_init_device() {
     float2 h[kRootTableLen];

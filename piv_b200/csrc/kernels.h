@@ -28,6 +28,10 @@ struct CorrParams {
 bool corr_supported(int n);
 cudaError_t corr_init_device();  // uploads the root-of-unity table to the current device
 cudaError_t launch_correlate(int n, const CorrParams& p, cudaStream_t s);
+// Launch variants of one window size (identical results; different geometry), for the autotuner.
+int corr_num_variants(int n);
+const char* corr_variant_name(int n, int v);
+cudaError_t launch_correlate_variant(int n, int v, const CorrParams& p, cudaStream_t s);
 // Number of kernel launches launch_correlate issues (for launch accounting).
 constexpr int kCorrLaunches = 1;
 

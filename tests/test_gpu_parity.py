@@ -171,3 +171,21 @@ def test_matches_oracle_on_synthetic_particles():
         fa, fb = an.prepare(a, P.RAW), an.prepare(b, P.RAW)
         _, traces = an.analyze_traced(fa, fb)
         _stage_check(an, traces, a, b, windows)
+
+
+def test_autotuned_variants_give_identical_results():
+    """Launch-geometry autotuning never changes results: variants differ only in geometry."""
+    import piv_b200 as P
+    from piv_b200 import synthetic as S
+    a, b = S.particle_pair(384, 384, 21, 0.05, 0.75, lambda x, y: (3.1 + 0.01 * y, -2.2))
+    for windows in ([128, 64, 32, 16], [96, 48, 24, 12], [64, 32, 16, 8]):
+        an = P.PivAnalyzer(P.PivConfig(windows=windows, overlap=0.75, final_iterations=1))
+        fa, fb = an.prepare(a, P.RAW), an.prepare(b, P.RAW)
+        r0, t0 = an.analyze_traced(fa, fb)
+        chosen = an.autotune(fa, fb)
+        assert set(chosen) == set(windows)
+        r1, t1 = an.analyze_traced(fa, fb)
+        for x, y in zip(t0, t1):
+            assert np.array_equal(x.raw.flags, y.raw.flags)
+            assert same_floats(x.raw.dx, y.raw.dx) and same_floats(x.raw.dy, y.raw.dy)
+            assert same_floats(x.raw.peak_ratio, y.raw.peak_ratio)
