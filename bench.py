@@ -202,6 +202,29 @@ def cpu_baseline(wl, a, b, budget_s=12.0, crop=1024):
                       f"oracle/piv_oracle.cpp, {nthreads} OpenMP threads, {dt:.1f} s"}
 
 
+def run_profile_case(args, wl):
+    """An untimed run for profilers: one pair of the workload, analysed --steps times through the
+    host C ABI with the default launch variants (inputs cached under /tmp between processes)."""
+    import piv_b200 as P
+    w = dict(wl)
+    if args.profile_case != "all":
+        w["windows"] = [int(x) for x in args.profile_case.split(",")]
+    cache = f"/tmp/piv_b200_{args.workload}_pair.npz"
+    if os.path.exists(cache):
+        z = np.load(cache)
+        a, b = z["a"], z["b"]
+    else:
+        a, b = make_inputs(wl)
+        np.savez(cache, a=a, b=b)
+    an = P.PivAnalyzer(piv_config(w), device=0)
+    fa, fb = an.prepare(a, P.RAW), an.prepare(b, P.RAW)
+    for _ in range(max(args.steps, 1)):
+        r = an.analyze(fa, fb)
+    print(json.dumps({"profile_case": w["windows"], "vectors": int(r.field.dx.size), "summary": r.summary.as_dict(),
+                      "launches": an.launches()}))
+    return 0
+
+
 def run_reference(args, wl):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -239,9 +262,14 @@ def main():
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--ref-step-s", type=float, default=3.0)
     ap.add_argument("--ref-crop", type=int, default=1024)
+    ap.add_argument("--profile-case", default=None, metavar="WINDOWS",
+                    help="profiler workload: analyse the workload's pair --steps times with the given comma-separated "
+                         "window schedule (or 'all'), through the host API, untimed")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     wl = WORKLOADS[args.workload]
+    if args.profile_case:
+        return run_profile_case(args, wl)
     if args.impl == "reference":
         return run_reference(args, wl)
 

@@ -173,6 +173,42 @@ int32_t piv_analyze(PivAnalyzer* an, const PivFrame* a, const PivFrame* b, float
 int32_t piv_analyze_device(PivAnalyzer* an, const PivFrame* a, const PivFrame* b, float* dx, float* dy,
                            float* peak_ratio, uint8_t* flags, uint64_t* summary_dev);
 
+/* ----------------------------------------------------------------------------- batching form
+ * No counterpart in the reference, which analyses one pair per call (multipass.rs:136) and
+ * parallelises only inside it. PivAnalyzer::analyze for `count` pairs of equal-size frames in
+ * one go: every stage of every pass is one kernel launch covering all pairs. Outputs are DEVICE
+ * arrays, pair k's final field at offset k * nx*ny (output_grid); summaries_dev (nullable) gets
+ * 8 uint64 per pair (the first 5 as in piv_analyze_device). Asynchronous. */
+int32_t piv_analyze_batch_device(PivAnalyzer* an, const PivFrame* const* a, const PivFrame* const* b, int32_t count,
+                                 float* dx, float* dy, float* peak_ratio, uint8_t* flags, uint64_t* summaries_dev);
+
+/* A fixed batch for streams of frames, replayed from a CUDA graph. It owns a private copy of the
+ * analyzer (configuration and tuned launch variants), a device slab for the raw samples of its
+ * frames (sequential: pairs+1 frames, pair k = (frame k, frame k+1); otherwise 2*pairs frames,
+ * pair k = (frame 2k, frame 2k+1)), the prepared frames, the workspace and an output slab. The
+ * first run executes eagerly (allocating everything), then captures preparation of every frame
+ * and every pass of every pair into one graph; later runs launch that graph. */
+typedef struct PivBatch PivBatch;
+int32_t piv_batch_create(const PivAnalyzer* an, int64_t height, int64_t width, int32_t pairs, int32_t sequential,
+                         int32_t dtype, const PivPreprocessC* pre, PivBatch** out);
+void piv_batch_destroy(PivBatch* batch);
+/* Device slab of raw samples (frames back to back) and its size in bytes. */
+void* piv_batch_input_device(PivBatch* batch);
+int64_t piv_batch_input_bytes(const PivBatch* batch);
+/* Runs the batch on its stream (asynchronous). */
+int32_t piv_batch_run(PivBatch* batch);
+int32_t piv_batch_sync(PivBatch* batch);
+/* Device output slabs: dx, dy, peak ratio (f32) and flags (u8), pairs*nx*ny each; 8 uint64
+ * summary counters per pair; nx*ny is piv_output_grid's. */
+int32_t piv_batch_outputs_device(PivBatch* batch, float** dx, float** dy, float** peak_ratio, uint8_t** flags,
+                                 uint64_t** summaries);
+/* Host convenience: copies `raw` (all frames, pinned memory recommended) into the slab, runs,
+ * copies the results back; any output may be NULL. Blocking. */
+int32_t piv_batch_run_host(PivBatch* batch, const void* raw, float* dx, float* dy, float* peak_ratio, uint8_t* flags,
+                           PivSummaryC* summaries);
+/* Kernels executed per run (counted on the eager first run; the graph replays the same set). */
+int64_t piv_batch_kernels(const PivBatch* batch);
+
 /* PivAnalyzer::analyze_traced (multipass.rs:142-150, PassTrace :72-81): HOST arrays holding
  * every pass back to back (pass 0 cells, then pass 1 ...; piv_pass_grid gives each count):
  * origins 4 floats per cell [ax, ay, bx, by]; raw_* before validation; the rest after.

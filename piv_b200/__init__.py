@@ -10,6 +10,7 @@ from .api import (  # noqa: F401
     MaskConfig,
     PairResult,
     PassTrace,
+    PivBatch,
     PivAnalyzer,
     PivConfig,
     PivError,

@@ -21,7 +21,9 @@ EXPORTS = [
     "piv_analyzer_profile", "piv_analyzer_autotune", "piv_analyzer_variant",
     "piv_frame_create", "piv_frame_destroy", "piv_frame_prepare", "piv_frame_prepare_device",
     "piv_frame_set_prepared", "piv_frame_download", "piv_frame_image_device", "piv_background_device",
-    "piv_analyze", "piv_analyze_device", "piv_analyze_traced",
+    "piv_analyze", "piv_analyze_device", "piv_analyze_traced", "piv_analyze_batch_device",
+    "piv_batch_create", "piv_batch_destroy", "piv_batch_input_device", "piv_batch_input_bytes", "piv_batch_run",
+    "piv_batch_sync", "piv_batch_outputs_device", "piv_batch_run_host", "piv_batch_kernels",
     "piv_place_windows", "piv_correlate_origins", "piv_validate_field", "piv_validate_field_noalloc",
 ]
 
@@ -108,6 +110,16 @@ def load():
         "piv_analyze": ([vp, vp, vp, vp, vp, vp, vp, P(PivSummaryC)], i32),
         "piv_analyze_device": ([vp, vp, vp, vp, vp, vp, vp, vp], i32),
         "piv_analyze_traced": ([vp, vp, vp, P(PivTraceC), P(PivSummaryC)], i32),
+        "piv_analyze_batch_device": ([vp, vp, vp, i32, vp, vp, vp, vp, vp], i32),
+        "piv_batch_create": ([vp, i64, i64, i32, i32, i32, P(PivPreprocessC), P(vp)], i32),
+        "piv_batch_destroy": ([vp], None),
+        "piv_batch_input_device": ([vp], vp),
+        "piv_batch_input_bytes": ([vp], i64),
+        "piv_batch_run": ([vp], i32),
+        "piv_batch_sync": ([vp], i32),
+        "piv_batch_outputs_device": ([vp, P(vp), P(vp), P(vp), P(vp), P(vp)], i32),
+        "piv_batch_run_host": ([vp, vp, vp, vp, vp, vp, vp], i32),
+        "piv_batch_kernels": ([vp], i64),
         "piv_place_windows": ([vp, i64, i64, P(PivGridC), P(PivGridC), vp, vp, vp], i32),
         "piv_correlate_origins": ([vp, vp, vp, i64, vp, i64, vp, vp, vp, vp], i32),
         "piv_validate_field": ([vp, i64, i64, vp, vp, vp, vp, vp, vp, vp, P(PivSummaryC)], i32),

@@ -464,3 +464,64 @@ def _profile_methods():
 
 
 _profile_methods()
+
+
+class PivBatch:
+    """The batching form: a fixed set of frames (sequential pairs (i, i+1), or independent pairs
+    (2k, 2k+1)) analysed by one CUDA graph replay per run. Results are those of
+    PivAnalyzer.analyze on each pair."""
+
+    def __init__(self, analyzer: PivAnalyzer, height, width, pairs, sequential=True, dtype=np.uint16,
+                 cfg: PreprocessConfig = None):
+        cfg = RAW if cfg is None else cfg
+        self.height, self.width, self.pairs, self.sequential = int(height), int(width), int(pairs), bool(sequential)
+        self.dtype = np.dtype(dtype)
+        self.nframes = pairs + 1 if sequential else 2 * pairs
+        self.grid = analyzer.output_grid(height, width)
+        h = ctypes.c_void_p()
+        pc = cfg._c()
+        _check(_lib.load().piv_batch_create(analyzer._h, self.height, self.width, self.pairs, int(self.sequential),
+                                            _dtype_code(np.empty(0, self.dtype)), ctypes.byref(pc), ctypes.byref(h)))
+        self._h = h
+
+    def input_device(self) -> int:
+        return int(_lib.load().piv_batch_input_device(self._h))
+
+    def run(self):
+        _check(_lib.load().piv_batch_run(self._h))
+
+    def sync(self):
+        _check(_lib.load().piv_batch_sync(self._h))
+
+    def kernels(self) -> int:
+        return int(_lib.load().piv_batch_kernels(self._h))
+
+    def outputs_device(self):
+        ptrs = [ctypes.c_void_p() for _ in range(5)]
+        _check(_lib.load().piv_batch_outputs_device(self._h, *[ctypes.byref(p) for p in ptrs]))
+        return [p.value for p in ptrs]
+
+    def run_host(self, frames):
+        """frames: [nframes, H, W] samples. Returns a list of PairResult, one per pair."""
+        frames = np.ascontiguousarray(frames, dtype=self.dtype)
+        if frames.shape != (self.nframes, self.height, self.width):
+            raise ShapeMismatchError(f"expected {(self.nframes, self.height, self.width)}, got {frames.shape}")
+        g = self.grid
+        sh = (self.pairs, g.ny, g.nx)
+        dx, dy, ppr = (np.empty(sh, np.float32) for _ in range(3))
+        fl = np.empty(sh, np.uint8)
+        sums = (_lib.PivSummaryC * self.pairs)()
+        _check(_lib.load().piv_batch_run_host(self._h, _ptr(frames), _ptr(dx), _ptr(dy), _ptr(ppr), _ptr(fl), sums))
+        return [PairResult(VectorField(g, dx[k], dy[k], ppr[k], fl[k]), ValidationSummary._from_c(sums[k]))
+                for k in range(self.pairs)]
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.load().piv_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

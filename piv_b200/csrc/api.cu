@@ -106,7 +106,8 @@ struct PivAnalyzer {
     cudaStream_t cur = nullptr;
     // per-pair workspace, sized for (H, W)
     int64_t H = 0, W = 0;
-    std::vector<PassBuf> passes;
+    int K = 0;                                // pairs the workspace holds
+    std::vector<std::vector<PassBuf>> pairs;  // [pair][pass]
     void* arena = nullptr;
     unsigned long long* d_counts = nullptr;
     long long launches = 0;
@@ -145,6 +146,29 @@ struct PivFrame {
     float* d_bg = nullptr;
 };
 
+struct PivBatch {
+    PivAnalyzer* an = nullptr;  // private analyzer: its workspace is never resized by other calls
+    int64_t H = 0, W = 0;
+    int K = 0;
+    bool sequential = false;
+    int32_t dtype = PIV_DTYPE_U16;
+    PivPreprocessC pre{};
+    size_t frame_bytes = 0;
+    void* raw = nullptr;
+    std::vector<PivFrame*> frames;
+    int64_t cells = 0;
+    void* out = nullptr;
+    float* dx = nullptr;
+    float* dy = nullptr;
+    float* ppr = nullptr;
+    uint8_t* flags = nullptr;
+    unsigned long long* sums = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    long long kernels = 0;  // kernel launches of the eager run
+    int runs = 0;
+};
+
 namespace {
 
 int check_cfg(const PivConfigC* c) {
@@ -168,16 +192,19 @@ int use_device(PivAnalyzer* an) {
     return PIV_OK;
 }
 
-int ensure_workspace(PivAnalyzer* an, int64_t H, int64_t W) {
-    if (an->arena && an->H == H && an->W == W) return PIV_OK;
+// Per-pair workspace for up to K pairs of (H, W) frames: for every pass, origins, signal status,
+// raw field, two flag snapshots and the validated field; 8 summary counters per pair.
+int ensure_workspace(PivAnalyzer* an, int64_t H, int64_t W, int K) {
+    if (an->arena && an->H == H && an->W == W && an->K >= K) return PIV_OK;
     if (an->arena) {
         CUDA_TRY(cudaStreamSynchronize(an->cur));
         CUDA_TRY(cudaFree(an->arena));
         an->arena = nullptr;
     }
-    an->passes.clear();
+    an->pairs.clear();
     const auto wins = an->pass_windows();
-    size_t total = align256(sizeof(unsigned long long) * 8);
+    std::vector<PassBuf> proto;
+    size_t per_pair = 0;
     for (int32_t n : wins) {
         PassBuf pb{};
         int st = make_grid(H, W, n, an->overlap, &pb.grid);
@@ -185,9 +212,10 @@ int ensure_workspace(PivAnalyzer* an, int64_t H, int64_t W) {
         pb.cells = pb.grid.nx * pb.grid.ny;
         if (pb.cells > (int64_t)1 << 30) return fail(PIV_ERR_UNSUPPORTED, "too many windows in one pass");
         const size_t c = (size_t)pb.cells;
-        total += align256(16 * c) + align256(c) + 3 * align256(4 * c) + 3 * align256(c) + 2 * align256(4 * c) + align256(c);
-        an->passes.push_back(pb);
+        per_pair += align256(16 * c) + align256(c) + 3 * align256(4 * c) + 3 * align256(c) + 2 * align256(4 * c) + align256(c);
+        proto.push_back(pb);
     }
+    const size_t total = align256(sizeof(unsigned long long) * 8 * (size_t)K) + per_pair * (size_t)K;
     CUDA_TRY(cudaMalloc(&an->arena, total));
     char* p = (char*)an->arena;
     auto take = [&](size_t bytes) {
@@ -195,23 +223,28 @@ int ensure_workspace(PivAnalyzer* an, int64_t H, int64_t W) {
         p += align256(bytes);
         return r;
     };
-    an->d_counts = (unsigned long long*)take(sizeof(unsigned long long) * 8);
-    for (auto& pb : an->passes) {
-        const size_t c = (size_t)pb.cells;
-        pb.origins = (float4*)take(16 * c);
-        pb.status = (uint8_t*)take(c);
-        pb.raw_dx = (float*)take(4 * c);
-        pb.raw_dy = (float*)take(4 * c);
-        pb.raw_ppr = (float*)take(4 * c);
-        pb.raw_flags = (uint8_t*)take(c);
-        pb.f1 = (uint8_t*)take(c);
-        pb.f2 = (uint8_t*)take(c);
-        pb.dx = (float*)take(4 * c);
-        pb.dy = (float*)take(4 * c);
-        pb.flags = (uint8_t*)take(c);
+    an->d_counts = (unsigned long long*)take(sizeof(unsigned long long) * 8 * (size_t)K);
+    for (int k = 0; k < K; ++k) {
+        std::vector<PassBuf> passes = proto;
+        for (auto& pb : passes) {
+            const size_t c = (size_t)pb.cells;
+            pb.origins = (float4*)take(16 * c);
+            pb.status = (uint8_t*)take(c);
+            pb.raw_dx = (float*)take(4 * c);
+            pb.raw_dy = (float*)take(4 * c);
+            pb.raw_ppr = (float*)take(4 * c);
+            pb.raw_flags = (uint8_t*)take(c);
+            pb.f1 = (uint8_t*)take(c);
+            pb.f2 = (uint8_t*)take(c);
+            pb.dx = (float*)take(4 * c);
+            pb.dy = (float*)take(4 * c);
+            pb.flags = (uint8_t*)take(c);
+        }
+        an->pairs.push_back(passes);
     }
     an->H = H;
     an->W = W;
+    an->K = K;
     return PIV_OK;
 }
 
@@ -227,44 +260,65 @@ int alloc_stats(PivFrame* f) {
     return PIV_OK;
 }
 
-// The multipass loop (multipass.rs:152-192): every pass is placement -> correlation ->
-// validation on the analyzer's stream; the predictor is the previous pass's validated field.
-int run_passes(PivAnalyzer* an, const PivFrame* a, const PivFrame* b, bool tune = false) {
-    if (!a || !b) return fail(PIV_ERR_ARGUMENT, "null frame");
-    if (a->H != b->H || a->W != b->W)
-        return fail(PIV_ERR_SHAPE_MISMATCH, "frames have different shapes: (%lld, %lld) vs (%lld, %lld)", (long long)a->H,
-                    (long long)a->W, (long long)b->H, (long long)b->W);
+// The multipass loop (multipass.rs:152-192) for K pairs of equal size at once: every pass is
+// placement -> correlation -> validation, each stage ONE launch covering all K pairs, on the
+// analyzer's stream; the predictor of pair k is its own previous pass's validated field.
+int run_passes(PivAnalyzer* an, const PivFrame* const* a, const PivFrame* const* b, int K, bool tune = false) {
+    if (K <= 0) return fail(PIV_ERR_ARGUMENT, "no pairs");
+    for (int k = 0; k < K; ++k) {
+        if (!a[k] || !b[k]) return fail(PIV_ERR_ARGUMENT, "null frame");
+        if (a[k]->H != b[k]->H || a[k]->W != b[k]->W)
+            return fail(PIV_ERR_SHAPE_MISMATCH, "frames have different shapes: (%lld, %lld) vs (%lld, %lld)",
+                        (long long)a[k]->H, (long long)a[k]->W, (long long)b[k]->H, (long long)b[k]->W);
+        if (a[k]->H != a[0]->H || a[k]->W != a[0]->W)
+            return fail(PIV_ERR_SHAPE_MISMATCH, "all pairs of a batch must have the same frame size");
+    }
+    const int64_t H = a[0]->H, W = a[0]->W;
     int st = use_device(an);
     if (st) return st;
-    st = ensure_workspace(an, a->H, a->W);
+    st = ensure_workspace(an, H, W, K);
     if (st) return st;
-    const bool use_stats = needs_stats(an, a) || needs_stats(an, b);
-    if (use_stats && !(a->stats_valid && b->stats_valid))
-        return fail(PIV_ERR_ARGUMENT, "frame statistics missing for the signal mask");
-    for (size_t i = 0; i < an->passes.size(); ++i) {
-        PassBuf& pb = an->passes[i];
-        PlaceParams pp{};
-        pp.grid = to_gp(pb.grid);
-        pp.H = (int)a->H;
-        pp.W = (int)a->W;
-        pp.has_pred = i > 0;
-        if (i > 0) {
-            pp.pgrid = to_gp(an->passes[i - 1].grid);
-            pp.pdx = an->passes[i - 1].dx;
-            pp.pdy = an->passes[i - 1].dy;
+    std::vector<int> use_stats(K);
+    for (int k = 0; k < K; ++k) {
+        use_stats[k] = needs_stats(an, a[k]) || needs_stats(an, b[k]);
+        if (use_stats[k] && !(a[k]->stats_valid && b[k]->stats_valid))
+            return fail(PIV_ERR_ARGUMENT, "frame statistics missing for the signal mask");
+    }
+    const size_t npass = an->pairs[0].size();
+    std::vector<PlaceParams> pps(K);
+    std::vector<CorrParams> cps(K);
+    std::vector<ValidateParams> vps(K);
+    for (size_t i = 0; i < npass; ++i) {
+        for (int k = 0; k < K; ++k) {
+            PassBuf& pb = an->pairs[k][i];
+            PlaceParams& pp = pps[k];
+            pp = PlaceParams{};
+            pp.grid = to_gp(pb.grid);
+            pp.H = (int)H;
+            pp.W = (int)W;
+            pp.has_pred = i > 0;
+            if (i > 0) {
+                pp.pgrid = to_gp(an->pairs[k][i - 1].grid);
+                pp.pdx = an->pairs[k][i - 1].dx;
+                pp.pdy = an->pairs[k][i - 1].dy;
+            }
+            pp.origins = pb.origins;
+            pp.status = pb.status;
+            pp.use_stats = use_stats[k];
+            if (use_stats[k]) {
+                pp.sa = stats_of(a[k]);
+                pp.sb = stats_of(b[k]);
+            }
+            pp.min_mean = an->min_mean;
+            pp.min_std = an->min_std;
+            cps[k] = CorrParams{a[k]->image, b[k]->image, (int)H, (int)W, pb.origins, pb.status, (int)pb.cells,
+                                pb.raw_dx, pb.raw_dy, pb.raw_ppr, pb.raw_flags};
+            vps[k] = ValidateParams{(int)pb.grid.nx, (int)pb.grid.ny, pb.raw_dx, pb.raw_dy, pb.raw_ppr, pb.raw_flags,
+                                    pb.f1, pb.f2, pb.dx, pb.dy, pb.flags, (float)an->windows[0] / 2.0f,
+                                    an->ppr_threshold, an->median_threshold, an->median_eps, an->replace};
         }
-        pp.origins = pb.origins;
-        pp.status = pb.status;
-        pp.use_stats = use_stats;
-        if (use_stats) {
-            pp.sa = stats_of(a);
-            pp.sb = stats_of(b);
-        }
-        pp.min_mean = an->min_mean;
-        pp.min_std = an->min_std;
-        CUDA_TRY(launch_place(pp, an->cur));
-        CorrParams cp{a->image, b->image, (int)a->H, (int)a->W, pb.origins, pb.status, (int)pb.cells,
-                      pb.raw_dx, pb.raw_dy, pb.raw_ppr, pb.raw_flags};
+        int nl = 0;
+        CUDA_TRY(launch_place_items(pps.data(), K, an->cur, &nl));
         cudaEvent_t ev0 = nullptr, ev1 = nullptr;
         if (an->profiling) {
             for (cudaEvent_t* ev : {&ev0, &ev1}) {
@@ -277,7 +331,7 @@ int run_passes(PivAnalyzer* an, const PivFrame* a, const PivFrame* b, bool tune 
             }
             CUDA_TRY(cudaEventRecord(ev0, an->cur));
         }
-        const int nwin = (int)pb.grid.window;
+        const int nwin = (int)an->pairs[0][i].grid.window;
         if (tune) {
             // Time every launch variant of this window size on this pass's data (all compute the
             // same results) and keep the fastest for later calls.
@@ -287,14 +341,13 @@ int run_passes(PivAnalyzer* an, const PivFrame* a, const PivFrame* b, bool tune 
             float best = 1e30f;
             int best_v = 0;
             for (int v = 0; v < corr_num_variants(nwin); ++v) {
-                CUDA_TRY(launch_correlate_variant(nwin, v, cp, an->cur));
+                CUDA_TRY(launch_correlate_items(nwin, v, cps.data(), K, an->cur, &nl));
                 CUDA_TRY(cudaEventRecord(t0, an->cur));
-                for (int r = 0; r < 3; ++r) CUDA_TRY(launch_correlate_variant(nwin, v, cp, an->cur));
+                for (int r = 0; r < 3; ++r) CUDA_TRY(launch_correlate_items(nwin, v, cps.data(), K, an->cur, &nl));
                 CUDA_TRY(cudaEventRecord(t1, an->cur));
                 CUDA_TRY(cudaEventSynchronize(t1));
                 float ms = 0.0f;
                 CUDA_TRY(cudaEventElapsedTime(&ms, t0, t1));
-                an->launches += 4;
                 if (ms < best) {
                     best = ms;
                     best_v = v;
@@ -304,22 +357,28 @@ int run_passes(PivAnalyzer* an, const PivFrame* a, const PivFrame* b, bool tune 
             cudaEventDestroy(t1);
             an->variant[nwin] = best_v;
         }
-        CUDA_TRY(launch_correlate_variant(nwin, an->variant[nwin], cp, an->cur));
+        CUDA_TRY(launch_correlate_items(nwin, an->variant[nwin], cps.data(), K, an->cur, &nl));
         if (an->profiling) {
             CUDA_TRY(cudaEventRecord(ev1, an->cur));
-            if (an->pending.size() < an->passes.size()) an->pending.resize(an->passes.size());
+            if (an->pending.size() < npass) an->pending.resize(npass);
             an->pending[i].push_back({ev0, ev1});
         }
-        ValidateParams vp{(int)pb.grid.nx, (int)pb.grid.ny, pb.raw_dx, pb.raw_dy, pb.raw_ppr, pb.raw_flags, pb.f1, pb.f2,
-                          pb.dx, pb.dy, pb.flags, (float)an->windows[0] / 2.0f, an->ppr_threshold,
-                          an->median_threshold, an->median_eps, an->replace};
-        CUDA_TRY(launch_validate(vp, an->cur));
-        an->launches += 1 + kCorrLaunches + kValidateLaunches;
+        CUDA_TRY(launch_validate_items(vps.data(), K, an->cur, &nl));
+        an->launches += nl;
     }
-    const PassBuf& last = an->passes.back();
-    CUDA_TRY(launch_summary(last.flags, (int)last.cells, an->d_counts, an->cur));
-    an->launches += kSummaryLaunches;
+    std::vector<SummaryItem> sums(K);
+    for (int k = 0; k < K; ++k) {
+        const PassBuf& last = an->pairs[k].back();
+        sums[k] = SummaryItem{last.flags, (int)last.cells, an->d_counts + 8 * (size_t)k};
+    }
+    int nl = 0;
+    CUDA_TRY(launch_summary_items(sums.data(), K, an->cur, &nl));
+    an->launches += nl;
     return PIV_OK;
+}
+
+int run_passes(PivAnalyzer* an, const PivFrame* a, const PivFrame* b, bool tune = false) {
+    return run_passes(an, &a, &b, 1, tune);
 }
 
 int copy_summary(PivAnalyzer* an, PivSummaryC* s) {
@@ -687,7 +746,7 @@ int32_t piv_analyze_device(PivAnalyzer* an, const PivFrame* a, const PivFrame* b
     if (!an) return fail(PIV_ERR_ARGUMENT, "null analyzer");
     int st = run_passes(an, a, b);
     if (st) return st;
-    const PassBuf& last = an->passes.back();
+    const PassBuf& last = an->pairs[0].back();
     const size_t c = (size_t)last.cells;
     if (dx) CUDA_TRY(cudaMemcpyAsync(dx, last.dx, 4 * c, cudaMemcpyDeviceToDevice, an->cur));
     if (dy) CUDA_TRY(cudaMemcpyAsync(dy, last.dy, 4 * c, cudaMemcpyDeviceToDevice, an->cur));
@@ -703,7 +762,7 @@ int32_t piv_analyze(PivAnalyzer* an, const PivFrame* a, const PivFrame* b, float
     if (!an) return fail(PIV_ERR_ARGUMENT, "null analyzer");
     int st = run_passes(an, a, b);
     if (st) return st;
-    const PassBuf& last = an->passes.back();
+    const PassBuf& last = an->pairs[0].back();
     const size_t c = (size_t)last.cells;
     if (dx) CUDA_TRY(cudaMemcpyAsync(dx, last.dx, 4 * c, cudaMemcpyDeviceToHost, an->cur));
     if (dy) CUDA_TRY(cudaMemcpyAsync(dy, last.dy, 4 * c, cudaMemcpyDeviceToHost, an->cur));
@@ -720,7 +779,7 @@ int32_t piv_analyze_traced(PivAnalyzer* an, const PivFrame* a, const PivFrame* b
     int st = run_passes(an, a, b);
     if (st) return st;
     size_t off = 0;
-    for (const PassBuf& pb : an->passes) {
+    for (const PassBuf& pb : an->pairs[0]) {
         const size_t c = (size_t)pb.cells;
         auto d2h = [&](void* dst, const void* src, size_t es) -> cudaError_t {
             if (!dst) return cudaSuccess;
@@ -897,5 +956,221 @@ int32_t piv_validate_field(PivAnalyzer* an, int64_t ny, int64_t nx, const float*
     }
     return PIV_OK;
 }
+
+int32_t piv_analyze_batch_device(PivAnalyzer* an, const PivFrame* const* a, const PivFrame* const* b, int32_t count,
+                                 float* dx, float* dy, float* peak_ratio, uint8_t* flags, uint64_t* summaries_dev) {
+    if (!an || !a || !b) return fail(PIV_ERR_ARGUMENT, "null argument");
+    int st = run_passes(an, a, b, count);
+    if (st) return st;
+    for (int k = 0; k < count; ++k) {
+        const PassBuf& last = an->pairs[k].back();
+        const size_t c = (size_t)last.cells;
+        if (dx) CUDA_TRY(cudaMemcpyAsync(dx + k * c, last.dx, 4 * c, cudaMemcpyDeviceToDevice, an->cur));
+        if (dy) CUDA_TRY(cudaMemcpyAsync(dy + k * c, last.dy, 4 * c, cudaMemcpyDeviceToDevice, an->cur));
+        if (peak_ratio) CUDA_TRY(cudaMemcpyAsync(peak_ratio + k * c, last.raw_ppr, 4 * c, cudaMemcpyDeviceToDevice, an->cur));
+        if (flags) CUDA_TRY(cudaMemcpyAsync(flags + k * c, last.flags, c, cudaMemcpyDeviceToDevice, an->cur));
+    }
+    if (summaries_dev)
+        CUDA_TRY(cudaMemcpyAsync(summaries_dev, an->d_counts, 8 * sizeof(unsigned long long) * (size_t)count,
+                                 cudaMemcpyDeviceToDevice, an->cur));
+    return PIV_OK;
+}
+
+namespace {
+
+// One run of a batch: prepare every frame from the slab, all passes of all pairs, outputs.
+int batch_record(PivBatch* bt) {
+    PivAnalyzer* an = bt->an;
+    const int nf = (int)bt->frames.size();
+    for (int i = 0; i < nf; ++i) {
+        int st = prepare_common(an, bt->frames[i], (const char*)bt->raw + (size_t)i * bt->frame_bytes, bt->dtype, &bt->pre,
+                                nullptr);
+        if (st) return st;
+    }
+    std::vector<const PivFrame*> fa(bt->K), fb(bt->K);
+    for (int k = 0; k < bt->K; ++k) {
+        fa[k] = bt->sequential ? bt->frames[k] : bt->frames[2 * k];
+        fb[k] = bt->sequential ? bt->frames[k + 1] : bt->frames[2 * k + 1];
+    }
+    return piv_analyze_batch_device(an, fa.data(), fb.data(), bt->K, bt->dx, bt->dy, bt->ppr, bt->flags,
+                                    (uint64_t*)bt->sums);
+}
+
+}  // namespace
+
+int32_t piv_batch_create(const PivAnalyzer* parent, int64_t height, int64_t width, int32_t pairs, int32_t sequential,
+                         int32_t dtype, const PivPreprocessC* pre, PivBatch** out) {
+    if (!parent || !out || pairs <= 0) return fail(PIV_ERR_ARGUMENT, "bad argument");
+    *out = nullptr;
+    const size_t es = dtype_size(dtype);
+    if (!es) return fail(PIV_ERR_ARGUMENT, "unknown dtype %d", dtype);
+    PivGridC g;
+    int st = make_grid(height, width, parent->windows.back(), parent->overlap, &g);
+    if (st) return st;
+    for (int32_t n : parent->windows) {
+        st = make_grid(height, width, n, parent->overlap, &g);
+        if (st) return st;
+    }
+    make_grid(height, width, parent->windows.back(), parent->overlap, &g);
+    CUDA_TRY(cudaSetDevice(parent->device));
+    PivBatch* bt = new PivBatch();
+    PivAnalyzer* an = new PivAnalyzer();
+    an->windows = parent->windows;
+    an->overlap = parent->overlap;
+    an->final_iterations = parent->final_iterations;
+    an->min_mean = parent->min_mean;
+    an->min_std = parent->min_std;
+    an->ppr_threshold = parent->ppr_threshold;
+    an->median_threshold = parent->median_threshold;
+    an->median_eps = parent->median_eps;
+    an->replace = parent->replace;
+    an->device = parent->device;
+    for (int i = 0; i < 129; ++i) an->variant[i] = parent->variant[i];
+    bt->an = an;
+    bt->H = height;
+    bt->W = width;
+    bt->K = pairs;
+    bt->sequential = sequential != 0;
+    bt->dtype = dtype;
+    bt->pre = pre ? *pre : PivPreprocessC{1.0f, 4, 0.02f, 0.0};
+    bt->frame_bytes = es * (size_t)height * (size_t)width;
+    bt->cells = g.nx * g.ny;
+    const int nf = bt->sequential ? pairs + 1 : 2 * pairs;
+    const size_t c = (size_t)bt->cells * (size_t)pairs;
+    cudaError_t e = cudaStreamCreateWithFlags(&an->own, cudaStreamNonBlocking);
+    an->cur = an->own;
+    if (e == cudaSuccess) e = cudaMalloc(&bt->raw, bt->frame_bytes * (size_t)nf);
+    if (e == cudaSuccess)
+        e = cudaMalloc(&bt->out, align256(4 * c) * 3 + align256(c) + align256(8 * sizeof(unsigned long long) * pairs));
+    if (e != cudaSuccess) {
+        piv_batch_destroy(bt);
+        return fail(PIV_ERR_CUDA, "batch allocation: %s", cudaGetErrorString(e));
+    }
+    char* p = (char*)bt->out;
+    bt->dx = (float*)p;
+    p += align256(4 * c);
+    bt->dy = (float*)p;
+    p += align256(4 * c);
+    bt->ppr = (float*)p;
+    p += align256(4 * c);
+    bt->flags = (uint8_t*)p;
+    p += align256(c);
+    bt->sums = (unsigned long long*)p;
+    for (int i = 0; i < nf; ++i) {
+        PivFrame* f = nullptr;
+        st = piv_frame_create(an, height, width, &f);
+        if (st) {
+            piv_batch_destroy(bt);
+            return st;
+        }
+        bt->frames.push_back(f);
+    }
+    *out = bt;
+    return PIV_OK;
+}
+
+void piv_batch_destroy(PivBatch* bt) {
+    if (!bt) return;
+    if (bt->an) {
+        cudaSetDevice(bt->an->device);
+        if (bt->an->own) cudaStreamSynchronize(bt->an->own);
+    }
+    if (bt->exec) cudaGraphExecDestroy(bt->exec);
+    if (bt->graph) cudaGraphDestroy(bt->graph);
+    for (PivFrame* f : bt->frames) piv_frame_destroy(f);
+    cudaFree(bt->raw);
+    cudaFree(bt->out);
+    piv_analyzer_destroy(bt->an);
+    delete bt;
+}
+
+void* piv_batch_input_device(PivBatch* bt) { return bt ? bt->raw : nullptr; }
+
+int64_t piv_batch_input_bytes(const PivBatch* bt) {
+    return bt ? (int64_t)(bt->frame_bytes * bt->frames.size()) : 0;
+}
+
+int32_t piv_batch_run(PivBatch* bt) {
+    if (!bt) return fail(PIV_ERR_ARGUMENT, "null batch");
+    PivAnalyzer* an = bt->an;
+    int st = use_device(an);
+    if (st) return st;
+    if (bt->exec) {
+        CUDA_TRY(cudaGraphLaunch(bt->exec, an->cur));
+        ++bt->runs;
+        return PIV_OK;
+    }
+    // First run: eager (allocates the workspace and frame buffers), then capture the same work.
+    const long long l0 = an->launches;
+    st = batch_record(bt);
+    if (st) return st;
+    bt->kernels = an->launches - l0;
+    CUDA_TRY(cudaStreamSynchronize(an->cur));
+    CUDA_TRY(cudaStreamBeginCapture(an->cur, cudaStreamCaptureModeRelaxed));
+    st = batch_record(bt);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(an->cur, &graph);
+    if (st) {
+        if (graph) cudaGraphDestroy(graph);
+        return st;
+    }
+    if (ce != cudaSuccess) return fail(PIV_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+    bt->graph = graph;
+    CUDA_TRY(cudaGraphInstantiate(&bt->exec, bt->graph, 0));
+    ++bt->runs;
+    return PIV_OK;
+}
+
+int32_t piv_batch_sync(PivBatch* bt) {
+    if (!bt) return fail(PIV_ERR_ARGUMENT, "null batch");
+    CUDA_TRY(cudaSetDevice(bt->an->device));
+    CUDA_TRY(cudaStreamSynchronize(bt->an->cur));
+    return PIV_OK;
+}
+
+int32_t piv_batch_outputs_device(PivBatch* bt, float** dx, float** dy, float** peak_ratio, uint8_t** flags,
+                                 uint64_t** summaries) {
+    if (!bt) return fail(PIV_ERR_ARGUMENT, "null batch");
+    if (dx) *dx = bt->dx;
+    if (dy) *dy = bt->dy;
+    if (peak_ratio) *peak_ratio = bt->ppr;
+    if (flags) *flags = bt->flags;
+    if (summaries) *summaries = (uint64_t*)bt->sums;
+    return PIV_OK;
+}
+
+int32_t piv_batch_run_host(PivBatch* bt, const void* raw, float* dx, float* dy, float* peak_ratio, uint8_t* flags,
+                           PivSummaryC* summaries) {
+    if (!bt || !raw) return fail(PIV_ERR_ARGUMENT, "null argument");
+    PivAnalyzer* an = bt->an;
+    int st = use_device(an);
+    if (st) return st;
+    CUDA_TRY(cudaMemcpyAsync(bt->raw, raw, bt->frame_bytes * bt->frames.size(), cudaMemcpyHostToDevice, an->cur));
+    st = piv_batch_run(bt);
+    if (st) return st;
+    const size_t c = (size_t)bt->cells * (size_t)bt->K;
+    if (dx) CUDA_TRY(cudaMemcpyAsync(dx, bt->dx, 4 * c, cudaMemcpyDeviceToHost, an->cur));
+    if (dy) CUDA_TRY(cudaMemcpyAsync(dy, bt->dy, 4 * c, cudaMemcpyDeviceToHost, an->cur));
+    if (peak_ratio) CUDA_TRY(cudaMemcpyAsync(peak_ratio, bt->ppr, 4 * c, cudaMemcpyDeviceToHost, an->cur));
+    if (flags) CUDA_TRY(cudaMemcpyAsync(flags, bt->flags, c, cudaMemcpyDeviceToHost, an->cur));
+    std::vector<unsigned long long> hs;
+    if (summaries) {
+        hs.resize(8 * (size_t)bt->K);
+        CUDA_TRY(cudaMemcpyAsync(hs.data(), bt->sums, sizeof(unsigned long long) * hs.size(), cudaMemcpyDeviceToHost,
+                                 an->cur));
+    }
+    CUDA_TRY(cudaStreamSynchronize(an->cur));
+    if (summaries)
+        for (int k = 0; k < bt->K; ++k) {
+            summaries[k].no_signal = (int64_t)hs[8 * k + 0];
+            summaries[k].low_ppr = (int64_t)hs[8 * k + 1];
+            summaries[k].median_outliers = (int64_t)hs[8 * k + 2];
+            summaries[k].out_of_range = (int64_t)hs[8 * k + 3];
+            summaries[k].replaced = (int64_t)hs[8 * k + 4];
+        }
+    return PIV_OK;
+}
+
+int64_t piv_batch_kernels(const PivBatch* bt) { return bt ? bt->kernels : 0; }
 
 }  // extern "C"

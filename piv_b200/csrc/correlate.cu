@@ -41,14 +41,27 @@ struct CorrCfg {
     static constexpr int P = N / T;
     static constexpr int NT = N * T;
     static constexpr int THREADS = G * NT;
-    static constexpr int LD = N + 1;
     static constexpr int WPG = PAIR ? 2 : 1;
+    // Shared-memory plane layout (in float2 units), chosen so that every access pattern of a
+    // half-warp (16 lanes = 16/T lines x T lanes) hits 16 distinct 8-byte bank pairs:
+    //   A(row, col) = row*LD + (row/P)*Q + col           transposes, correlation plane
+    //   B(ky, kx)   = ky*LD + (ky/P)*Q + kx + (kx/P)      Hermitian-partner exchange (T > 1)
+    // with LD = N + 1 for T = 1; otherwise LD >= N + T - 1, LD = T (mod 16) (lines of a
+    // half-warp step by T banks, its T lanes fill the gap) and Q making a block of P rows step
+    // by 16/T bank pairs.
+    static constexpr int LD = (T == 1) ? N + 1 : ((N + T - 1 + 15 - T) / 16) * 16 + T;
+    static constexpr int Q = (T == 1) ? 0 : ((16 / T - (P * LD) % 16) % 16 + 16) % 16;
+    static constexpr int PLANE_ELEMS = ((N * LD + (T - 1) * Q) + 1) / 2 * 2;
     // Shuffle segment: largest power of two dividing NT, at most a warp.
     static constexpr int SW = (NT % 32 == 0) ? 32 : (NT % 16 == 0) ? 16 : (NT % 8 == 0) ? 8 : (NT % 4 == 0) ? 4 : (NT % 2 == 0) ? 2 : 1;
     static constexpr int NSEG = NT / SW;
     // plane0: float2 N x LD; plane1: float2 (PAIR) or float (single) N x LD.
-    static constexpr size_t PLANE0 = sizeof(float2) * (size_t)N * LD;
-    static constexpr size_t PLANE1 = (PAIR ? sizeof(float2) : sizeof(float)) * (size_t)N * LD;
+    static constexpr size_t PLANE0 = sizeof(float2) * (size_t)PLANE_ELEMS;
+    static constexpr size_t PLANE1 = ((PAIR ? sizeof(float2) : sizeof(float)) * (size_t)PLANE_ELEMS + 15) / 16 * 16;
+    __host__ __device__ static constexpr int A(int row, int col) { return row * LD + (row / P) * Q + col; }
+    __host__ __device__ static constexpr int B(int ky, int kx) {
+        return T == 1 ? ky * LD + kx : ky * LD + (ky / P) * Q + kx + kx / P;
+    }
     static constexpr size_t SMEM = (size_t)G * (PLANE0 + PLANE1) + sizeof(float2) * N + sizeof(float) * (size_t)G * NSEG * 4 + 64;
 };
 
@@ -265,8 +278,11 @@ __device__ __forceinline__ float2 cross4(float2 z, float2 m) {
 }
 
 template <class C>
-__global__ void __launch_bounds__(C::THREADS, C::MINB) correlate_kernel(const CorrParams prm) {
-    constexpr int N = C::N, T = C::T, G = C::G, P = C::P, NT = C::NT, LD = C::LD, WPG = C::WPG;
+__global__ void __launch_bounds__(C::THREADS, C::MINB) correlate_kernel(const __grid_constant__ CorrBatch batch) {
+    constexpr int N = C::N, T = C::T, G = C::G, P = C::P, NT = C::NT, WPG = C::WPG;
+    const int item = batch_item(batch.block_start, batch.n, (int)blockIdx.x);
+    const CorrParams& prm = batch.item[item];
+    const int block = (int)blockIdx.x - batch.block_start[item];
     constexpr bool PAIR = C::PAIR;
     extern __shared__ float4 smem_f4[];
     char* sbase = reinterpret_cast<char*>(smem_f4);
@@ -285,7 +301,7 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB) correlate_kernel(const Co
     for (int i = tid; i < N; i += C::THREADS) s_roots[i] = c_roots[root_off(N) + i];
     __syncthreads();
 
-    const long long base_cell = ((long long)blockIdx.x * G + g) * WPG;
+    const long long base_cell = ((long long)block * G + g) * WPG;
     float4 org[WPG];
     bool ok[WPG];
     float scale[WPG];
@@ -360,14 +376,14 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB) correlate_kernel(const Co
     if constexpr (PAIR) fft_line_interleaved<N, T, 1>(z1, t, s_roots);
 #pragma unroll
     for (int k = 0; k < P; ++k) {
-        plane0[(k + P * rt) * LD + line] = z0[k];
-        if constexpr (PAIR) plane1[(k + P * rt) * LD + line] = z1[k];
+        plane0[C::A(k + P * rt, line)] = z0[k];
+        if constexpr (PAIR) plane1[C::A(k + P * rt, line)] = z1[k];
     }
     __syncthreads();
 #pragma unroll
     for (int q = 0; q < P; ++q) {
-        z0[q] = plane0[line * LD + t + T * q];
-        if constexpr (PAIR) z1[q] = plane1[line * LD + t + T * q];
+        z0[q] = plane0[C::A(line, t + T * q)];
+        if constexpr (PAIR) z1[q] = plane1[C::A(line, t + T * q)];
     }
     __syncthreads();
     fft_line_interleaved<N, T, 1>(z0, t, s_roots);
@@ -375,8 +391,8 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB) correlate_kernel(const Co
     // ------------------------------------------------------------------ cross spectra
 #pragma unroll
     for (int k = 0; k < P; ++k) {
-        plane0[line * LD + k + P * rt] = z0[k];
-        if constexpr (PAIR) plane1[line * LD + k + P * rt] = z1[k];
+        plane0[C::B(line, k + P * rt)] = z0[k];
+        if constexpr (PAIR) plane1[C::B(line, k + P * rt)] = z1[k];
     }
     __syncthreads();
     {
@@ -384,9 +400,9 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB) correlate_kernel(const Co
 #pragma unroll
         for (int k = 0; k < P; ++k) {
             const int kx = (N - (k + P * rt)) % N;
-            const float2 c0 = cross4(z0[k], plane0[my * LD + kx]);
+            const float2 c0 = cross4(z0[k], plane0[C::B(my, kx)]);
             if constexpr (PAIR) {
-                const float2 c1 = cross4(z1[k], plane1[my * LD + kx]);
+                const float2 c1 = cross4(z1[k], plane1[C::B(my, kx)]);
                 z0[k] = make_float2(c0.x - c1.y, c0.y + c1.x);  // D = C0 + i*C1
             } else {
                 z0[k] = c0;
@@ -398,10 +414,10 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB) correlate_kernel(const Co
     // ------------------------------------------------------------------ inverse 2-D FFT
     fft_line_blocked<N, T, -1>(z0, t, s_roots);
 #pragma unroll
-    for (int k = 0; k < P; ++k) plane0[line * LD + t + T * k] = z0[k];
+    for (int k = 0; k < P; ++k) plane0[C::A(line, t + T * k)] = z0[k];
     __syncthreads();
 #pragma unroll
-    for (int q = 0; q < P; ++q) z0[q] = plane0[(t + T * q) * LD + line];
+    for (int q = 0; q < P; ++q) z0[q] = plane0[C::A(t + T * q, line)];
     __syncthreads();
     fft_line_interleaved<N, T, -1>(z0, t, s_roots);
     // Lane now holds corr[y = k + P*rt][x = line]; scale as the reference does (c *= scale).
@@ -409,7 +425,7 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB) correlate_kernel(const Co
     for (int k = 0; k < P; ++k) {
         z0[k].x = z0[k].x * scale[0];
         z0[k].y = PAIR ? z0[k].y * scale[WPG - 1] : 0.0f;
-        plane0[(k + P * rt) * LD + line] = z0[k];
+        plane0[C::A(k + P * rt, line)] = z0[k];
     }
 
     // ------------------------------------------------------------------ find_peak
@@ -428,7 +444,7 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB) correlate_kernel(const Co
     if (!(best.y > -INFINITY)) bi1 = 0;
     __syncthreads();  // the scaled planes are complete in shared memory
     auto at = [&](int ch, int y, int x) -> float {
-        const float2 v = plane0[(y % N) * LD + (x % N)];
+        const float2 v = plane0[C::A(y % N, x % N)];
         return ch == 0 ? v.x : v.y;
     };
     // Footprint of the primary peak (correlate.rs:242-254): half-width along +-y, +-x.
@@ -465,7 +481,7 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB) correlate_kernel(const Co
             const float2 a = k == 0 ? up : z0[k - 1];
             const float2 b = k == P - 1 ? dn : z0[k + 1];
             const float m0 = fmaxf(fmaxf(a.x, b.x), z0[k].x);
-            const int o = (k + P * rt) * LD + line;
+            const int o = C::A(k + P * rt, line);
             if constexpr (PAIR) {
                 reinterpret_cast<float2*>(vm)[o] = make_float2(m0, fmaxf(fmaxf(a.y, b.y), z0[k].y));
             } else {
@@ -497,12 +513,12 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB) correlate_kernel(const Co
             const int y = k + P * rt;
             if constexpr (PAIR) {
                 const float2* v2 = reinterpret_cast<const float2*>(vm);
-                const float2 l = v2[y * LD + xl], c = v2[y * LD + line], r = v2[y * LD + xr];
+                const float2 l = v2[C::A(y, xl)], c = v2[C::A(y, line)], r = v2[C::A(y, xr)];
                 const float h0 = fmaxf(fmaxf(l.x, r.x), c.x), h1 = fmaxf(fmaxf(l.y, r.y), c.y);
                 if (z0[k].x == h0 && max(circ(y, by0), cx0) > ex0) second.x = fmaxf(second.x, z0[k].x);
                 if (z0[k].y == h1 && max(circ(y, by1), cx1) > ex1) second.y = fmaxf(second.y, z0[k].y);
             } else {
-                const float h0 = fmaxf(fmaxf(vm[y * LD + xl], vm[y * LD + xr]), vm[y * LD + line]);
+                const float h0 = fmaxf(fmaxf(vm[C::A(y, xl)], vm[C::A(y, xr)]), vm[C::A(y, line)]);
                 if (z0[k].x == h0 && max(circ(y, by0), cx0) > ex0) second.x = fmaxf(second.x, z0[k].x);
             }
         }
@@ -541,17 +557,24 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB) correlate_kernel(const Co
     }
 }
 
+// One launch over all items of the batch: item i owns blocks [block_start[i], block_start[i+1]).
 template <class C>
-static cudaError_t launch_t(const CorrParams& p, cudaStream_t s) {
+static cudaError_t launch_t(CorrBatch b, cudaStream_t s) {
     static_assert(C::SMEM <= 227 * 1024, "shared memory");
-    if (p.ncells <= 0) return cudaSuccess;
+    const long long per_block = (long long)C::G * C::WPG;
+    long long total = 0;
+    for (int i = 0; i < b.n; ++i) {
+        b.block_start[i] = (int)total;
+        total += (b.item[i].ncells + per_block - 1) / per_block;
+    }
+    b.block_start[b.n] = (int)total;
+    if (total <= 0) return cudaSuccess;
+    if (total > 0x7fffffffll) return cudaErrorInvalidValue;
     auto kern = correlate_kernel<C>;
     // Attribute setting is idempotent and per device; done on every launch for simplicity.
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
     if (e != cudaSuccess) return e;
-    const long long per_block = (long long)C::G * C::WPG;
-    const long long blocks = (p.ncells + per_block - 1) / per_block;
-    kern<<<(unsigned)blocks, C::THREADS, C::SMEM, s>>>(p);
+    kern<<<(unsigned)total, C::THREADS, C::SMEM, s>>>(b);
     return cudaGetLastError();
 }
 
@@ -569,7 +592,7 @@ bool corr_supported(int n) {
 // ---------------------------------------------------------------------------------------------
 struct CorrVariant {
     const char* name;
-    cudaError_t (*launch)(const CorrParams&, cudaStream_t);
+    cudaError_t (*launch)(CorrBatch, cudaStream_t);
 };
 
 #define PIV_V(N, T, PR, G, MB, SH) {#N "/T" #T "/G" #G "/B" #MB "/" #SH, &launch_t<CorrCfg<N, T, PR, G, MB, SH>>}
@@ -626,11 +649,23 @@ const char* corr_variant_name(int n, int v) {
     return (vs && v >= 0 && v < c) ? vs[v].name : "";
 }
 
-cudaError_t launch_correlate_variant(int n, int v, const CorrParams& p, cudaStream_t s) {
+cudaError_t launch_correlate_items(int n, int v, const CorrParams* items, int count, cudaStream_t s, int* launches) {
     int c = 0;
     const CorrVariant* vs = variants(n, &c);
     if (!vs || v < 0 || v >= c) return cudaErrorInvalidValue;
-    return vs[v].launch(p, s);
+    for (int off = 0; off < count; off += kMaxBatch) {
+        CorrBatch b;
+        b.n = count - off < kMaxBatch ? count - off : kMaxBatch;
+        for (int i = 0; i < b.n; ++i) b.item[i] = items[off + i];
+        const cudaError_t e = vs[v].launch(b, s);
+        if (e != cudaSuccess) return e;
+        if (launches) ++*launches;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t launch_correlate_variant(int n, int v, const CorrParams& p, cudaStream_t s) {
+    return launch_correlate_items(n, v, &p, 1, s, nullptr);
 }
 
 cudaError_t launch_correlate(int n, const CorrParams& p, cudaStream_t s) { return launch_correlate_variant(n, 0, p, s); }

@@ -70,10 +70,31 @@ __device__ bool has_signal(const StatsView& s, float x, float y, int n, float mi
     return mean >= min_mean && sd >= min_std;
 }
 
-__global__ void place_kernel(const PlaceParams p) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    const int cells = p.grid.nx * p.grid.ny;
-    if (k >= cells) return;
+// Batches of items of any grid size: item i owns cells [cell_start[i], cell_start[i+1]).
+struct PlaceBatch {
+    int n;
+    int cell_start[kMaxBatch + 1];
+    PlaceParams item[kMaxBatch];
+};
+
+struct ValidateBatch {
+    int n;
+    int cell_start[kMaxBatch + 1];
+    ValidateParams item[kMaxBatch];
+};
+
+struct SummaryBatch {
+    int n;
+    int cell_start[kMaxBatch + 1];
+    SummaryItem item[kMaxBatch];
+};
+
+__global__ void place_kernel(const __grid_constant__ PlaceBatch b) {
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= b.cell_start[b.n]) return;
+    const int it = batch_item(b.cell_start, b.n, u);
+    const PlaceParams& p = b.item[it];
+    const int k = u - b.cell_start[it];
     const int ix = k % p.grid.nx, iy = k / p.grid.nx;
     const int n = p.grid.window;
     // max = (w - n).saturating_sub(1) (multipass.rs:207-208)
@@ -103,12 +124,28 @@ __global__ void mask_kernel(const PlaceParams p, const float4* origins, int ncel
     p.status[k] = st;
 }
 
-cudaError_t launch_place(const PlaceParams& p, cudaStream_t s) {
-    const int cells = p.grid.nx * p.grid.ny;
-    if (cells <= 0) return cudaSuccess;
-    place_kernel<<<(cells + 255) / 256, 256, 0, s>>>(p);
-    return cudaGetLastError();
+cudaError_t launch_place_items(const PlaceParams* items, int count, cudaStream_t s, int* launches) {
+    for (int off = 0; off < count; off += kMaxBatch) {
+        PlaceBatch b;
+        b.n = min(count - off, kMaxBatch);
+        long long total = 0;
+        for (int i = 0; i < b.n; ++i) {
+            b.item[i] = items[off + i];
+            b.cell_start[i] = (int)total;
+            total += (long long)b.item[i].grid.nx * b.item[i].grid.ny;
+        }
+        b.cell_start[b.n] = (int)total;
+        if (total <= 0) continue;
+        if (total > 0x7fffffffll) return cudaErrorInvalidValue;
+        place_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(b);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        if (launches) ++*launches;
+    }
+    return cudaSuccess;
 }
+
+cudaError_t launch_place(const PlaceParams& p, cudaStream_t s) { return launch_place_items(&p, 1, s, nullptr); }
 
 cudaError_t launch_mask(const PlaceParams& p, const float4* origins, int ncells, cudaStream_t s) {
     if (ncells <= 0) return cudaSuccess;
@@ -158,9 +195,7 @@ __device__ float residual(float value, float* nb, int n, float eps) {
 }
 
 // Per-vector tests (validate.rs:59-78).
-__global__ void validate_vector_kernel(const ValidateParams p) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= p.nx * p.ny) return;
+__device__ __forceinline__ void validate_vector(const ValidateParams& p, int k) {
     uint8_t f = p.flags0[k];
     if (!(f & F_NO_SIGNAL)) {
         if (hypotf(p.dx[k], p.dy[k]) > p.max_displacement) f |= F_OUT_OF_RANGE;
@@ -170,9 +205,7 @@ __global__ void validate_vector_kernel(const ValidateParams p) {
 }
 
 // Normalized median test on a snapshot of the flags (validate.rs:80-100).
-__global__ void validate_median_kernel(const ValidateParams p) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= p.nx * p.ny) return;
+__device__ __forceinline__ void validate_median(const ValidateParams& p, int k) {
     const int ix = k % p.nx, iy = k / p.nx;
     uint8_t f = p.flags1[k];
     if ((f & F_INVALID) == 0) {
@@ -188,9 +221,7 @@ __global__ void validate_median_kernel(const ValidateParams p) {
 }
 
 // Replacement by the median of usable neighbours at radius 1, then 2 (validate.rs:102-128).
-__global__ void validate_replace_kernel(const ValidateParams p) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= p.nx * p.ny) return;
+__device__ __forceinline__ void validate_replace(const ValidateParams& p, int k) {
     const int ix = k % p.nx, iy = k / p.nx;
     uint8_t f = p.flags2[k];
     float u = p.dx[k], v = p.dy[k];
@@ -216,49 +247,100 @@ __global__ void validate_replace_kernel(const ValidateParams p) {
     p.out_flags[k] = f;
 }
 
-cudaError_t launch_validate(const ValidateParams& p, cudaStream_t s) {
-    const int cells = p.nx * p.ny;
-    if (cells <= 0) return cudaSuccess;
-    const int blocks = (cells + 255) / 256;
-    validate_vector_kernel<<<blocks, 256, 0, s>>>(p);
-    validate_median_kernel<<<blocks, 256, 0, s>>>(p);
-    validate_replace_kernel<<<blocks, 256, 0, s>>>(p);
-    return cudaGetLastError();
+template <int STAGE>
+__global__ void validate_kernel(const __grid_constant__ ValidateBatch b) {
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= b.cell_start[b.n]) return;
+    const int it = batch_item(b.cell_start, b.n, u);
+    const int k = u - b.cell_start[it];
+    if (STAGE == 0) validate_vector(b.item[it], k);
+    if (STAGE == 1) validate_median(b.item[it], k);
+    if (STAGE == 2) validate_replace(b.item[it], k);
 }
+
+cudaError_t launch_validate_items(const ValidateParams* items, int count, cudaStream_t s, int* launches) {
+    for (int off = 0; off < count; off += kMaxBatch) {
+        ValidateBatch b;
+        b.n = min(count - off, kMaxBatch);
+        long long total = 0;
+        for (int i = 0; i < b.n; ++i) {
+            b.item[i] = items[off + i];
+            b.cell_start[i] = (int)total;
+            total += (long long)b.item[i].nx * b.item[i].ny;
+        }
+        b.cell_start[b.n] = (int)total;
+        if (total <= 0) continue;
+        if (total > 0x7fffffffll) return cudaErrorInvalidValue;
+        const unsigned blocks = (unsigned)((total + 255) / 256);
+        validate_kernel<0><<<blocks, 256, 0, s>>>(b);
+        validate_kernel<1><<<blocks, 256, 0, s>>>(b);
+        validate_kernel<2><<<blocks, 256, 0, s>>>(b);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        if (launches) *launches += 3;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t launch_validate(const ValidateParams& p, cudaStream_t s) { return launch_validate_items(&p, 1, s, nullptr); }
 
 // ---------------------------------------------------------------------------------------------
 // Summary counts (validate.rs:40-46), from the final flags as `validate` counts them.
 // ---------------------------------------------------------------------------------------------
-__global__ void summary_zero_kernel(unsigned long long* c) {
-    if (threadIdx.x < 5) c[threadIdx.x] = 0;
+__global__ void summary_zero_kernel(const __grid_constant__ SummaryBatch b) {
+    const int i = threadIdx.x / 5, j = threadIdx.x % 5;
+    if (i < b.n) b.item[i].counts5[j] = 0;
 }
 
-__global__ void summary_kernel(const uint8_t* flags, int n, unsigned long long* c) {
+__global__ void summary_kernel(const __grid_constant__ SummaryBatch b) {
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool in = u < b.cell_start[b.n];
+    const int it = in ? batch_item(b.cell_start, b.n, u) : 0;
     unsigned int loc[5] = {0, 0, 0, 0, 0};
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const uint8_t f = flags[k];
+    if (in) {
+        const uint8_t f = b.item[it].flags[u - b.cell_start[it]];
         if (f & F_NO_SIGNAL) {
-            loc[0]++;
-            continue;
+            loc[0] = 1;
+        } else {
+            loc[1] = (f & F_LOW_PPR) ? 1 : 0;
+            loc[2] = (f & F_MEDIAN_OUTLIER) ? 1 : 0;
+            loc[3] = (f & F_OUT_OF_RANGE) ? 1 : 0;
+            loc[4] = (f & F_REPLACED) ? 1 : 0;
         }
-        if (f & F_LOW_PPR) loc[1]++;
-        if (f & F_MEDIAN_OUTLIER) loc[2]++;
-        if (f & F_OUT_OF_RANGE) loc[3]++;
-        if (f & F_REPLACED) loc[4]++;
     }
+    // Lanes of one item reduce together; the leader of each item's lanes adds the totals.
+    const unsigned same = __match_any_sync(0xffffffffu, in ? it : -1);
+    const int leader = __ffs(same) - 1;
 #pragma unroll
     for (int i = 0; i < 5; ++i) {
-        unsigned int v = loc[i];
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if ((threadIdx.x & 31) == 0 && v) atomicAdd(&c[i], (unsigned long long)v);
+        const unsigned int v = __reduce_add_sync(same, loc[i]);
+        if (in && (int)(threadIdx.x & 31) == leader && v) atomicAdd(&b.item[it].counts5[i], (unsigned long long)v);
     }
+}
+
+cudaError_t launch_summary_items(const SummaryItem* items, int count, cudaStream_t s, int* launches) {
+    for (int off = 0; off < count; off += kMaxBatch) {
+        SummaryBatch b;
+        b.n = min(count - off, kMaxBatch);
+        long long total = 0;
+        for (int i = 0; i < b.n; ++i) {
+            b.item[i] = items[off + i];
+            b.cell_start[i] = (int)total;
+            total += b.item[i].n;
+        }
+        b.cell_start[b.n] = (int)total;
+        summary_zero_kernel<<<1, 5 * kMaxBatch, 0, s>>>(b);
+        if (total > 0) summary_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(b);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        if (launches) *launches += total > 0 ? 2 : 1;
+    }
+    return cudaSuccess;
 }
 
 cudaError_t launch_summary(const uint8_t* flags, int n, unsigned long long* counts5, cudaStream_t s) {
-    summary_zero_kernel<<<1, 32, 0, s>>>(counts5);
-    const int blocks = n > 0 ? min((n + 255) / 256, 592) : 1;
-    summary_kernel<<<blocks, 256, 0, s>>>(flags, n, counts5);
-    return cudaGetLastError();
+    SummaryItem it{flags, n, counts5};
+    return launch_summary_items(&it, 1, s, nullptr);
 }
 
 }  // namespace pivb200

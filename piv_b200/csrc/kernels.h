@@ -25,6 +25,27 @@ struct CorrParams {
     uint8_t* raw_flags;      // 0 or NO_SIGNAL
 };
 
+// Kernels take a batch of independent work items (pairs, passes or requests, of any sizes) by
+// value, so that one launch covers many items and the launch can be captured in a CUDA graph
+// without any device-side descriptor table. Launchers split longer lists into batches.
+constexpr int kMaxBatch = 64;
+
+// Item index that owns global unit `u` (block or cell) given exclusive prefix starts.
+__host__ __device__ __forceinline__ int batch_item(const int* start, int n, int u) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (start[mid] <= u) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+struct CorrBatch {
+    int n;
+    int block_start[kMaxBatch + 1];
+    CorrParams item[kMaxBatch];
+};
+
 bool corr_supported(int n);
 cudaError_t corr_init_device();  // uploads the root-of-unity table to the current device
 cudaError_t launch_correlate(int n, const CorrParams& p, cudaStream_t s);
@@ -32,6 +53,8 @@ cudaError_t launch_correlate(int n, const CorrParams& p, cudaStream_t s);
 int corr_num_variants(int n);
 const char* corr_variant_name(int n, int v);
 cudaError_t launch_correlate_variant(int n, int v, const CorrParams& p, cudaStream_t s);
+// All items share window size n; returns the number of launches issued in *launches.
+cudaError_t launch_correlate_items(int n, int v, const CorrParams* items, int count, cudaStream_t s, int* launches);
 // Number of kernel launches launch_correlate issues (for launch accounting).
 constexpr int kCorrLaunches = 1;
 
@@ -61,6 +84,7 @@ struct PlaceParams {
 };
 
 cudaError_t launch_place(const PlaceParams& p, cudaStream_t s);
+cudaError_t launch_place_items(const PlaceParams* items, int count, cudaStream_t s, int* launches);
 // Mask only (origins given): fills status from origins.
 cudaError_t launch_mask(const PlaceParams& p, const float4* origins, int ncells, cudaStream_t s);
 
@@ -80,12 +104,19 @@ struct ValidateParams {
 };
 
 cudaError_t launch_validate(const ValidateParams& p, cudaStream_t s);
+cudaError_t launch_validate_items(const ValidateParams* items, int count, cudaStream_t s, int* launches);
 constexpr int kValidateLaunches = 3;
 
 // Summary counts from a validated flag field (validate.rs:40-46): no_signal, low_ppr,
 // median_outliers, out_of_range, replaced.
 cudaError_t launch_summary(const uint8_t* flags, int n, unsigned long long* counts5, cudaStream_t s);
 constexpr int kSummaryLaunches = 2;
+struct SummaryItem {
+    const uint8_t* flags;
+    int n;
+    unsigned long long* counts5;
+};
+cudaError_t launch_summary_items(const SummaryItem* items, int count, cudaStream_t s, int* launches);
 
 // ----------------------------------------------------------------------------- preprocessing
 enum RawType { RAW_U8 = 0, RAW_U16 = 1, RAW_F32 = 2 };
