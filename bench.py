@@ -40,6 +40,16 @@ WORKLOADS = {
         name="4096x4096 u16 12-bit particle pair, 128->64->32->16 px at 75% overlap, FP32 plain",
         h=4096, w=4096, bits=12, windows=[128, 64, 32, 16], overlap=0.75, final_iterations=1, ppp=0.05,
         dmin=2.0, dmax=4.0, vmax=10.0, shear=0.01, outlier_frac=0.02, seed=5),
+    "c3": dict(
+        name="1280x800 u16 video stream, sequential pairs, 64->32 px at 50% overlap, 32 pairs per CUDA-graph replay",
+        h=800, w=1280, bits=12, windows=[64, 32], overlap=0.5, final_iterations=1, ppp=0.04, dmin=2.0, dmax=5.0,
+        amplitude=6.0, wavelength=320.0, phase_step=0.02, frames=33, stream=True, seed=3, outlier_frac=0.0),
+    "c4": dict(
+        name="serving: Poisson arrivals 400 pairs/s, u16 pairs of 512x512 / 1024x768 / 2048x2048, schedules "
+             "[32] / [64,32] / [64,32,16] at 50% overlap, 60 GB admission budget, continuous batching",
+        rate=400.0, duration=60.0, sizes=[(512, 512), (768, 1024), (2048, 2048)],
+        schedules=[[32], [64, 32], [64, 32, 16]], pool=3, budget=60 << 30, max_in_flight=256, seed=4,
+        serving=True, windows=[32], overlap=0.5, final_iterations=1, h=512, w=512, outlier_frac=0.0),
     "c2": dict(
         name="1024x1024 u16 12-bit Lamb-Oseen pair, 64->32->16 px at 50% overlap, FP32 plain",
         h=1024, w=1024, bits=12, windows=[64, 32, 16], overlap=0.5, final_iterations=1, ppp=0.03,
@@ -66,6 +76,190 @@ def make_inputs(wl, seed_offset=0):
         cells = np.stack([g.x0 + (k % g.nx) * g.step, g.y0 + (k // g.nx) * g.step], 1)
     return S.baseline_pair(h, w, wl["seed"] + seed_offset, field, ppp=wl["ppp"], dmin=wl["dmin"], dmax=wl["dmax"],
                            bits=wl["bits"], outlier_cells=cells, outlier_window=wl["windows"][-1])
+
+
+class _DeviceBuffer:
+    """A raw device allocation exposed to torch through __cuda_array_interface__."""
+
+    def __init__(self, ptr, count, typestr):
+        self.__cuda_array_interface__ = {"shape": (int(count),), "typestr": typestr, "data": (int(ptr), False),
+                                         "version": 3, "strides": None}
+
+
+def make_stream(wl):
+    """A synthetic high-speed video: particles advected frame to frame by Taylor-Green vortices
+    u = A sin(kx + phi_i) cos(ky), v = -A cos(kx + phi_i) sin(ky) whose phase drifts slowly.
+    Returns [frames, H, W] u16 (12-bit)."""
+    from piv_b200 import synthetic as S
+    h, w, full = wl["h"], wl["w"], (1 << wl["bits"]) - 1
+    x, y, s, a = S._blobs(h, w, wl["seed"], wl["ppp"], wl["dmin"], wl["dmax"], (120 / 255) * full, full)
+    k = 2 * math.pi / wl["wavelength"]
+    out = []
+    for i in range(wl["frames"]):
+        f = S.render(h, w, x, y, s, a)
+        out.append(S.quantise(S.add_noise(f, (4 / 255) * full, wl["seed"] + 7 * i), full, np.uint16))
+        phi = wl["phase_step"] * i
+        amp = wl["amplitude"]
+
+        def field(X, Y, phi=phi):
+            X = np.asarray(X, np.float64)
+            Y = np.asarray(Y, np.float64)
+            return ((amp * np.sin(k * X + phi) * np.cos(k * Y)).astype(np.float32),
+                    (-amp * np.cos(k * X + phi) * np.sin(k * Y)).astype(np.float32))
+        x, y = S.displace(x, y, field)
+    return np.stack(out)
+
+
+def run_stream(args, wl):
+    """The batching form on a video stream: all sequential pairs of wl['frames'] frames analysed by
+    one CUDA-graph replay per step (prepare every frame, every pass of every pair)."""
+    import torch
+
+    import piv_b200 as P
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(0)
+    frames = make_stream(wl)
+    nf, h, w = frames.shape
+    k = nf - 1
+    an = P.PivAnalyzer(piv_config(wl), device=0)
+    fa, fb = an.prepare(frames[0], P.RAW), an.prepare(frames[1], P.RAW)
+    tuned = an.autotune(fa, fb) if not args.no_autotune else {}
+    batch = P.PivBatch(an, h, w, k, sequential=True)
+    # the raw frames go once into the batch's device input slab (inputs resident in HBM)
+    slab = torch.as_tensor(_DeviceBuffer(batch.input_device(), frames.nbytes // 2, "<i2"), device=dev)
+    slab.copy_(torch.from_numpy(frames.reshape(-1).view(np.int16)).to(dev))
+    torch.cuda.synchronize()
+    bstream = torch.cuda.ExternalStream(batch.stream(), device=dev)
+    nvec = k * final_vectors(wl)
+    for _ in range(args.warmup):
+        batch.run()
+    batch.sync()
+    gpu_uuid = str(torch.cuda.get_device_properties(0).uuid)
+    sampler = ClockSampler(gpu_uuid if gpu_uuid.startswith("GPU-") else f"GPU-{gpu_uuid}")
+    sampler.start()
+    time.sleep(0.3)
+    t0 = time.perf_counter()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ev[0].record(bstream)
+    for _ in range(args.steps):
+        batch.run()
+    ev[1].record(bstream)
+    ev[1].synchronize()
+    wall = time.perf_counter() - t0
+    clocks = sampler.stop()
+    ms = ev[0].elapsed_time(ev[1])
+    value = args.steps * nvec / (ms * 1e-3)
+    # end to end: pinned host frames -> input slab -> graph -> results to host, every step
+    pin = torch.from_numpy(frames.view(np.int16)).pin_memory().numpy().view(np.uint16)
+    res = batch.run_host(pin)
+    ev2 = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    e2e_steps = max(3, args.steps // 4)
+    ev2[0].record(bstream)
+    for _ in range(e2e_steps):
+        res = batch.run_host(pin)
+    ev2[1].record(bstream)
+    ev2[1].synchronize()
+    e2e_ms = ev2[0].elapsed_time(ev2[1])
+    line = {"metric": METRIC, "value": value, "unit": "vectors/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": wl["name"], "frames_per_step": nf, "pairs_per_step": k,
+                       "final_pass_vectors_per_pair": final_vectors(wl), "windows": pass_windows(wl),
+                       "l2": "inputs > L2: 33 frames = 66 MiB of samples + 132 MiB prepared per step"},
+            "e2e": {"value": e2e_steps * nvec / (e2e_ms * 1e-3), "unit": "vectors/s",
+                    "h2d_bytes_per_step": int(pin.nbytes), "d2h_bytes_per_step": int(nvec * 13 + k * 40),
+                    "ms_per_step": e2e_ms / e2e_steps},
+            "gpu_launches": int(batch.kernels() * args.steps), "graph_launches": args.steps,
+            "clocks": clocks, "autotuned_variants": tuned, "wall_ms_per_step": 1e3 * wall / args.steps,
+            "valid_fraction_last_pair": float(np.mean((res[-1].field.flags & P.flags.INVALID) == 0))}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_serving(args, wl):
+    """The serving form under a Poisson load: requests of mixed sizes and window schedules are
+    submitted at their arrival times to one PivServer (continuous batching); latency is submit ->
+    results in host memory. vectors/s counts the final-pass vectors of all completed requests
+    over the span from the first submission to the last completion."""
+    import threading as th
+
+    import torch
+
+    import piv_b200 as P
+    from piv_b200 import synthetic as S
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(wl["seed"])
+    duration = args.duration if args.duration else wl["duration"]
+    pool = {}
+    for si, (h, w) in enumerate(wl["sizes"]):
+        for j in range(wl["pool"]):
+            shear, off = float(rng.uniform(0, 0.02)), float(rng.uniform(0, 4))
+            f = (lambda sh, of, hh: (lambda X, Y: (np.float32(of) + sh * (np.asarray(Y, np.float32) - hh / 2),
+                                                   np.float32(0.5 * of))))(shear, off, h)
+            a, b = S.baseline_pair(h, w, 1000 * si + j, f, ppp=0.05, dmin=2.0, dmax=4.0, bits=12)
+            pool[(si, j)] = tuple(torch.from_numpy(x.view(np.int16)).pin_memory().numpy().view(np.uint16) for x in (a, b))
+    cfgs = [P.PivConfig(windows=s, overlap=wl["overlap"], final_iterations=1) for s in wl["schedules"]]
+    n = int(rng.poisson(wl["rate"] * duration))
+    arrivals = np.cumsum(rng.exponential(1.0 / wl["rate"], n))
+    kinds = [(int(rng.integers(0, len(wl["sizes"]))), int(rng.integers(0, len(cfgs))), int(rng.integers(0, wl["pool"])))
+             for _ in range(n)]
+    vec = {(si, ci): len(P.Grid.new(wl["sizes"][si][0], wl["sizes"][si][1], cfgs[ci].windows[-1], cfgs[ci].overlap))
+           for si in range(len(wl["sizes"])) for ci in range(len(cfgs))}
+    sv = P.PivServer(memory_budget_bytes=wl["budget"], max_in_flight=wl["max_in_flight"], device=0)
+    # warm-up: one request of every kind
+    for si in range(len(wl["sizes"])):
+        for ci in range(len(cfgs)):
+            sv.wait(sv.submit(*pool[(si, 0)], cfgs[ci]))
+    tickets = []
+    lat = []
+    done = th.Event()
+
+    def waiter():
+        i = 0
+        while i < n:
+            while i >= len(tickets):
+                if done.is_set() and i >= len(tickets):
+                    return
+                time.sleep(0.0002)
+            _, l = sv.wait(tickets[i])
+            lat.append(l)
+            i += 1
+
+    wt = th.Thread(target=waiter)
+    wt.start()
+    gpu_uuid = str(torch.cuda.get_device_properties(0).uuid)
+    sampler = ClockSampler(gpu_uuid if gpu_uuid.startswith("GPU-") else f"GPU-{gpu_uuid}")
+    sampler.start()
+    s0 = sv.stats()
+    t0 = time.perf_counter()
+    for i in range(n):
+        now = time.perf_counter() - t0
+        if arrivals[i] > now:
+            time.sleep(arrivals[i] - now)
+        si, ci, pj = kinds[i]
+        tickets.append(sv.submit(*pool[(si, pj)], cfgs[ci]))
+    done.set()
+    wt.join()
+    span = time.perf_counter() - t0
+    clocks = sampler.stop()
+    s1 = sv.stats()
+    sv.close()
+    total_vec = sum(vec[(si, ci)] for si, ci, _ in kinds)
+    lat_a = np.array(lat)
+    line = {"metric": METRIC, "value": total_vec / span, "unit": "vectors/s", "n_gpus": 1, "steps": n, "warmup": 9,
+            "ms_per_step": 1e3 * span / max(n, 1), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": wl["name"], "requests": n, "duration_s": duration, "rate_per_s": wl["rate"]},
+            "latency_ms": {"p50": float(np.percentile(lat_a, 50)), "p90": float(np.percentile(lat_a, 90)),
+                           "p99": float(np.percentile(lat_a, 99)), "max": float(lat_a.max()), "mean": float(lat_a.mean())},
+            "achieved_rate_per_s": n / span,
+            "e2e": {"value": total_vec / span, "unit": "vectors/s",
+                    "h2d_bytes_per_step": int(np.mean([pool[(si, pj)][0].nbytes * 2 for si, _, pj in kinds])),
+                    "d2h_bytes_per_step": int(np.mean([vec[(si, ci)] * 13 for si, ci, _ in kinds]))},
+            "gpu_launches": int(s1["kernel_launches"] - s0["kernel_launches"]), "server_steps": int(s1["steps"] - s0["steps"]),
+            "clocks": clocks}
+    print(json.dumps(line), flush=True)
+    return 0
 
 
 def piv_config(wl):
@@ -229,8 +423,10 @@ def run_reference(args, wl):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    from piv_b200 import synthetic as S  # noqa: F401
-    a, b = make_inputs(wl)
+    if wl.get("stream"):
+        a, b = make_stream(dict(wl, frames=2))
+    else:
+        a, b = make_inputs(wl)
     for _ in range(args.warmup):
         pass  # the oracle has no warm-up state; warm-up steps run no work
     base = None
@@ -260,6 +456,7 @@ def main():
     ap.add_argument("--workload", default="c5", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--duration", type=float, default=None, help="serving workload: seconds of arrivals")
     ap.add_argument("--ref-step-s", type=float, default=3.0)
     ap.add_argument("--ref-crop", type=int, default=1024)
     ap.add_argument("--profile-case", default=None, metavar="WINDOWS",
@@ -272,6 +469,10 @@ def main():
         return run_profile_case(args, wl)
     if args.impl == "reference":
         return run_reference(args, wl)
+    if wl.get("stream"):
+        return run_stream(args, wl)
+    if wl.get("serving"):
+        return run_serving(args, wl)
 
     import torch
     import torch.distributed as dist

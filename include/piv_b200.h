@@ -197,6 +197,8 @@ void* piv_batch_input_device(PivBatch* batch);
 int64_t piv_batch_input_bytes(const PivBatch* batch);
 /* Runs the batch on its stream (asynchronous). */
 int32_t piv_batch_run(PivBatch* batch);
+/* The batch's CUDA stream (a cudaStream_t), for callers that order their own work after it. */
+void* piv_batch_stream(PivBatch* batch);
 int32_t piv_batch_sync(PivBatch* batch);
 /* Device output slabs: dx, dy, peak ratio (f32) and flags (u8), pairs*nx*ny each; 8 uint64
  * summary counters per pair; nx*ny is piv_output_grid's. */
@@ -208,6 +210,48 @@ int32_t piv_batch_run_host(PivBatch* batch, const void* raw, float* dx, float* d
                            PivSummaryC* summaries);
 /* Kernels executed per run (counted on the eager first run; the graph replays the same set). */
 int64_t piv_batch_kernels(const PivBatch* batch);
+
+/* ----------------------------------------------------------------------------- serving form
+ * No counterpart in the reference. A request loop on one GPU with continuous batching: frame
+ * pairs of any size with their own PivConfig are submitted at any time; a scheduler thread
+ * admits them (FIFO) while the in-flight count and a device-memory budget allow, keeps each
+ * request's state (prepared frames, per-pass origins and predictor fields) on the device, and
+ * advances ALL admitted requests by one pass per step: one placement launch for all of them,
+ * one correlation launch per window size, one validation chain. A request joins at the next
+ * step boundary and leaves when its last pass is done, so requests that arrive while others run
+ * share kernel launches with them. Window pairs are independent inside a launch, so each
+ * result is bit-identical to PivAnalyzer::analyze of that pair alone. */
+typedef struct PivServer PivServer;
+typedef struct {
+    int32_t device;              /* CUDA device ordinal (-1: current) */
+    int64_t memory_budget_bytes; /* device memory admitted requests may hold together */
+    int32_t max_in_flight;       /* admitted requests at most */
+} PivServerConfigC;
+typedef struct {
+    PivConfigC config;           /* window schedule, overlap, mask, validation of this request */
+    PivPreprocessC preprocess;
+    int32_t dtype;               /* PIV_DTYPE_* of the samples */
+    int64_t height, width;
+    const void* frame_a;         /* HOST samples (pinned memory recommended); valid until done */
+    const void* frame_b;
+    float* dx;                   /* HOST outputs of output_grid's nx*ny elements; valid until done */
+    float* dy;
+    float* peak_ratio;
+    uint8_t* flags;
+} PivRequestC;
+typedef struct {
+    int64_t submitted, admitted, completed, failed, queued, in_flight;
+    int64_t memory_in_use_bytes, steps, kernel_launches;
+} PivServerStatsC;
+int32_t piv_server_create(const PivServerConfigC* cfg, PivServer** out);
+/* Finishes the admitted and queued requests, then stops the scheduler and frees the server. */
+void piv_server_destroy(PivServer* server);
+/* Queues a request; fails at once for an invalid config or a request larger than the budget. */
+int32_t piv_server_submit(PivServer* server, const PivRequestC* request, uint64_t* id);
+/* Blocks until request `id` is done; fills its summary and its latency (submit to results in
+ * host memory, milliseconds). Returns the request's own status. Each id may be waited once. */
+int32_t piv_server_wait(PivServer* server, uint64_t id, PivSummaryC* summary, double* latency_ms);
+int32_t piv_server_stats(PivServer* server, PivServerStatsC* stats);
 
 /* PivAnalyzer::analyze_traced (multipass.rs:142-150, PassTrace :72-81): HOST arrays holding
  * every pass back to back (pass 0 cells, then pass 1 ...; piv_pass_grid gives each count):

@@ -44,6 +44,7 @@ class OrcConfig(ctypes.Structure):
         ("median_threshold", ctypes.c_float),
         ("median_eps", ctypes.c_float),
         ("replace", ctypes.c_int32),
+        ("deform", ctypes.c_int32),
     ]
 
 
@@ -87,6 +88,11 @@ def lib():
         L.orc_analyze.argtypes = [ctypes.POINTER(OrcConfig), _f32p, _f32p, _f32p, _f32p, _i64, _i64, ctypes.c_int,
                                   ctypes.c_int, _f32p, _f32p, _f32p, _u8p, ctypes.POINTER(OrcSummary)] + [vp] * 9
         L.orc_analyze.restype = ctypes.c_int
+        L.orc_place_deform.argtypes = [ctypes.POINTER(OrcGrid), _i64, _i64, ctypes.c_void_p, ctypes.c_void_p,
+                                       ctypes.c_void_p, _f32p, _f32p]
+        L.orc_correlate_pass_deform.argtypes = [_f32p, _f32p, _f32p, _f32p, _i64, _i64, ctypes.POINTER(OrcGrid), _f32p,
+                                                _f32p, ctypes.c_float, ctypes.c_float, ctypes.c_int, ctypes.c_int, _f32p,
+                                                _f32p, _f32p, _u8p]
         L.orc_splitmix_next.argtypes = [ctypes.POINTER(ctypes.c_uint64)]
         L.orc_splitmix_next.restype = ctypes.c_uint64
         _lib = L
@@ -188,6 +194,30 @@ def correlate_pass(image_a, image_b, base_a, base_b, n, origins, min_mean=0.0, m
     return dx, dy, ppr, flags
 
 
+def place_deform(g, h, w, pgrid=None, pdx=None, pdy=None):
+    """Origins and the predictor at each window's four corner pixels (deformed windows)."""
+    out = np.empty((g.ny * g.nx, 4), np.float32)
+    corners = np.empty((g.ny * g.nx, 8), np.float32)
+    pdx = None if pdx is None else _f(pdx)
+    pdy = None if pdy is None else _f(pdy)
+    lib().orc_place_deform(ctypes.byref(g), h, w, ctypes.byref(pgrid) if pgrid is not None else None, _ptr(pdx),
+                           _ptr(pdy), out, corners)
+    return out, corners
+
+
+def correlate_pass_deform(image_a, image_b, base_a, base_b, g, origins, corners, min_mean=0.0, min_std=0.0, mode=REF,
+                          nthreads=0):
+    image_a, image_b, base_a, base_b = map(_f, (image_a, image_b, base_a, base_b))
+    origins, corners = _f(origins), _f(corners)
+    cells = g.nx * g.ny
+    dx, dy, ppr = (np.empty(cells, np.float32) for _ in range(3))
+    flags = np.empty(cells, np.uint8)
+    h, w = image_a.shape
+    lib().orc_correlate_pass_deform(image_a, image_b, base_a, base_b, h, w, ctypes.byref(g), origins, corners, min_mean,
+                                    min_std, mode, nthreads, dx, dy, ppr, flags)
+    return dx, dy, ppr, flags
+
+
 def correlate_window(a, ax, ay, b, bx, by, n, mode=REF):
     a, b = _f(a), _f(b)
     pk = np.empty(4, np.float32)
@@ -238,12 +268,13 @@ class OracleConfig:
     median_threshold: float = 2.0
     median_eps: float = 0.1
     replace: bool = True
+    deform: bool = False
 
     def c(self):
         self._w = (ctypes.c_int32 * len(self.windows))(*self.windows)
         return OrcConfig(self._w, len(self.windows), self.overlap, self.final_iterations, self.min_mean,
                          self.min_std, self.ppr_threshold, self.median_threshold, self.median_eps,
-                         int(bool(self.replace)))
+                         int(bool(self.replace)), int(bool(self.deform)))
 
     def passes(self):
         return list(self.windows) + [self.windows[-1]] * (self.final_iterations - 1)

@@ -301,13 +301,25 @@ struct Workspace {
     // Returns false when either window is flat. Fills corr with the scaled plane.
     bool plane(const float* ia, int64_t wa, float ax, float ay, const float* ib, int64_t wb, float bx,
                float by);
+    bool finish(double ea, double eb);
 };
+
+template <>
+bool Workspace<float>::finish(double ea, double eb);
+template <>
+bool Workspace<double>::finish(double ea, double eb);
 
 template <>
 bool Workspace<float>::plane(const float* ia, int64_t wa, float ax, float ay, const float* ib,
                              int64_t wb, float bx, float by) {
     const double ea = load_window_f32(ia, wa, ax, ay, n, a.data());
     const double eb = load_window_f32(ib, wb, bx, by, n, b.data());
+    return finish(ea, eb);
+}
+
+// correlate.rs:110-137 on windows already in a and b.
+template <>
+bool Workspace<float>::finish(double ea, double eb) {
     if (ea <= 1e-12 || eb <= 1e-12) return false;
     forward(a.data(), ta);
     forward(b.data(), tb);
@@ -324,6 +336,11 @@ bool Workspace<double>::plane(const float* ia, int64_t wa, float ax, float ay, c
                               int64_t wb, float bx, float by) {
     const double ea = load_window_f64(ia, wa, ax, ay, n, a.data());
     const double eb = load_window_f64(ib, wb, bx, by, n, b.data());
+    return finish(ea, eb);
+}
+
+template <>
+bool Workspace<double>::finish(double ea, double eb) {
     if (ea <= 1e-12 || eb <= 1e-12) return false;
     forward(a.data(), ta);
     forward(b.data(), tb);
@@ -548,6 +565,86 @@ void orc_box_stats(const float* frame, int64_t h, int64_t w, int64_t bx, int64_t
     ii.stats(bx, by, bw, bh, mean, sd);
 }
 
+}  // extern "C"
+
+namespace {
+
+// VectorField::sample (field.rs:56-81): bilinear on the predictor grid, clamped, NaN skipped.
+void sample_pred(const OrcGrid* pg, const float* pdx, const float* pdy, float x, float y, float* px, float* py) {
+    *px = 0.0f;
+    *py = 0.0f;
+    const float fx = clampf((x - center(pg->x0, 0, pg->step, pg->window)) / (float)pg->step, 0.0f, (float)(pg->nx - 1));
+    const float fy = clampf((y - center(pg->y0, 0, pg->step, pg->window)) / (float)pg->step, 0.0f, (float)(pg->ny - 1));
+    const int64_t jx = (int64_t)std::floor(fx), jy = (int64_t)std::floor(fy);
+    const float tx = fx - (float)jx, ty = fy - (float)jy;
+    const int64_t jx1 = std::min(jx + 1, pg->nx - 1), jy1 = std::min(jy + 1, pg->ny - 1);
+    const int64_t rr[4] = {jy, jy, jy1, jy1};
+    const int64_t cc[4] = {jx, jx1, jx, jx1};
+    const float ww[4] = {(1.0f - tx) * (1.0f - ty), tx * (1.0f - ty), (1.0f - tx) * ty, tx * ty};
+    float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f;
+    for (int j = 0; j < 4; ++j) {
+        const float u = pdx[rr[j] * pg->nx + cc[j]], v = pdy[rr[j] * pg->nx + cc[j]];
+        if (ww[j] > 0.0f && std::isfinite(u) && std::isfinite(v)) {
+            a0 = a0 + ww[j] * u;
+            a1 = a1 + ww[j] * v;
+            a2 = a2 + ww[j];
+        }
+    }
+    if (a2 > 0.0f) {
+        *px = a0 / a2;
+        *py = a1 / a2;
+    }
+}
+
+// Deformed-window helpers (see piv_oracle.h).
+template <class T>
+T blend(const float* c, int k, T u, T v) {
+    const T w00 = ((T)1 - u) * ((T)1 - v), w10 = u * ((T)1 - v), w01 = ((T)1 - u) * v, w11 = u * v;
+    return w00 * (T)c[k] + w10 * (T)c[2 + k] + w01 * (T)c[4 + k] + w11 * (T)c[6 + k];
+}
+
+template <class T>
+T bilinear_clamped(const float* img, int64_t h, int64_t w, T px, T py) {
+    px = std::min(std::max(px, (T)0), (T)(w - 1));
+    py = std::min(std::max(py, (T)0), (T)(h - 1));
+    int64_t ix = (int64_t)std::floor(px), iy = (int64_t)std::floor(py);
+    ix = std::min(ix, std::max<int64_t>(w - 2, 0));
+    iy = std::min(iy, std::max<int64_t>(h - 2, 0));
+    const T tx = px - (T)ix, ty = py - (T)iy;
+    const int64_t ix1 = std::min(ix + 1, w - 1), iy1 = std::min(iy + 1, h - 1);
+    const T w00 = ((T)1 - tx) * ((T)1 - ty), w01 = tx * ((T)1 - ty), w10 = ((T)1 - tx) * ty, w11 = tx * ty;
+    return w00 * (T)img[iy * w + ix] + w01 * (T)img[iy * w + ix1] + w10 * (T)img[iy1 * w + ix] +
+           w11 * (T)img[iy1 * w + ix1];
+}
+
+// Window sample of the deformed window (sign -1: frame A, +1: frame B), then mean removal and
+// energy as load_window (correlate.rs:203-209).
+template <class T>
+double load_window_deform(const float* img, int64_t h, int64_t w, int64_t x0, int64_t y0, int64_t n,
+                          const float* corners, T sign, T* dst) {
+    for (int64_t r = 0; r < n; ++r)
+        for (int64_t c = 0; c < n; ++c) {
+            const T u = (T)c / (T)(n - 1), v = (T)r / (T)(n - 1);
+            const T px = (T)(x0 + c) + sign * ((T)0.5 * blend<T>(corners, 0, u, v));
+            const T py = (T)(y0 + r) + sign * ((T)0.5 * blend<T>(corners, 1, u, v));
+            dst[r * n + c] = bilinear_clamped<T>(img, h, w, px, py);
+        }
+    double s = 0.0;
+    for (int64_t i = 0; i < n * n; ++i) s += (double)dst[i];
+    const double mean = s / (double)(n * n);
+    const T mf = (T)mean;
+    double energy = 0.0;
+    for (int64_t i = 0; i < n * n; ++i) {
+        dst[i] -= mf;
+        energy += (double)dst[i] * (double)dst[i];
+    }
+    return energy;
+}
+
+}  // namespace
+
+extern "C" {
+
 void orc_place(const OrcGrid* g, int64_t h, int64_t w, const OrcGrid* pg, const float* pdx,
                const float* pdy, float* origins) {
     // multipass.rs:204-231, field.rs:56-81
@@ -557,33 +654,9 @@ void orc_place(const OrcGrid* g, int64_t h, int64_t w, const OrcGrid* pg, const 
     for (int64_t iy = 0; iy < g->ny; ++iy)
         for (int64_t ix = 0; ix < g->nx; ++ix) {
             float px = 0.0f, py = 0.0f;
-            if (pg && pdx && pdy) {
-                const float x = center(g->x0, ix, g->step, g->window);
-                const float y = center(g->y0, iy, g->step, g->window);
-                const float fx = clampf((x - center(pg->x0, 0, pg->step, pg->window)) / (float)pg->step,
-                                        0.0f, (float)(pg->nx - 1));
-                const float fy = clampf((y - center(pg->y0, 0, pg->step, pg->window)) / (float)pg->step,
-                                        0.0f, (float)(pg->ny - 1));
-                const int64_t jx = (int64_t)std::floor(fx), jy = (int64_t)std::floor(fy);
-                const float tx = fx - (float)jx, ty = fy - (float)jy;
-                const int64_t jx1 = std::min(jx + 1, pg->nx - 1), jy1 = std::min(jy + 1, pg->ny - 1);
-                const int64_t rr[4] = {jy, jy, jy1, jy1};
-                const int64_t cc[4] = {jx, jx1, jx, jx1};
-                const float ww[4] = {(1.0f - tx) * (1.0f - ty), tx * (1.0f - ty), (1.0f - tx) * ty, tx * ty};
-                float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f;
-                for (int j = 0; j < 4; ++j) {
-                    const float u = pdx[rr[j] * pg->nx + cc[j]], v = pdy[rr[j] * pg->nx + cc[j]];
-                    if (ww[j] > 0.0f && std::isfinite(u) && std::isfinite(v)) {
-                        a0 = a0 + ww[j] * u;
-                        a1 = a1 + ww[j] * v;
-                        a2 = a2 + ww[j];
-                    }
-                }
-                if (a2 > 0.0f) {
-                    px = a0 / a2;
-                    py = a1 / a2;
-                }
-            }
+            if (pg && pdx && pdy)
+                sample_pred(pg, pdx, pdy, center(g->x0, ix, g->step, g->window), center(g->y0, iy, g->step, g->window),
+                            &px, &py);
             auto place = [](int64_t origin, float shift, float mx, float* a, float* b) {
                 const float s = clampf(shift, -mx, mx);
                 const float a0 = clampf((float)origin - s / 2.0f, std::fmax(-s, 0.0f), std::fmin(mx - s, mx));
@@ -645,6 +718,83 @@ void orc_correlate_pass(const float* image_a, const float* image_b, const float*
                 dx[k] = bx - ax + pk[0];
                 dy[k] = by - ay + pk[1];
                 ppr[k] = pk[3];
+                flags[k] = 0;
+            }
+        }
+    }
+}
+
+void orc_place_deform(const OrcGrid* g, int64_t h, int64_t w, const OrcGrid* pg, const float* pdx,
+                      const float* pdy, float* origins, float* corners) {
+    orc_place(g, h, w, pg, pdx, pdy, origins);
+    const int64_t n = g->window;
+    for (int64_t iy = 0; iy < g->ny; ++iy)
+        for (int64_t ix = 0; ix < g->nx; ++ix) {
+            float* c = corners + 8 * (iy * g->nx + ix);
+            const float x0 = (float)(g->x0 + ix * g->step), y0 = (float)(g->y0 + iy * g->step);
+            const float xs[4] = {x0, x0 + (float)(n - 1), x0, x0 + (float)(n - 1)};
+            const float ys[4] = {y0, y0, y0 + (float)(n - 1), y0 + (float)(n - 1)};
+            for (int j = 0; j < 4; ++j) {
+                c[2 * j] = 0.0f;
+                c[2 * j + 1] = 0.0f;
+                if (pg && pdx && pdy) sample_pred(pg, pdx, pdy, xs[j], ys[j], &c[2 * j], &c[2 * j + 1]);
+            }
+        }
+}
+
+void orc_correlate_pass_deform(const float* image_a, const float* image_b, const float* base_a,
+                               const float* base_b, int64_t h, int64_t w, const OrcGrid* g,
+                               const float* origins, const float* corners, float min_mean, float min_std,
+                               int mode, int nthreads, float* dx, float* dy, float* ppr, uint8_t* flags) {
+    Integral sa(base_a, h, w), sb(base_b, h, w);
+    const int64_t n = g->window, ncells = g->nx * g->ny;
+    const int nt = num_threads(nthreads);
+#pragma omp parallel num_threads(nt)
+    {
+        Workspace<float> wsf(mode == ORC_REF ? n : 2);
+        Workspace<double> wsd(mode == ORC_FP64 ? n : 2);
+#pragma omp for schedule(dynamic, 16)
+        for (int64_t k = 0; k < ncells; ++k) {
+            const float* o = origins + 4 * k;
+            const float* c = corners + 8 * k;
+            const int64_t x0 = g->x0 + (k % g->nx) * g->step, y0 = g->y0 + (k / g->nx) * g->step;
+            auto has_signal = [&](const Integral& s, float x, float y) {
+                float mean, sd;
+                s.stats((int64_t)std::round(x), (int64_t)std::round(y), n, n, &mean, &sd);
+                return mean >= min_mean && sd >= min_std;
+            };
+            bool ok = has_signal(sa, o[0], o[1]) && has_signal(sb, o[2], o[3]);
+            if (ok) {
+                if (mode == ORC_REF) {
+                    const double ea = load_window_deform<float>(image_a, h, w, x0, y0, n, c, -1.0f, wsf.a.data());
+                    const double eb = load_window_deform<float>(image_b, h, w, x0, y0, n, c, 1.0f, wsf.b.data());
+                    ok = wsf.finish(ea, eb);
+                    if (ok) {
+                        float pk[4];
+                        find_peak_t<float>(wsf.corr.data(), n, pk);
+                        dx[k] = blend<float>(c, 0, 0.5f, 0.5f) + pk[0];
+                        dy[k] = blend<float>(c, 1, 0.5f, 0.5f) + pk[1];
+                        ppr[k] = pk[3];
+                    }
+                } else {
+                    const double ea = load_window_deform<double>(image_a, h, w, x0, y0, n, c, -1.0, wsd.a.data());
+                    const double eb = load_window_deform<double>(image_b, h, w, x0, y0, n, c, 1.0, wsd.b.data());
+                    ok = wsd.finish(ea, eb);
+                    if (ok) {
+                        double pd[4];
+                        find_peak_t<double>(wsd.corr.data(), n, pd);
+                        dx[k] = (float)(blend<double>(c, 0, 0.5, 0.5) + pd[0]);
+                        dy[k] = (float)(blend<double>(c, 1, 0.5, 0.5) + pd[1]);
+                        ppr[k] = (float)pd[3];
+                    }
+                }
+            }
+            if (!ok) {
+                dx[k] = NAN;
+                dy[k] = NAN;
+                ppr[k] = 0.0f;
+                flags[k] = NO_SIGNAL;
+            } else {
                 flags[k] = 0;
             }
         }
@@ -787,11 +937,19 @@ int orc_analyze(const OrcConfig* cfg, const float* image_a, const float* image_b
         const int64_t cells = g.nx * g.ny;
         std::vector<float> origins(4 * cells), dx(cells), dy(cells), ppr(cells);
         std::vector<uint8_t> fl(cells);
-        orc_place(&g, h, w, have_pred ? &pg : nullptr, have_pred ? pdx.data() : nullptr,
-                  have_pred ? pdy.data() : nullptr, origins.data());
-        orc_correlate_pass(image_a, image_b, base_a, base_b, h, w, win, cells, origins.data(),
-                           cfg->min_mean, cfg->min_std, mode, nthreads, dx.data(), dy.data(), ppr.data(),
-                           fl.data());
+        if (cfg->deform && have_pred) {
+            std::vector<float> corners(8 * cells);
+            orc_place_deform(&g, h, w, &pg, pdx.data(), pdy.data(), origins.data(), corners.data());
+            orc_correlate_pass_deform(image_a, image_b, base_a, base_b, h, w, &g, origins.data(), corners.data(),
+                                      cfg->min_mean, cfg->min_std, mode, nthreads, dx.data(), dy.data(), ppr.data(),
+                                      fl.data());
+        } else {
+            orc_place(&g, h, w, have_pred ? &pg : nullptr, have_pred ? pdx.data() : nullptr,
+                      have_pred ? pdy.data() : nullptr, origins.data());
+            orc_correlate_pass(image_a, image_b, base_a, base_b, h, w, win, cells, origins.data(),
+                               cfg->min_mean, cfg->min_std, mode, nthreads, dx.data(), dy.data(), ppr.data(),
+                               fl.data());
+        }
         if (trace_origins) std::memcpy(trace_origins + 4 * toff, origins.data(), sizeof(float) * 4 * cells);
         if (trace_raw_dx) std::memcpy(trace_raw_dx + toff, dx.data(), sizeof(float) * cells);
         if (trace_raw_dy) std::memcpy(trace_raw_dy + toff, dy.data(), sizeof(float) * cells);

@@ -47,6 +47,7 @@ typedef struct {
     float min_mean, min_std;             /* MaskConfig */
     float ppr_threshold, median_threshold, median_eps; /* ValidationConfig */
     int32_t replace;
+    int32_t deform; /* 0: the reference's uniform window shift; 1: deformed windows */
 } OrcConfig;
 
 int orc_grid(int64_t height, int64_t width, int64_t window, float overlap, OrcGrid* out);
@@ -96,6 +97,27 @@ void orc_find_peak(const float* corr, int64_t n, float* peak);
 /* Full correlation plane (scaled) for one window pair; returns 0 for a flat window. */
 int orc_correlation_plane(const float* a, int64_t ha, int64_t wa, float ax, float ay, const float* b,
                           int64_t hb, int64_t wb, float bx, float by, int64_t n, int mode, float* plane);
+
+/* Window deformation (not in the reference, whose windows only shift: multipass.rs:224-231;
+ * deformation is deferred in docs/phase1-plan.md:104,248). Parity of these is unpinned against the
+ * reference and pinned against this restatement only.
+ *
+ * orc_place_deform: as orc_place, plus the predictor (field.rs:56-81 sampling) at the four corner
+ * pixels of each window's grid position (x0, y0), (x0+n-1, y0), (x0, y0+n-1), (x0+n-1, y0+n-1):
+ * corners[8k..8k+7] = dx00, dy00, dx10, dy10, dx01, dy01, dx11, dy11. Without a predictor all zero.
+ *
+ * orc_correlate_pass_deform: every pixel (r, c) of the window at grid position (x0, y0) is
+ * displaced by the bilinear blend of the corners, D = (1-u)(1-v) D00 + u(1-v) D10 + (1-u)v D01
+ * + uv D11 with u = c/(n-1), v = r/(n-1) (f32, left to right); window A samples frame A at
+ * (x0+c, y0+r) - D/2 and window B frame B at + D/2, bilinearly with coordinates clamped to the
+ * image; the vector is D(center) + peak, D(center) the blend at u = v = 1/2. The signal mask
+ * uses the undeformed origins (`origins`, from orc_place). */
+void orc_place_deform(const OrcGrid* grid, int64_t h, int64_t w, const OrcGrid* pgrid, const float* pdx,
+                      const float* pdy, float* origins, float* corners);
+void orc_correlate_pass_deform(const float* image_a, const float* image_b, const float* base_a,
+                               const float* base_b, int64_t h, int64_t w, const OrcGrid* grid,
+                               const float* origins, const float* corners, float min_mean, float min_std,
+                               int mode, int nthreads, float* dx, float* dy, float* ppr, uint8_t* flags);
 
 /* validate (validate.rs:51-130) in place. */
 void orc_validate(float* dx, float* dy, const float* ppr, uint8_t* flags, int64_t ny, int64_t nx,

@@ -14,6 +14,7 @@ from .api import (  # noqa: F401
     PivAnalyzer,
     PivConfig,
     PivError,
+    PivServer,
     PreparedFrame,
     PreprocessConfig,
     ShapeMismatchError,

@@ -23,8 +23,9 @@ EXPORTS = [
     "piv_frame_set_prepared", "piv_frame_download", "piv_frame_image_device", "piv_background_device",
     "piv_analyze", "piv_analyze_device", "piv_analyze_traced", "piv_analyze_batch_device",
     "piv_batch_create", "piv_batch_destroy", "piv_batch_input_device", "piv_batch_input_bytes", "piv_batch_run",
-    "piv_batch_sync", "piv_batch_outputs_device", "piv_batch_run_host", "piv_batch_kernels",
+    "piv_batch_sync", "piv_batch_outputs_device", "piv_batch_run_host", "piv_batch_kernels", "piv_batch_stream",
     "piv_place_windows", "piv_correlate_origins", "piv_validate_field", "piv_validate_field_noalloc",
+    "piv_server_create", "piv_server_destroy", "piv_server_submit", "piv_server_wait", "piv_server_stats",
 ]
 
 
@@ -67,6 +68,24 @@ class PivTraceC(ctypes.Structure):
         ("raw_peak_ratio", ctypes.c_void_p), ("raw_flags", ctypes.c_void_p), ("dx", ctypes.c_void_p),
         ("dy", ctypes.c_void_p), ("peak_ratio", ctypes.c_void_p), ("flags", ctypes.c_void_p),
     ]
+
+
+class PivServerConfigC(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("memory_budget_bytes", ctypes.c_int64), ("max_in_flight", ctypes.c_int32)]
+
+
+class PivRequestC(ctypes.Structure):
+    _fields_ = [
+        ("config", PivConfigC), ("preprocess", PivPreprocessC), ("dtype", ctypes.c_int32),
+        ("height", ctypes.c_int64), ("width", ctypes.c_int64), ("frame_a", ctypes.c_void_p),
+        ("frame_b", ctypes.c_void_p), ("dx", ctypes.c_void_p), ("dy", ctypes.c_void_p),
+        ("peak_ratio", ctypes.c_void_p), ("flags", ctypes.c_void_p),
+    ]
+
+
+class PivServerStatsC(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int64) for n in ("submitted", "admitted", "completed", "failed", "queued", "in_flight",
+                                                "memory_in_use_bytes", "steps", "kernel_launches")]
 
 
 _lib = None
@@ -120,10 +139,16 @@ def load():
         "piv_batch_outputs_device": ([vp, P(vp), P(vp), P(vp), P(vp), P(vp)], i32),
         "piv_batch_run_host": ([vp, vp, vp, vp, vp, vp, vp], i32),
         "piv_batch_kernels": ([vp], i64),
+        "piv_batch_stream": ([vp], vp),
         "piv_place_windows": ([vp, i64, i64, P(PivGridC), P(PivGridC), vp, vp, vp], i32),
         "piv_correlate_origins": ([vp, vp, vp, i64, vp, i64, vp, vp, vp, vp], i32),
         "piv_validate_field": ([vp, i64, i64, vp, vp, vp, vp, vp, vp, vp, P(PivSummaryC)], i32),
         "piv_validate_field_noalloc": ([i64, i64, vp, vp, vp, vp, f32, f32, f32, f32, i32, vp, vp, vp, vp], i32),
+        "piv_server_create": ([P(PivServerConfigC), P(vp)], i32),
+        "piv_server_destroy": ([vp], None),
+        "piv_server_submit": ([vp, P(PivRequestC), P(ctypes.c_uint64)], i32),
+        "piv_server_wait": ([vp, ctypes.c_uint64, P(PivSummaryC), P(ctypes.c_double)], i32),
+        "piv_server_stats": ([vp, P(PivServerStatsC)], i32),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)

@@ -496,6 +496,10 @@ class PivBatch:
     def kernels(self) -> int:
         return int(_lib.load().piv_batch_kernels(self._h))
 
+    def stream(self) -> int:
+        """The batch's CUDA stream handle (for torch.cuda.ExternalStream)."""
+        return int(_lib.load().piv_batch_stream(self._h))
+
     def outputs_device(self):
         ptrs = [ctypes.c_void_p() for _ in range(5)]
         _check(_lib.load().piv_batch_outputs_device(self._h, *[ctypes.byref(p) for p in ptrs]))
@@ -518,6 +522,64 @@ class PivBatch:
     def close(self):
         if getattr(self, "_h", None):
             _lib.load().piv_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class PivServer:
+    """The serving form: continuous batching of frame pairs of any size and window schedule on one
+    GPU under a device-memory budget. submit() returns a ticket at once; wait(ticket) returns the
+    PairResult and the request's latency in milliseconds."""
+
+    def __init__(self, memory_budget_bytes=60 << 30, max_in_flight=64, device=-1):
+        h = ctypes.c_void_p()
+        c = _lib.PivServerConfigC(int(device), int(memory_budget_bytes), int(max_in_flight))
+        _check(_lib.load().piv_server_create(ctypes.byref(c), ctypes.byref(h)))
+        self._h = h
+        self._pending = {}
+
+    def submit(self, a, b, cfg: PivConfig = None, pre: PreprocessConfig = None, out=None):
+        """Queues the pair (a, b) of host samples (u8/u16/f32, pinned memory recommended). `out`
+        optionally gives the four result arrays (dx, dy, peak_ratio, flags) to fill."""
+        cfg = PivConfig() if cfg is None else cfg
+        pre = RAW if pre is None else pre
+        a = np.ascontiguousarray(a)
+        b = np.ascontiguousarray(b)
+        if a.shape != b.shape or a.dtype != b.dtype:
+            raise ShapeMismatchError(f"frames differ: {a.shape} {a.dtype} vs {b.shape} {b.dtype}")
+        h, w = a.shape
+        g = Grid.new(h, w, cfg.windows[-1], cfg.overlap)
+        if out is None:
+            out = (np.empty((g.ny, g.nx), np.float32), np.empty((g.ny, g.nx), np.float32),
+                   np.empty((g.ny, g.nx), np.float32), np.empty((g.ny, g.nx), np.uint8))
+        cc = cfg._c()
+        q = _lib.PivRequestC(cc, pre._c(), _dtype_code(a), h, w, a.ctypes.data, b.ctypes.data, out[0].ctypes.data,
+                             out[1].ctypes.data, out[2].ctypes.data, out[3].ctypes.data)
+        rid = ctypes.c_uint64()
+        _check(_lib.load().piv_server_submit(self._h, ctypes.byref(q), ctypes.byref(rid)))
+        self._pending[rid.value] = (a, b, out, g, cc)
+        return rid.value
+
+    def wait(self, ticket):
+        a, b, out, g, cc = self._pending.pop(ticket)
+        s = _lib.PivSummaryC()
+        lat = ctypes.c_double()
+        _check(_lib.load().piv_server_wait(self._h, ctypes.c_uint64(ticket), ctypes.byref(s), ctypes.byref(lat)))
+        return PairResult(VectorField(g, out[0], out[1], out[2], out[3]), ValidationSummary._from_c(s)), lat.value
+
+    def stats(self):
+        s = _lib.PivServerStatsC()
+        _check(_lib.load().piv_server_stats(self._h, ctypes.byref(s)))
+        return {n: getattr(s, n) for n, _ in s._fields_}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.load().piv_server_destroy(self._h)
             self._h = None
 
     def __del__(self):

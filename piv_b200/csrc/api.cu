@@ -3,9 +3,15 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
 #include <cstring>
+#include <deque>
+#include <map>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/piv_b200.h"
@@ -1121,6 +1127,8 @@ int32_t piv_batch_run(PivBatch* bt) {
     return PIV_OK;
 }
 
+void* piv_batch_stream(PivBatch* bt) { return bt ? (void*)bt->an->cur : nullptr; }
+
 int32_t piv_batch_sync(PivBatch* bt) {
     if (!bt) return fail(PIV_ERR_ARGUMENT, "null batch");
     CUDA_TRY(cudaSetDevice(bt->an->device));
@@ -1172,5 +1180,469 @@ int32_t piv_batch_run_host(PivBatch* bt, const void* raw, float* dx, float* dy, 
 }
 
 int64_t piv_batch_kernels(const PivBatch* bt) { return bt ? bt->kernels : 0; }
+
+// ---------------------------------------------------------------------------------------------
+// Serving form: continuous batching of independent requests on one stream.
+// ---------------------------------------------------------------------------------------------
+}  // extern "C"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+    uint64_t id = 0;
+    PivAnalyzer cfg;  // configuration only (no stream of its own)
+    PivPreprocessC pre{};
+    int32_t dtype = 0;
+    int64_t H = 0, W = 0;
+    const void* host_a = nullptr;
+    const void* host_b = nullptr;
+    float* out_dx = nullptr;
+    float* out_dy = nullptr;
+    float* out_ppr = nullptr;
+    uint8_t* out_flags = nullptr;
+    size_t bytes = 0;
+    void* mem = nullptr;
+    PivFrame fa, fb;
+    std::vector<PassBuf> passes;
+    unsigned long long* d_counts = nullptr;
+    unsigned long long h_counts[8] = {};
+    bool use_stats = false;
+    int next_pass = 0;
+    cudaEvent_t done_ev = nullptr;
+    bool final_launched = false;
+    bool done = false;
+    int status = PIV_OK;
+    std::string error;
+    Clock::time_point t_submit, t_done;
+};
+
+// Device footprint of a request and the layout of its single allocation.
+size_t request_bytes(const Request& r, bool stats, bool chain, bool both, size_t es) {
+    const size_t hw = (size_t)r.H * (size_t)r.W;
+    size_t b = 2 * align256(es * hw) + 2 * align256(4 * hw);
+    if (chain) b += 2 * align256(4 * hw);
+    if (both) b += 2 * align256(4 * hw);
+    if (stats) b += 4 * align256(8 * (size_t)(r.H + 1) * (size_t)(r.W + 1));
+    b += 2 * align256(4 * (4 + 512 + 4)) + 2 * align256(8);
+    for (const PassBuf& pb : r.passes) {
+        const size_t c = (size_t)pb.cells;
+        b += align256(16 * c) + align256(c) + 3 * align256(4 * c) + 3 * align256(c) + 2 * align256(4 * c) + align256(c);
+    }
+    return b + align256(8 * sizeof(unsigned long long));
+}
+
+}  // namespace
+
+struct PivServer {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int64_t budget = 0;
+    int max_in_flight = 1;
+    std::mutex mu;
+    std::condition_variable cv_submit, cv_done;
+    std::deque<Request*> queue;
+    std::vector<Request*> active;
+    std::map<uint64_t, Request*> by_id;
+    uint64_t next_id = 1;
+    bool stop = false;
+    std::thread worker;
+    int64_t in_use = 0;
+    PivServerStatsC stats{};
+    int variant[129] = {};
+    std::vector<cudaEvent_t> step_events;  // completion of recent steps (bounded run-ahead)
+
+    void loop();
+    bool admit_locked(Request* r, std::string* err);
+    void launch_step(std::vector<Request*>& work);
+    void retire();
+};
+
+namespace {
+
+// Allocates the request's device memory on the server stream and queues the uploads and frame
+// preparation (preprocess.rs:138-158) for both frames.
+int admit_request(PivServer* sv, Request* r) {
+    const size_t es = dtype_size(r->dtype);
+    const size_t hw = (size_t)r->H * (size_t)r->W;
+    const bool chain = r->pre.smooth_sigma > 0.0f || r->pre.normalize_radius > 0;
+    const bool both = r->pre.smooth_sigma > 0.0f && r->pre.normalize_radius > 0;
+    CUDA_TRY(cudaMallocAsync(&r->mem, r->bytes, sv->stream));
+    char* p = (char*)r->mem;
+    auto take = [&](size_t bytes) {
+        void* q = p;
+        p += align256(bytes);
+        return q;
+    };
+    for (PivFrame* f : {&r->fa, &r->fb}) {
+        f->an = &r->cfg;
+        f->device = sv->device;
+        f->H = r->H;
+        f->W = r->W;
+        f->d_raw = take(es * hw);
+        f->d_raw_bytes = es * hw;
+        f->image = (float*)take(4 * hw);
+        f->base = f->image;
+        if (chain) f->base_store = (float*)take(4 * hw);
+        if (both) f->tmp = (float*)take(4 * hw);
+        if (r->use_stats) {
+            f->sum = (long long*)take(8 * (size_t)(r->H + 1) * (size_t)(r->W + 1));
+            f->sumsq = (long long*)take(8 * (size_t)(r->H + 1) * (size_t)(r->W + 1));
+        }
+        f->words = (unsigned int*)take(4 * (4 + 512 + 4));
+        f->scales = (int*)take(8);
+    }
+    for (PassBuf& pb : r->passes) {
+        const size_t c = (size_t)pb.cells;
+        pb.origins = (float4*)take(16 * c);
+        pb.status = (uint8_t*)take(c);
+        pb.raw_dx = (float*)take(4 * c);
+        pb.raw_dy = (float*)take(4 * c);
+        pb.raw_ppr = (float*)take(4 * c);
+        pb.raw_flags = (uint8_t*)take(c);
+        pb.f1 = (uint8_t*)take(c);
+        pb.f2 = (uint8_t*)take(c);
+        pb.dx = (float*)take(4 * c);
+        pb.dy = (float*)take(4 * c);
+        pb.flags = (uint8_t*)take(c);
+    }
+    r->d_counts = (unsigned long long*)take(8 * sizeof(unsigned long long));
+    r->cfg.cur = sv->stream;
+    CUDA_TRY(cudaMemcpyAsync(r->fa.d_raw, r->host_a, es * hw, cudaMemcpyHostToDevice, sv->stream));
+    CUDA_TRY(cudaMemcpyAsync(r->fb.d_raw, r->host_b, es * hw, cudaMemcpyHostToDevice, sv->stream));
+    int st = prepare_common(&r->cfg, &r->fa, r->fa.d_raw, r->dtype, &r->pre, nullptr);
+    if (!st) st = prepare_common(&r->cfg, &r->fb, r->fb.d_raw, r->dtype, &r->pre, nullptr);
+    return st;
+}
+
+}  // namespace
+
+bool PivServer::admit_locked(Request* r, std::string* err) {
+    const int st = admit_request(this, r);
+    if (st) {
+        *err = g_last_error;
+        return false;
+    }
+    return true;
+}
+
+// One step: the next pass of every admitted request (multipass.rs:194-259 and validate.rs:51),
+// batched across requests: one placement launch, one correlation launch per window size, one
+// validation chain; requests whose last pass this is get their summary and their results copied
+// to host memory, followed by a completion event.
+void PivServer::launch_step(std::vector<Request*>& work) {
+    std::vector<PlaceParams> pps;
+    std::map<int, std::vector<CorrParams>> cps;
+    std::vector<ValidateParams> vps;
+    for (Request* r : work) {
+        const int i = r->next_pass;
+        PassBuf& pb = r->passes[i];
+        PlaceParams pp{};
+        pp.grid = to_gp(pb.grid);
+        pp.H = (int)r->H;
+        pp.W = (int)r->W;
+        pp.has_pred = i > 0;
+        if (i > 0) {
+            pp.pgrid = to_gp(r->passes[i - 1].grid);
+            pp.pdx = r->passes[i - 1].dx;
+            pp.pdy = r->passes[i - 1].dy;
+        }
+        pp.origins = pb.origins;
+        pp.status = pb.status;
+        pp.use_stats = r->use_stats;
+        if (r->use_stats) {
+            pp.sa = stats_of(&r->fa);
+            pp.sb = stats_of(&r->fb);
+        }
+        pp.min_mean = r->cfg.min_mean;
+        pp.min_std = r->cfg.min_std;
+        pps.push_back(pp);
+        cps[(int)pb.grid.window].push_back(CorrParams{r->fa.image, r->fb.image, (int)r->H, (int)r->W, pb.origins, pb.status,
+                                                      (int)pb.cells, pb.raw_dx, pb.raw_dy, pb.raw_ppr, pb.raw_flags});
+        vps.push_back(ValidateParams{(int)pb.grid.nx, (int)pb.grid.ny, pb.raw_dx, pb.raw_dy, pb.raw_ppr, pb.raw_flags, pb.f1,
+                                     pb.f2, pb.dx, pb.dy, pb.flags, (float)r->cfg.windows[0] / 2.0f, r->cfg.ppr_threshold,
+                                     r->cfg.median_threshold, r->cfg.median_eps, r->cfg.replace});
+    }
+    int nl = 0;
+    cudaError_t e = launch_place_items(pps.data(), (int)pps.size(), stream, &nl);
+    for (auto& kv : cps)
+        if (e == cudaSuccess) e = launch_correlate_items(kv.first, variant[kv.first], kv.second.data(), (int)kv.second.size(),
+                                                         stream, &nl);
+    if (e == cudaSuccess) e = launch_validate_items(vps.data(), (int)vps.size(), stream, &nl);
+    std::vector<SummaryItem> sums;
+    for (Request* r : work) {
+        r->next_pass++;
+        if (r->next_pass == (int)r->passes.size()) {
+            const PassBuf& last = r->passes.back();
+            sums.push_back(SummaryItem{last.flags, (int)last.cells, r->d_counts});
+        }
+    }
+    if (e == cudaSuccess && !sums.empty()) e = launch_summary_items(sums.data(), (int)sums.size(), stream, &nl);
+    for (Request* r : work) {
+        if (r->next_pass != (int)r->passes.size() || e != cudaSuccess) continue;
+        const PassBuf& last = r->passes.back();
+        const size_t c = (size_t)last.cells;
+        if (r->out_dx) e = cudaMemcpyAsync(r->out_dx, last.dx, 4 * c, cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess && r->out_dy) e = cudaMemcpyAsync(r->out_dy, last.dy, 4 * c, cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess && r->out_ppr)
+            e = cudaMemcpyAsync(r->out_ppr, last.raw_ppr, 4 * c, cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess && r->out_flags) e = cudaMemcpyAsync(r->out_flags, last.flags, c, cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(r->h_counts, r->d_counts, sizeof(r->h_counts), cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&r->done_ev, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventRecord(r->done_ev, stream);
+        r->final_launched = true;
+    }
+    stats.steps++;
+    stats.kernel_launches += nl;
+    if (e != cudaSuccess) {
+        for (Request* r : work) {
+            r->status = PIV_ERR_CUDA;
+            r->error = cudaGetErrorString(e);
+            r->final_launched = true;
+        }
+    }
+}
+
+// Requests whose completion event has fired: results are in host memory, memory goes back.
+void PivServer::retire() {
+    std::vector<Request*> keep;
+    bool any = false;
+    for (Request* r : active) {
+        bool fin = false;
+        if (r->final_launched) {
+            if (!r->done_ev) {
+                fin = true;  // failed before recording
+            } else {
+                const cudaError_t q = cudaEventQuery(r->done_ev);
+                if (q == cudaSuccess) fin = true;
+                else if (q != cudaErrorNotReady) {
+                    r->status = PIV_ERR_CUDA;
+                    r->error = cudaGetErrorString(q);
+                    fin = true;
+                }
+            }
+        }
+        if (!fin) {
+            keep.push_back(r);
+            continue;
+        }
+        r->t_done = Clock::now();
+        if (r->done_ev) cudaEventDestroy(r->done_ev);
+        r->done_ev = nullptr;
+        if (r->mem) cudaFreeAsync(r->mem, stream);
+        r->mem = nullptr;
+        in_use -= (int64_t)r->bytes;
+        std::lock_guard<std::mutex> lk(mu);
+        r->done = true;
+        if (r->status == PIV_OK) stats.completed++; else stats.failed++;
+        stats.in_flight--;
+        any = true;
+    }
+    active.swap(keep);
+    if (any) cv_done.notify_all();
+}
+
+void PivServer::loop() {
+    cudaSetDevice(device);
+    for (;;) {
+        // admission at a step boundary (FIFO while slots and memory allow)
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            if (queue.empty() && active.empty()) {
+                if (stop) break;
+                cv_submit.wait_for(lk, std::chrono::milliseconds(50));
+                continue;
+            }
+            while (!queue.empty() && (int)active.size() < max_in_flight &&
+                   in_use + (int64_t)queue.front()->bytes <= budget) {
+                Request* r = queue.front();
+                queue.pop_front();
+                stats.queued--;
+                lk.unlock();
+                std::string err;
+                const bool ok = admit_locked(r, &err);
+                lk.lock();
+                if (!ok) {
+                    r->status = PIV_ERR_CUDA;
+                    r->error = err;
+                    r->done = true;
+                    r->t_done = Clock::now();
+                    stats.failed++;
+                    cv_done.notify_all();
+                    continue;
+                }
+                in_use += (int64_t)r->bytes;
+                stats.admitted++;
+                stats.in_flight++;
+                active.push_back(r);
+            }
+            stats.memory_in_use_bytes = in_use;
+        }
+        std::vector<Request*> work;
+        for (Request* r : active)
+            if (r->next_pass < (int)r->passes.size() && !r->final_launched) work.push_back(r);
+        if (!work.empty()) {
+            launch_step(work);
+            // bounded run-ahead: keep at most two steps queued on the device
+            cudaEvent_t ev;
+            if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess) {
+                cudaEventRecord(ev, stream);
+                step_events.push_back(ev);
+                while (step_events.size() > 2) {
+                    cudaEventSynchronize(step_events.front());
+                    cudaEventDestroy(step_events.front());
+                    step_events.erase(step_events.begin());
+                }
+            }
+        } else {
+            std::this_thread::sleep_for(std::chrono::microseconds(20));
+        }
+        retire();
+    }
+    for (cudaEvent_t ev : step_events) cudaEventDestroy(ev);
+    step_events.clear();
+}
+
+extern "C" {
+
+int32_t piv_server_create(const PivServerConfigC* cfg, PivServer** out) {
+    if (!cfg || !out) return fail(PIV_ERR_ARGUMENT, "null argument");
+    *out = nullptr;
+    if (cfg->memory_budget_bytes <= 0 || cfg->max_in_flight <= 0) return fail(PIV_ERR_ARGUMENT, "bad server config");
+    int dev = cfg->device;
+    if (dev < 0) CUDA_TRY(cudaGetDevice(&dev));
+    CUDA_TRY(cudaSetDevice(dev));
+    int st = ensure_device_init(dev);
+    if (st) return st;
+    // keep freed request memory in the pool instead of returning it to the driver
+    cudaMemPool_t pool;
+    CUDA_TRY(cudaDeviceGetDefaultMemPool(&pool, dev));
+    uint64_t threshold = UINT64_MAX;
+    CUDA_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
+    PivServer* sv = new PivServer();
+    sv->device = dev;
+    sv->budget = cfg->memory_budget_bytes;
+    sv->max_in_flight = cfg->max_in_flight;
+    cudaError_t e = cudaStreamCreateWithFlags(&sv->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete sv;
+        return fail(PIV_ERR_CUDA, "server stream: %s", cudaGetErrorString(e));
+    }
+    sv->worker = std::thread([sv] { sv->loop(); });
+    *out = sv;
+    return PIV_OK;
+}
+
+void piv_server_destroy(PivServer* sv) {
+    if (!sv) return;
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        sv->stop = true;
+    }
+    sv->cv_submit.notify_all();
+    if (sv->worker.joinable()) sv->worker.join();
+    cudaSetDevice(sv->device);
+    cudaStreamSynchronize(sv->stream);
+    for (auto& kv : sv->by_id) delete kv.second;
+    cudaStreamDestroy(sv->stream);
+    delete sv;
+}
+
+int32_t piv_server_submit(PivServer* sv, const PivRequestC* q, uint64_t* id) {
+    if (!sv || !q || !id) return fail(PIV_ERR_ARGUMENT, "null argument");
+    int st = check_cfg(&q->config);
+    if (st) return st;
+    const size_t es = dtype_size(q->dtype);
+    if (!es) return fail(PIV_ERR_ARGUMENT, "unknown dtype %d", q->dtype);
+    if (!q->frame_a || !q->frame_b) return fail(PIV_ERR_ARGUMENT, "null frame");
+    if (q->preprocess.clip_percentile > 0.0 && q->dtype == PIV_DTYPE_F32)
+        return fail(PIV_ERR_UNSUPPORTED, "percentile clipping needs integer (u8/u16) samples");
+    Request* r = new Request();
+    PivAnalyzer& c = r->cfg;
+    c.windows.assign(q->config.windows, q->config.windows + q->config.n_windows);
+    c.overlap = q->config.overlap;
+    c.final_iterations = q->config.final_iterations;
+    c.min_mean = q->config.min_mean;
+    c.min_std = q->config.min_std;
+    c.ppr_threshold = q->config.ppr_threshold;
+    c.median_threshold = q->config.median_threshold;
+    c.median_eps = q->config.median_eps;
+    c.replace = q->config.replace;
+    c.device = sv->device;
+    r->pre = q->preprocess;
+    r->dtype = q->dtype;
+    r->H = q->height;
+    r->W = q->width;
+    r->host_a = q->frame_a;
+    r->host_b = q->frame_b;
+    r->out_dx = q->dx;
+    r->out_dy = q->dy;
+    r->out_ppr = q->peak_ratio;
+    r->out_flags = q->flags;
+    for (int32_t n : c.pass_windows()) {
+        PassBuf pb{};
+        st = make_grid(r->H, r->W, n, c.overlap, &pb.grid);
+        if (st) {
+            delete r;
+            return st;
+        }
+        pb.cells = pb.grid.nx * pb.grid.ny;
+        r->passes.push_back(pb);
+    }
+    const bool chain = r->pre.smooth_sigma > 0.0f || r->pre.normalize_radius > 0;
+    const bool both = r->pre.smooth_sigma > 0.0f && r->pre.normalize_radius > 0;
+    r->fa.nonneg = r->fb.nonneg = r->dtype != PIV_DTYPE_F32;
+    r->use_stats = !c.mask_trivial() || r->dtype == PIV_DTYPE_F32;
+    r->bytes = request_bytes(*r, r->use_stats, chain, both, es);
+    if ((int64_t)r->bytes > sv->budget) {
+        const size_t b = r->bytes;
+        delete r;
+        return fail(PIV_ERR_UNSUPPORTED, "request needs %zu bytes of device memory, above the budget", b);
+    }
+    r->t_submit = Clock::now();
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        r->id = sv->next_id++;
+        sv->by_id[r->id] = r;
+        sv->queue.push_back(r);
+        sv->stats.submitted++;
+        sv->stats.queued++;
+    }
+    sv->cv_submit.notify_all();
+    *id = r->id;
+    return PIV_OK;
+}
+
+int32_t piv_server_wait(PivServer* sv, uint64_t id, PivSummaryC* summary, double* latency_ms) {
+    if (!sv) return fail(PIV_ERR_ARGUMENT, "null server");
+    std::unique_lock<std::mutex> lk(sv->mu);
+    auto it = sv->by_id.find(id);
+    if (it == sv->by_id.end()) return fail(PIV_ERR_ARGUMENT, "unknown request %llu", (unsigned long long)id);
+    Request* r = it->second;
+    sv->cv_done.wait(lk, [r] { return r->done; });
+    sv->by_id.erase(it);
+    lk.unlock();
+    const int st = r->status;
+    if (st) fail(st, "request %llu: %s", (unsigned long long)id, r->error.c_str());
+    if (summary) {
+        summary->no_signal = (int64_t)r->h_counts[0];
+        summary->low_ppr = (int64_t)r->h_counts[1];
+        summary->median_outliers = (int64_t)r->h_counts[2];
+        summary->out_of_range = (int64_t)r->h_counts[3];
+        summary->replaced = (int64_t)r->h_counts[4];
+    }
+    if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count();
+    delete r;
+    return st;
+}
+
+int32_t piv_server_stats(PivServer* sv, PivServerStatsC* out) {
+    if (!sv || !out) return fail(PIV_ERR_ARGUMENT, "null argument");
+    std::lock_guard<std::mutex> lk(sv->mu);
+    *out = sv->stats;
+    return PIV_OK;
+}
 
 }  // extern "C"

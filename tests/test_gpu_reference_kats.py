@@ -1,0 +1,274 @@
+"""The reference's own known-answer unit tests, run on the CUDA path through the C ABI.
+
+Ported from correlate.rs:310-402, multipass.rs:319-475, validate.rs:187-242 and
+preprocess.rs:486-519 (same inputs and assertions), plus the GPU counterparts of the oracle-only
+definitions added by this project (percentile clip, background estimator).
+"""
+import numpy as np
+import pytest
+
+from piv_b200 import synthetic as S
+
+pytestmark = pytest.mark.gpu
+
+
+def _an(windows=(32,), final_iterations=1, **kw):
+    import piv_b200 as P
+    return P.PivAnalyzer(P.PivConfig(windows=list(windows), final_iterations=final_iterations, **kw))
+
+
+def _window(an, a, b, n, ax=0.0, ay=0.0, bx=None, by=None):
+    import piv_b200 as P
+    fa = an.frame(*a.shape).set_prepared(a)
+    fb = an.frame(*b.shape).set_prepared(b)
+    o = np.array([[ax, ay, ax if bx is None else bx, ay if by is None else by]], np.float32)
+    dx, dy, ppr, fl = an.correlate_origins(fa, fb, n, o)
+    return float(dx[0]), float(dy[0]), float(ppr[0]), int(fl[0])
+
+
+# ------------------------------------------------------------------ correlate.rs:310-402
+def test_integer_shift_is_exact_for_circular_content():
+    n = 32
+    rng = S.Rng(7)
+    a = np.array([[rng.uniform() for _ in range(n)] for _ in range(n)], np.float32)
+    b = np.array([[a[(y + 3) % n, (x + n - 5) % n] for x in range(n)] for y in range(n)], np.float32)
+    dx, dy, ppr, fl = _window(_an([n]), a, b, n)
+    assert fl == 0 and abs(dx - 5.0) < 0.02 and abs(dy + 3.0) < 0.02 and ppr > 2.0
+
+
+def test_subpixel_shift_of_particles():
+    a, b = S.particle_pair(64, 64, 3, 0.05, 1.2, lambda x, y: (0.4, -0.3))
+    dx, dy, _, _ = _window(_an([32]), a, b, 32, 16, 16)
+    assert abs(dx - 0.4) < 0.08 and abs(dy + 0.3) < 0.08
+
+
+def test_isolated_particle_is_unbiased():
+    a = S.render(64, 64, [31.3], [30.7], [1.5], [1.0])
+    b = S.render(64, 64, [31.7], [30.45], [1.5], [1.0])
+    dx, dy, _, _ = _window(_an([64]), a, b, 64)
+    assert abs(dx - 0.4) < 1e-3 and abs(dy + 0.25) < 1e-3
+
+
+def test_flat_window_has_no_peak():
+    import piv_b200 as P
+    a = np.full((32, 32), 0.3, np.float32)
+    _, _, _, fl = _window(_an([32]), a, a, 32)
+    assert fl == P.flags.NO_SIGNAL
+
+
+# ------------------------------------------------------------------ multipass.rs:319-475
+def _errors(field, truth, margin, size):
+    g = field.grid
+    s, worst, n = 0.0, 0.0, 0
+    for iy, y in enumerate(g.ys()):
+        for ix, x in enumerate(g.xs()):
+            if x < margin or y < margin or x > size - margin or y > size - margin:
+                continue
+            u, v = truth(x, y)
+            e = float(np.hypot(field.dx[iy, ix] - u, field.dy[iy, ix] - v))
+            s += e * e
+            worst = max(worst, e)
+            n += 1
+    return (s / n) ** 0.5, worst, n
+
+
+def _run(a, b, windows, pre=None, **kw):
+    import piv_b200 as P
+    an = _an(windows, 1 if len(windows) == 1 else 2, **kw)
+    pre = P.RAW if pre is None else pre
+    return an.analyze(an.prepare(a, pre), an.prepare(b, pre))
+
+
+@pytest.mark.parametrize("i,uv", list(enumerate([(0.25, 0.0), (0.0, 0.5), (3.7, 0.0), (3.7, -1.3), (-2.2, 2.6)])))
+def test_uniform_shifts_particles(i, uv):
+    u, v = uv
+    a, b = S.particle_pair(256, 256, 10 + i, 0.04, 1.2, lambda x, y: (u, v))
+    r = _run(a, b, [64, 32])
+    rms, worst, n = _errors(r.field, lambda x, y: (u, v), 20.0, 256.0)
+    assert n > 100 and rms < 0.05, (rms, worst)
+    assert r.summary.median_outliers * 50 <= r.field.dx.size
+
+
+def test_uniform_shift_fog_texture_with_noise():
+    import piv_b200 as P
+    u, v = 2.4, -1.7
+    a, b = S.fog_pair(256, 256, 4, lambda x, y: (u, v))
+    a, b = S.add_noise(a, 0.01, 1), S.add_noise(b, 0.01, 2)
+    an = P.PivAnalyzer(P.PivConfig())
+    r = an.analyze(an.prepare(a, P.PreprocessConfig()), an.prepare(b, P.PreprocessConfig()))
+    rms, _, _ = _errors(r.field, lambda x, y: (u, v), 20.0, 256.0)
+    assert rms < 0.1
+
+
+def test_window_as_large_as_the_image():
+    u, v = 1.5, -0.5
+    a, b = S.particle_pair(64, 64, 3, 0.04, 1.2, lambda x, y: (u, v))
+    r = _run(a, b, [64])
+    assert r.field.dx.size == 1
+    assert abs(r.field.dx[0, 0] - u) < 0.2 and abs(r.field.dy[0, 0] - v) < 0.2
+    assert np.isfinite(_run(a, b, [64, 64]).field.dx[0, 0])
+
+
+def test_large_shift_recovered_by_multipass():
+    u, v = 20.0, -6.0
+    a, b = S.particle_pair(320, 320, 5, 0.04, 1.2, lambda x, y: (u, v))
+    rms, _, _ = _errors(_run(a, b, [64, 32]).field, lambda x, y: (u, v), 48.0, 320.0)
+    assert rms < 0.1
+    rms1, _, _ = _errors(_run(a, b, [32]).field, lambda x, y: (u, v), 48.0, 320.0)
+    assert rms1 > 1.0
+
+
+@pytest.mark.parametrize("kind", ["rotation", "shear"])
+def test_rotation_and_shear_with_directions(kind):
+    c = 127.5
+    truth = (lambda x, y: (-0.03 * (y - c), 0.03 * (x - c))) if kind == "rotation" else (lambda x, y: (0.025 * (y - c), 0.0))
+    a, b = S.particle_pair(256, 256, 6 if kind == "rotation" else 8, 0.04, 1.2, truth)
+    r = _run(a, b, [64, 32])
+    rms, _, _ = _errors(r.field, truth, 20.0, 256.0)
+    assert rms < 0.15
+    g = r.field.grid
+    for iy, y in enumerate(g.ys()):
+        for ix, x in enumerate(g.xs()):
+            u, v = truth(x, y)
+            if np.hypot(u, v) > 0.5:
+                assert u * r.field.dx[iy, ix] + v * r.field.dy[iy, ix] > 0
+
+
+def test_blank_regions_get_no_signal():
+    import piv_b200 as P
+    a, b = S.particle_pair(128, 128, 9, 0.04, 1.2, lambda x, y: (1.0, 0.0))
+    a[:, :64] = 0.0
+    b[:, :64] = 0.0
+    a, b = S.add_noise(a, 0.002, 3), S.add_noise(b, 0.002, 4)
+    an = P.PivAnalyzer(P.PivConfig(mask=P.MaskConfig(0.01, 0.01)))
+    r = an.analyze(an.prepare(a, P.RAW), an.prepare(b, P.RAW))
+    g = r.field.grid
+    for ix, x in enumerate(g.xs()):
+        col = r.field.flags[:, ix]
+        if x + 16.0 < 64.0:
+            assert np.all(col == P.flags.NO_SIGNAL) and np.all(np.isnan(r.field.dx[:, ix]))
+        elif x - 16.0 >= 64.0:
+            assert np.all((col & P.flags.NO_SIGNAL) == 0)
+
+
+# ------------------------------------------------------------------ validate.rs:187-242
+def _uniform_field(u, v):
+    import piv_b200 as P
+    g = P.Grid.new(160, 160, 32, 0.5)
+    sh = (g.ny, g.nx)
+    return (np.full(sh, u, np.float32), np.full(sh, v, np.float32), np.full(sh, 5.0, np.float32),
+            np.zeros(sh, np.uint8))
+
+
+def test_catches_and_replaces_injected_outliers():
+    import piv_b200 as P
+    dx, dy, ppr, fl = _uniform_field(2.0, -1.0)
+    flat = dx.reshape(-1)
+    for i in range(flat.size):
+        flat[i] += np.float32(0.05) * np.float32((i * 7 % 5) - 2.0)
+    outliers = [(2, 3), (5, 5), (8, 0)]
+    for iy, ix in outliers:
+        dx[iy, ix], dy[iy, ix] = 9.0, 4.0
+    # the reference test runs without a range limit; windows[0]/2 = 64 px is far above the values
+    an = P.PivAnalyzer(P.PivConfig(windows=[128]))
+    odx, ody, ofl, s = an.validate_field(dx, dy, ppr, fl)
+    assert s.median_outliers == len(outliers) and s.replaced == len(outliers)
+    for iy, ix in outliers:
+        assert ofl[iy, ix] & P.flags.MEDIAN_OUTLIER and ofl[iy, ix] & P.flags.REPLACED
+        assert abs(odx[iy, ix] - 2.0) < 0.2 and abs(ody[iy, ix] + 1.0) < 1e-6
+
+
+def test_low_peak_ratio_is_flagged_and_no_signal_untouched():
+    import piv_b200 as P
+    dx, dy, ppr, fl = _uniform_field(1.0, 1.0)
+    ppr[4, 4] = 1.05
+    fl[0, 0] = P.flags.NO_SIGNAL
+    dx[0, 0] = dy[0, 0] = np.nan
+    an = P.PivAnalyzer(P.PivConfig(windows=[128]))
+    odx, _, ofl, s = an.validate_field(dx, dy, ppr, fl)
+    assert (s.low_ppr, s.no_signal, s.median_outliers) == (1, 1, 0)
+    assert ofl[4, 4] == P.flags.LOW_PPR | P.flags.REPLACED
+    assert ofl[0, 0] == P.flags.NO_SIGNAL and np.isnan(odx[0, 0])
+
+
+def test_out_of_range_vectors_are_flagged_and_replaced():
+    import piv_b200 as P
+    dx, dy, ppr, fl = _uniform_field(1.0, 0.5)
+    dx[3, 3] = 40.0
+    an = P.PivAnalyzer(P.PivConfig(windows=[64]))  # max_displacement = 32
+    odx, _, ofl, s = an.validate_field(dx, dy, ppr, fl)
+    assert s.out_of_range == 1
+    assert ofl[3, 3] & P.flags.OUT_OF_RANGE and ofl[3, 3] & P.flags.REPLACED
+    assert odx[3, 3] == 1.0
+
+
+# ------------------------------------------------------------------ preprocess.rs:486-519
+def _prep(img, sigma, radius, eps=0.0):
+    import piv_b200 as P
+    an = P.PivAnalyzer(P.PivConfig(windows=[8]))
+    return an.prepare(img.astype(np.float32), P.PreprocessConfig(sigma, radius, eps)).image
+
+
+def test_blur_preserves_constant_and_mass():
+    b = _prep(np.full((20, 30), 0.5, np.float32), 1.5, 0)
+    assert np.all(np.abs(b - 0.5) < 1e-6)
+    d = np.zeros((21, 21), np.float32)
+    d[10, 10] = 1.0
+    b = _prep(d, 1.0, 0)
+    assert abs(b.sum() - 1.0) < 1e-5
+    assert b[10, 10] > b[10, 11] > b[10, 12]
+
+
+def test_normalize_removes_gradient():
+    f = np.fromfunction(lambda y, x: 0.01 * x + 0.002 * y, (40, 40)).astype(np.float32)
+    n = _prep(f, 0.0, 5, 0.0)
+    assert abs(n[20, 20]) < 1e-3
+
+
+def test_preprocessing_matches_oracle_bit_for_bit_on_random_frames():
+    from oracle import oracle as O
+    rng = np.random.default_rng(3)
+    for h, w, sigma, r, eps in ((97, 131, 1.0, 4, 0.02), (64, 64, 2.5, 7, 0.01), (200, 150, 0.0, 3, 0.05)):
+        img = rng.random((h, w), np.float32)
+        bg = (0.1 * rng.random((h, w))).astype(np.float32)
+        import piv_b200 as P
+        an = P.PivAnalyzer(P.PivConfig(windows=[8]))
+        got = an.prepare(img, P.PreprocessConfig(sigma, r, eps), bg).image
+        ref, _ = O.prepare(img, sigma, r, eps, bg)
+        assert np.abs(got - ref).max() <= 1e-5 * max(1.0, np.abs(ref).max())
+        assert np.mean(got.view(np.uint32) == ref.view(np.uint32)) > 0.999
+
+
+def test_percentile_clip_matches_oracle():
+    import piv_b200 as P
+    from oracle import oracle as O
+    rng = np.random.default_rng(5)
+    raw = np.minimum(rng.gamma(2.0, 300.0, (256, 300)), 4095).astype(np.uint16)
+    raw[10, 10] = 4095
+    for pct in (99.0, 50.0, 100.0, 0.5):
+        an = P.PivAnalyzer(P.PivConfig(windows=[8]))
+        got = an.prepare(raw, P.PreprocessConfig(0.0, 0, 0.0, clip_percentile=pct)).image
+        clipped, _ = O.percentile_clip_u16(raw, pct)
+        assert np.array_equal(got, O.u16_to_f32(clipped))
+
+
+def test_background_estimator_matches_oracle():
+    import ctypes
+
+    import torch
+
+    import piv_b200 as P
+    from oracle import oracle as O
+    rng = np.random.default_rng(8)
+    frames = rng.integers(0, 4096, (5, 64, 96)).astype(np.uint16)
+    an = P.PivAnalyzer(P.PivConfig(windows=[8]))
+    dev = torch.device("cuda", 0)
+    src = torch.from_numpy(frames.view(np.int16)).to(dev)
+    for mode, name in ((0, "min"), (1, "mean")):
+        out = torch.empty((64, 96), device=dev)
+        st = P.load_library().piv_background_device(an._h, ctypes.c_void_p(src.data_ptr()), 1, 5, 64, 96, mode,
+                                                    ctypes.c_void_p(out.data_ptr()))
+        assert st == 0
+        an.sync()
+        ref = O.background(O.u16_to_f32(frames), name)
+        assert np.array_equal(out.cpu().numpy(), ref)

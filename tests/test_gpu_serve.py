@@ -1,0 +1,88 @@
+"""The serving form: continuous batching of mixed requests. Each result must be the same alone
+and in the mix (bit-identical: window pairs are independent inside a launch and every launch
+variant of a window size computes the same arithmetic), and must equal PivAnalyzer.analyze of
+that pair. Admission must respect the device-memory budget."""
+import numpy as np
+import pytest
+
+from conftest import same_floats
+
+pytestmark = pytest.mark.gpu
+
+
+def _pin(a):
+    import torch
+    t = torch.from_numpy(np.ascontiguousarray(a).view(np.int16) if a.dtype == np.uint16 else np.ascontiguousarray(a))
+    return t.pin_memory().numpy().view(a.dtype)
+
+
+def _pair(h, w, seed, shear=0.01, offset=2.0):
+    from piv_b200 import synthetic as S
+    f = lambda X, Y: (np.float32(offset) + shear * (np.asarray(Y, np.float32) - h / 2), np.float32(0.5 * offset))
+    a, b = S.baseline_pair(h, w, seed, f, ppp=0.05, dmin=2.0, dmax=4.0, bits=12)
+    return _pin(a), _pin(b)
+
+
+SCHEDULES = ([32], [64, 32], [64, 32, 16])
+
+
+def _cfg(sched):
+    import piv_b200 as P
+    return P.PivConfig(windows=list(sched), overlap=0.5, final_iterations=1)
+
+
+def _same(r, q):
+    assert np.array_equal(r.field.flags, q.field.flags)
+    assert same_floats(r.field.dx, q.field.dx) and same_floats(r.field.dy, q.field.dy)
+    assert same_floats(r.field.peak_ratio, q.field.peak_ratio)
+    assert r.summary.as_dict() == q.summary.as_dict()
+
+
+def test_results_are_the_same_alone_and_in_the_mix():
+    import piv_b200 as P
+    rng = np.random.default_rng(0)
+    sizes = [(256, 256), (384, 288), (512, 512)]
+    reqs = []
+    for i in range(18):
+        h, w = sizes[i % 3]
+        sched = SCHEDULES[int(rng.integers(0, 3))]
+        reqs.append((h, w, sched, _pair(h, w, 100 + i, shear=float(rng.uniform(0, 0.02)), offset=float(rng.uniform(0, 4)))))
+    # alone: a fresh server per request
+    alone = []
+    for h, w, sched, (a, b) in reqs[:4]:
+        sv = P.PivServer(memory_budget_bytes=1 << 30, max_in_flight=4)
+        t = sv.submit(a, b, _cfg(sched))
+        alone.append(sv.wait(t)[0])
+        sv.close()
+    # in the mix: everything at once on one server
+    sv = P.PivServer(memory_budget_bytes=1 << 30, max_in_flight=64)
+    tickets = [sv.submit(a, b, _cfg(sched)) for h, w, sched, (a, b) in reqs]
+    mixed = [sv.wait(t) for t in tickets]
+    st = sv.stats()
+    sv.close()
+    for r, (q, lat) in zip(alone, mixed[:4]):
+        _same(r, q)
+    assert all(lat > 0 for _, lat in mixed)
+    assert st["completed"] == len(reqs) and st["failed"] == 0
+    assert st["steps"] < sum(len(s) for _, _, s, _ in reqs)  # passes of different requests shared steps
+    # and every request equals the per-pair analysis
+    for (h, w, sched, (a, b)), (q, _) in zip(reqs, mixed):
+        an = P.PivAnalyzer(_cfg(sched))
+        r = an.analyze(an.prepare(a, P.RAW), an.prepare(b, P.RAW))
+        _same(r, q)
+
+
+def test_admission_respects_the_memory_budget():
+    import piv_b200 as P
+    a, b = _pair(512, 512, 7)
+    sv = P.PivServer(memory_budget_bytes=12 << 20, max_in_flight=64)  # room for about two requests
+    tickets = [sv.submit(a, b, _cfg([64, 32, 16])) for _ in range(6)]
+    res = [sv.wait(t) for t in tickets]
+    st = sv.stats()
+    assert st["completed"] == 6
+    for q, _ in res[1:]:
+        _same(res[0][0], q)
+    big_a, big_b = _pair(2048, 2048, 9)
+    with pytest.raises(P.UnsupportedError):
+        sv.submit(big_a, big_b, _cfg([32]))
+    sv.close()
