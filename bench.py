@@ -264,7 +264,8 @@ def run_serving(args, wl):
 
 def piv_config(wl):
     import piv_b200 as P
-    return P.PivConfig(windows=list(wl["windows"]), overlap=wl["overlap"], final_iterations=wl["final_iterations"])
+    return P.PivConfig(windows=list(wl["windows"]), overlap=wl["overlap"], final_iterations=wl["final_iterations"],
+                       deform=bool(wl.get("deform", False)))
 
 
 def final_vectors(wl, h=None, w=None):
@@ -373,27 +374,58 @@ def load_traffic(workload):
         return None
 
 
-def cpu_baseline(wl, a, b, budget_s=12.0, crop=1024):
-    """Times the oracle port (reference operation order, OpenMP over windows) on a crop of the
-    workload with the same pass schedule; returns final-pass vectors/s and the sample used."""
+def _oracle_inputs(wl, a, b, crop):
     from oracle import oracle as O
     ch, cw = min(crop, wl["h"]), min(crop, wl["w"])
     fa = O.u16_to_f32(np.ascontiguousarray(a[:ch, :cw])) if a.dtype == np.uint16 else O.u8_to_f32(a[:ch, :cw])
     fb = O.u16_to_f32(np.ascontiguousarray(b[:ch, :cw])) if b.dtype == np.uint16 else O.u8_to_f32(b[:ch, :cw])
-    cfg = O.OracleConfig(tuple(wl["windows"]), wl["overlap"], wl["final_iterations"])
+    cfg = O.OracleConfig(tuple(wl["windows"]), wl["overlap"], wl["final_iterations"],
+                         deform=int(bool(wl.get("deform", False))))
+    return O, fa, fb, cfg, ch, cw
+
+
+def cpu_baseline(wl, a, b, budget_s=12.0, crop=1024, single_s=0.0):
+    """Times the oracle port (reference operation order, OpenMP over windows) on a crop of the
+    workload with the same pass schedule; returns final-pass vectors/s and the sample used, plus a
+    single-thread figure when single_s > 0."""
+    O, fa, fb, cfg, ch, cw = _oracle_inputs(wl, a, b, crop)
     nthreads = os.cpu_count() or 1
     vec = final_vectors(wl, ch, cw)
-    t0 = time.perf_counter()
-    reps = 0
-    while True:
-        O.analyze(cfg, fa, fb, nthreads=nthreads)
-        reps += 1
-        if time.perf_counter() - t0 >= budget_s:
-            break
-    dt = time.perf_counter() - t0
-    return {"value": vec * reps / dt, "unit": "vectors/s", "cores": nthreads, "kind": "port",
-            "sample": f"{reps} x full {len(pass_windows(wl))}-pass analysis of a {ch}x{cw} crop ({vec} final vectors), "
-                      f"oracle/piv_oracle.cpp, {nthreads} OpenMP threads, {dt:.1f} s"}
+
+    def timed(nt, budget):
+        t0 = time.perf_counter()
+        reps = 0
+        while True:
+            O.analyze(cfg, fa, fb, nthreads=nt)
+            reps += 1
+            if time.perf_counter() - t0 >= budget:
+                break
+        return reps, time.perf_counter() - t0
+
+    reps, dt = timed(nthreads, budget_s)
+    out = {"value": vec * reps / dt, "unit": "vectors/s", "cores": nthreads, "kind": "port",
+           "sample": f"{reps} x full {len(pass_windows(wl))}-pass analysis of a {ch}x{cw} crop ({vec} final vectors), "
+                     f"oracle/piv_oracle.cpp, {nthreads} OpenMP threads, {dt:.1f} s"}
+    if single_s > 0:
+        r1, d1 = timed(1, single_s)
+        out["single_thread_value"] = vec * r1 / d1
+        out["single_thread_sample"] = f"{r1} x the same analysis on 1 thread, {d1:.1f} s"
+    return out
+
+
+def accuracy_vs_fp64(wl, a, b, an, crop=1024):
+    """The GPU's final field on a crop of the pair against the FP64 oracle's (every correlation
+    step in f64): RMS and max |d| over cells both mark valid, and the share of equal flags."""
+    import piv_b200 as P
+    O, fa, fb, cfg, ch, cw = _oracle_inputs(wl, a, b, crop)
+    ref, _, _ = O.analyze(cfg, fa, fb, mode=O.FP64)
+    r = an.analyze(an.prepare(np.ascontiguousarray(a[:ch, :cw]), P.RAW), an.prepare(np.ascontiguousarray(b[:ch, :cw]), P.RAW))
+    ok = (ref["flags"] == 0) & (r.field.flags == 0)
+    d = np.hypot(r.field.dx[ok] - ref["dx"][ok], r.field.dy[ok] - ref["dy"][ok])
+    return {"rms_px_vs_fp64": float(np.sqrt(np.mean(d * d))) if d.size else None,
+            "max_px_vs_fp64": float(d.max()) if d.size else None,
+            "flag_agreement": float(np.mean(ref["flags"] == r.field.flags)),
+            "sample": f"final field of a {ch}x{cw} crop ({ok.sum()} cells valid in both), FP64 oracle"}
 
 
 def run_profile_case(args, wl):
@@ -456,6 +488,8 @@ def main():
     ap.add_argument("--workload", default="c5", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--deform", type=int, choices=[0, 1], default=None,
+                    help="window deformation from the second pass on (default: the workload's setting)")
     ap.add_argument("--duration", type=float, default=None, help="serving workload: seconds of arrivals")
     ap.add_argument("--ref-step-s", type=float, default=3.0)
     ap.add_argument("--ref-crop", type=int, default=1024)
@@ -464,7 +498,10 @@ def main():
                          "window schedule (or 'all'), through the host API, untimed")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
-    wl = WORKLOADS[args.workload]
+    wl = dict(WORKLOADS[args.workload])
+    if args.deform is not None:
+        wl["deform"] = bool(args.deform)
+        wl["name"] = wl["name"] + (", deformed windows" if args.deform else ", uniform windows")
     if args.profile_case:
         return run_profile_case(args, wl)
     if args.impl == "reference":
@@ -640,7 +677,8 @@ def main():
                     "ms_per_step": float(ms2_t.item()) / e2e_steps, "wall_ms_per_step": 1e3 * t_wall / e2e_steps},
             "gpu_launches": int(launches), "roofline": roof, "clocks": clocks, "autotuned_variants": tuned}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(wl, a0, b0)
+        line["cpu_baseline"] = cpu_baseline(wl, a0, b0, single_s=4.0)
+        line["accuracy"] = accuracy_vs_fp64(wl, a0, b0, an)
     if rank == 0:
         print(json.dumps(line), flush=True)
     an.close()

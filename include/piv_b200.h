@@ -71,6 +71,9 @@ typedef struct {
     float median_eps;
     int32_t replace;
     int32_t device;         /* CUDA device ordinal; -1 = current device */
+    int32_t deform;         /* 0: windows shift uniformly (the reference, multipass.rs:224-231);
+                             * 1: from the second pass on, windows deform with the predictor
+                             * (see piv_correlate_deform) */
 } PivConfigC;
 
 /* PreprocessConfig (preprocess.rs:5-29) plus the percentile clip of integer codes
@@ -283,6 +286,25 @@ int32_t piv_place_windows(PivAnalyzer* an, int64_t height, int64_t width, const 
 int32_t piv_correlate_origins(PivAnalyzer* an, const PivFrame* a, const PivFrame* b, int64_t window,
                               const float* origins, int64_t ncells, float* dx, float* dy, float* peak_ratio,
                               uint8_t* flags);
+/* Window deformation (no counterpart in the reference, whose windows only shift,
+ * multipass.rs:224-231; deformation is listed as deferred in docs/phase1-plan.md:104,248).
+ * A deformed window's base position (x0, y0) is its zero-shift origin under the placement clamp
+ * (multipass.rs:207-208): the grid origin clamped to [0, W - n - 1] x [0, H - n - 1].
+ * piv_place_windows_deform: as piv_place_windows, plus the predictor (field.rs:56-81 sampling) at
+ * the four corner pixels of each window's base position (x0, y0), (x0+n-1, y0), (x0, y0+n-1),
+ * (x0+n-1, y0+n-1): corners[8k..8k+7] = dx00, dy00, dx10, dy10, dx01, dy01, dx11, dy11 (zero
+ * without a predictor).
+ * piv_correlate_deform: correlates the deformed windows of `grid`: pixel (r, c) of the window at
+ * base position (x0, y0) is displaced by D, the bilinear blend of the corners at u = c/(n-1),
+ * v = r/(n-1); window A samples frame A at (x0+c, y0+r) - D/2 and window B frame B at + D/2
+ * (bilinear, clamped to the image). The signal mask uses `origins` (4 floats per cell, as
+ * piv_place_windows returns them); the vector is D(centre) + peak. */
+int32_t piv_place_windows_deform(PivAnalyzer* an, int64_t height, int64_t width, const PivGridC* grid,
+                                 const PivGridC* pred_grid, const float* pred_dx, const float* pred_dy, float* origins,
+                                 float* corners);
+int32_t piv_correlate_deform(PivAnalyzer* an, const PivFrame* a, const PivFrame* b, const PivGridC* grid,
+                             const float* origins, const float* corners, float* dx, float* dy, float* peak_ratio,
+                             uint8_t* flags);
 /* validate (validate.rs:51-130) of a raw field with the analyzer's thresholds and
  * max_displacement = windows[0] / 2. Outputs validated dx, dy, flags. */
 int32_t piv_validate_field(PivAnalyzer* an, int64_t ny, int64_t nx, const float* dx, const float* dy,

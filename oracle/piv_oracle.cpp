@@ -597,6 +597,12 @@ void sample_pred(const OrcGrid* pg, const float* pdx, const float* pdy, float x,
 }
 
 // Deformed-window helpers (see piv_oracle.h).
+// Base position of a deformed window: its zero-shift origin under the placement clamp
+// (multipass.rs:207-208, 224-231 with shift 0), i.e. the grid origin clamped to w - n - 1.
+int64_t deform_base(int64_t origin, int64_t extent, int64_t n) {
+    return std::min(std::max<int64_t>(origin, 0), std::max<int64_t>(extent - n - 1, 0));
+}
+
 template <class T>
 T blend(const float* c, int k, T u, T v) {
     const T w00 = ((T)1 - u) * ((T)1 - v), w10 = u * ((T)1 - v), w01 = ((T)1 - u) * v, w11 = u * v;
@@ -731,7 +737,8 @@ void orc_place_deform(const OrcGrid* g, int64_t h, int64_t w, const OrcGrid* pg,
     for (int64_t iy = 0; iy < g->ny; ++iy)
         for (int64_t ix = 0; ix < g->nx; ++ix) {
             float* c = corners + 8 * (iy * g->nx + ix);
-            const float x0 = (float)(g->x0 + ix * g->step), y0 = (float)(g->y0 + iy * g->step);
+            const float x0 = (float)deform_base(g->x0 + ix * g->step, w, n);
+            const float y0 = (float)deform_base(g->y0 + iy * g->step, h, n);
             const float xs[4] = {x0, x0 + (float)(n - 1), x0, x0 + (float)(n - 1)};
             const float ys[4] = {y0, y0, y0 + (float)(n - 1), y0 + (float)(n - 1)};
             for (int j = 0; j < 4; ++j) {
@@ -757,7 +764,8 @@ void orc_correlate_pass_deform(const float* image_a, const float* image_b, const
         for (int64_t k = 0; k < ncells; ++k) {
             const float* o = origins + 4 * k;
             const float* c = corners + 8 * k;
-            const int64_t x0 = g->x0 + (k % g->nx) * g->step, y0 = g->y0 + (k / g->nx) * g->step;
+            const int64_t x0 = deform_base(g->x0 + (k % g->nx) * g->step, w, n);
+            const int64_t y0 = deform_base(g->y0 + (k / g->nx) * g->step, h, n);
             auto has_signal = [&](const Integral& s, float x, float y) {
                 float mean, sd;
                 s.stats((int64_t)std::round(x), (int64_t)std::round(y), n, n, &mean, &sd);

@@ -102,11 +102,14 @@ int orc_correlation_plane(const float* a, int64_t ha, int64_t wa, float ax, floa
  * deformation is deferred in docs/phase1-plan.md:104,248). Parity of these is unpinned against the
  * reference and pinned against this restatement only.
  *
+ * A deformed window's base position (x0, y0) is its zero-shift origin under the placement clamp
+ * (multipass.rs:207-208): the grid origin clamped to [0, w - n - 1] x [0, h - n - 1].
+ *
  * orc_place_deform: as orc_place, plus the predictor (field.rs:56-81 sampling) at the four corner
- * pixels of each window's grid position (x0, y0), (x0+n-1, y0), (x0, y0+n-1), (x0+n-1, y0+n-1):
+ * pixels of each window's base position (x0, y0), (x0+n-1, y0), (x0, y0+n-1), (x0+n-1, y0+n-1):
  * corners[8k..8k+7] = dx00, dy00, dx10, dy10, dx01, dy01, dx11, dy11. Without a predictor all zero.
  *
- * orc_correlate_pass_deform: every pixel (r, c) of the window at grid position (x0, y0) is
+ * orc_correlate_pass_deform: every pixel (r, c) of the window at base position (x0, y0) is
  * displaced by the bilinear blend of the corners, D = (1-u)(1-v) D00 + u(1-v) D10 + (1-u)v D01
  * + uv D11 with u = c/(n-1), v = r/(n-1) (f32, left to right); window A samples frame A at
  * (x0+c, y0+r) - D/2 and window B frame B at + D/2, bilinearly with coordinates clamped to the

@@ -92,6 +92,9 @@ class PivConfig:
     final_iterations: int = 2
     mask: MaskConfig = dc_field(default_factory=MaskConfig)
     validation: ValidationConfig = dc_field(default_factory=ValidationConfig)
+    # False: windows shift uniformly (the reference). True: from the second pass on, each window
+    # is deformed by the bilinear blend of the predictor at its four corner pixels.
+    deform: bool = False
 
     def passes(self):
         return list(self.windows) + [self.windows[-1]] * (self.final_iterations - 1)
@@ -101,7 +104,8 @@ class PivConfig:
         c = _lib.PivConfigC(w, len(self.windows), float(self.overlap), int(self.final_iterations),
                             float(self.mask.min_mean), float(self.mask.min_std),
                             float(self.validation.ppr_threshold), float(self.validation.median_threshold),
-                            float(self.validation.median_eps), int(bool(self.validation.replace)), int(device))
+                            float(self.validation.median_eps), int(bool(self.validation.replace)), int(device),
+                            int(bool(self.deform)))
         c._keep = w
         return c
 
@@ -411,6 +415,38 @@ class PivAnalyzer:
         fl = np.empty(c, np.uint8)
         _check(_lib.load().piv_correlate_origins(self._h, a._h, b._h, int(window), _ptr(origins), c, _ptr(dx), _ptr(dy),
                                                  _ptr(ppr), _ptr(fl)))
+        return dx, dy, ppr, fl
+
+    def place_windows_deform(self, height, width, grid: Grid, predictor: Optional[VectorField] = None):
+        """Origins [cells, 4] and the predictor at each window's corner pixels [cells, 8]
+        (dx00, dy00, dx10, dy10, dx01, dy01, dx11, dy11)."""
+        out = np.empty((len(grid), 4), np.float32)
+        corners = np.empty((len(grid), 8), np.float32)
+        gc = grid._c()
+        if predictor is None:
+            _check(_lib.load().piv_place_windows_deform(self._h, int(height), int(width), ctypes.byref(gc), None, None,
+                                                        None, _ptr(out), _ptr(corners)))
+        else:
+            pg = predictor.grid._c()
+            pdx = np.ascontiguousarray(predictor.dx, np.float32)
+            pdy = np.ascontiguousarray(predictor.dy, np.float32)
+            _check(_lib.load().piv_place_windows_deform(self._h, int(height), int(width), ctypes.byref(gc),
+                                                        ctypes.byref(pg), _ptr(pdx), _ptr(pdy), _ptr(out),
+                                                        _ptr(corners)))
+        return out, corners
+
+    def correlate_deform(self, a: PreparedFrame, b: PreparedFrame, grid: Grid, origins, corners):
+        """Raw field of the deformed windows of `grid` (mask on `origins`): dx, dy, ppr, flags."""
+        origins = np.ascontiguousarray(origins, np.float32).reshape(-1, 4)
+        corners = np.ascontiguousarray(corners, np.float32).reshape(-1, 8)
+        c = len(grid)
+        if origins.shape[0] != c or corners.shape[0] != c:
+            raise PivError("origins and corners need one row per grid cell")
+        dx, dy, ppr = (np.empty(c, np.float32) for _ in range(3))
+        fl = np.empty(c, np.uint8)
+        gc = grid._c()
+        _check(_lib.load().piv_correlate_deform(self._h, a._h, b._h, ctypes.byref(gc), _ptr(origins), _ptr(corners),
+                                                _ptr(dx), _ptr(dy), _ptr(ppr), _ptr(fl)))
         return dx, dy, ppr, fl
 
     def validate_field(self, dx, dy, peak_ratio, fl):

@@ -84,6 +84,7 @@ struct PassBuf {
     float* dx;
     float* dy;
     uint8_t* flags;
+    float4* corners;  // deformed windows: predictor at the 4 corner pixels (2 float4 per cell)
 };
 
 std::mutex g_init_mu;
@@ -107,6 +108,7 @@ struct PivAnalyzer {
     float min_mean = 0.0f, min_std = 0.0f;
     float ppr_threshold = 1.3f, median_threshold = 2.0f, median_eps = 0.1f;
     int32_t replace = 1;
+    int32_t deform = 0;
     int device = 0;
     cudaStream_t own = nullptr;
     cudaStream_t cur = nullptr;
@@ -122,8 +124,8 @@ struct PivAnalyzer {
     std::vector<std::vector<std::pair<cudaEvent_t, cudaEvent_t>>> pending;
     std::vector<cudaEvent_t> spare;
 
-    // correlation launch variant chosen per window size (0 until autotuned)
-    int variant[129] = {};
+    // correlation launch variant chosen per window size (0 until autotuned), uniform / deformed
+    int variant[2][129] = {};
 
     bool mask_trivial() const { return min_mean <= 0.0f && min_std <= 0.0f; }
     std::vector<int32_t> pass_windows() const {
@@ -186,6 +188,7 @@ int check_cfg(const PivConfigC* c) {
             return fail(PIV_ERR_CONFIG, "window size %d must be even and >= 8", c->windows[i]);
     if (!(c->overlap >= 0.0f && c->overlap < 1.0f)) return fail(PIV_ERR_CONFIG, "overlap %g must be in [0, 1)", c->overlap);
     if (c->final_iterations < 1) return fail(PIV_ERR_CONFIG, "final_iterations must be at least 1");
+    if (c->deform != 0 && c->deform != 1) return fail(PIV_ERR_CONFIG, "deform must be 0 or 1");
     for (int i = 0; i < c->n_windows; ++i)
         if (!corr_supported(c->windows[i]))
             return fail(PIV_ERR_UNSUPPORTED, "window size %d is not supported on the GPU (8, 12, 16, 24, 32, 48, 64, 96, 128)",
@@ -218,7 +221,8 @@ int ensure_workspace(PivAnalyzer* an, int64_t H, int64_t W, int K) {
         pb.cells = pb.grid.nx * pb.grid.ny;
         if (pb.cells > (int64_t)1 << 30) return fail(PIV_ERR_UNSUPPORTED, "too many windows in one pass");
         const size_t c = (size_t)pb.cells;
-        per_pair += align256(16 * c) + align256(c) + 3 * align256(4 * c) + 3 * align256(c) + 2 * align256(4 * c) + align256(c);
+        per_pair += align256(16 * c) + align256(c) + 3 * align256(4 * c) + 3 * align256(c) + 2 * align256(4 * c) + align256(c) +
+                    (an->deform ? align256(32 * c) : 0);
         proto.push_back(pb);
     }
     const size_t total = align256(sizeof(unsigned long long) * 8 * (size_t)K) + per_pair * (size_t)K;
@@ -245,6 +249,7 @@ int ensure_workspace(PivAnalyzer* an, int64_t H, int64_t W, int K) {
             pb.dx = (float*)take(4 * c);
             pb.dy = (float*)take(4 * c);
             pb.flags = (uint8_t*)take(c);
+            pb.corners = an->deform ? (float4*)take(32 * c) : nullptr;
         }
         an->pairs.push_back(passes);
     }
@@ -310,6 +315,8 @@ int run_passes(PivAnalyzer* an, const PivFrame* const* a, const PivFrame* const*
             }
             pp.origins = pb.origins;
             pp.status = pb.status;
+            // Deformed windows need a predictor; the first pass is the uniform placement.
+            pp.corners = (an->deform && i > 0) ? pb.corners : nullptr;
             pp.use_stats = use_stats[k];
             if (use_stats[k]) {
                 pp.sa = stats_of(a[k]);
@@ -318,7 +325,8 @@ int run_passes(PivAnalyzer* an, const PivFrame* const* a, const PivFrame* const*
             pp.min_mean = an->min_mean;
             pp.min_std = an->min_std;
             cps[k] = CorrParams{a[k]->image, b[k]->image, (int)H, (int)W, pb.origins, pb.status, (int)pb.cells,
-                                pb.raw_dx, pb.raw_dy, pb.raw_ppr, pb.raw_flags};
+                                pb.raw_dx, pb.raw_dy, pb.raw_ppr, pb.raw_flags, pp.corners, (int)pb.grid.x0,
+                                (int)pb.grid.y0, (int)pb.grid.step, (int)pb.grid.nx};
             vps[k] = ValidateParams{(int)pb.grid.nx, (int)pb.grid.ny, pb.raw_dx, pb.raw_dy, pb.raw_ppr, pb.raw_flags,
                                     pb.f1, pb.f2, pb.dx, pb.dy, pb.flags, (float)an->windows[0] / 2.0f,
                                     an->ppr_threshold, an->median_threshold, an->median_eps, an->replace};
@@ -338,6 +346,7 @@ int run_passes(PivAnalyzer* an, const PivFrame* const* a, const PivFrame* const*
             CUDA_TRY(cudaEventRecord(ev0, an->cur));
         }
         const int nwin = (int)an->pairs[0][i].grid.window;
+        const int kind = cps[0].corners ? 1 : 0;
         if (tune) {
             // Time every launch variant of this window size on this pass's data (all compute the
             // same results) and keep the fastest for later calls.
@@ -346,7 +355,7 @@ int run_passes(PivAnalyzer* an, const PivFrame* const* a, const PivFrame* const*
             CUDA_TRY(cudaEventCreate(&t1));
             float best = 1e30f;
             int best_v = 0;
-            for (int v = 0; v < corr_num_variants(nwin); ++v) {
+            for (int v = 0; v < corr_num_variants(nwin, kind); ++v) {
                 CUDA_TRY(launch_correlate_items(nwin, v, cps.data(), K, an->cur, &nl));
                 CUDA_TRY(cudaEventRecord(t0, an->cur));
                 for (int r = 0; r < 3; ++r) CUDA_TRY(launch_correlate_items(nwin, v, cps.data(), K, an->cur, &nl));
@@ -361,9 +370,9 @@ int run_passes(PivAnalyzer* an, const PivFrame* const* a, const PivFrame* const*
             }
             cudaEventDestroy(t0);
             cudaEventDestroy(t1);
-            an->variant[nwin] = best_v;
+            an->variant[kind][nwin] = best_v;
         }
-        CUDA_TRY(launch_correlate_items(nwin, an->variant[nwin], cps.data(), K, an->cur, &nl));
+        CUDA_TRY(launch_correlate_items(nwin, an->variant[kind][nwin], cps.data(), K, an->cur, &nl));
         if (an->profiling) {
             CUDA_TRY(cudaEventRecord(ev1, an->cur));
             if (an->pending.size() < npass) an->pending.resize(npass);
@@ -524,6 +533,7 @@ int32_t piv_analyzer_create(const PivConfigC* cfg, PivAnalyzer** out) {
     an->median_threshold = cfg->median_threshold;
     an->median_eps = cfg->median_eps;
     an->replace = cfg->replace;
+    an->deform = cfg->deform;
     an->device = dev;
     cudaError_t e = cudaStreamCreateWithFlags(&an->own, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
@@ -595,7 +605,8 @@ int32_t piv_analyzer_autotune(PivAnalyzer* an, const PivFrame* a, const PivFrame
 int32_t piv_analyzer_variant(const PivAnalyzer* an, int32_t window, char* name, int32_t capacity) {
     if (!an || !name || capacity <= 0) return fail(PIV_ERR_ARGUMENT, "bad argument");
     if (!corr_supported(window)) return fail(PIV_ERR_UNSUPPORTED, "window size %d", window);
-    snprintf(name, (size_t)capacity, "%s", corr_variant_name(window, an->variant[window]));
+    const int kind = an->deform ? 1 : 0;
+    snprintf(name, (size_t)capacity, "%s", corr_variant_name(window, an->variant[kind][window], kind));
     return PIV_OK;
 }
 
@@ -808,15 +819,21 @@ int32_t piv_analyze_traced(PivAnalyzer* an, const PivFrame* a, const PivFrame* b
     return PIV_OK;
 }
 
-int32_t piv_place_windows(PivAnalyzer* an, int64_t height, int64_t width, const PivGridC* grid,
-                          const PivGridC* pred_grid, const float* pred_dx, const float* pred_dy, float* origins) {
+namespace {
+
+int place_windows(PivAnalyzer* an, int64_t height, int64_t width, const PivGridC* grid, const PivGridC* pred_grid,
+                  const float* pred_dx, const float* pred_dy, float* origins, float* corners) {
     if (!an || !grid || !origins) return fail(PIV_ERR_ARGUMENT, "null argument");
+    if (grid->nx <= 0 || grid->ny <= 0 || grid->window <= 0 || grid->step <= 0)
+        return fail(PIV_ERR_ARGUMENT, "empty grid");
+    if (pred_grid && (pred_grid->nx <= 0 || pred_grid->ny <= 0 || pred_grid->step <= 0))
+        return fail(PIV_ERR_ARGUMENT, "empty predictor grid");
     int st = use_device(an);
     if (st) return st;
     const size_t c = (size_t)(grid->nx * grid->ny);
     const size_t pc = pred_grid ? (size_t)(pred_grid->nx * pred_grid->ny) : 0;
     void* buf = nullptr;
-    CUDA_TRY(cudaMalloc(&buf, align256(16 * c) + align256(c) + 2 * align256(4 * pc + 4)));
+    CUDA_TRY(cudaMalloc(&buf, align256(16 * c) + align256(c) + 2 * align256(4 * pc + 4) + align256(32 * c)));
     char* p = (char*)buf;
     float4* d_org = (float4*)p;
     p += align256(16 * c);
@@ -825,6 +842,8 @@ int32_t piv_place_windows(PivAnalyzer* an, int64_t height, int64_t width, const 
     float* d_pdx = (float*)p;
     p += align256(4 * pc + 4);
     float* d_pdy = (float*)p;
+    p += align256(4 * pc + 4);
+    float4* d_corners = (float4*)p;
     PlaceParams pp{};
     pp.grid = to_gp(*grid);
     pp.H = (int)height;
@@ -840,14 +859,30 @@ int32_t piv_place_windows(PivAnalyzer* an, int64_t height, int64_t width, const 
     }
     pp.origins = d_org;
     pp.status = d_st;
+    pp.corners = corners ? d_corners : nullptr;
     pp.use_stats = 0;
     if (e == cudaSuccess) e = launch_place(pp, an->cur);
     an->launches += 1;
     if (e == cudaSuccess) e = cudaMemcpyAsync(origins, d_org, 16 * c, cudaMemcpyDeviceToHost, an->cur);
+    if (e == cudaSuccess && corners) e = cudaMemcpyAsync(corners, d_corners, 32 * c, cudaMemcpyDeviceToHost, an->cur);
     if (e == cudaSuccess) e = cudaStreamSynchronize(an->cur);
     cudaFree(buf);
     if (e != cudaSuccess) return fail(PIV_ERR_CUDA, "place: %s", cudaGetErrorString(e));
     return PIV_OK;
+}
+
+}  // namespace
+
+int32_t piv_place_windows(PivAnalyzer* an, int64_t height, int64_t width, const PivGridC* grid,
+                          const PivGridC* pred_grid, const float* pred_dx, const float* pred_dy, float* origins) {
+    return place_windows(an, height, width, grid, pred_grid, pred_dx, pred_dy, origins, nullptr);
+}
+
+int32_t piv_place_windows_deform(PivAnalyzer* an, int64_t height, int64_t width, const PivGridC* grid,
+                                 const PivGridC* pred_grid, const float* pred_dx, const float* pred_dy, float* origins,
+                                 float* corners) {
+    if (!corners) return fail(PIV_ERR_ARGUMENT, "null corners");
+    return place_windows(an, height, width, grid, pred_grid, pred_dx, pred_dy, origins, corners);
 }
 
 int32_t piv_correlate_origins(PivAnalyzer* an, const PivFrame* a, const PivFrame* b, int64_t window,
@@ -899,6 +934,76 @@ int32_t piv_correlate_origins(PivAnalyzer* an, const PivFrame* a, const PivFrame
     if (e == cudaSuccess) e = launch_mask(pp, d_org, (int)ncells, an->cur);
     CorrParams cp{a->image, b->image, (int)a->H, (int)a->W, d_org, d_st, (int)ncells, d_dx, d_dy, d_ppr, d_fl};
     if (e == cudaSuccess) e = launch_correlate((int)window, cp, an->cur);
+    an->launches += 2;
+    if (e == cudaSuccess && dx) e = cudaMemcpyAsync(dx, d_dx, 4 * c, cudaMemcpyDeviceToHost, an->cur);
+    if (e == cudaSuccess && dy) e = cudaMemcpyAsync(dy, d_dy, 4 * c, cudaMemcpyDeviceToHost, an->cur);
+    if (e == cudaSuccess && peak_ratio) e = cudaMemcpyAsync(peak_ratio, d_ppr, 4 * c, cudaMemcpyDeviceToHost, an->cur);
+    if (e == cudaSuccess && flags) e = cudaMemcpyAsync(flags, d_fl, c, cudaMemcpyDeviceToHost, an->cur);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(an->cur);
+    cudaFree(buf);
+    if (e != cudaSuccess) return fail(PIV_ERR_CUDA, "correlate: %s", cudaGetErrorString(e));
+    return PIV_OK;
+}
+
+int32_t piv_correlate_deform(PivAnalyzer* an, const PivFrame* a, const PivFrame* b, const PivGridC* grid,
+                             const float* origins, const float* corners, float* dx, float* dy, float* peak_ratio,
+                             uint8_t* flags) {
+    if (!an || !a || !b || !grid || !origins || !corners) return fail(PIV_ERR_ARGUMENT, "bad argument");
+    if (a->H != b->H || a->W != b->W) return fail(PIV_ERR_SHAPE_MISMATCH, "frames have different shapes");
+    const int64_t window = grid->window;
+    if (!corr_supported((int)window)) return fail(PIV_ERR_UNSUPPORTED, "window size %lld", (long long)window);
+    if (grid->nx <= 0 || grid->ny <= 0 || grid->step <= 0 || grid->x0 < 0 || grid->y0 < 0 ||
+        grid->x0 + (grid->nx - 1) * grid->step + window > a->W || grid->y0 + (grid->ny - 1) * grid->step + window > a->H)
+        return fail(PIV_ERR_ARGUMENT, "grid does not fit the image");
+    const int64_t ncells = grid->nx * grid->ny;
+    for (int64_t k = 0; k < ncells; ++k) {
+        for (int j = 0; j < 4; ++j) {
+            const float v = origins[4 * k + j];
+            const float lim = (float)((j % 2 == 0 ? a->W : a->H) - window);
+            if (!(v >= 0.0f && v <= lim)) return fail(PIV_ERR_ARGUMENT, "origin %lld out of the image", (long long)k);
+        }
+        for (int j = 0; j < 8; ++j)
+            if (!std::isfinite(corners[8 * k + j])) return fail(PIV_ERR_ARGUMENT, "corner %lld not finite", (long long)k);
+    }
+    int st = use_device(an);
+    if (st) return st;
+    const bool use_stats = needs_stats(an, a) || needs_stats(an, b);
+    if (use_stats && !(a->stats_valid && b->stats_valid)) return fail(PIV_ERR_ARGUMENT, "frame statistics missing");
+    const size_t c = (size_t)ncells;
+    void* buf = nullptr;
+    CUDA_TRY(cudaMalloc(&buf, align256(16 * c) + align256(32 * c) + align256(c) + 3 * align256(4 * c) + align256(c) + 256));
+    char* p = (char*)buf;
+    float4* d_org = (float4*)p;
+    p += align256(16 * c);
+    float4* d_cor = (float4*)p;
+    p += align256(32 * c);
+    uint8_t* d_st = (uint8_t*)p;
+    p += align256(c);
+    float* d_dx = (float*)p;
+    p += align256(4 * c);
+    float* d_dy = (float*)p;
+    p += align256(4 * c);
+    float* d_ppr = (float*)p;
+    p += align256(4 * c);
+    uint8_t* d_fl = (uint8_t*)p;
+    cudaError_t e = cudaMemcpyAsync(d_org, origins, 16 * c, cudaMemcpyHostToDevice, an->cur);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_cor, corners, 32 * c, cudaMemcpyHostToDevice, an->cur);
+    PlaceParams pp{};
+    pp.grid.window = (int)window;
+    pp.H = (int)a->H;
+    pp.W = (int)a->W;
+    pp.status = d_st;
+    pp.use_stats = use_stats;
+    if (use_stats) {
+        pp.sa = stats_of(a);
+        pp.sb = stats_of(b);
+    }
+    pp.min_mean = an->min_mean;
+    pp.min_std = an->min_std;
+    if (e == cudaSuccess) e = launch_mask(pp, d_org, (int)ncells, an->cur);
+    CorrParams cp{a->image, b->image, (int)a->H, (int)a->W, d_org, d_st, (int)ncells, d_dx, d_dy, d_ppr, d_fl,
+                  d_cor, (int)grid->x0, (int)grid->y0, (int)grid->step, (int)grid->nx};
+    if (e == cudaSuccess) e = launch_correlate_items((int)window, an->variant[1][window], &cp, 1, an->cur, nullptr);
     an->launches += 2;
     if (e == cudaSuccess && dx) e = cudaMemcpyAsync(dx, d_dx, 4 * c, cudaMemcpyDeviceToHost, an->cur);
     if (e == cudaSuccess && dy) e = cudaMemcpyAsync(dy, d_dy, 4 * c, cudaMemcpyDeviceToHost, an->cur);
@@ -1030,8 +1135,10 @@ int32_t piv_batch_create(const PivAnalyzer* parent, int64_t height, int64_t widt
     an->median_threshold = parent->median_threshold;
     an->median_eps = parent->median_eps;
     an->replace = parent->replace;
+    an->deform = parent->deform;
     an->device = parent->device;
-    for (int i = 0; i < 129; ++i) an->variant[i] = parent->variant[i];
+    for (int k = 0; k < 2; ++k)
+        for (int i = 0; i < 129; ++i) an->variant[k][i] = parent->variant[k][i];
     bt->an = an;
     bt->H = height;
     bt->W = width;
@@ -1228,7 +1335,8 @@ size_t request_bytes(const Request& r, bool stats, bool chain, bool both, size_t
     b += 2 * align256(4 * (4 + 512 + 4)) + 2 * align256(8);
     for (const PassBuf& pb : r.passes) {
         const size_t c = (size_t)pb.cells;
-        b += align256(16 * c) + align256(c) + 3 * align256(4 * c) + 3 * align256(c) + 2 * align256(4 * c) + align256(c);
+        b += align256(16 * c) + align256(c) + 3 * align256(4 * c) + 3 * align256(c) + 2 * align256(4 * c) + align256(c) +
+             (r.cfg.deform ? align256(32 * c) : 0);
     }
     return b + align256(8 * sizeof(unsigned long long));
 }
@@ -1250,7 +1358,7 @@ struct PivServer {
     std::thread worker;
     int64_t in_use = 0;
     PivServerStatsC stats{};
-    int variant[129] = {};
+    int variant[2][129] = {};
     std::vector<cudaEvent_t> step_events;  // completion of recent steps (bounded run-ahead)
 
     void loop();
@@ -1306,6 +1414,7 @@ int admit_request(PivServer* sv, Request* r) {
         pb.dx = (float*)take(4 * c);
         pb.dy = (float*)take(4 * c);
         pb.flags = (uint8_t*)take(c);
+        pb.corners = r->cfg.deform ? (float4*)take(32 * c) : nullptr;
     }
     r->d_counts = (unsigned long long*)take(8 * sizeof(unsigned long long));
     r->cfg.cur = sv->stream;
@@ -1330,10 +1439,11 @@ bool PivServer::admit_locked(Request* r, std::string* err) {
 // One step: the next pass of every admitted request (multipass.rs:194-259 and validate.rs:51),
 // batched across requests: one placement launch, one correlation launch per window size, one
 // validation chain; requests whose last pass this is get their summary and their results copied
-// to host memory, followed by a completion event.
+// to host memory, followed by a completion event. Correlation launches are keyed by window size
+// and window kind (uniform shift / deformed).
 void PivServer::launch_step(std::vector<Request*>& work) {
     std::vector<PlaceParams> pps;
-    std::map<int, std::vector<CorrParams>> cps;
+    std::map<std::pair<int, int>, std::vector<CorrParams>> cps;
     std::vector<ValidateParams> vps;
     for (Request* r : work) {
         const int i = r->next_pass;
@@ -1350,6 +1460,7 @@ void PivServer::launch_step(std::vector<Request*>& work) {
         }
         pp.origins = pb.origins;
         pp.status = pb.status;
+        pp.corners = (r->cfg.deform && i > 0) ? pb.corners : nullptr;
         pp.use_stats = r->use_stats;
         if (r->use_stats) {
             pp.sa = stats_of(&r->fa);
@@ -1358,8 +1469,10 @@ void PivServer::launch_step(std::vector<Request*>& work) {
         pp.min_mean = r->cfg.min_mean;
         pp.min_std = r->cfg.min_std;
         pps.push_back(pp);
-        cps[(int)pb.grid.window].push_back(CorrParams{r->fa.image, r->fb.image, (int)r->H, (int)r->W, pb.origins, pb.status,
-                                                      (int)pb.cells, pb.raw_dx, pb.raw_dy, pb.raw_ppr, pb.raw_flags});
+        cps[{(int)pb.grid.window, pp.corners ? 1 : 0}].push_back(
+            CorrParams{r->fa.image, r->fb.image, (int)r->H, (int)r->W, pb.origins, pb.status, (int)pb.cells, pb.raw_dx,
+                       pb.raw_dy, pb.raw_ppr, pb.raw_flags, pp.corners, (int)pb.grid.x0, (int)pb.grid.y0,
+                       (int)pb.grid.step, (int)pb.grid.nx});
         vps.push_back(ValidateParams{(int)pb.grid.nx, (int)pb.grid.ny, pb.raw_dx, pb.raw_dy, pb.raw_ppr, pb.raw_flags, pb.f1,
                                      pb.f2, pb.dx, pb.dy, pb.flags, (float)r->cfg.windows[0] / 2.0f, r->cfg.ppr_threshold,
                                      r->cfg.median_threshold, r->cfg.median_eps, r->cfg.replace});
@@ -1367,8 +1480,9 @@ void PivServer::launch_step(std::vector<Request*>& work) {
     int nl = 0;
     cudaError_t e = launch_place_items(pps.data(), (int)pps.size(), stream, &nl);
     for (auto& kv : cps)
-        if (e == cudaSuccess) e = launch_correlate_items(kv.first, variant[kv.first], kv.second.data(), (int)kv.second.size(),
-                                                         stream, &nl);
+        if (e == cudaSuccess)
+            e = launch_correlate_items(kv.first.first, variant[kv.first.second][kv.first.first], kv.second.data(),
+                                       (int)kv.second.size(), stream, &nl);
     if (e == cudaSuccess) e = launch_validate_items(vps.data(), (int)vps.size(), stream, &nl);
     std::vector<SummaryItem> sums;
     for (Request* r : work) {
@@ -1570,6 +1684,7 @@ int32_t piv_server_submit(PivServer* sv, const PivRequestC* q, uint64_t* id) {
     c.median_threshold = q->config.median_threshold;
     c.median_eps = q->config.median_eps;
     c.replace = q->config.replace;
+    c.deform = q->config.deform;
     c.device = sv->device;
     r->pre = q->preprocess;
     r->dtype = q->dtype;

@@ -34,10 +34,10 @@ namespace pivb200 {
 // single windows, groups per CTA G, minimum resident CTAs per SM (register cap), sampler.
 // G and MINB only change the launch geometry, never the arithmetic; N, T and PAIR fix the FFT
 // decomposition and therefore the rounding of the results.
-template <int N_, int T_, bool PAIR_, int G_, int MINB_, bool SHFL_ = false>
+template <int N_, int T_, bool PAIR_, int G_, int MINB_, bool SHFL_ = false, bool DEFORM_ = false>
 struct CorrCfg {
     static constexpr int N = N_, T = T_, G = G_, MINB = MINB_;
-    static constexpr bool PAIR = PAIR_, SHFL_SAMPLE = SHFL_;
+    static constexpr bool PAIR = PAIR_, SHFL_SAMPLE = SHFL_, DEFORM = DEFORM_;
     static constexpr int P = N / T;
     static constexpr int NT = N * T;
     static constexpr int THREADS = G * NT;
@@ -62,7 +62,8 @@ struct CorrCfg {
     __host__ __device__ static constexpr int B(int ky, int kx) {
         return T == 1 ? ky * LD + kx : ky * LD + (ky / P) * Q + kx + kx / P;
     }
-    static constexpr size_t SMEM = (size_t)G * (PLANE0 + PLANE1) + sizeof(float2) * N + sizeof(float) * (size_t)G * NSEG * 4 + 64;
+    static constexpr size_t SMEM = (size_t)G * (PLANE0 + PLANE1) + sizeof(float2) * N + sizeof(float) * (size_t)G * NSEG * 4 +
+                                   (DEFORM ? sizeof(float) * N : 0) + 64;
 };
 
 // ---------------------------------------------------------------------------------------------
@@ -256,6 +257,62 @@ __device__ __forceinline__ void sample_column(const float* __restrict__ img, int
     }
 }
 
+// ---------------------------------------------------------------------------------------------
+// Deformed windows (no counterpart in the reference, whose windows only shift): pixel (r, c) of
+// the window at base position (x0, y0) (the grid origin under the placement clamp to W - n - 1,
+// as a zero shift is placed by multipass.rs:207-231) is displaced by the bilinear blend D of the predictor at
+// the window's four corner pixels, with u = c/(n-1), v = r/(n-1):
+//   D = (1-u)(1-v) D00 + u(1-v) D10 + (1-u)v D01 + uv D11      (f32, summed left to right)
+// frame A is sampled at (x0+c, y0+r) - D/2 and frame B at + D/2, bilinearly, coordinates
+// clamped into the image and the tap clamped to the last full cell. Every operation is a
+// round-to-nearest intrinsic in that order, so the samples are bit-identical to a sequential f32
+// evaluation. Both frames' samples of one pixel share D: lane (x, t) fills z[p] = (A, B) at
+// column x, row t + T*p.
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ float corner_blend(float c00, float c10, float c01, float c11, float u, float v) {
+    const float ou = __fsub_rn(1.0f, u), ov = __fsub_rn(1.0f, v);
+    float d = __fmul_rn(__fmul_rn(ou, ov), c00);
+    d = __fadd_rn(d, __fmul_rn(__fmul_rn(u, ov), c10));
+    d = __fadd_rn(d, __fmul_rn(__fmul_rn(ou, v), c01));
+    return __fadd_rn(d, __fmul_rn(__fmul_rn(u, v), c11));
+}
+
+__device__ __forceinline__ float bilinear_clamped(const float* __restrict__ img, int H, int W, float px, float py) {
+    px = px < 0.0f ? 0.0f : px;
+    px = (float)(W - 1) < px ? (float)(W - 1) : px;
+    py = py < 0.0f ? 0.0f : py;
+    py = (float)(H - 1) < py ? (float)(H - 1) : py;
+    const int ix = min((int)floorf(px), max(W - 2, 0)), iy = min((int)floorf(py), max(H - 2, 0));
+    const float tx = __fsub_rn(px, (float)ix), ty = __fsub_rn(py, (float)iy);
+    const int ix1 = min(ix + 1, W - 1), iy1 = min(iy + 1, H - 1);
+    const float ux = __fsub_rn(1.0f, tx), uy = __fsub_rn(1.0f, ty);
+    const float* top = img + (size_t)iy * W;
+    const float* bot = img + (size_t)iy1 * W;
+    float s = __fmul_rn(__fmul_rn(ux, uy), __ldg(top + ix));
+    s = __fadd_rn(s, __fmul_rn(__fmul_rn(tx, uy), __ldg(top + ix1)));
+    s = __fadd_rn(s, __fmul_rn(__fmul_rn(ux, ty), __ldg(bot + ix)));
+    return __fadd_rn(s, __fmul_rn(__fmul_rn(tx, ty), __ldg(bot + ix1)));
+}
+
+template <int N, int T>
+__device__ __forceinline__ void sample_deformed(const float* __restrict__ img_a, const float* __restrict__ img_b, int H,
+                                                int W, int x0, int y0, float4 k0, float4 k1, int x, int t,
+                                                const float* s_ramp, float2 (&z)[N / T]) {
+    constexpr int P = N / T;
+    const float u = s_ramp[x];
+    const float xf = (float)(x0 + x);
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+        const int r = t + T * p;
+        const float v = s_ramp[r];
+        const float hx = __fmul_rn(0.5f, corner_blend(k0.x, k0.z, k1.x, k1.z, u, v));
+        const float hy = __fmul_rn(0.5f, corner_blend(k0.y, k0.w, k1.y, k1.w, u, v));
+        const float yf = (float)(y0 + r);
+        z[p].x = bilinear_clamped(img_a, H, W, __fsub_rn(xf, hx), __fsub_rn(yf, hy));
+        z[p].y = bilinear_clamped(img_b, H, W, __fadd_rn(xf, hx), __fadd_rn(yf, hy));
+    }
+}
+
 // 3-point Gaussian sub-pixel offset, parabolic when a value is not positive (correlate.rs:269-281).
 __device__ __forceinline__ float subpixel(float m, float c, float p) {
     float d;
@@ -296,13 +353,17 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB) correlate_kernel(const __
     char* plane1_raw = sbase + (size_t)g * (C::PLANE0 + C::PLANE1) + C::PLANE0;
     float2* s_roots = reinterpret_cast<float2*>(sbase + (size_t)G * (C::PLANE0 + C::PLANE1));
     float* s_red = reinterpret_cast<float*>(s_roots + N);
+    float* s_ramp = s_red + G * C::NSEG * 4;  // c / (N - 1) for c < N (deformed windows only)
     __shared__ int s_hw[G][8];
 
-    for (int i = tid; i < N; i += C::THREADS) s_roots[i] = c_roots[root_off(N) + i];
+    for (int i = tid; i < N; i += C::THREADS) {
+        s_roots[i] = c_roots[root_off(N) + i];
+        if constexpr (C::DEFORM) s_ramp[i] = __fdiv_rn((float)i, (float)(N - 1));
+    }
     __syncthreads();
 
     const long long base_cell = ((long long)block * G + g) * WPG;
-    float4 org[WPG];
+    float4 org[WPG];  // uniform shift: origins; deformed: (D(centre).x, D(centre).y, -, -)
     bool ok[WPG];
     float scale[WPG];
     float2 z0[P];
@@ -313,10 +374,29 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB) correlate_kernel(const __
     for (int wi = 0; wi < WPG; ++wi) {
         const long long cell = base_cell + wi;
         const bool active = cell < prm.ncells;
-        org[wi] = active ? prm.origins[cell] : make_float4(0.f, 0.f, 0.f, 0.f);
+        if constexpr (!C::DEFORM) org[wi] = active ? prm.origins[cell] : make_float4(0.f, 0.f, 0.f, 0.f);
         ok[wi] = active && prm.status[cell] != 0;
     }
-    if constexpr (C::SHFL_SAMPLE) {
+    if constexpr (C::DEFORM) {
+#pragma unroll
+        for (int wi = 0; wi < WPG; ++wi) {
+            const long long cell = base_cell + wi;
+            const bool active = cell < prm.ncells;
+            const int ci = active ? (int)cell : 0;
+            const float4 k0 = active ? prm.corners[2 * (size_t)ci] : make_float4(0.f, 0.f, 0.f, 0.f);
+            const float4 k1 = active ? prm.corners[2 * (size_t)ci + 1] : make_float4(0.f, 0.f, 0.f, 0.f);
+            // base position: the grid origin under the placement clamp (multipass.rs:207-208)
+            const int gx = min(prm.gx0 + (ci % prm.gnx) * prm.gstep, max(prm.W - N - 1, 0));
+            const int gy = min(prm.gy0 + (ci / prm.gnx) * prm.gstep, max(prm.H - N - 1, 0));
+            org[wi] = make_float4(corner_blend(k0.x, k0.z, k1.x, k1.z, 0.5f, 0.5f),
+                                  corner_blend(k0.y, k0.w, k1.y, k1.w, 0.5f, 0.5f), 0.f, 0.f);
+            if (wi == 0) {
+                sample_deformed<N, T>(prm.img_a, prm.img_b, prm.H, prm.W, gx, gy, k0, k1, line, t, s_ramp, z0);
+            } else if constexpr (PAIR) {
+                sample_deformed<N, T>(prm.img_a, prm.img_b, prm.H, prm.W, gx, gy, k0, k1, line, t, s_ramp, z1);
+            }
+        }
+    } else if constexpr (C::SHFL_SAMPLE) {
         sample_column<N, T, false>(prm.img_a, prm.H, prm.W, org[0].x, org[0].y, line, t, z0);
         sample_column<N, T, true>(prm.img_b, prm.H, prm.W, org[0].z, org[0].w, line, t, z0);
         if constexpr (PAIR) {
@@ -543,8 +623,13 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB) correlate_kernel(const __
                 const float wy = by >= N / 2 ? (float)by - (float)N : (float)by;
                 const float pdx = __fadd_rn(wx, sx), pdy = __fadd_rn(wy, sy);
                 const float ppr = sv > 0.0f ? fminf(__fdiv_rn(bv, sv), MAX_PPR) : MAX_PPR;
-                prm.raw_dx[cell] = __fadd_rn(__fsub_rn(o.z, o.x), pdx);
-                prm.raw_dy[cell] = __fadd_rn(__fsub_rn(o.w, o.y), pdy);
+                if constexpr (C::DEFORM) {
+                    prm.raw_dx[cell] = __fadd_rn(o.x, pdx);  // D(centre) + peak
+                    prm.raw_dy[cell] = __fadd_rn(o.y, pdy);
+                } else {
+                    prm.raw_dx[cell] = __fadd_rn(__fsub_rn(o.z, o.x), pdx);
+                    prm.raw_dy[cell] = __fadd_rn(__fsub_rn(o.w, o.y), pdy);
+                }
                 prm.raw_ppr[cell] = ppr;
                 prm.raw_flags[cell] = 0;
             } else {
@@ -613,23 +698,35 @@ static const CorrVariant kV64[] = {PIV_V(64, 4, true, 1, 2, true), PIV_V(64, 4, 
                                    PIV_V(64, 4, true, 1, 1, true)};
 static const CorrVariant kV96[] = {PIV_V(96, 4, true, 1, 1, true), PIV_V(96, 4, true, 1, 1, false)};
 static const CorrVariant kV128[] = {PIV_V(128, 4, false, 1, 1, false), PIV_V(128, 4, false, 1, 1, true)};
+// Deformed-window variants: the same FFT decomposition per size, the deformed sampler.
+#define PIV_D(N, T, PR, G, MB) {#N "/T" #T "/G" #G "/B" #MB "/deform", &launch_t<CorrCfg<N, T, PR, G, MB, false, true>>}
+static const CorrVariant kD8[] = {PIV_D(8, 1, true, 32, 1)};
+static const CorrVariant kD12[] = {PIV_D(12, 1, true, 16, 1)};
+static const CorrVariant kD16[] = {PIV_D(16, 1, true, 16, 2), PIV_D(16, 1, true, 8, 4)};
+static const CorrVariant kD24[] = {PIV_D(24, 2, true, 4, 2)};
+static const CorrVariant kD32[] = {PIV_D(32, 2, true, 4, 2), PIV_D(32, 2, true, 2, 4)};
+static const CorrVariant kD48[] = {PIV_D(48, 4, true, 1, 2)};
+static const CorrVariant kD64[] = {PIV_D(64, 4, true, 1, 2), PIV_D(64, 4, true, 1, 1)};
+static const CorrVariant kD96[] = {PIV_D(96, 4, true, 1, 1)};
+static const CorrVariant kD128[] = {PIV_D(128, 4, false, 1, 1)};
+#undef PIV_D
 #undef PIV_V
 
-static const CorrVariant* variants(int n, int* count) {
-#define PIV_CASE(N, A)                          \
-    case N:                                     \
-        *count = (int)(sizeof(A) / sizeof(A[0])); \
-        return A;
+static const CorrVariant* variants(int n, bool deform, int* count) {
+#define PIV_CASE(N, A, D)                                                       \
+    case N:                                                                     \
+        *count = deform ? (int)(sizeof(D) / sizeof(D[0])) : (int)(sizeof(A) / sizeof(A[0])); \
+        return deform ? D : A;
     switch (n) {
-        PIV_CASE(8, kV8)
-        PIV_CASE(12, kV12)
-        PIV_CASE(16, kV16)
-        PIV_CASE(24, kV24)
-        PIV_CASE(32, kV32)
-        PIV_CASE(48, kV48)
-        PIV_CASE(64, kV64)
-        PIV_CASE(96, kV96)
-        PIV_CASE(128, kV128)
+        PIV_CASE(8, kV8, kD8)
+        PIV_CASE(12, kV12, kD12)
+        PIV_CASE(16, kV16, kD16)
+        PIV_CASE(24, kV24, kD24)
+        PIV_CASE(32, kV32, kD32)
+        PIV_CASE(48, kV48, kD48)
+        PIV_CASE(64, kV64, kD64)
+        PIV_CASE(96, kV96, kD96)
+        PIV_CASE(128, kV128, kD128)
         default:
             *count = 0;
             return nullptr;
@@ -637,21 +734,28 @@ static const CorrVariant* variants(int n, int* count) {
 #undef PIV_CASE
 }
 
-int corr_num_variants(int n) {
+int corr_num_variants(int n, bool deform) {
     int c = 0;
-    variants(n, &c);
+    variants(n, deform, &c);
     return c;
 }
 
-const char* corr_variant_name(int n, int v) {
+const char* corr_variant_name(int n, int v, bool deform) {
     int c = 0;
-    const CorrVariant* vs = variants(n, &c);
+    const CorrVariant* vs = variants(n, deform, &c);
     return (vs && v >= 0 && v < c) ? vs[v].name : "";
 }
 
 cudaError_t launch_correlate_items(int n, int v, const CorrParams* items, int count, cudaStream_t s, int* launches) {
+    if (count <= 0) return cudaSuccess;
+    const bool deform = items[0].corners != nullptr;
+    for (int i = 1; i < count; ++i)
+        if ((items[i].corners != nullptr) != deform) return cudaErrorInvalidValue;
+    if (deform)
+        for (int i = 0; i < count; ++i)
+            if (items[i].gnx <= 0 || items[i].gstep <= 0) return cudaErrorInvalidValue;
     int c = 0;
-    const CorrVariant* vs = variants(n, &c);
+    const CorrVariant* vs = variants(n, deform, &c);
     if (!vs || v < 0 || v >= c) return cudaErrorInvalidValue;
     for (int off = 0; off < count; off += kMaxBatch) {
         CorrBatch b;

@@ -107,6 +107,22 @@ __global__ void place_kernel(const __grid_constant__ PlaceBatch b) {
     const float2 ys = place1(p.grid.y0 + iy * p.grid.step, shift.y, max_y);
     const float4 o = make_float4(xs.x, ys.x, xs.y, ys.y);
     p.origins[k] = o;
+    if (p.corners) {
+        // Predictor at the corner pixels (x0, y0), (x0+n-1, y0), (x0, y0+n-1), (x0+n-1, y0+n-1) of
+        // the deformed window's base position: the zero-shift origin under the placement clamp.
+        const float xa = (float)min(p.grid.x0 + ix * p.grid.step, max(p.W - n - 1, 0));
+        const float ya = (float)min(p.grid.y0 + iy * p.grid.step, max(p.H - n - 1, 0));
+        const float xb = __fadd_rn(xa, (float)(n - 1)), yb = __fadd_rn(ya, (float)(n - 1));
+        float2 c00 = make_float2(0.0f, 0.0f), c10 = c00, c01 = c00, c11 = c00;
+        if (p.has_pred) {
+            c00 = sample_predictor(p.pdx, p.pdy, p.pgrid, xa, ya);
+            c10 = sample_predictor(p.pdx, p.pdy, p.pgrid, xb, ya);
+            c01 = sample_predictor(p.pdx, p.pdy, p.pgrid, xa, yb);
+            c11 = sample_predictor(p.pdx, p.pdy, p.pgrid, xb, yb);
+        }
+        p.corners[2 * (size_t)k] = make_float4(c00.x, c00.y, c10.x, c10.y);
+        p.corners[2 * (size_t)k + 1] = make_float4(c01.x, c01.y, c11.x, c11.y);
+    }
     uint8_t st = 1;
     if (p.use_stats)
         st = has_signal(p.sa, o.x, o.y, n, p.min_mean, p.min_std) && has_signal(p.sb, o.z, o.w, n, p.min_mean, p.min_std);

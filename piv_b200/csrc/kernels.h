@@ -23,6 +23,11 @@ struct CorrParams {
     float* raw_dy;
     float* raw_ppr;
     uint8_t* raw_flags;      // 0 or NO_SIGNAL
+    // Deformed windows (null = the reference's uniform shift): 2 float4 per cell holding the
+    // predictor at the window's four corner pixels (dx00, dy00, dx10, dy10 | dx01, dy01, dx11,
+    // dy11), and the pass grid that gives each cell's undeformed position.
+    const float4* corners;
+    int gx0, gy0, gstep, gnx;
 };
 
 // Kernels take a batch of independent work items (pairs, passes or requests, of any sizes) by
@@ -50,10 +55,11 @@ bool corr_supported(int n);
 cudaError_t corr_init_device();  // uploads the root-of-unity table to the current device
 cudaError_t launch_correlate(int n, const CorrParams& p, cudaStream_t s);
 // Launch variants of one window size (identical results; different geometry), for the autotuner.
-int corr_num_variants(int n);
-const char* corr_variant_name(int n, int v);
+int corr_num_variants(int n, bool deform = false);
+const char* corr_variant_name(int n, int v, bool deform = false);
 cudaError_t launch_correlate_variant(int n, int v, const CorrParams& p, cudaStream_t s);
-// All items share window size n; returns the number of launches issued in *launches.
+// All items share window size n and either all have corners (deformed windows) or none; v
+// indexes the variants of that kind. Returns the number of launches issued in *launches.
 cudaError_t launch_correlate_items(int n, int v, const CorrParams* items, int count, cudaStream_t s, int* launches);
 // Number of kernel launches launch_correlate issues (for launch accounting).
 constexpr int kCorrLaunches = 1;
@@ -77,6 +83,7 @@ struct PlaceParams {
     const float* pdy;
     float4* origins;
     uint8_t* status;
+    float4* corners;  // nullable: predictor at the four corner pixels of each window (deformation)
     // signal mask (multipass.rs:233-241); use_stats = 0 means every window has signal
     int use_stats;
     StatsView sa, sb;
