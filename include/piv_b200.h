@@ -56,6 +56,15 @@ typedef enum {
 
 typedef enum { PIV_DTYPE_U8 = 0, PIV_DTYPE_U16 = 1, PIV_DTYPE_F32 = 2 } PivDtype;
 
+/* Arithmetic of the window correlation (no counterpart in the reference, which has FP32 only):
+ * PIV_PRECISION_FP32 runs the FFTs on the FP32 cores in the reference's precision;
+ * PIV_PRECISION_BF16X3 runs the 2-D DFTs as DFT-matrix products on the tensor cores with every
+ * operand split into two BF16 halves and three products summed in FP32 (about 16 significant
+ * bits) for window sizes 16 and 32 and uniform windows; other sizes and deformed windows keep
+ * the FP32 kernel. */
+#define PIV_PRECISION_FP32 0
+#define PIV_PRECISION_BF16X3 1
+
 /* PivConfig + MaskConfig + ValidationConfig (multipass.rs:22-63, validate.rs:7-37).
  * Defaults of the reference: windows {96, 64}, overlap 0.5, final_iterations 2, mask 0/0,
  * ppr 1.3, median threshold 2, median eps 0.1, replace 1. */
@@ -74,6 +83,7 @@ typedef struct {
     int32_t deform;         /* 0: windows shift uniformly (the reference, multipass.rs:224-231);
                              * 1: from the second pass on, windows deform with the predictor
                              * (see piv_correlate_deform) */
+    int32_t precision;      /* PIV_PRECISION_FP32 (the reference) or PIV_PRECISION_BF16X3 */
 } PivConfigC;
 
 /* PreprocessConfig (preprocess.rs:5-29) plus the percentile clip of integer codes
@@ -310,6 +320,12 @@ int32_t piv_correlate_deform(PivAnalyzer* an, const PivFrame* a, const PivFrame*
 int32_t piv_validate_field(PivAnalyzer* an, int64_t ny, int64_t nx, const float* dx, const float* dy,
                            const float* peak_ratio, const uint8_t* flags, float* out_dx, float* out_dy,
                            uint8_t* out_flags, PivSummaryC* summary);
+
+/* Diagnostics (no counterpart in the reference): D (128 x n) = A (128 x k) * B (n x k)^T on the
+ * tensor cores of `device` with BF16 operands (inputs rounded to BF16) and FP32 accumulation, A
+ * stored K-major (a_mn = 0) or MN-major (a_mn = 1) as the tensor-core correlation stores its
+ * operands. a, b, d are row-major DEVICE arrays; n, k multiples of 16 in [16, 256]. Blocking. */
+int32_t piv_tc_selftest(int32_t device, int32_t a_mn, int32_t n, int32_t k, const float* a, const float* b, float* d);
 
 /* ----------------------------------------------------------------------------- no allocation
  * No counterpart in the reference. Validation of a raw field (the same rules as

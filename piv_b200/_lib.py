@@ -25,7 +25,7 @@ EXPORTS = [
     "piv_batch_create", "piv_batch_destroy", "piv_batch_input_device", "piv_batch_input_bytes", "piv_batch_run",
     "piv_batch_sync", "piv_batch_outputs_device", "piv_batch_run_host", "piv_batch_kernels", "piv_batch_stream",
     "piv_place_windows", "piv_correlate_origins", "piv_place_windows_deform", "piv_correlate_deform",
-    "piv_validate_field", "piv_validate_field_noalloc",
+    "piv_validate_field", "piv_tc_selftest", "piv_validate_field_noalloc",
     "piv_server_create", "piv_server_destroy", "piv_server_submit", "piv_server_wait", "piv_server_stats",
 ]
 
@@ -44,6 +44,7 @@ class PivConfigC(ctypes.Structure):
         ("replace", ctypes.c_int32),
         ("device", ctypes.c_int32),
         ("deform", ctypes.c_int32),
+        ("precision", ctypes.c_int32),
     ]
 
 
@@ -146,6 +147,7 @@ def load():
         "piv_correlate_origins": ([vp, vp, vp, i64, vp, i64, vp, vp, vp, vp], i32),
         "piv_place_windows_deform": ([vp, i64, i64, P(PivGridC), P(PivGridC), vp, vp, vp, vp], i32),
         "piv_correlate_deform": ([vp, vp, vp, P(PivGridC), vp, vp, vp, vp, vp, vp], i32),
+        "piv_tc_selftest": ([i32, i32, i32, i32, vp, vp, vp], i32),
         "piv_validate_field": ([vp, i64, i64, vp, vp, vp, vp, vp, vp, vp, P(PivSummaryC)], i32),
         "piv_validate_field_noalloc": ([i64, i64, vp, vp, vp, vp, f32, f32, f32, f32, i32, vp, vp, vp, vp], i32),
         "piv_server_create": ([P(PivServerConfigC), P(vp)], i32),

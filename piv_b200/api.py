@@ -85,6 +85,9 @@ class ValidationConfig:
     replace: bool = True
 
 
+_PRECISIONS = {"fp32": 0, "bf16x3": 1}
+
+
 @dataclass
 class PivConfig:
     windows: List[int] = dc_field(default_factory=lambda: [96, 64])
@@ -95,6 +98,9 @@ class PivConfig:
     # False: windows shift uniformly (the reference). True: from the second pass on, each window
     # is deformed by the bilinear blend of the predictor at its four corner pixels.
     deform: bool = False
+    # "fp32": FFTs on the FP32 cores (the reference's precision). "bf16x3": DFTs on the tensor
+    # cores with operands split into two BF16 halves (window sizes 16 and 32, uniform windows).
+    precision: str = "fp32"
 
     def passes(self):
         return list(self.windows) + [self.windows[-1]] * (self.final_iterations - 1)
@@ -105,7 +111,7 @@ class PivConfig:
                             float(self.mask.min_mean), float(self.mask.min_std),
                             float(self.validation.ppr_threshold), float(self.validation.median_threshold),
                             float(self.validation.median_eps), int(bool(self.validation.replace)), int(device),
-                            int(bool(self.deform)))
+                            int(bool(self.deform)), _PRECISIONS.get(self.precision, -1))
         c._keep = w
         return c
 

@@ -19,12 +19,13 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relax
           "-I", CSRC, "-I", os.path.join(ROOT, "include")]
 UNITS = {
     "correlate.cu": [],
+    "correlate_tc.cu": [],
     "field.cu": ["--fmad=false"],
     "prep.cu": ["--fmad=false"],
     "api.cu": ["--fmad=false"],
     "noalloc.cu": ["--fmad=false"],
 }
-HEADERS = ["common.cuh", "fft.cuh", "kernels.h"]
+HEADERS = ["common.cuh", "fft.cuh", "kernels.h", "window.cuh", "tc.cuh"]
 
 
 def _nvcc():

@@ -95,6 +95,7 @@ int ensure_device_init(int dev) {
     for (int d : g_inited_devices)
         if (d == dev) return PIV_OK;
     CUDA_TRY(corr_init_device());
+    CUDA_TRY(corr_tc_init_device());
     g_inited_devices.push_back(dev);
     return PIV_OK;
 }
@@ -109,6 +110,7 @@ struct PivAnalyzer {
     float ppr_threshold = 1.3f, median_threshold = 2.0f, median_eps = 0.1f;
     int32_t replace = 1;
     int32_t deform = 0;
+    int32_t precision = PIV_PRECISION_FP32;
     int device = 0;
     cudaStream_t own = nullptr;
     cudaStream_t cur = nullptr;
@@ -189,6 +191,8 @@ int check_cfg(const PivConfigC* c) {
     if (!(c->overlap >= 0.0f && c->overlap < 1.0f)) return fail(PIV_ERR_CONFIG, "overlap %g must be in [0, 1)", c->overlap);
     if (c->final_iterations < 1) return fail(PIV_ERR_CONFIG, "final_iterations must be at least 1");
     if (c->deform != 0 && c->deform != 1) return fail(PIV_ERR_CONFIG, "deform must be 0 or 1");
+    if (c->precision != PIV_PRECISION_FP32 && c->precision != PIV_PRECISION_BF16X3)
+        return fail(PIV_ERR_CONFIG, "precision must be PIV_PRECISION_FP32 or PIV_PRECISION_BF16X3");
     for (int i = 0; i < c->n_windows; ++i)
         if (!corr_supported(c->windows[i]))
             return fail(PIV_ERR_UNSUPPORTED, "window size %d is not supported on the GPU (8, 12, 16, 24, 32, 48, 64, 96, 128)",
@@ -347,7 +351,8 @@ int run_passes(PivAnalyzer* an, const PivFrame* const* a, const PivFrame* const*
         }
         const int nwin = (int)an->pairs[0][i].grid.window;
         const int kind = cps[0].corners ? 1 : 0;
-        if (tune) {
+        const bool tensor = kind == 0 && an->precision == PIV_PRECISION_BF16X3 && corr_tc_supported(nwin);
+        if (tune && !tensor) {
             // Time every launch variant of this window size on this pass's data (all compute the
             // same results) and keep the fastest for later calls.
             cudaEvent_t t0, t1;
@@ -372,7 +377,10 @@ int run_passes(PivAnalyzer* an, const PivFrame* const* a, const PivFrame* const*
             cudaEventDestroy(t1);
             an->variant[kind][nwin] = best_v;
         }
-        CUDA_TRY(launch_correlate_items(nwin, an->variant[kind][nwin], cps.data(), K, an->cur, &nl));
+        if (tensor)
+            CUDA_TRY(launch_correlate_tc_items(nwin, cps.data(), K, an->cur, &nl));
+        else
+            CUDA_TRY(launch_correlate_items(nwin, an->variant[kind][nwin], cps.data(), K, an->cur, &nl));
         if (an->profiling) {
             CUDA_TRY(cudaEventRecord(ev1, an->cur));
             if (an->pending.size() < npass) an->pending.resize(npass);
@@ -394,6 +402,13 @@ int run_passes(PivAnalyzer* an, const PivFrame* const* a, const PivFrame* const*
 
 int run_passes(PivAnalyzer* an, const PivFrame* a, const PivFrame* b, bool tune = false) {
     return run_passes(an, &a, &b, 1, tune);
+}
+
+// After a synchronisation: a tensor-core kernel whose bounded wait ran out leaves its results
+// undefined and sets the device's error word.
+int check_device_error(int dev) {
+    if (corr_tc_error(dev)) return fail(PIV_ERR_CUDA, "a tensor-core correlation wait timed out on device %d", dev);
+    return PIV_OK;
 }
 
 int copy_summary(PivAnalyzer* an, PivSummaryC* s) {
@@ -534,6 +549,7 @@ int32_t piv_analyzer_create(const PivConfigC* cfg, PivAnalyzer** out) {
     an->median_eps = cfg->median_eps;
     an->replace = cfg->replace;
     an->deform = cfg->deform;
+    an->precision = cfg->precision;
     an->device = dev;
     cudaError_t e = cudaStreamCreateWithFlags(&an->own, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
@@ -589,7 +605,7 @@ int32_t piv_analyzer_sync(PivAnalyzer* an) {
     int st = use_device(an);
     if (st) return st;
     CUDA_TRY(cudaStreamSynchronize(an->cur));
-    return PIV_OK;
+    return check_device_error(an->device);
 }
 
 int64_t piv_analyzer_launches(const PivAnalyzer* an) { return an ? an->launches : 0; }
@@ -788,7 +804,7 @@ int32_t piv_analyze(PivAnalyzer* an, const PivFrame* a, const PivFrame* b, float
     st = copy_summary(an, summary);
     if (st) return st;
     CUDA_TRY(cudaStreamSynchronize(an->cur));
-    return PIV_OK;
+    return check_device_error(an->device);
 }
 
 int32_t piv_analyze_traced(PivAnalyzer* an, const PivFrame* a, const PivFrame* b, PivTraceC* tr, PivSummaryC* summary) {
@@ -933,7 +949,10 @@ int32_t piv_correlate_origins(PivAnalyzer* an, const PivFrame* a, const PivFrame
     pp.min_std = an->min_std;
     if (e == cudaSuccess) e = launch_mask(pp, d_org, (int)ncells, an->cur);
     CorrParams cp{a->image, b->image, (int)a->H, (int)a->W, d_org, d_st, (int)ncells, d_dx, d_dy, d_ppr, d_fl};
-    if (e == cudaSuccess) e = launch_correlate((int)window, cp, an->cur);
+    if (e == cudaSuccess)
+        e = (an->precision == PIV_PRECISION_BF16X3 && corr_tc_supported((int)window))
+                ? launch_correlate_tc_items((int)window, &cp, 1, an->cur, nullptr)
+                : launch_correlate((int)window, cp, an->cur);
     an->launches += 2;
     if (e == cudaSuccess && dx) e = cudaMemcpyAsync(dx, d_dx, 4 * c, cudaMemcpyDeviceToHost, an->cur);
     if (e == cudaSuccess && dy) e = cudaMemcpyAsync(dy, d_dy, 4 * c, cudaMemcpyDeviceToHost, an->cur);
@@ -942,7 +961,7 @@ int32_t piv_correlate_origins(PivAnalyzer* an, const PivFrame* a, const PivFrame
     if (e == cudaSuccess) e = cudaStreamSynchronize(an->cur);
     cudaFree(buf);
     if (e != cudaSuccess) return fail(PIV_ERR_CUDA, "correlate: %s", cudaGetErrorString(e));
-    return PIV_OK;
+    return check_device_error(an->device);
 }
 
 int32_t piv_correlate_deform(PivAnalyzer* an, const PivFrame* a, const PivFrame* b, const PivGridC* grid,
@@ -1013,6 +1032,20 @@ int32_t piv_correlate_deform(PivAnalyzer* an, const PivFrame* a, const PivFrame*
     cudaFree(buf);
     if (e != cudaSuccess) return fail(PIV_ERR_CUDA, "correlate: %s", cudaGetErrorString(e));
     return PIV_OK;
+}
+
+int32_t piv_tc_selftest(int32_t device, int32_t a_mn, int32_t n, int32_t k, const float* a, const float* b, float* d) {
+    if (!a || !b || !d) return fail(PIV_ERR_ARGUMENT, "null pointer");
+    if (n < 16 || n > 256 || n % 16 || k < 16 || k > 256 || k % 16)
+        return fail(PIV_ERR_ARGUMENT, "n and k must be multiples of 16 in [16, 256]");
+    int dev = device;
+    if (dev < 0) CUDA_TRY(cudaGetDevice(&dev));
+    CUDA_TRY(cudaSetDevice(dev));
+    int st = ensure_device_init(dev);
+    if (st) return st;
+    CUDA_TRY(tc_selftest(a_mn != 0, n, k, a, b, d));
+    CUDA_TRY(cudaDeviceSynchronize());
+    return check_device_error(dev);
 }
 
 int32_t piv_validate_field(PivAnalyzer* an, int64_t ny, int64_t nx, const float* dx, const float* dy,
@@ -1136,6 +1169,7 @@ int32_t piv_batch_create(const PivAnalyzer* parent, int64_t height, int64_t widt
     an->median_eps = parent->median_eps;
     an->replace = parent->replace;
     an->deform = parent->deform;
+    an->precision = parent->precision;
     an->device = parent->device;
     for (int k = 0; k < 2; ++k)
         for (int i = 0; i < 129; ++i) an->variant[k][i] = parent->variant[k][i];
@@ -1469,7 +1503,10 @@ void PivServer::launch_step(std::vector<Request*>& work) {
         pp.min_mean = r->cfg.min_mean;
         pp.min_std = r->cfg.min_std;
         pps.push_back(pp);
-        cps[{(int)pb.grid.window, pp.corners ? 1 : 0}].push_back(
+        const int kind = pp.corners ? 1
+                         : (r->cfg.precision == PIV_PRECISION_BF16X3 && corr_tc_supported((int)pb.grid.window)) ? 2
+                                                                                                              : 0;
+        cps[{(int)pb.grid.window, kind}].push_back(
             CorrParams{r->fa.image, r->fb.image, (int)r->H, (int)r->W, pb.origins, pb.status, (int)pb.cells, pb.raw_dx,
                        pb.raw_dy, pb.raw_ppr, pb.raw_flags, pp.corners, (int)pb.grid.x0, (int)pb.grid.y0,
                        (int)pb.grid.step, (int)pb.grid.nx});
@@ -1481,8 +1518,10 @@ void PivServer::launch_step(std::vector<Request*>& work) {
     cudaError_t e = launch_place_items(pps.data(), (int)pps.size(), stream, &nl);
     for (auto& kv : cps)
         if (e == cudaSuccess)
-            e = launch_correlate_items(kv.first.first, variant[kv.first.second][kv.first.first], kv.second.data(),
-                                       (int)kv.second.size(), stream, &nl);
+            e = kv.first.second == 2
+                    ? launch_correlate_tc_items(kv.first.first, kv.second.data(), (int)kv.second.size(), stream, &nl)
+                    : launch_correlate_items(kv.first.first, variant[kv.first.second][kv.first.first], kv.second.data(),
+                                             (int)kv.second.size(), stream, &nl);
     if (e == cudaSuccess) e = launch_validate_items(vps.data(), (int)vps.size(), stream, &nl);
     std::vector<SummaryItem> sums;
     for (Request* r : work) {
@@ -1685,6 +1724,7 @@ int32_t piv_server_submit(PivServer* sv, const PivRequestC* q, uint64_t* id) {
     c.median_eps = q->config.median_eps;
     c.replace = q->config.replace;
     c.deform = q->config.deform;
+    c.precision = q->config.precision;
     c.device = sv->device;
     r->pre = q->preprocess;
     r->dtype = q->dtype;

@@ -1,0 +1,667 @@
+// Split-precision tensor-core form of the window correlation (no counterpart in the reference,
+// whose FFTs run on CPU cores: correlate.rs:99-178 through realfft/rustfft).
+//
+// The 2-D DFTs of CorrelationPlan::correlate become dense DFT-matrix products on the 5th-
+// generation tensor cores (tcgen05.mma kind::f16, BF16 operands in shared memory, FP32
+// accumulators in TMEM). Every operand x is split into hi = bf16(x) and lo = bf16(x - hi), and a
+// product A*B is evaluated as hi*hi + lo*hi + hi*lo (about 16 significant bits, FP32 sums).
+//
+// One warpgroup owns a 128-row tile of 128/N windows; thread i is row i of every operand and
+// TMEM lane i. Real input makes the transforms half-size, so every stage is a 128 x N x K GEMM
+// with the exchanges between stages either inside a thread or between the two lanes of a pair:
+//   F1  r2c along x of both frames (rows (w, r), K = x): packed half spectrum per row,
+//       columns [re(kx=0..N/2-1) | im(kx=1..N/2-1) with the Nyquist real value in the im(0) slot]
+//   F2  complex DFT along y (rows (w, kx', frame), K = [re(r) | im(r)]): row kx' = 0 carries
+//       DC + i*Nyquist and is separated inside the thread (Hermitian partner at -ky);
+//   --  cross spectrum conj(FA)*FB between the two frame lanes (lane ^ 1), window mean removed by
+//       zeroing the DC bin; the frame-1 lane multiplies by (-1)^ky so that the next stage gives
+//       it the upper half of the outputs;
+//   I1  inverse complex DFT along ky, each lane half of the y outputs;
+//   I2  c2r along kx (rows (w, y), K = packed kx): the correlation plane, row y per thread.
+// find_peak (correlate.rs:215-303) then runs on the plane as in the FP32 kernel.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.h"
+#include "tc.cuh"
+#include "window.cuh"
+
+namespace pivb200 {
+
+template <int N_>
+struct TcCfg {
+    static constexpr int N = N_, H2 = N / 2;
+    static constexpr int WPT = 128 / N;  // windows (cells) per tile
+    static constexpr int NWG = 4;        // warpgroups per CTA, each on its own tiles
+    static constexpr int THREADS = 128 * NWG;
+    // DFT matrices, B operands (rows = outputs, K-major), element offsets of hi (or lo) parts
+    static constexpr int R1_OFF = 0;                 // N x N
+    static constexpr int R2_OFF = R1_OFF + N * N;    // 2N x 2N
+    static constexpr int R3_OFF = R2_OFF + 4 * N * N;  // N x 2N
+    static constexpr int R4_OFF = R3_OFF + 2 * N * N;  // N x N
+    static constexpr int RMAT = R4_OFF + N * N;
+    static constexpr size_t MAT_BYTES = (size_t)RMAT * 2;
+    static constexpr int ABUF = 128 * 2 * N;  // operand elements per part per warpgroup
+    static constexpr size_t A_BYTES = (size_t)ABUF * 2;
+    static constexpr int TCOLS = (2 * N < 32) ? 32 : 2 * N;  // TMEM columns per warpgroup
+    static constexpr int PLD = N + 1;                        // FP32 plane row pitch (floats)
+    static constexpr size_t BAR_OFF = 2 * MAT_BYTES + (size_t)NWG * 2 * A_BYTES;
+    static constexpr size_t SMEM = BAR_OFF + 8 * NWG + 16 + sizeof(int) * NWG * WPT * 4 + 64;
+    static_assert((size_t)128 * PLD * 4 <= 2 * A_BYTES, "plane fits in the operand buffers");
+    static_assert(N % 16 == 0 && 128 % N == 0, "tile shape");
+};
+
+// K-major operand of `rows` rows: byte offset of the 16-byte chunk holding (row, k..k+7).
+__device__ __forceinline__ uint32_t kmaj_chunk(int rows, int row, int k) {
+    return (uint32_t)((k >> 3) * (rows >> 3) * 128 + (row >> 3) * 128 + (row & 7) * 16);
+}
+// MN-major operand of `rows` rows: byte offset of the chunk holding (m..m+7, k), m % 8 == 0.
+__device__ __forceinline__ uint32_t mnmaj_chunk(int rows, int m, int k) {
+    return (uint32_t)((k >> 3) * (rows >> 3) * 128 + (m >> 3) * 128 + (k & 7) * 16);
+}
+
+__device__ __forceinline__ void wg_sync(int wg) { asm volatile("bar.sync %0, 128;" ::"r"(wg + 1) : "memory"); }
+
+__device__ __forceinline__ void store_split(uint8_t* hi, uint8_t* lo, uint32_t off, const float (&v)[8]) {
+    uint4 h, l;
+    tc::split8_bf16(v, h, l);
+    *reinterpret_cast<uint4*>(hi + off) = h;
+    *reinterpret_cast<uint4*>(lo + off) = l;
+}
+
+// Issues D (+)= A * B^T over `ksteps` K=16 steps for the three split products.
+__device__ __forceinline__ void mma_split(uint32_t d, uint32_t a_hi, uint32_t a_lo, uint32_t a_lbo, uint32_t b_hi,
+                                          uint32_t b_lo, uint32_t b_lbo, int ksteps, uint32_t idesc) {
+    uint32_t acc = 0;
+    const uint32_t as[3] = {a_hi, a_lo, a_hi};
+    const uint32_t bs[3] = {b_hi, b_hi, b_lo};
+#pragma unroll
+    for (int part = 0; part < 3; ++part)
+        for (int s = 0; s < ksteps; ++s) {
+            const uint64_t ad = tc::smem_desc(as[part] + 2 * s * a_lbo, a_lbo, 128);
+            const uint64_t bd = tc::smem_desc(bs[part] + 2 * s * b_lbo, b_lbo, 128);
+            tc::mma_f16(d, ad, bd, idesc, acc);
+            acc = 1;
+        }
+}
+
+template <int N>
+__global__ void __launch_bounds__(TcCfg<N>::THREADS, 1)
+    correlate_tc_kernel(const __grid_constant__ CorrBatch batch, const uint4* __restrict__ mats, int total_tiles,
+                        unsigned int* err) {
+    using C = TcCfg<N>;
+    constexpr int H2 = C::H2;
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint8_t* mat_hi = smem;
+    uint8_t* mat_lo = smem + C::MAT_BYTES;
+    const int wg = threadIdx.x >> 7;
+    const int i = threadIdx.x & 127;  // row of the tile, TMEM lane
+    uint8_t* a_hi = smem + 2 * C::MAT_BYTES + (size_t)wg * 2 * C::A_BYTES;
+    uint8_t* a_lo = a_hi + C::A_BYTES;
+    float* plane = reinterpret_cast<float*>(a_hi);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + C::BAR_OFF) + wg;
+    uint32_t* tbase = reinterpret_cast<uint32_t*>(smem + C::BAR_OFF + 8 * C::NWG);
+    int* s_hw = reinterpret_cast<int*>(smem + C::BAR_OFF + 8 * C::NWG + 16) + wg * C::WPT * 4;
+
+    for (int j = threadIdx.x; j < (int)(2 * C::MAT_BYTES / 16); j += C::THREADS)
+        reinterpret_cast<uint4*>(smem)[j] = mats[j];
+    if (threadIdx.x == 0) {
+        for (int g = 0; g < C::NWG; ++g) tc::mbar_init(reinterpret_cast<uint64_t*>(smem + C::BAR_OFF) + g, 1);
+        tc::fence_mbar_init();
+    }
+    if (threadIdx.x < 32) {
+        tc::tmem_alloc(tbase, C::NWG * C::TCOLS);
+        tc::tmem_relinquish();
+    }
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = *tbase + (uint32_t)(wg * C::TCOLS);
+    const uint32_t trow = tmem + ((uint32_t)(i & ~31) << 16);  // this warp's lane quarter
+    uint32_t phase = 0;
+
+    const uint32_t mh = tc::smem_u32(mat_hi), ml = tc::smem_u32(mat_lo);
+    const uint32_t ah = tc::smem_u32(a_hi), al = tc::smem_u32(a_lo);
+    constexpr uint32_t LBO_A = (128 / 8) * 128;  // 128-row operands
+    const int c = i / N;                          // window of the tile for this thread
+    const int q = i % N;                          // column (sampling) / row (later stages) in the window
+
+    auto mma_wait = [&]() {
+        tc::mbar_wait(bar, phase, err);
+        phase ^= 1u;
+        tc::fence_after_sync();
+    };
+    auto sync_for_mma = [&]() {
+        tc::fence_async_smem();
+        tc::fence_before_sync();
+        wg_sync(wg);
+    };
+
+    for (int tile = blockIdx.x * C::NWG + wg; tile < total_tiles; tile += gridDim.x * C::NWG) {
+        const int item = batch_item(batch.block_start, batch.n, tile);
+        const CorrParams& prm = batch.item[item];
+        const long long cell = (long long)(tile - batch.block_start[item]) * C::WPT + c;
+        const bool active = cell < prm.ncells;
+        const float4 org = active ? prm.origins[cell] : make_float4(0.f, 0.f, 0.f, 0.f);
+        bool ok = active && prm.status[cell] != 0;
+
+        // ------------------------------------------------ sampling (lane = column q of window c)
+        float2 z[N];
+        sample_column_direct<N, 1, false>(prm.img_a, prm.H, prm.W, org.x, org.y, q, 0, z);
+        sample_column_direct<N, 1, true>(prm.img_b, prm.H, prm.W, org.z, org.w, q, 0, z);
+        float2 e;
+        {
+            float2 s = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int p = 0; p < N; ++p) {
+                s.x += z[p].x;
+                s.y += z[p].y;
+            }
+#pragma unroll
+            for (int o = N / 2; o > 0; o >>= 1) {
+                s.x += __shfl_xor_sync(0xffffffffu, s.x, o);
+                s.y += __shfl_xor_sync(0xffffffffu, s.y, o);
+            }
+            constexpr float inv = 1.0f / (float)(N * N);
+            const float ma = s.x * inv, mb = s.y * inv;
+            e = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int p = 0; p < N; ++p) {
+                z[p].x = __fsub_rn(z[p].x, ma);
+                z[p].y = __fsub_rn(z[p].y, mb);
+                e.x += z[p].x * z[p].x;
+                e.y += z[p].y * z[p].y;
+            }
+#pragma unroll
+            for (int o = N / 2; o > 0; o >>= 1) {
+                e.x += __shfl_xor_sync(0xffffffffu, e.x, o);
+                e.y += __shfl_xor_sync(0xffffffffu, e.y, o);
+            }
+        }
+        ok = ok && e.x > 1e-12f && e.y > 1e-12f;
+        const float scale = 1.0f / ((float)(N * N) * (sqrtf(e.x) * sqrtf(e.y)));
+        // F1 operands, MN-major (m = c*N + r, k = column q); frame b after frame a.
+#pragma unroll
+        for (int j = 0; j < N / 8; ++j) {
+            float va[8], vb[8];
+#pragma unroll
+            for (int t = 0; t < 8; ++t) {
+                va[t] = z[8 * j + t].x;
+                vb[t] = z[8 * j + t].y;
+            }
+            const uint32_t off = mnmaj_chunk(128, c * N + 8 * j, q);
+            store_split(a_hi, a_lo, off, va);
+            store_split(a_hi + 128 * N * 2, a_lo + 128 * N * 2, off, vb);
+        }
+        sync_for_mma();
+        if (i == 0) {
+            tc::fence_after_sync();
+            constexpr uint32_t id = tc::idesc_f16(128, N, true, true);
+            constexpr uint32_t lb = (N / 8) * 128;
+            for (int f = 0; f < 2; ++f)
+                mma_split(tmem + f * N, ah + f * 128 * N * 2, al + f * 128 * N * 2, LBO_A, mh + C::R1_OFF * 2,
+                          ml + C::R1_OFF * 2, lb, N / 16, id);
+            tc::mma_commit(bar);
+        }
+        mma_wait();
+
+        // ------------------------------------------------ F1 -> F2 operand (row r = q of window c)
+        {
+            float d[2 * N];
+#pragma unroll
+            for (int j = 0; j < 2 * N; j += 16) tc::tmem_ld16(trow + j, d + j);
+            tc::wait_ld();
+            // m = c*N + 2*kx' + f; k = r (real parts), N + r (imaginary parts)
+#pragma unroll
+            for (int j = 0; j < N / 8; ++j) {
+                float vr[8], vi[8];
+#pragma unroll
+                for (int t = 0; t < 8; ++t) {
+                    vr[t] = d[(t & 1) * N + 4 * j + (t >> 1)];
+                    vi[t] = d[(t & 1) * N + H2 + 4 * j + (t >> 1)];
+                }
+                store_split(a_hi, a_lo, mnmaj_chunk(128, c * N + 8 * j, q), vr);
+                store_split(a_hi, a_lo, mnmaj_chunk(128, c * N + 8 * j, N + q), vi);
+            }
+        }
+        sync_for_mma();
+        if (i == 0) {
+            tc::fence_after_sync();
+            constexpr uint32_t id = tc::idesc_f16(128, 2 * N, true, true);
+            constexpr uint32_t lb = (2 * N / 8) * 128;
+            mma_split(tmem, ah, al, LBO_A, mh + C::R2_OFF * 2, ml + C::R2_OFF * 2, lb, 2 * N / 16, id);
+            tc::mma_commit(bar);
+        }
+        mma_wait();
+
+        // ------------------------------------------------ spectra -> cross spectrum -> I1 operand
+        {
+            const int kxp = q >> 1, fr = q & 1;  // row (w, kx', frame)
+            const bool dcrow = kxp == 0;
+            float zr[N], zi[N];
+#pragma unroll
+            for (int j = 0; j < N; j += 16) {
+                tc::tmem_ld16(trow + j, zr + j);
+                tc::tmem_ld16(trow + N + j, zi + j);
+            }
+            tc::wait_ld();
+#pragma unroll
+            for (int j = 0; j < N / 8; ++j) {
+                float pr[8], pi[8];
+#pragma unroll
+                for (int t = 0; t < 8; ++t) {
+                    const int ky = 8 * j + t, my = (N - ky) % N;
+                    // own frame's spectrum at (kx', ky); the DC row also yields the Nyquist row
+                    float ar = zr[ky], ai = zi[ky], br = 0.f, bi = 0.f;
+                    if (dcrow) {
+                        ar = 0.5f * (zr[ky] + zr[my]);
+                        ai = 0.5f * (zi[ky] - zi[my]);
+                        br = 0.5f * (zi[ky] + zi[my]);
+                        bi = 0.5f * (zr[my] - zr[ky]);
+                        if (ky == 0) ar = ai = 0.f;  // mean removed: DC bin is zero
+                    }
+                    const float oar = __shfl_xor_sync(0xffffffffu, ar, 1), oai = __shfl_xor_sync(0xffffffffu, ai, 1);
+                    const float obr = __shfl_xor_sync(0xffffffffu, br, 1), obi = __shfl_xor_sync(0xffffffffu, bi, 1);
+                    // FA from the frame-0 lane, FB from the frame-1 lane
+                    const float far_ = fr ? oar : ar, fai = fr ? oai : ai, fbr = fr ? ar : oar, fbi = fr ? ai : oai;
+                    const float gar = fr ? obr : br, gai = fr ? obi : bi, gbr = fr ? br : obr, gbi = fr ? bi : obi;
+                    float cr = far_ * fbr + fai * fbi, ci = far_ * fbi - fai * fbr;  // conj(FA) * FB
+                    if (dcrow) {
+                        const float nr = gar * gbr + gai * gbi, ni = gar * gbi - gai * gbr;
+                        const float t0 = cr - ni, t1 = ci + nr;  // C(0, ky) + i C(N/2, ky)
+                        cr = t0;
+                        ci = t1;
+                    }
+                    if (fr && (ky & 1)) {
+                        cr = -cr;
+                        ci = -ci;
+                    }
+                    pr[t] = cr;
+                    pi[t] = ci;
+                }
+                store_split(a_hi, a_lo, kmaj_chunk(128, i, 8 * j), pr);
+                store_split(a_hi, a_lo, kmaj_chunk(128, i, N + 8 * j), pi);
+            }
+        }
+        sync_for_mma();
+        if (i == 0) {
+            tc::fence_after_sync();
+            constexpr uint32_t id = tc::idesc_f16(128, N, true, false);
+            constexpr uint32_t lb = (N / 8) * 128;
+            mma_split(tmem, ah, al, LBO_A, mh + C::R3_OFF * 2, ml + C::R3_OFF * 2, lb, 2 * N / 16, id);
+            tc::mma_commit(bar);
+        }
+        mma_wait();
+
+        // ------------------------------------------------ I1 -> I2 operand
+        {
+            const int kxp = q >> 1, fr = q & 1;
+            float g[N];
+#pragma unroll
+            for (int j = 0; j < N; j += 16) tc::tmem_ld16(trow + j, g + j);
+            tc::wait_ld();
+            // m = c*N + y with y = fr*N/2 + j; k = kx' (real), N/2 + kx' (imaginary)
+#pragma unroll
+            for (int j = 0; j < H2 / 8; ++j) {
+                float vr[8], vi[8];
+#pragma unroll
+                for (int t = 0; t < 8; ++t) {
+                    vr[t] = g[8 * j + t];
+                    vi[t] = g[H2 + 8 * j + t];
+                }
+                const int m = c * N + fr * H2 + 8 * j;
+                store_split(a_hi, a_lo, mnmaj_chunk(128, m, kxp), vr);
+                store_split(a_hi, a_lo, mnmaj_chunk(128, m, H2 + kxp), vi);
+            }
+        }
+        sync_for_mma();
+        if (i == 0) {
+            tc::fence_after_sync();
+            constexpr uint32_t id = tc::idesc_f16(128, N, true, true);
+            constexpr uint32_t lb = (N / 8) * 128;
+            mma_split(tmem, ah, al, LBO_A, mh + C::R4_OFF * 2, ml + C::R4_OFF * 2, lb, N / 16, id);
+            tc::mma_commit(bar);
+        }
+        mma_wait();
+
+        // ------------------------------------------------ correlation plane, row y = q
+        float v[N];
+#pragma unroll
+        for (int j = 0; j < N; j += 16) tc::tmem_ld16(trow + j, v + j);
+        tc::wait_ld();
+        tc::fence_before_sync();
+        const int y = q;
+        float* prow = plane + (size_t)(c * N) * C::PLD;  // window c's plane
+#pragma unroll
+        for (int x = 0; x < N; ++x) {
+            v[x] = v[x] * scale;
+            prow[y * C::PLD + x] = v[x];
+        }
+        // argmax, lowest row-major index on ties
+        float best = -INFINITY;
+        int bi = 0x7fffffff;
+#pragma unroll
+        for (int x = 0; x < N; ++x)
+            if (v[x] > best) {
+                best = v[x];
+                bi = y * N + x;
+            }
+#pragma unroll
+        for (int o = N / 2; o > 0; o >>= 1) {
+            const float ob = __shfl_xor_sync(0xffffffffu, best, o);
+            const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+            amax_combine(best, bi, ob, oi);
+        }
+        if (!(best > -INFINITY)) bi = 0;
+        const int by = bi / N, bx = bi % N;
+        wg_sync(wg);  // plane complete
+        auto at = [&](int yy, int xx) -> float { return prow[((yy + N) % N) * C::PLD + (xx + N) % N]; };
+        if (q < 4) {  // footprint (correlate.rs:242-254): half-width along +y, -y, +x, -x
+            const int sy = q == 0 ? 1 : (q == 1 ? N - 1 : 0);
+            const int sx = q == 2 ? 1 : (q == 3 ? N - 1 : 0);
+            const float half = 0.5f * best;
+            int k = 0;
+            while (k < N / 2 && at(by + k * sy, bx + k * sx) > half) ++k;
+            s_hw[c * 4 + q] = k;
+        }
+        // vertical 3-maximum from the neighbouring rows
+        float vm[N];
+        {
+            const float* up = prow + ((y + N - 1) % N) * C::PLD;
+            const float* dn = prow + ((y + 1) % N) * C::PLD;
+#pragma unroll
+            for (int x = 0; x < N; ++x) vm[x] = fmaxf(fmaxf(up[x], dn[x]), v[x]);
+        }
+        wg_sync(wg);  // footprints written
+        const int hw = max(max(s_hw[c * 4 + 0], s_hw[c * 4 + 1]), max(s_hw[c * 4 + 2], s_hw[c * 4 + 3]));
+        const int ex = max((int)ceilf(1.5f * (float)hw), 2);
+        float second = -INFINITY;
+        {
+            auto circ = [](int a, int b) {
+                const int d = abs(a - b);
+                return min(d, N - d);
+            };
+            const int cy = circ(y, by);
+#pragma unroll
+            for (int x = 0; x < N; ++x) {
+                const float h = fmaxf(fmaxf(vm[(x + N - 1) % N], vm[(x + 1) % N]), vm[x]);
+                if (v[x] == h && max(cy, circ(x, bx)) > ex) second = fmaxf(second, v[x]);
+            }
+        }
+#pragma unroll
+        for (int o = N / 2; o > 0; o >>= 1) second = fmaxf(second, __shfl_xor_sync(0xffffffffu, second, o));
+        if (q == 0 && active) {
+            if (ok) {
+                const float sx = subpixel(at(by, bx - 1), best, at(by, bx + 1));
+                const float sy = subpixel(at(by - 1, bx), best, at(by + 1, bx));
+                const float wx = bx >= N / 2 ? (float)bx - (float)N : (float)bx;
+                const float wy = by >= N / 2 ? (float)by - (float)N : (float)by;
+                const float pdx = __fadd_rn(wx, sx), pdy = __fadd_rn(wy, sy);
+                prm.raw_dx[cell] = __fadd_rn(__fsub_rn(org.z, org.x), pdx);
+                prm.raw_dy[cell] = __fadd_rn(__fsub_rn(org.w, org.y), pdy);
+                prm.raw_ppr[cell] = second > 0.0f ? fminf(__fdiv_rn(best, second), MAX_PPR) : MAX_PPR;
+                prm.raw_flags[cell] = 0;
+            } else {
+                prm.raw_dx[cell] = NAN;
+                prm.raw_dy[cell] = NAN;
+                prm.raw_ppr[cell] = 0.0f;
+                prm.raw_flags[cell] = F_NO_SIGNAL;
+            }
+        }
+        wg_sync(wg);  // plane and footprints read before the next tile reuses them
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        tc::fence_after_sync();
+        tc::tmem_dealloc(*tbase, C::NWG * C::TCOLS);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Host side: DFT matrices (split into bf16 hi / lo, laid out as the K-major shared-memory image).
+// ---------------------------------------------------------------------------------------------
+static uint16_t bf16_rne(float f) {
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    if ((u & 0x7fffffffu) > 0x7f800000u) return (uint16_t)((u >> 16) | 0x40);  // NaN
+    const uint32_t r = 0x7fffu + ((u >> 16) & 1u);
+    return (uint16_t)((u + r) >> 16);
+}
+static float bf16_f(uint16_t h) {
+    const uint32_t u = (uint32_t)h << 16;
+    float f;
+    std::memcpy(&f, &u, 4);
+    return f;
+}
+
+// cos / sin of 2*pi*k/n with the phase reduced exactly first.
+static double cs(long long k, int n, bool sine) {
+    const long long r = ((k % n) + n) % n;
+    const double a = 2.0 * M_PI * (double)r / (double)n;
+    return sine ? std::sin(a) : std::cos(a);
+}
+
+template <int N>
+static std::vector<uint16_t> build_mats() {
+    using C = TcCfg<N>;
+    constexpr int H2 = N / 2;
+    std::vector<uint16_t> img(2 * (size_t)C::RMAT, 0);  // [hi image | lo image]
+    auto put = [&](int off, int rows, int row, int k, double val) {
+        const size_t e = (size_t)off + (size_t)(k >> 3) * (rows >> 3) * 64 + (size_t)(row >> 3) * 64 + (row & 7) * 8 +
+                         (k & 7);  // element index of the K-major layout (64 elements per core)
+        const uint16_t h = bf16_rne((float)val);
+        const uint16_t l = bf16_rne((float)(val - (double)bf16_f(h)));
+        img[e] = h;
+        img[(size_t)C::RMAT + e] = l;
+    };
+    for (int n = 0; n < N; ++n)  // R1: r2c along x, packed half spectrum
+        for (int x = 0; x < N; ++x) {
+            double v;
+            if (n < H2) v = cs((long long)n * x, N, false);
+            else if (n == H2) v = (x & 1) ? -1.0 : 1.0;
+            else v = -cs((long long)(n - H2) * x, N, true);
+            put(C::R1_OFF, N, n, x, v);
+        }
+    for (int n = 0; n < 2 * N; ++n)  // R2: forward complex DFT along y
+        for (int k = 0; k < 2 * N; ++k) {
+            const int ky = n % N, r = k % N;
+            const bool out_im = n >= N, in_im = k >= N;
+            double v;
+            if (!out_im) v = in_im ? cs((long long)ky * r, N, true) : cs((long long)ky * r, N, false);
+            else v = in_im ? cs((long long)ky * r, N, false) : -cs((long long)ky * r, N, true);
+            put(C::R2_OFF, 2 * N, n, k, v);
+        }
+    for (int n = 0; n < N; ++n)  // R3: inverse complex DFT along ky, outputs y < N/2
+        for (int k = 0; k < 2 * N; ++k) {
+            const int yy = n % H2, ky = k % N;
+            const bool out_im = n >= H2, in_im = k >= N;
+            double v;
+            if (!out_im) v = in_im ? -cs((long long)ky * yy, N, true) : cs((long long)ky * yy, N, false);
+            else v = in_im ? cs((long long)ky * yy, N, false) : cs((long long)ky * yy, N, true);
+            put(C::R3_OFF, N, n, k, v);
+        }
+    for (int x = 0; x < N; ++x)  // R4: c2r along kx from the packed half spectrum
+        for (int k = 0; k < N; ++k) {
+            double v;
+            if (k == 0) v = 1.0;
+            else if (k < H2) v = 2.0 * cs((long long)k * x, N, false);
+            else if (k == H2) v = (x & 1) ? -1.0 : 1.0;
+            else v = -2.0 * cs((long long)(k - H2) * x, N, true);
+            put(C::R4_OFF, N, x, k, v);
+        }
+    return img;
+}
+
+namespace {
+constexpr int kMaxDevices = 64;
+const uint4* g_mats16[kMaxDevices] = {};
+const uint4* g_mats32[kMaxDevices] = {};
+unsigned int* g_err_host[kMaxDevices] = {};
+unsigned int* g_err_dev[kMaxDevices] = {};
+
+template <int N>
+cudaError_t upload(const uint4** slot) {
+    if (*slot) return cudaSuccess;
+    const std::vector<uint16_t> img = build_mats<N>();
+    void* d = nullptr;
+    cudaError_t e = cudaMalloc(&d, img.size() * 2);
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpy(d, img.data(), img.size() * 2, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        cudaFree(d);
+        return e;
+    }
+    *slot = reinterpret_cast<const uint4*>(d);
+    return cudaSuccess;
+}
+}  // namespace
+
+bool corr_tc_supported(int n) { return n == 16 || n == 32; }
+
+cudaError_t corr_tc_init_device() {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    e = upload<16>(&g_mats16[dev]);
+    if (e == cudaSuccess) e = upload<32>(&g_mats32[dev]);
+    if (e == cudaSuccess && !g_err_host[dev]) {
+        e = cudaHostAlloc(reinterpret_cast<void**>(&g_err_host[dev]), sizeof(unsigned int), cudaHostAllocMapped);
+        if (e == cudaSuccess) {
+            *g_err_host[dev] = 0;
+            e = cudaHostGetDevicePointer(reinterpret_cast<void**>(&g_err_dev[dev]), g_err_host[dev], 0);
+        }
+    }
+    return e;
+}
+
+unsigned int corr_tc_error(int device) {
+    return (device >= 0 && device < kMaxDevices && g_err_host[device]) ? *(volatile unsigned int*)g_err_host[device] : 0u;
+}
+
+template <int N>
+static cudaError_t launch_tc(CorrBatch b, cudaStream_t s, const uint4* mats, unsigned int* err) {
+    using C = TcCfg<N>;
+    long long total = 0;
+    for (int i = 0; i < b.n; ++i) {
+        b.block_start[i] = (int)total;
+        total += (b.item[i].ncells + C::WPT - 1) / C::WPT;
+    }
+    b.block_start[b.n] = (int)total;
+    if (total <= 0) return cudaSuccess;
+    if (total > 0x7fffffffll) return cudaErrorInvalidValue;
+    int dev = 0, sms = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    auto kern = correlate_tc_kernel<N>;
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+    if (e != cudaSuccess) return e;
+    const long long ctas = std::min<long long>((total + C::NWG - 1) / C::NWG, (long long)sms);
+    kern<<<(unsigned)ctas, C::THREADS, C::SMEM, s>>>(b, mats, (int)total, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_correlate_tc_items(int n, const CorrParams* items, int count, cudaStream_t s, int* launches) {
+    if (count <= 0) return cudaSuccess;
+    if (!corr_tc_supported(n)) return cudaErrorInvalidValue;
+    for (int i = 0; i < count; ++i)
+        if (items[i].corners) return cudaErrorInvalidValue;  // deformed windows: FP32 kernel only
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices || !g_err_dev[dev]) return cudaErrorInitializationError;
+    for (int off = 0; off < count; off += kMaxBatch) {
+        CorrBatch b;
+        b.n = count - off < kMaxBatch ? count - off : kMaxBatch;
+        for (int i = 0; i < b.n; ++i) b.item[i] = items[off + i];
+        e = n == 16 ? launch_tc<16>(b, s, g_mats16[dev], g_err_dev[dev]) : launch_tc<32>(b, s, g_mats32[dev], g_err_dev[dev]);
+        if (e != cudaSuccess) return e;
+        if (launches) ++*launches;
+    }
+    return cudaSuccess;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Self-test of the tensor-core building blocks: D (128 x n) = A (128 x k) * B (n x k)^T with
+// BF16 operands (the inputs are rounded to bf16 on the way in) and FP32 accumulation, A stored
+// K-major or MN-major exactly as the correlation kernel stores its operands.
+// ---------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(128, 1)
+    tc_selftest_kernel(const float* __restrict__ a, const float* __restrict__ b, float* __restrict__ d, int n, int k,
+                       int a_mn, unsigned int* err) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    // A: 128 x k, B: n x k (bf16), then the barrier and the TMEM address
+    uint8_t* sa = smem;
+    uint8_t* sb = smem + 128 * k * 2;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sb + n * k * 2);
+    uint32_t* tbase = reinterpret_cast<uint32_t*>(bar + 1);
+    const int i = threadIdx.x;
+    // element writes (scalar; this is a test)
+    for (int e = i; e < 128 * k; e += 128) {
+        const int m = e / k, kk = e % k;
+        const uint32_t off = a_mn ? mnmaj_chunk(128, m & ~7, kk) + (m & 7) * 2 : kmaj_chunk(128, m, kk & ~7) + (kk & 7) * 2;
+        *reinterpret_cast<__nv_bfloat16*>(sa + off) = __float2bfloat16_rn(a[e]);
+    }
+    for (int e = i; e < n * k; e += 128) {
+        const int r = e / k, kk = e % k;
+        *reinterpret_cast<__nv_bfloat16*>(sb + kmaj_chunk(n, r, kk & ~7) + (kk & 7) * 2) = __float2bfloat16_rn(b[e]);
+    }
+    if (i == 0) {
+        tc::mbar_init(bar, 1);
+        tc::fence_mbar_init();
+    }
+    if (i < 32) {
+        tc::tmem_alloc(tbase, 256);
+        tc::tmem_relinquish();
+    }
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = *tbase;
+    if (i == 0) {
+        const uint32_t id = tc::idesc_f16(128, n, true, a_mn != 0);
+        const uint32_t la = 16 * 128, lb = (uint32_t)(n / 8) * 128;
+        const uint32_t a0 = tc::smem_u32(sa), b0 = tc::smem_u32(sb);
+        for (int s = 0; s < k / 16; ++s)
+            tc::mma_f16(tmem, tc::smem_desc(a0 + 2 * s * la, la, 128), tc::smem_desc(b0 + 2 * s * lb, lb, 128), id,
+                        s > 0 ? 1u : 0u);
+        tc::mma_commit(bar);
+    }
+    tc::mbar_wait(bar, 0, err);
+    tc::fence_after_sync();
+    for (int j = 0; j < n; j += 16) {
+        float v[16];
+        tc::tmem_ld16(tmem + ((uint32_t)(i & ~31) << 16) + j, v);
+        tc::wait_ld();
+        for (int t = 0; t < 16; ++t) d[i * n + j + t] = v[t];
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (i < 32) {
+        tc::fence_after_sync();
+        tc::tmem_dealloc(tmem, 256);
+    }
+}
+
+cudaError_t tc_selftest(int a_mn, int n, int k, const float* a, const float* b, float* d) {
+    if (n < 16 || n > 256 || n % 16 || k < 16 || k > 256 || k % 16) return cudaErrorInvalidValue;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices || !g_err_dev[dev]) return cudaErrorInitializationError;
+    const size_t smem = (size_t)128 * k * 2 + (size_t)n * k * 2 + 64;
+    e = cudaFuncSetAttribute(tc_selftest_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    tc_selftest_kernel<<<1, 128, smem>>>(a, b, d, n, k, a_mn, g_err_dev[dev]);
+    return cudaGetLastError();
+}
+
+}  // namespace pivb200
