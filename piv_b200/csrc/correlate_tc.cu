@@ -48,9 +48,11 @@ struct TcCfg {
     static constexpr int ABUF = 128 * 2 * N;  // operand elements per part per warpgroup
     static constexpr size_t A_BYTES = (size_t)ABUF * 2;
     static constexpr int TCOLS = (2 * N < 32) ? 32 : 2 * N;  // TMEM columns per warpgroup
-    static constexpr int PLD = N + 1;                        // FP32 plane row pitch (floats)
+    static constexpr int PLD = N + 4;  // FP32 plane row pitch (floats): 16-byte rows, 8 rows on distinct banks
     static constexpr size_t BAR_OFF = 2 * MAT_BYTES + (size_t)NWG * 2 * A_BYTES;
-    static constexpr size_t SMEM = BAR_OFF + 8 * NWG + 16 + sizeof(int) * NWG * WPT * 4 + 64;
+    // staged DC + i*Nyquist spectra: per warpgroup, window and frame, 2N floats
+    static constexpr size_t ZST_OFF = (BAR_OFF + 8 * NWG + 16 + sizeof(int) * NWG * WPT * 4 + 15) / 16 * 16;
+    static constexpr size_t SMEM = ZST_OFF + sizeof(float) * NWG * WPT * 4 * N + 64;
     static_assert((size_t)128 * PLD * 4 <= 2 * A_BYTES, "plane fits in the operand buffers");
     static_assert(N % 16 == 0 && 128 % N == 0, "tile shape");
 };
@@ -62,6 +64,40 @@ __device__ __forceinline__ uint32_t kmaj_chunk(int rows, int row, int k) {
 // MN-major operand of `rows` rows: byte offset of the chunk holding (m..m+7, k), m % 8 == 0.
 __device__ __forceinline__ uint32_t mnmaj_chunk(int rows, int m, int k) {
     return (uint32_t)((k >> 3) * (rows >> 3) * 128 + (m >> 3) * 128 + (k & 7) * 16);
+}
+
+// Window sampling for the tensor-core tier (correlate.rs:182-202 semantics: integer copy when
+// both fractional parts are < 1e-4, bilinear otherwise), one lane per column streaming down the
+// rows: each pixel of the patch is loaded once, the right-hand neighbour comes from the next lane
+// and the row below is carried to the next iteration. The bilinear weights are applied as two
+// linear interpolations with FMA (rounding differs from the reference's weight sum by an ulp,
+// far below the split-BF16 precision); zero fractions make it an exact copy. The last column of
+// a window (and lane 31) loads its right neighbour itself.
+template <int N, bool IMAG>
+__device__ __forceinline__ void sample_rows(const float* __restrict__ img, int H, int W, float ox, float oy, int x,
+                                            float2 (&z)[N]) {
+    const float fx0 = floorf(ox), fy0 = floorf(oy);
+    const int x0 = min(max((int)fx0, 0), W - 1), y0 = min(max((int)fy0, 0), H - 1);
+    float tx = ox - fx0, ty = oy - fy0;
+    if (tx < 1e-4f && ty < 1e-4f) tx = ty = 0.0f;
+    const int c0 = min(x0 + x, W - 1), c1 = min(x0 + x + 1, W - 1);
+    const bool edge = (threadIdx.x & 31) == 31 || x == N - 1;
+    int off = y0 * W;  // H * W < 2^31
+    float top = __ldg(img + off + c0);
+    float topr = __shfl_down_sync(0xffffffffu, top, 1);
+    if (edge) topr = __ldg(img + off + c1);
+    float ht = fmaf(tx, topr - top, top);
+#pragma unroll
+    for (int p = 0; p < N; ++p) {
+        off = min(y0 + p + 1, H - 1) * W;
+        const float bot = __ldg(img + off + c0);
+        float botr = __shfl_down_sync(0xffffffffu, bot, 1);
+        if (edge) botr = __ldg(img + off + c1);
+        const float hb = fmaf(tx, botr - bot, bot);
+        const float v = fmaf(ty, hb - ht, ht);
+        if (IMAG) z[p].y = v; else z[p].x = v;
+        ht = hb;
+    }
 }
 
 __device__ __forceinline__ void wg_sync(int wg) { asm volatile("bar.sync %0, 128;" ::"r"(wg + 1) : "memory"); }
@@ -106,6 +142,7 @@ __global__ void __launch_bounds__(TcCfg<N>::THREADS, 1)
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem + C::BAR_OFF) + wg;
     uint32_t* tbase = reinterpret_cast<uint32_t*>(smem + C::BAR_OFF + 8 * C::NWG);
     int* s_hw = reinterpret_cast<int*>(smem + C::BAR_OFF + 8 * C::NWG + 16) + wg * C::WPT * 4;
+    float* zst = reinterpret_cast<float*>(smem + C::ZST_OFF) + (size_t)wg * C::WPT * 4 * N;
 
     for (int j = threadIdx.x; j < (int)(2 * C::MAT_BYTES / 16); j += C::THREADS)
         reinterpret_cast<uint4*>(smem)[j] = mats[j];
@@ -152,8 +189,8 @@ __global__ void __launch_bounds__(TcCfg<N>::THREADS, 1)
 
         // ------------------------------------------------ sampling (lane = column q of window c)
         float2 z[N];
-        sample_column_direct<N, 1, false>(prm.img_a, prm.H, prm.W, org.x, org.y, q, 0, z);
-        sample_column_direct<N, 1, true>(prm.img_b, prm.H, prm.W, org.z, org.w, q, 0, z);
+        sample_rows<N, false>(prm.img_a, prm.H, prm.W, org.x, org.y, q, z);
+        sample_rows<N, true>(prm.img_b, prm.H, prm.W, org.z, org.w, q, z);
         float2 e;
         {
             float2 s = make_float2(0.f, 0.f);
@@ -241,8 +278,8 @@ __global__ void __launch_bounds__(TcCfg<N>::THREADS, 1)
 
         // ------------------------------------------------ spectra -> cross spectrum -> I1 operand
         {
-            const int kxp = q >> 1, fr = q & 1;  // row (w, kx', frame)
-            const bool dcrow = kxp == 0;
+            const int fr = q & 1;  // row (w, kx' = q/2, frame fr)
+            const bool dcrow = q < 2;
             float zr[N], zi[N];
 #pragma unroll
             for (int j = 0; j < N; j += 16) {
@@ -250,42 +287,62 @@ __global__ void __launch_bounds__(TcCfg<N>::THREADS, 1)
                 tc::tmem_ld16(trow + N + j, zi + j);
             }
             tc::wait_ld();
+            if (dcrow) {  // DC + i*Nyquist rows: staged for the separation below
+                float* st = zst + (c * 2 + fr) * 2 * N;
+#pragma unroll
+                for (int j = 0; j < N; j += 4) {
+                    *reinterpret_cast<float4*>(st + j) = make_float4(zr[j], zr[j + 1], zr[j + 2], zr[j + 3]);
+                    *reinterpret_cast<float4*>(st + N + j) = make_float4(zi[j], zi[j + 1], zi[j + 2], zi[j + 3]);
+                }
+            }
+            // conj(FA) * FB with FA from the frame-0 lane and FB from the frame-1 lane (lane ^ 1)
 #pragma unroll
             for (int j = 0; j < N / 8; ++j) {
                 float pr[8], pi[8];
 #pragma unroll
                 for (int t = 0; t < 8; ++t) {
-                    const int ky = 8 * j + t, my = (N - ky) % N;
-                    // own frame's spectrum at (kx', ky); the DC row also yields the Nyquist row
-                    float ar = zr[ky], ai = zi[ky], br = 0.f, bi = 0.f;
-                    if (dcrow) {
-                        ar = 0.5f * (zr[ky] + zr[my]);
-                        ai = 0.5f * (zi[ky] - zi[my]);
-                        br = 0.5f * (zi[ky] + zi[my]);
-                        bi = 0.5f * (zr[my] - zr[ky]);
-                        if (ky == 0) ar = ai = 0.f;  // mean removed: DC bin is zero
-                    }
-                    const float oar = __shfl_xor_sync(0xffffffffu, ar, 1), oai = __shfl_xor_sync(0xffffffffu, ai, 1);
-                    const float obr = __shfl_xor_sync(0xffffffffu, br, 1), obi = __shfl_xor_sync(0xffffffffu, bi, 1);
-                    // FA from the frame-0 lane, FB from the frame-1 lane
-                    const float far_ = fr ? oar : ar, fai = fr ? oai : ai, fbr = fr ? ar : oar, fbi = fr ? ai : oai;
-                    const float gar = fr ? obr : br, gai = fr ? obi : bi, gbr = fr ? br : obr, gbi = fr ? bi : obi;
-                    float cr = far_ * fbr + fai * fbi, ci = far_ * fbi - fai * fbr;  // conj(FA) * FB
-                    if (dcrow) {
-                        const float nr = gar * gbr + gai * gbi, ni = gar * gbi - gai * gbr;
-                        const float t0 = cr - ni, t1 = ci + nr;  // C(0, ky) + i C(N/2, ky)
-                        cr = t0;
-                        ci = t1;
-                    }
-                    if (fr && (ky & 1)) {
-                        cr = -cr;
-                        ci = -ci;
-                    }
-                    pr[t] = cr;
-                    pi[t] = ci;
+                    const int ky = 8 * j + t;
+                    const float oar = __shfl_xor_sync(0xffffffffu, zr[ky], 1);
+                    const float oai = __shfl_xor_sync(0xffffffffu, zi[ky], 1);
+                    const float far_ = fr ? oar : zr[ky], fai = fr ? oai : zi[ky];
+                    const float fbr = fr ? zr[ky] : oar, fbi = fr ? zi[ky] : oai;
+                    const float sg = (fr && (ky & 1)) ? -1.0f : 1.0f;  // frame-1 lane: (-1)^ky
+                    pr[t] = sg * (far_ * fbr + fai * fbi);
+                    pi[t] = sg * (far_ * fbi - fai * fbr);
                 }
-                store_split(a_hi, a_lo, kmaj_chunk(128, i, 8 * j), pr);
-                store_split(a_hi, a_lo, kmaj_chunk(128, i, N + 8 * j), pi);
+                if (!dcrow) {
+                    store_split(a_hi, a_lo, kmaj_chunk(128, i, 8 * j), pr);
+                    store_split(a_hi, a_lo, kmaj_chunk(128, i, N + 8 * j), pi);
+                }
+            }
+        }
+        wg_sync(wg);  // staged DC rows complete
+        {
+            // Lane q of window c separates column ky = q of the DC + i*Nyquist rows of both frames:
+            // F(0, ky) = (Z + conj Z[-ky]) / 2, F(N/2, ky) = (Z - conj Z[-ky]) / 2i, the DC bin
+            // zeroed (mean removal), and writes C(0, ky) + i C(N/2, ky) into rows (w, 0, 0) and,
+            // times (-1)^ky, (w, 0, 1).
+            const int ky = q, my = (N - q) % N;
+            const float* sa = zst + (c * 2 + 0) * 2 * N;
+            const float* sb = zst + (c * 2 + 1) * 2 * N;
+            float a0r = 0.5f * (sa[ky] + sa[my]), a0i = 0.5f * (sa[N + ky] - sa[N + my]);
+            const float anr = 0.5f * (sa[N + ky] + sa[N + my]), ani = 0.5f * (sa[my] - sa[ky]);
+            float b0r = 0.5f * (sb[ky] + sb[my]), b0i = 0.5f * (sb[N + ky] - sb[N + my]);
+            const float bnr = 0.5f * (sb[N + ky] + sb[N + my]), bni = 0.5f * (sb[my] - sb[ky]);
+            if (ky == 0) a0r = a0i = b0r = b0i = 0.0f;
+            const float c0r = a0r * b0r + a0i * b0i, c0i = a0r * b0i - a0i * b0r;
+            const float cnr = anr * bnr + ani * bni, cni = anr * bni - ani * bnr;
+            const float prr = c0r - cni, pri = c0i + cnr;
+            const float sg = (ky & 1) ? -1.0f : 1.0f;
+            const float vals[4] = {prr, pri, sg * prr, sg * pri};
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int row = c * N + (u >> 1), k = (u & 1) * N + ky;
+                const uint32_t off = kmaj_chunk(128, row, k) + (k & 7) * 2;
+                const __nv_bfloat16 h = __float2bfloat16_rn(vals[u]);
+                const __nv_bfloat16 l = __float2bfloat16_rn(vals[u] - __bfloat162float(h));
+                *reinterpret_cast<__nv_bfloat16*>(a_hi + off) = h;
+                *reinterpret_cast<__nv_bfloat16*>(a_lo + off) = l;
             }
         }
         sync_for_mma();
@@ -338,9 +395,12 @@ __global__ void __launch_bounds__(TcCfg<N>::THREADS, 1)
         const int y = q;
         float* prow = plane + (size_t)(c * N) * C::PLD;  // window c's plane
 #pragma unroll
-        for (int x = 0; x < N; ++x) {
-            v[x] = v[x] * scale;
-            prow[y * C::PLD + x] = v[x];
+        for (int x = 0; x < N; x += 4) {
+            v[x] *= scale;
+            v[x + 1] *= scale;
+            v[x + 2] *= scale;
+            v[x + 3] *= scale;
+            *reinterpret_cast<float4*>(prow + y * C::PLD + x) = make_float4(v[x], v[x + 1], v[x + 2], v[x + 3]);
         }
         // argmax, lowest row-major index on ties
         float best = -INFINITY;
@@ -375,22 +435,37 @@ __global__ void __launch_bounds__(TcCfg<N>::THREADS, 1)
             const float* up = prow + ((y + N - 1) % N) * C::PLD;
             const float* dn = prow + ((y + 1) % N) * C::PLD;
 #pragma unroll
-            for (int x = 0; x < N; ++x) vm[x] = fmaxf(fmaxf(up[x], dn[x]), v[x]);
+            for (int x = 0; x < N; x += 4) {
+                const float4 a4 = *reinterpret_cast<const float4*>(up + x), b4 = *reinterpret_cast<const float4*>(dn + x);
+                vm[x] = fmaxf(fmaxf(a4.x, b4.x), v[x]);
+                vm[x + 1] = fmaxf(fmaxf(a4.y, b4.y), v[x + 1]);
+                vm[x + 2] = fmaxf(fmaxf(a4.z, b4.z), v[x + 2]);
+                vm[x + 3] = fmaxf(fmaxf(a4.w, b4.w), v[x + 3]);
+            }
         }
         wg_sync(wg);  // footprints written
         const int hw = max(max(s_hw[c * 4 + 0], s_hw[c * 4 + 1]), max(s_hw[c * 4 + 2], s_hw[c * 4 + 3]));
         const int ex = max((int)ceilf(1.5f * (float)hw), 2);
         float second = -INFINITY;
         {
-            auto circ = [](int a, int b) {
-                const int d = abs(a - b);
-                return min(d, N - d);
-            };
-            const int cy = circ(y, by);
+            // columns outside the footprint: circular distance from bx above ex, or every column
+            // when this row is already farther than ex from by
+            const int dy = abs(y - by), cy = min(dy, N - dy);
+            uint32_t allowed = 0xffffffffu;
+            if (cy <= ex) {
+                uint32_t band = 0xffffffffu;  // columns bx - ex .. bx + ex (circular)
+                if (2 * ex + 1 < N) {
+                    const uint32_t run = (1u << (2 * ex + 1)) - 1u;
+                    const int s0 = (bx - ex + N) % N;
+                    band = (run << s0) | (s0 ? run >> (N - s0) : 0u);
+                    if constexpr (N < 32) band &= (1u << (N & 31)) - 1u;
+                }
+                allowed = ~band;
+            }
 #pragma unroll
             for (int x = 0; x < N; ++x) {
                 const float h = fmaxf(fmaxf(vm[(x + N - 1) % N], vm[(x + 1) % N]), vm[x]);
-                if (v[x] == h && max(cy, circ(x, bx)) > ex) second = fmaxf(second, v[x]);
+                if (v[x] == h && (allowed & (1u << x))) second = fmaxf(second, v[x]);
             }
         }
 #pragma unroll
