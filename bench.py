@@ -116,12 +116,16 @@ def run_stream(args, wl):
     import torch
 
     import piv_b200 as P
-    dev = torch.device("cuda", 0)
-    torch.cuda.set_device(0)
-    frames = make_stream(wl)
+    from piv_b200.replicas import Ranks
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(local)
+    ranks = Ranks(backend="nccl", device=dev)
+    # replicas: every rank analyses its own stream (weak scaling), nothing crosses GPUs
+    frames = make_stream(dict(wl, seed=wl["seed"] + 101 * ranks.rank))
     nf, h, w = frames.shape
     k = nf - 1
-    an = P.PivAnalyzer(piv_config(wl), device=0)
+    an = P.PivAnalyzer(piv_config(wl), device=local)
     fa, fb = an.prepare(frames[0], P.RAW), an.prepare(frames[1], P.RAW)
     tuned = an.autotune(fa, fb) if not args.no_autotune else {}
     batch = P.PivBatch(an, h, w, k, sequential=True)
@@ -134,10 +138,12 @@ def run_stream(args, wl):
     for _ in range(args.warmup):
         batch.run()
     batch.sync()
-    gpu_uuid = str(torch.cuda.get_device_properties(0).uuid)
+    gpu_uuid = str(torch.cuda.get_device_properties(local).uuid)
     sampler = ClockSampler(gpu_uuid if gpu_uuid.startswith("GPU-") else f"GPU-{gpu_uuid}")
     sampler.start()
     time.sleep(0.3)
+    ranks.barrier()
+    torch.cuda.synchronize()
     t0 = time.perf_counter()
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
     ev[0].record(bstream)
@@ -147,32 +153,38 @@ def run_stream(args, wl):
     ev[1].synchronize()
     wall = time.perf_counter() - t0
     clocks = sampler.stop()
-    ms = ev[0].elapsed_time(ev[1])
-    value = args.steps * nvec / (ms * 1e-3)
+    ms = ranks.max(ev[0].elapsed_time(ev[1]))
+    value = ranks.world * args.steps * nvec / (ms * 1e-3)
     # end to end: pinned host frames -> input slab -> graph -> results to host, every step
     pin = torch.from_numpy(frames.view(np.int16)).pin_memory().numpy().view(np.uint16)
     res = batch.run_host(pin)
     ev2 = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
     e2e_steps = max(3, args.steps // 4)
+    ranks.barrier()
+    torch.cuda.synchronize()
     ev2[0].record(bstream)
     for _ in range(e2e_steps):
         res = batch.run_host(pin)
     ev2[1].record(bstream)
     ev2[1].synchronize()
-    e2e_ms = ev2[0].elapsed_time(ev2[1])
-    line = {"metric": METRIC, "value": value, "unit": "vectors/s", "n_gpus": 1, "steps": args.steps,
+    e2e_ms = ranks.max(ev2[0].elapsed_time(ev2[1]))
+    line = {"metric": METRIC, "value": value, "unit": "vectors/s", "n_gpus": ranks.world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": wl["name"], "frames_per_step": nf, "pairs_per_step": k,
                        "final_pass_vectors_per_pair": final_vectors(wl), "windows": pass_windows(wl),
                        "l2": "inputs > L2: 33 frames = 66 MiB of samples + 132 MiB prepared per step"},
-            "e2e": {"value": e2e_steps * nvec / (e2e_ms * 1e-3), "unit": "vectors/s",
+            "e2e": {"value": ranks.world * e2e_steps * nvec / (e2e_ms * 1e-3), "unit": "vectors/s",
                     "h2d_bytes_per_step": int(pin.nbytes), "d2h_bytes_per_step": int(nvec * 13 + k * 40),
                     "ms_per_step": e2e_ms / e2e_steps},
             "gpu_launches": int(batch.kernels() * args.steps), "graph_launches": args.steps,
             "clocks": clocks, "autotuned_variants": tuned, "wall_ms_per_step": 1e3 * wall / args.steps,
-            "valid_fraction_last_pair": float(np.mean((res[-1].field.flags & P.flags.INVALID) == 0))}
-    print(json.dumps(line), flush=True)
+            "valid_fraction_last_pair": float(np.mean((res[-1].field.flags & P.flags.INVALID) == 0)),
+            "parallelism": f"replicas x{ranks.world}"}
+    if ranks.rank == 0:
+        print(json.dumps(line), flush=True)
+    del batch
+    ranks.close()
     return 0
 
 
@@ -187,8 +199,12 @@ def run_serving(args, wl):
 
     import piv_b200 as P
     from piv_b200 import synthetic as S
-    torch.cuda.set_device(0)
-    rng = np.random.default_rng(wl["seed"])
+    from piv_b200.replicas import Ranks
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    ranks = Ranks(backend="nccl", device=torch.device("cuda", local))
+    # replicas: every rank serves its own Poisson stream on its own GPU
+    rng = np.random.default_rng(wl["seed"] + 101 * ranks.rank)
     duration = args.duration if args.duration else wl["duration"]
     pool = {}
     for si, (h, w) in enumerate(wl["sizes"]):
@@ -205,7 +221,7 @@ def run_serving(args, wl):
              for _ in range(n)]
     vec = {(si, ci): len(P.Grid.new(wl["sizes"][si][0], wl["sizes"][si][1], cfgs[ci].windows[-1], cfgs[ci].overlap))
            for si in range(len(wl["sizes"])) for ci in range(len(cfgs))}
-    sv = P.PivServer(memory_budget_bytes=wl["budget"], max_in_flight=wl["max_in_flight"], device=0)
+    sv = P.PivServer(memory_budget_bytes=wl["budget"], max_in_flight=wl["max_in_flight"], device=local)
     # warm-up: one request of every kind
     for si in range(len(wl["sizes"])):
         for ci in range(len(cfgs)):
@@ -227,10 +243,11 @@ def run_serving(args, wl):
 
     wt = th.Thread(target=waiter)
     wt.start()
-    gpu_uuid = str(torch.cuda.get_device_properties(0).uuid)
+    gpu_uuid = str(torch.cuda.get_device_properties(local).uuid)
     sampler = ClockSampler(gpu_uuid if gpu_uuid.startswith("GPU-") else f"GPU-{gpu_uuid}")
     sampler.start()
     s0 = sv.stats()
+    ranks.barrier()
     t0 = time.perf_counter()
     for i in range(n):
         now = time.perf_counter() - t0
@@ -244,21 +261,27 @@ def run_serving(args, wl):
     clocks = sampler.stop()
     s1 = sv.stats()
     sv.close()
-    total_vec = sum(vec[(si, ci)] for si, ci, _ in kinds)
-    lat_a = np.array(lat)
-    line = {"metric": METRIC, "value": total_vec / span, "unit": "vectors/s", "n_gpus": 1, "steps": n, "warmup": 9,
-            "ms_per_step": 1e3 * span / max(n, 1), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic",
-            "config": {"workload": wl["name"], "requests": n, "duration_s": duration, "rate_per_s": wl["rate"]},
+    total_vec = ranks.sum(sum(vec[(si, ci)] for si, ci, _ in kinds))
+    span = ranks.max(span)
+    n_all = int(ranks.sum(n))
+    launches = ranks.sum(s1["kernel_launches"] - s0["kernel_launches"])
+    lat_a = np.concatenate([np.asarray(x) for x in ranks.gather(lat)])
+    line = {"metric": METRIC, "value": total_vec / span, "unit": "vectors/s", "n_gpus": ranks.world, "steps": n_all,
+            "warmup": 9, "ms_per_step": 1e3 * span / max(n_all, 1), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": wl["name"], "requests": n_all, "duration_s": duration,
+                       "rate_per_s": wl["rate"] * ranks.world, "parallelism": f"replicas x{ranks.world}"},
             "latency_ms": {"p50": float(np.percentile(lat_a, 50)), "p90": float(np.percentile(lat_a, 90)),
                            "p99": float(np.percentile(lat_a, 99)), "max": float(lat_a.max()), "mean": float(lat_a.mean())},
-            "achieved_rate_per_s": n / span,
+            "achieved_rate_per_s": n_all / span,
             "e2e": {"value": total_vec / span, "unit": "vectors/s",
                     "h2d_bytes_per_step": int(np.mean([pool[(si, pj)][0].nbytes * 2 for si, _, pj in kinds])),
                     "d2h_bytes_per_step": int(np.mean([vec[(si, ci)] * 13 for si, ci, _ in kinds]))},
-            "gpu_launches": int(s1["kernel_launches"] - s0["kernel_launches"]), "server_steps": int(s1["steps"] - s0["steps"]),
+            "gpu_launches": int(launches), "server_steps": int(s1["steps"] - s0["steps"]),
             "clocks": clocks}
-    print(json.dumps(line), flush=True)
+    if ranks.rank == 0:
+        print(json.dumps(line), flush=True)
+    ranks.close()
     return 0
 
 
@@ -518,18 +541,15 @@ def main():
         return run_serving(args, wl)
 
     import torch
-    import torch.distributed as dist
 
     import piv_b200 as P
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
+    from piv_b200.replicas import Ranks
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+    ranks = Ranks(backend="nccl", device=dev)
+    rank, world = ranks.rank, ranks.world
 
     # ---------------------------------------------------------------- inputs (host, then device)
     a0, b0 = make_inputs(wl, seed_offset=rank)
@@ -574,8 +594,7 @@ def main():
     an.set_profiling(True)
     for p in range(npass):
         an.profile(p)  # reset
-    if world > 1:
-        dist.barrier()
+    ranks.barrier()
     torch.cuda.synchronize()
     gpu_uuid = str(torch.cuda.get_device_properties(local).uuid)
     sampler = ClockSampler(gpu_uuid if gpu_uuid.startswith("GPU-") else f"GPU-{gpu_uuid}")
@@ -594,11 +613,7 @@ def main():
     ms = e0.elapsed_time(e1)
     corr = [an.profile(p) for p in range(npass)]
     an.set_profiling(False)
-    ms_t = torch.tensor([ms], device=dev, dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-        dist.barrier()
-    ms_max = float(ms_t.item())
+    ms_max = ranks.max(ms)
     value = world * args.steps * nvec / (ms_max * 1e-3)
 
     # ---------------------------------------------------------------- timed: end to end (host buffers)
@@ -625,8 +640,7 @@ def main():
     for i in range(args.warmup):
         e2e_step(i)
     e2e_steps = max(3, args.steps // 4)
-    if world > 1:
-        dist.barrier()
+    ranks.barrier()
     torch.cuda.synchronize()
     e2 = torch.cuda.Event(enable_timing=True)
     e3 = torch.cuda.Event(enable_timing=True)
@@ -637,11 +651,8 @@ def main():
     e3.record(stream)
     e3.synchronize()
     t_wall = time.perf_counter() - t_wall
-    ms2 = e2.elapsed_time(e3)
-    ms2_t = torch.tensor([ms2], device=dev, dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(ms2_t, op=dist.ReduceOp.MAX)
-    e2e_value = world * e2e_steps * nvec / (float(ms2_t.item()) * 1e-3)
+    ms2 = ranks.max(e2.elapsed_time(e3))
+    e2e_value = world * e2e_steps * nvec / (ms2 * 1e-3)
     h2d = sum(x.nbytes for x in pin[0])
     d2h = hdx.nbytes + hdy.nbytes + hppr.nbytes + hfl.nbytes + 5 * 8
 
@@ -680,7 +691,7 @@ def main():
                        "l2": "inputs > L2: 2 alternating pairs, 192 MiB of samples + prepared images per step"},
             "e2e": {"value": e2e_value, "unit": "vectors/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
-                    "ms_per_step": float(ms2_t.item()) / e2e_steps, "wall_ms_per_step": 1e3 * t_wall / e2e_steps},
+                    "ms_per_step": ms2 / e2e_steps, "wall_ms_per_step": 1e3 * t_wall / e2e_steps},
             "gpu_launches": int(launches), "roofline": roof, "clocks": clocks, "autotuned_variants": tuned}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(wl, a0, b0, single_s=4.0)
@@ -688,9 +699,7 @@ def main():
     if rank == 0:
         print(json.dumps(line), flush=True)
     an.close()
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    ranks.close()
     return 0
 
 

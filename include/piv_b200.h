@@ -321,6 +321,35 @@ int32_t piv_validate_field(PivAnalyzer* an, int64_t ny, int64_t nx, const float*
                            const float* peak_ratio, const uint8_t* flags, float* out_dx, float* out_dy,
                            uint8_t* out_flags, PivSummaryC* summary);
 
+/* ----------------------------------------------------------------------------- post-processing
+ * The path's next components, on DEVICE arrays of validated fields (row-major [ny, nx] per pair,
+ * pairs stacked [nt, ny, nx]); work is queued on `stream` (NULL = default stream).
+ *
+ * piv_flow_stats_device: FlowStats of one pair (flowstats.rs:67-101) in px/s units from
+ * displacements in px (flow.rs:20-36: u = dx * f32(1/dt_s)), over the usable vectors (finite,
+ * accepted or REPLACED: flow.rs:13-17); `step` is the grid spacing in px. `vorticity` (nullable,
+ * device, [ny, nx]) receives the vorticity field (flowstats.rs:44-64). Blocking. */
+typedef struct {
+    float vorticity_mean, vorticity_abs_mean, ke_mean, ke_sum, coverage;
+    int64_t n_usable, n_vorticity;
+} PivFlowStatsC;
+int32_t piv_flow_stats_device(int64_t ny, int64_t nx, int64_t step, double dt_s, const float* dx, const float* dy,
+                              const uint8_t* flags, float* vorticity, PivFlowStatsC* stats, void* stream);
+/* temporal (smooth.rs:44-128): moving mean (median = 0) or median over `window` (odd, <= 63)
+ * consecutive pairs; `usable` marks contributing raw vectors, `gate` where outputs are wanted;
+ * outputs with fewer than min_support contributions are NaN; `leave_out` lists time offsets to
+ * skip (each non-zero one replaced by the next further out). Asynchronous. */
+int32_t piv_temporal_smooth_device(int64_t nt, int64_t ny, int64_t nx, const float* dx, const float* dy,
+                                   const uint8_t* usable, const uint8_t* gate, int32_t median, int32_t window,
+                                   int32_t min_support, const int32_t* leave_out, int32_t n_leave_out, float* out_dx,
+                                   float* out_dy, uint16_t* support, void* stream);
+/* spatial (smooth.rs:130-207): Gaussian normalized convolution of each pair's field, sigma in
+ * grid cells (<= 12), outputs need min_weight of the kernel's weight; leave_out < 0: none, else
+ * the Chebyshev radius left out. Asynchronous. */
+int32_t piv_spatial_smooth_device(int64_t nt, int64_t ny, int64_t nx, const float* dx, const float* dy,
+                                  const uint8_t* gate, float sigma, float min_weight, int32_t leave_out, float* out_dx,
+                                  float* out_dy, uint16_t* support, void* stream);
+
 /* Diagnostics (no counterpart in the reference): D (128 x n) = A (128 x k) * B (n x k)^T on the
  * tensor cores of `device` with BF16 operands (inputs rounded to BF16) and FP32 accumulation, A
  * stored K-major (a_mn = 0) or MN-major (a_mn = 1) as the tensor-core correlation stores its

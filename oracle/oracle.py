@@ -93,6 +93,14 @@ def lib():
         L.orc_correlate_pass_deform.argtypes = [_f32p, _f32p, _f32p, _f32p, _i64, _i64, ctypes.POINTER(OrcGrid), _f32p,
                                                 _f32p, ctypes.c_float, ctypes.c_float, ctypes.c_int, ctypes.c_int, _f32p,
                                                 _f32p, _f32p, _u8p]
+        L.orc_usable.argtypes = [_f32p, _u8p, _i64, _u8p]
+        L.orc_vorticity.argtypes = [_f32p, _f32p, _u8p, _i64, _i64, ctypes.c_float, _f32p]
+        L.orc_flow_stats.argtypes = [_f32p, _f32p, _u8p, _i64, _i64, ctypes.c_float, ctypes.POINTER(OrcFlowStats)]
+        L.orc_pair_stats.argtypes = [_f32p, _f32p, _u8p, _i64, _i64, _i64, ctypes.c_double, ctypes.POINTER(OrcFlowStats)]
+        L.orc_temporal.argtypes = [_f32p, _f32p, _u8p, _u8p, _i64, _i64, _i64, ctypes.c_int32, ctypes.c_int32,
+                                   ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32, _f32p, _f32p, ctypes.c_void_p]
+        L.orc_spatial.argtypes = [_f32p, _f32p, _u8p, _i64, _i64, _i64, ctypes.c_float, ctypes.c_float, ctypes.c_int32,
+                                  _f32p, _f32p, ctypes.c_void_p]
         L.orc_splitmix_next.argtypes = [ctypes.POINTER(ctypes.c_uint64)]
         L.orc_splitmix_next.restype = ctypes.c_uint64
         _lib = L
@@ -321,3 +329,66 @@ def analyze(cfg: OracleConfig, image_a, image_b, base_a=None, base_b=None, mode=
                                flags=tr["flags"][sl].reshape(sh)))
             off += c
     return dict(dx=fdx, dy=fdy, ppr=fppr, flags=ffl), s.as_dict(), traces
+
+
+# --------------------------------------------------------------------------------- post-processing
+class OrcFlowStats(ctypes.Structure):
+    _fields_ = [("vorticity_mean", ctypes.c_float), ("vorticity_abs_mean", ctypes.c_float), ("ke_mean", ctypes.c_float),
+                ("ke_sum", ctypes.c_float), ("coverage", ctypes.c_float), ("n_usable", ctypes.c_int64),
+                ("n_vorticity", ctypes.c_int64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+def _b(a):
+    return np.ascontiguousarray(a, dtype=np.uint8)
+
+
+def usable(dx, flags):
+    dx, flags = _f(dx), _b(flags)
+    out = np.empty(dx.shape, np.uint8)
+    lib().orc_usable(dx.ravel(), flags.ravel(), dx.size, out.reshape(-1))
+    return out.astype(bool)
+
+
+def vorticity(u, v, ok, step):
+    u, v = _f(u), _f(v)
+    out = np.empty(u.shape, np.float32)
+    lib().orc_vorticity(u, v, _b(ok), u.shape[0], u.shape[1], step, out)
+    return out
+
+
+def flow_stats(u, v, ok, step):
+    u, v = _f(u), _f(v)
+    s = OrcFlowStats()
+    lib().orc_flow_stats(u, v, _b(ok), u.shape[0], u.shape[1], step, ctypes.byref(s))
+    return s.as_dict()
+
+
+def pair_stats(dx, dy, flags, step, dt_s):
+    dx, dy = _f(dx), _f(dy)
+    s = OrcFlowStats()
+    lib().orc_pair_stats(dx, dy, _b(flags), dx.shape[0], dx.shape[1], int(step), float(dt_s), ctypes.byref(s))
+    return s.as_dict()
+
+
+def temporal(dx, dy, ok, gate, median, window, min_support, leave_out=()):
+    dx, dy = _f(dx), _f(dy)
+    nt, ny, nx = dx.shape
+    lo = np.ascontiguousarray(leave_out, np.int32)
+    ox, oy = np.empty_like(dx), np.empty_like(dy)
+    sup = np.empty(dx.shape, np.uint16)
+    lib().orc_temporal(dx, dy, _b(ok), _b(gate), nt, ny, nx, int(bool(median)), int(window), int(min_support),
+                       _ptr(lo) if lo.size else None, int(lo.size), ox, oy, _ptr(sup))
+    return ox, oy, sup
+
+
+def spatial(dx, dy, gate, sigma, min_weight, leave_out=None):
+    dx, dy = _f(dx), _f(dy)
+    nt, ny, nx = dx.shape
+    ox, oy = np.empty_like(dx), np.empty_like(dy)
+    sup = np.empty(dx.shape, np.uint16)
+    lib().orc_spatial(dx, dy, _b(gate), nt, ny, nx, float(sigma), float(min_weight),
+                      -1 if leave_out is None else int(leave_out), ox, oy, _ptr(sup))
+    return ox, oy, sup

@@ -986,6 +986,231 @@ int orc_analyze(const OrcConfig* cfg, const float* image_a, const float* image_b
     return ORC_OK;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Post-processing of validated fields (the path's next components).
+// ---------------------------------------------------------------------------------------------
+void orc_usable(const float* dx, const uint8_t* flags, int64_t n, uint8_t* usable) {
+    // flow.rs:13-17: finite and accepted, or interpolated (REPLACED)
+    for (int64_t i = 0; i < n; ++i)
+        usable[i] = std::isfinite(dx[i]) && ((flags[i] & INVALID) == 0 || (flags[i] & REPLACED) != 0);
+}
+
+extern "C++" {
+namespace {
+// flowstats.rs:28-39: central difference where both neighbours are usable, one-sided otherwise.
+template <class At>
+bool derivative(int64_t i, int64_t n, float h, At at, float* out) {
+    float c, l, r;
+    if (!at(i, &c)) return false;
+    const bool hl = i >= 1 && at(i - 1, &l);
+    const bool hr = i + 1 < n && at(i + 1, &r);
+    if (hl && hr) *out = (r - l) / (2.0f * h);
+    else if (hl) *out = (c - l) / h;
+    else if (hr) *out = (r - c) / h;
+    else return false;
+    return true;
+}
+}  // namespace
+}  // extern "C++"
+
+void orc_vorticity(const float* u, const float* v, const uint8_t* usable, int64_t ny, int64_t nx, float step,
+                   float* w) {
+    // flowstats.rs:44-64: w = du/dy - dv/dx (image axes), NaN where either derivative is missing
+    auto get = [&](const float* a, int64_t iy, int64_t ix, float* o) {
+        const float x = a[iy * nx + ix];
+        if (!(usable[iy * nx + ix] && std::isfinite(x))) return false;
+        *o = x;
+        return true;
+    };
+    for (int64_t iy = 0; iy < ny; ++iy)
+        for (int64_t ix = 0; ix < nx; ++ix) {
+            float a, b;
+            const bool ha = derivative(iy, ny, step, [&](int64_t j, float* o) { return get(u, j, ix, o); }, &a);
+            const bool hb = derivative(ix, nx, step, [&](int64_t j, float* o) { return get(v, iy, j, o); }, &b);
+            w[iy * nx + ix] = (ha && hb) ? a - b : NAN;
+        }
+}
+
+void orc_flow_stats(const float* u, const float* v, const uint8_t* usable, int64_t ny, int64_t nx, float step,
+                    OrcFlowStats* out) {
+    // flowstats.rs:67-101
+    std::vector<float> w((size_t)(ny * nx));
+    orc_vorticity(u, v, usable, ny, nx, step, w.data());
+    double ws = 0.0, wa = 0.0, e = 0.0;
+    int64_t nw = 0, n = 0;
+    for (float x : w)
+        if (std::isfinite(x)) {
+            ws += (double)x;
+            wa += (double)std::fabs(x);
+            ++nw;
+        }
+    for (int64_t i = 0; i < ny * nx; ++i)
+        if (usable[i] && std::isfinite(u[i]) && std::isfinite(v[i])) {
+            e += 0.5 * ((double)u[i] * (double)u[i] + (double)v[i] * (double)v[i]);
+            ++n;
+        }
+    auto mean = [](double s, int64_t k) { return k > 0 ? (float)(s / (double)k) : NAN; };
+    out->vorticity_mean = mean(ws, nw);
+    out->vorticity_abs_mean = mean(wa, nw);
+    out->ke_mean = mean(e, n);
+    out->ke_sum = (float)(e * std::pow((double)step, 2.0));
+    out->coverage = (float)n / (float)std::max<int64_t>(ny * nx, 1);
+    out->n_usable = n;
+    out->n_vorticity = nw;
+}
+
+void orc_pair_stats(const float* dx, const float* dy, const uint8_t* flags, int64_t ny, int64_t nx, int64_t step,
+                    double dt_s, OrcFlowStats* out) {
+    // flow.rs:20-36: px/s from px with k = (1 / dt) as f32
+    const int64_t n = ny * nx;
+    const float k = (float)(1.0 / dt_s);
+    std::vector<float> u((size_t)n), v((size_t)n);
+    std::vector<uint8_t> us((size_t)n);
+    for (int64_t i = 0; i < n; ++i) {
+        u[i] = dx[i] * k;
+        v[i] = dy[i] * k;
+    }
+    orc_usable(dx, flags, n, us.data());
+    orc_flow_stats(u.data(), v.data(), us.data(), ny, nx, (float)step, out);
+}
+
+extern "C++" {
+namespace {
+float mean_seq(const float* v, int n) {
+    float s = 0.0f;
+    for (int i = 0; i < n; ++i) s += v[i];
+    return s / (float)n;
+}
+float median_sorted(float* v, int n) {
+    std::sort(v, v + n, [](float a, float b) { return a < b; });
+    return (n % 2 == 1) ? v[n / 2] : 0.5f * (v[n / 2 - 1] + v[n / 2]);
+}
+}  // namespace
+}  // extern "C++"
+
+int orc_temporal_offsets(int32_t window, const int32_t* leave_out, int32_t n_leave, int32_t* offsets) {
+    // smooth.rs:59-73: centre unless left out, then half offsets each side skipping left-out ones
+    auto left = [&](int32_t o) {
+        for (int32_t i = 0; i < n_leave; ++i)
+            if (leave_out[i] == o) return true;
+        return false;
+    };
+    int c = 0;
+    if (!left(0)) offsets[c++] = 0;
+    const int32_t half = window / 2;
+    for (int32_t sign : {-1, 1}) {
+        int32_t k = 1, taken = 0;
+        while (taken < half) {
+            if (!left(sign * k)) {
+                offsets[c++] = sign * k;
+                ++taken;
+            }
+            ++k;
+        }
+    }
+    return c;
+}
+
+void orc_temporal(const float* dx, const float* dy, const uint8_t* usable, const uint8_t* gate, int64_t nt,
+                  int64_t ny, int64_t nx, int32_t median, int32_t window, int32_t min_support, const int32_t* leave_out,
+                  int32_t n_leave, float* out_dx, float* out_dy, uint16_t* support) {
+    // smooth.rs:44-128
+    std::vector<int32_t> off((size_t)window + 1);
+    const int no = orc_temporal_offsets(window, leave_out, n_leave, off.data());
+    const int64_t plane = ny * nx;
+    std::vector<float> bu((size_t)no), bv((size_t)no);
+    for (int64_t t = 0; t < nt; ++t)
+        for (int64_t k = 0; k < plane; ++k) {
+            const int64_t o = t * plane + k;
+            out_dx[o] = NAN;
+            out_dy[o] = NAN;
+            support[o] = 0;
+            if (!gate[o]) continue;
+            int c = 0;
+            for (int j = 0; j < no; ++j) {
+                const int64_t s = t + off[j];
+                if (s < 0 || s >= nt || !usable[s * plane + k]) continue;
+                bu[c] = dx[s * plane + k];
+                bv[c] = dy[s * plane + k];
+                ++c;
+            }
+            support[o] = (uint16_t)c;
+            if (c >= std::max(min_support, 1)) {
+                out_dx[o] = median ? median_sorted(bu.data(), c) : mean_seq(bu.data(), c);
+                out_dy[o] = median ? median_sorted(bv.data(), c) : mean_seq(bv.data(), c);
+            }
+        }
+}
+
+int orc_spatial_kernel(float sigma, int32_t leave_out, float* weights, float* full, float* total) {
+    // smooth.rs:143-166: radius max(ceil(2.5 sigma), 1); weights exp(-(i^2+j^2) / (2 sigma^2))
+    const int r = std::max((int)std::ceil(2.5f * sigma), 1);
+    const int d = 2 * r + 1;
+    float f = 0.0f, t = 0.0f;
+    for (int j = -r; j <= r; ++j)
+        for (int i = -r; i <= r; ++i) {
+            const float w = std::exp(-((float)(i * i + j * j)) / (2.0f * sigma * sigma));
+            if (weights) weights[(j + r) * d + (i + r)] = w;
+        }
+    for (int j = -r; j <= r; ++j)
+        for (int i = -r; i <= r; ++i) {
+            const float w = std::exp(-((float)(i * i + j * j)) / (2.0f * sigma * sigma));
+            const bool ex = leave_out >= 0 && std::max(std::abs(i), std::abs(j)) <= leave_out;
+            if (!ex) f += w;
+            t += w;
+        }
+    *full = f;
+    *total = t;
+    return r;
+}
+
+void orc_spatial(const float* dx, const float* dy, const uint8_t* gate, int64_t nt, int64_t ny, int64_t nx,
+                 float sigma, float min_weight, int32_t leave_out, float* out_dx, float* out_dy, uint16_t* support) {
+    // smooth.rs:130-207: normalized convolution, NaN neighbours skipped
+    float full, total;
+    const int r = orc_spatial_kernel(sigma, leave_out, nullptr, &full, &total);
+    const int d = 2 * r + 1;
+    std::vector<float> kern((size_t)(d * d));
+    orc_spatial_kernel(sigma, leave_out, kern.data(), &full, &total);
+    const int64_t plane = ny * nx;
+    for (int64_t i = 0; i < nt * plane; ++i) {
+        out_dx[i] = NAN;
+        out_dy[i] = NAN;
+        support[i] = 0;
+    }
+    if (full < 0.5f * total) return;
+    for (int64_t t = 0; t < nt; ++t)
+        for (int64_t y = 0; y < ny; ++y)
+            for (int64_t x = 0; x < nx; ++x) {
+                const int64_t o = t * plane + y * nx + x;
+                if (!gate[o]) continue;
+                float su = 0.0f, sv = 0.0f, sw = 0.0f;
+                int n = 0;
+                for (int j = -r; j <= r; ++j) {
+                    const int64_t yy = y + j;
+                    if (yy < 0 || yy >= ny) continue;
+                    for (int i = -r; i <= r; ++i) {
+                        const int64_t xx = x + i;
+                        if (xx < 0 || xx >= nx || (leave_out >= 0 && std::max(std::abs(i), std::abs(j)) <= leave_out))
+                            continue;
+                        const float a = dx[t * plane + yy * nx + xx], b = dy[t * plane + yy * nx + xx];
+                        if (std::isfinite(a) && std::isfinite(b)) {
+                            const float w = kern[(j + r) * d + (i + r)];
+                            su += w * a;
+                            sv += w * b;
+                            sw += w;
+                            ++n;
+                        }
+                    }
+                }
+                support[o] = (uint16_t)n;
+                if (sw >= min_weight * full && sw > 0.0f) {
+                    out_dx[o] = su / sw;
+                    out_dy[o] = sv / sw;
+                }
+            }
+}
+
 uint64_t orc_splitmix_next(uint64_t* state) {
     // synthetic.rs:20-26
     *state += 0x9E3779B97F4A7C15ull;

@@ -139,6 +139,29 @@ int orc_analyze(const OrcConfig* cfg, const float* image_a, const float* image_b
                 uint8_t* trace_raw_flags, float* trace_dx, float* trace_dy, float* trace_ppr,
                 uint8_t* trace_flags);
 
+/* Post-processing of validated fields (the next components after the pair analysis).
+ * orc_usable: flow.rs:13-17. orc_vorticity / orc_flow_stats: flowstats.rs:28-101. orc_pair_stats:
+ * flow.rs:20-36 (displacement px -> px/s with k = f32(1/dt)). orc_temporal: smooth.rs:44-128
+ * (median != 0: median kernel). orc_spatial: smooth.rs:130-207 (leave_out < 0: none). */
+typedef struct {
+    float vorticity_mean, vorticity_abs_mean, ke_mean, ke_sum, coverage;
+    int64_t n_usable, n_vorticity;
+} OrcFlowStats;
+void orc_usable(const float* dx, const uint8_t* flags, int64_t n, uint8_t* usable);
+void orc_vorticity(const float* u, const float* v, const uint8_t* usable, int64_t ny, int64_t nx, float step,
+                   float* w);
+void orc_flow_stats(const float* u, const float* v, const uint8_t* usable, int64_t ny, int64_t nx, float step,
+                    OrcFlowStats* out);
+void orc_pair_stats(const float* dx, const float* dy, const uint8_t* flags, int64_t ny, int64_t nx, int64_t step,
+                    double dt_s, OrcFlowStats* out);
+int orc_temporal_offsets(int32_t window, const int32_t* leave_out, int32_t n_leave, int32_t* offsets);
+void orc_temporal(const float* dx, const float* dy, const uint8_t* usable, const uint8_t* gate, int64_t nt,
+                  int64_t ny, int64_t nx, int32_t median, int32_t window, int32_t min_support, const int32_t* leave_out,
+                  int32_t n_leave, float* out_dx, float* out_dy, uint16_t* support);
+int orc_spatial_kernel(float sigma, int32_t leave_out, float* weights, float* full, float* total);
+void orc_spatial(const float* dx, const float* dy, const uint8_t* gate, int64_t nt, int64_t ny, int64_t nx,
+                 float sigma, float min_weight, int32_t leave_out, float* out_dx, float* out_dy, uint16_t* support);
+
 /* SplitMix64 (synthetic.rs:10-36), exposed so tests can pin the Python restatement. */
 uint64_t orc_splitmix_next(uint64_t* state);
 

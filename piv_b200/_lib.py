@@ -25,7 +25,8 @@ EXPORTS = [
     "piv_batch_create", "piv_batch_destroy", "piv_batch_input_device", "piv_batch_input_bytes", "piv_batch_run",
     "piv_batch_sync", "piv_batch_outputs_device", "piv_batch_run_host", "piv_batch_kernels", "piv_batch_stream",
     "piv_place_windows", "piv_correlate_origins", "piv_place_windows_deform", "piv_correlate_deform",
-    "piv_validate_field", "piv_tc_selftest", "piv_validate_field_noalloc",
+    "piv_validate_field", "piv_flow_stats_device", "piv_temporal_smooth_device", "piv_spatial_smooth_device",
+    "piv_tc_selftest", "piv_validate_field_noalloc",
     "piv_server_create", "piv_server_destroy", "piv_server_submit", "piv_server_wait", "piv_server_stats",
 ]
 
@@ -71,6 +72,12 @@ class PivTraceC(ctypes.Structure):
         ("raw_peak_ratio", ctypes.c_void_p), ("raw_flags", ctypes.c_void_p), ("dx", ctypes.c_void_p),
         ("dy", ctypes.c_void_p), ("peak_ratio", ctypes.c_void_p), ("flags", ctypes.c_void_p),
     ]
+
+
+class PivFlowStatsC(ctypes.Structure):
+    _fields_ = [("vorticity_mean", ctypes.c_float), ("vorticity_abs_mean", ctypes.c_float), ("ke_mean", ctypes.c_float),
+                ("ke_sum", ctypes.c_float), ("coverage", ctypes.c_float), ("n_usable", ctypes.c_int64),
+                ("n_vorticity", ctypes.c_int64)]
 
 
 class PivServerConfigC(ctypes.Structure):
@@ -148,6 +155,10 @@ def load():
         "piv_place_windows_deform": ([vp, i64, i64, P(PivGridC), P(PivGridC), vp, vp, vp, vp], i32),
         "piv_correlate_deform": ([vp, vp, vp, P(PivGridC), vp, vp, vp, vp, vp, vp], i32),
         "piv_tc_selftest": ([i32, i32, i32, i32, vp, vp, vp], i32),
+        "piv_flow_stats_device": ([i64, i64, i64, ctypes.c_double, vp, vp, vp, vp, P(PivFlowStatsC), vp], i32),
+        "piv_temporal_smooth_device": ([i64, i64, i64, vp, vp, vp, vp, i32, i32, i32, vp, i32, vp, vp, vp, vp], i32),
+        "piv_spatial_smooth_device": ([i64, i64, i64, vp, vp, vp, ctypes.c_float, ctypes.c_float, i32, vp, vp, vp, vp],
+                                      i32),
         "piv_validate_field": ([vp, i64, i64, vp, vp, vp, vp, vp, vp, vp, P(PivSummaryC)], i32),
         "piv_validate_field_noalloc": ([i64, i64, vp, vp, vp, vp, f32, f32, f32, f32, i32, vp, vp, vp, vp], i32),
         "piv_server_create": ([P(PivServerConfigC), P(vp)], i32),

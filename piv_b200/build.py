@@ -24,6 +24,7 @@ UNITS = {
     "prep.cu": ["--fmad=false"],
     "api.cu": ["--fmad=false"],
     "noalloc.cu": ["--fmad=false"],
+    "post.cu": ["--fmad=false"],
 }
 HEADERS = ["common.cuh", "fft.cuh", "kernels.h", "window.cuh", "tc.cuh"]
 

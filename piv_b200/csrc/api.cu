@@ -1034,6 +1034,65 @@ int32_t piv_correlate_deform(PivAnalyzer* an, const PivFrame* a, const PivFrame*
     return PIV_OK;
 }
 
+int32_t piv_flow_stats_device(int64_t ny, int64_t nx, int64_t step, double dt_s, const float* dx, const float* dy,
+                              const uint8_t* flags, float* vorticity, PivFlowStatsC* stats, void* stream) {
+    if (!dx || !dy || !flags || !stats) return fail(PIV_ERR_ARGUMENT, "null pointer");
+    if (ny <= 0 || nx <= 0 || ny * nx > 0x7fffffffll) return fail(PIV_ERR_ARGUMENT, "bad field shape");
+    if (step <= 0 || !(dt_s > 0.0)) return fail(PIV_ERR_ARGUMENT, "step and dt_s must be positive");
+    FlowStatsHost h{};
+    CUDA_TRY(flow_stats_device((int)ny, (int)nx, (float)step, dt_s, dx, dy, flags, vorticity, &h, (cudaStream_t)stream));
+    stats->vorticity_mean = h.vorticity_mean;
+    stats->vorticity_abs_mean = h.vorticity_abs_mean;
+    stats->ke_mean = h.ke_mean;
+    stats->ke_sum = h.ke_sum;
+    stats->coverage = h.coverage;
+    stats->n_usable = h.n_usable;
+    stats->n_vorticity = h.n_vorticity;
+    return PIV_OK;
+}
+
+int32_t piv_temporal_smooth_device(int64_t nt, int64_t ny, int64_t nx, const float* dx, const float* dy,
+                                   const uint8_t* usable, const uint8_t* gate, int32_t median, int32_t window,
+                                   int32_t min_support, const int32_t* leave_out, int32_t n_leave_out, float* out_dx,
+                                   float* out_dy, uint16_t* support, void* stream) {
+    if (!dx || !dy || !usable || !gate || !out_dx || !out_dy || !support) return fail(PIV_ERR_ARGUMENT, "null pointer");
+    if (nt <= 0 || ny <= 0 || nx <= 0 || nt * ny * nx > 0x7fffffffll) return fail(PIV_ERR_ARGUMENT, "bad shape");
+    if (window < 1 || window % 2 == 0 || window > 63) return fail(PIV_ERR_ARGUMENT, "window must be odd, 1..63");
+    if (n_leave_out < 0 || (n_leave_out > 0 && !leave_out)) return fail(PIV_ERR_ARGUMENT, "bad leave_out list");
+    // smooth.rs:59-73: the offsets, centre first, then each side outwards skipping left-out ones
+    std::vector<int> off;
+    auto left = [&](int o) {
+        for (int i = 0; i < n_leave_out; ++i)
+            if (leave_out[i] == o) return true;
+        return false;
+    };
+    if (!left(0)) off.push_back(0);
+    for (int sign : {-1, 1}) {
+        int k = 1, taken = 0;
+        while (taken < window / 2) {
+            if (!left(sign * k)) {
+                off.push_back(sign * k);
+                ++taken;
+            }
+            ++k;
+        }
+    }
+    CUDA_TRY(temporal_smooth_device((int)nt, (int)ny, (int)nx, dx, dy, usable, gate, median != 0, off.data(),
+                                    (int)off.size(), min_support, out_dx, out_dy, support, (cudaStream_t)stream));
+    return PIV_OK;
+}
+
+int32_t piv_spatial_smooth_device(int64_t nt, int64_t ny, int64_t nx, const float* dx, const float* dy,
+                                  const uint8_t* gate, float sigma, float min_weight, int32_t leave_out, float* out_dx,
+                                  float* out_dy, uint16_t* support, void* stream) {
+    if (!dx || !dy || !gate || !out_dx || !out_dy || !support) return fail(PIV_ERR_ARGUMENT, "null pointer");
+    if (nt <= 0 || ny <= 0 || nx <= 0 || nt * ny * nx > 0x7fffffffll) return fail(PIV_ERR_ARGUMENT, "bad shape");
+    if (!(sigma > 0.0f && sigma <= 12.0f)) return fail(PIV_ERR_ARGUMENT, "sigma must be in (0, 12]");
+    CUDA_TRY(spatial_smooth_device((int)nt, (int)ny, (int)nx, dx, dy, gate, sigma, min_weight, leave_out, out_dx, out_dy,
+                                   support, (cudaStream_t)stream));
+    return PIV_OK;
+}
+
 int32_t piv_tc_selftest(int32_t device, int32_t a_mn, int32_t n, int32_t k, const float* a, const float* b, float* d) {
     if (!a || !b || !d) return fail(PIV_ERR_ARGUMENT, "null pointer");
     if (n < 16 || n > 256 || n % 16 || k < 16 || k > 256 || k % 16)

@@ -134,6 +134,23 @@ struct SummaryItem {
 };
 cudaError_t launch_summary_items(const SummaryItem* items, int count, cudaStream_t s, int* launches);
 
+// ----------------------------------------------------------------------------- post-processing
+// Flow statistics of one validated field (flowstats.rs:67-101 via flow.rs:20-36); blocking.
+struct FlowStatsHost {
+    float vorticity_mean, vorticity_abs_mean, ke_mean, ke_sum, coverage;
+    long long n_usable, n_vorticity;
+};
+cudaError_t flow_stats_device(int ny, int nx, float step, double dt_s, const float* dx, const float* dy,
+                              const uint8_t* flags, float* vort, FlowStatsHost* stats, cudaStream_t s);
+// Temporal filter (smooth.rs:44-128) with the offsets already resolved (leave-out applied).
+cudaError_t temporal_smooth_device(int nt, int ny, int nx, const float* dx, const float* dy, const uint8_t* usable,
+                                   const uint8_t* gate, int median, const int* offsets, int n_off, int min_support,
+                                   float* out_dx, float* out_dy, uint16_t* support, cudaStream_t s);
+// Spatial filter (smooth.rs:130-207); leave_out < 0 means none. sigma up to 12 grid cells.
+cudaError_t spatial_smooth_device(int nt, int ny, int nx, const float* dx, const float* dy, const uint8_t* gate,
+                                  float sigma, float min_weight, int leave_out, float* out_dx, float* out_dy,
+                                  uint16_t* support, cudaStream_t s);
+
 // ----------------------------------------------------------------------------- preprocessing
 enum RawType { RAW_U8 = 0, RAW_U16 = 1, RAW_F32 = 2 };
 
