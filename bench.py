@@ -651,8 +651,36 @@ def main():
     e3.record(stream)
     e3.synchronize()
     t_wall = time.perf_counter() - t_wall
-    ms2 = ranks.max(e2.elapsed_time(e3))
-    e2e_value = world * e2e_steps * nvec / (ms2 * 1e-3)
+    ms_serial = ranks.max(e2.elapsed_time(e3))
+
+    # pipelined: the same calls through PivPipeline (depth 3), so one pair's uploads and downloads
+    # overlap the others' kernels; host clock with the device synchronised at both ends
+    depth = 3
+    pl = P.PivPipeline(an, h, w, dtype=np.uint16, cfg=pre, depth=depth)
+    outs = [tuple(torch.empty(nvec, dtype=dt).pin_memory().numpy().reshape(g.ny, g.nx)
+                  for dt in (torch.float32, torch.float32, torch.float32, torch.uint8)) for _ in range(depth)]
+
+    def e2e_run(n):
+        tickets = []
+        for i in range(n):
+            if len(tickets) == depth:
+                pl.wait(tickets.pop(0))
+            ha, hb = pin[i % len(pin)]
+            tickets.append(pl.submit(ha, hb, out=outs[i % depth]))
+        for t in tickets:
+            pl.wait(t)
+
+    e2e_run(max(args.warmup, depth))
+    pipe_steps = max(12, args.steps // 2)
+    ranks.barrier()
+    torch.cuda.synchronize()
+    t_pipe = time.perf_counter()
+    e2e_run(pipe_steps)
+    torch.cuda.synchronize()
+    t_pipe = time.perf_counter() - t_pipe
+    ms2 = ranks.max(1e3 * t_pipe)
+    pl.close()
+    e2e_value = world * pipe_steps * nvec / (ms2 * 1e-3)
     h2d = sum(x.nbytes for x in pin[0])
     d2h = hdx.nbytes + hdy.nbytes + hppr.nbytes + hfl.nbytes + 5 * 8
 
@@ -690,8 +718,13 @@ def main():
                        "overlap": wl["overlap"], "final_pass_vectors": nvec, "parallelism": f"replicas x{world}",
                        "l2": "inputs > L2: 2 alternating pairs, 192 MiB of samples + prepared images per step"},
             "e2e": {"value": e2e_value, "unit": "vectors/s", "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
-                    "ms_per_step": ms2 / e2e_steps, "wall_ms_per_step": 1e3 * t_wall / e2e_steps},
+                    "d2h_bytes_per_step": int(d2h), "steps": pipe_steps,
+                    "ms_per_step": ms2 / pipe_steps,
+                    "how": "PivPipeline (3 slots) over pinned host frames: upload, preparation, all passes and "
+                           "download of the final field per pair; host clock, device synchronised at both ends",
+                    "serial_value": world * e2e_steps * nvec / (ms_serial * 1e-3),
+                    "serial_ms_per_step": ms_serial / e2e_steps,
+                    "serial_wall_ms_per_step": 1e3 * t_wall / e2e_steps},
             "gpu_launches": int(launches), "roofline": roof, "clocks": clocks, "autotuned_variants": tuned}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(wl, a0, b0, single_s=4.0)

@@ -224,6 +224,23 @@ int32_t piv_batch_run_host(PivBatch* batch, const void* raw, float* dx, float* d
 /* Kernels executed per run (counted on the eager first run; the graph replays the same set). */
 int64_t piv_batch_kernels(const PivBatch* batch);
 
+/* Pipelined pairs (no counterpart in the reference, which analyses pairs one after another,
+ * analyze.rs:441): pairs of HOST frames are submitted without waiting; `depth` slots, each with
+ * its own stream, prepared frames and workspace, let the uploads and downloads of one pair overlap
+ * the kernels of the others. Each result equals piv_analyze of that pair. Host buffers should be
+ * pinned (cudaHostAlloc) for the copies to be asynchronous, and must stay valid (outputs
+ * untouched) until piv_pipeline_wait returns for that ticket. Submitting blocks only when the
+ * next slot still holds an unfinished pair. */
+typedef struct PivPipeline PivPipeline;
+int32_t piv_pipeline_create(const PivAnalyzer* an, int64_t height, int64_t width, int32_t dtype,
+                            const PivPreprocessC* pre, int32_t depth, PivPipeline** out);
+void piv_pipeline_destroy(PivPipeline* pipeline);
+/* Outputs as piv_analyze (any may be NULL); returns a ticket for piv_pipeline_wait. */
+int32_t piv_pipeline_submit(PivPipeline* pipeline, const void* frame_a, const void* frame_b, float* dx, float* dy,
+                            float* peak_ratio, uint8_t* flags, uint64_t* ticket);
+/* Waits for the pair of `ticket`; every ticket is waited for exactly once. */
+int32_t piv_pipeline_wait(PivPipeline* pipeline, uint64_t ticket, PivSummaryC* summary);
+
 /* ----------------------------------------------------------------------------- serving form
  * No counterpart in the reference. A request loop on one GPU with continuous batching: frame
  * pairs of any size with their own PivConfig are submitted at any time; a scheduler thread

@@ -11,6 +11,7 @@ from .api import (  # noqa: F401
     PairResult,
     PassTrace,
     PivBatch,
+    PivPipeline,
     PivAnalyzer,
     PivConfig,
     PivError,

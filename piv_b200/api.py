@@ -573,6 +573,55 @@ class PivBatch:
             pass
 
 
+class PivPipeline:
+    """Pipelined pairs of one size: submit() queues a pair of host frames and returns a ticket at
+    once; `depth` slots (each with its own stream and workspace) overlap one pair's copies with the
+    others' kernels. wait(ticket) returns the PairResult, equal to PivAnalyzer.analyze of that pair.
+    Frames should be pinned host memory for the uploads to be asynchronous."""
+
+    def __init__(self, analyzer: PivAnalyzer, height, width, dtype=np.uint16, cfg: PreprocessConfig = None, depth=2):
+        cfg = RAW if cfg is None else cfg
+        self.height, self.width, self.dtype = int(height), int(width), np.dtype(dtype)
+        self.grid = analyzer.output_grid(height, width)
+        h = ctypes.c_void_p()
+        pc = cfg._c()
+        _check(_lib.load().piv_pipeline_create(analyzer._h, self.height, self.width, _dtype_code(np.empty(0, self.dtype)),
+                                               ctypes.byref(pc), int(depth), ctypes.byref(h)))
+        self._h = h
+        self._pending = {}
+
+    def submit(self, a, b, out=None):
+        a = np.ascontiguousarray(a, self.dtype)
+        b = np.ascontiguousarray(b, self.dtype)
+        if a.shape != (self.height, self.width) or b.shape != a.shape:
+            raise ShapeMismatchError(f"expected {(self.height, self.width)}, got {a.shape} and {b.shape}")
+        g = self.grid
+        if out is None:
+            out = (np.empty((g.ny, g.nx), np.float32), np.empty((g.ny, g.nx), np.float32),
+                   np.empty((g.ny, g.nx), np.float32), np.empty((g.ny, g.nx), np.uint8))
+        t = ctypes.c_uint64()
+        _check(_lib.load().piv_pipeline_submit(self._h, _ptr(a), _ptr(b), *[_ptr(x) for x in out], ctypes.byref(t)))
+        self._pending[t.value] = (a, b, out)  # keep the buffers alive until the pair is collected
+        return t.value
+
+    def wait(self, ticket):
+        a, b, out = self._pending.pop(ticket)
+        s = _lib.PivSummaryC()
+        _check(_lib.load().piv_pipeline_wait(self._h, ctypes.c_uint64(ticket), ctypes.byref(s)))
+        return PairResult(VectorField(self.grid, *out), ValidationSummary._from_c(s))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.load().piv_pipeline_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class PivServer:
     """The serving form: continuous batching of frame pairs of any size and window schedule on one
     GPU under a device-memory budget. submit() returns a ticket at once; wait(ticket) returns the

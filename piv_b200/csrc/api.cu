@@ -1201,6 +1201,29 @@ int batch_record(PivBatch* bt) {
 
 }  // namespace
 
+namespace {
+// A private analyzer with the parent's configuration and chosen launch variants (no workspace,
+// no stream yet): its workspace is never resized by the parent's calls.
+PivAnalyzer* clone_config(const PivAnalyzer* parent) {
+    PivAnalyzer* an = new PivAnalyzer();
+    an->windows = parent->windows;
+    an->overlap = parent->overlap;
+    an->final_iterations = parent->final_iterations;
+    an->min_mean = parent->min_mean;
+    an->min_std = parent->min_std;
+    an->ppr_threshold = parent->ppr_threshold;
+    an->median_threshold = parent->median_threshold;
+    an->median_eps = parent->median_eps;
+    an->replace = parent->replace;
+    an->deform = parent->deform;
+    an->precision = parent->precision;
+    an->device = parent->device;
+    for (int k = 0; k < 2; ++k)
+        for (int i = 0; i < 129; ++i) an->variant[k][i] = parent->variant[k][i];
+    return an;
+}
+}  // namespace
+
 int32_t piv_batch_create(const PivAnalyzer* parent, int64_t height, int64_t width, int32_t pairs, int32_t sequential,
                          int32_t dtype, const PivPreprocessC* pre, PivBatch** out) {
     if (!parent || !out || pairs <= 0) return fail(PIV_ERR_ARGUMENT, "bad argument");
@@ -1217,21 +1240,7 @@ int32_t piv_batch_create(const PivAnalyzer* parent, int64_t height, int64_t widt
     make_grid(height, width, parent->windows.back(), parent->overlap, &g);
     CUDA_TRY(cudaSetDevice(parent->device));
     PivBatch* bt = new PivBatch();
-    PivAnalyzer* an = new PivAnalyzer();
-    an->windows = parent->windows;
-    an->overlap = parent->overlap;
-    an->final_iterations = parent->final_iterations;
-    an->min_mean = parent->min_mean;
-    an->min_std = parent->min_std;
-    an->ppr_threshold = parent->ppr_threshold;
-    an->median_threshold = parent->median_threshold;
-    an->median_eps = parent->median_eps;
-    an->replace = parent->replace;
-    an->deform = parent->deform;
-    an->precision = parent->precision;
-    an->device = parent->device;
-    for (int k = 0; k < 2; ++k)
-        for (int i = 0; i < 129; ++i) an->variant[k][i] = parent->variant[k][i];
+    PivAnalyzer* an = clone_config(parent);
     bt->an = an;
     bt->H = height;
     bt->W = width;
@@ -1288,6 +1297,142 @@ void piv_batch_destroy(PivBatch* bt) {
     cudaFree(bt->out);
     piv_analyzer_destroy(bt->an);
     delete bt;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Pipelined pairs: `depth` slots, each a private analyzer with its own stream and frames. A
+// submitted pair's uploads, preparation, passes and downloads are queued on its slot's stream,
+// so the copies of one pair overlap the kernels of the others.
+// ---------------------------------------------------------------------------------------------
+struct PivPipeline {
+    struct Slot {
+        PivAnalyzer* an = nullptr;
+        PivFrame* fa = nullptr;
+        PivFrame* fb = nullptr;
+        unsigned long long* sums = nullptr;  // pinned: 5 counters of the slot's last pair
+        cudaEvent_t done = nullptr;
+        uint64_t ticket = 0;  // 0: idle
+    };
+    int device = 0;
+    int64_t H = 0, W = 0;
+    int32_t dtype = PIV_DTYPE_U16;
+    PivPreprocessC pre{};
+    std::vector<Slot> slots;
+    size_t next = 0;
+    uint64_t tickets = 0;
+    std::map<uint64_t, PivSummaryC> finished;  // pairs whose slot was reused before their wait
+};
+
+namespace {
+int retire_slot(PivPipeline* pl, PivPipeline::Slot& s, PivSummaryC* out) {
+    CUDA_TRY(cudaEventSynchronize(s.done));
+    int st = check_device_error(pl->device);
+    if (st) return st;
+    PivSummaryC r{(int64_t)s.sums[0], (int64_t)s.sums[1], (int64_t)s.sums[2], (int64_t)s.sums[3], (int64_t)s.sums[4]};
+    if (out) *out = r;
+    else pl->finished[s.ticket] = r;
+    s.ticket = 0;
+    return PIV_OK;
+}
+}  // namespace
+
+int32_t piv_pipeline_create(const PivAnalyzer* parent, int64_t height, int64_t width, int32_t dtype,
+                            const PivPreprocessC* pre, int32_t depth, PivPipeline** out) {
+    if (!parent || !out) return fail(PIV_ERR_ARGUMENT, "null argument");
+    *out = nullptr;
+    if (depth < 1 || depth > 8) return fail(PIV_ERR_ARGUMENT, "depth must be in [1, 8]");
+    if (!dtype_size(dtype)) return fail(PIV_ERR_ARGUMENT, "unknown dtype %d", dtype);
+    PivGridC g;
+    for (int32_t n : parent->windows) {
+        int st = make_grid(height, width, n, parent->overlap, &g);
+        if (st) return st;
+    }
+    CUDA_TRY(cudaSetDevice(parent->device));
+    PivPipeline* pl = new PivPipeline();
+    pl->device = parent->device;
+    pl->H = height;
+    pl->W = width;
+    pl->dtype = dtype;
+    pl->pre = pre ? *pre : PivPreprocessC{1.0f, 4, 0.02f, 0.0};
+    pl->slots.resize((size_t)depth);
+    for (auto& s : pl->slots) {
+        s.an = clone_config(parent);
+        cudaError_t e = cudaStreamCreateWithFlags(&s.an->own, cudaStreamNonBlocking);
+        s.an->cur = s.an->own;
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.sums, 8 * sizeof(unsigned long long), cudaHostAllocDefault);
+        int st = e == cudaSuccess ? PIV_OK : fail(PIV_ERR_CUDA, "pipeline slot: %s", cudaGetErrorString(e));
+        if (!st) st = piv_frame_create(s.an, height, width, &s.fa);
+        if (!st) st = piv_frame_create(s.an, height, width, &s.fb);
+        if (st) {
+            piv_pipeline_destroy(pl);
+            return st;
+        }
+    }
+    *out = pl;
+    return PIV_OK;
+}
+
+void piv_pipeline_destroy(PivPipeline* pl) {
+    if (!pl) return;
+    cudaSetDevice(pl->device);
+    for (auto& s : pl->slots) {
+        if (s.an && s.an->own) cudaStreamSynchronize(s.an->own);
+        if (s.fa) piv_frame_destroy(s.fa);
+        if (s.fb) piv_frame_destroy(s.fb);
+        if (s.done) cudaEventDestroy(s.done);
+        if (s.sums) cudaFreeHost(s.sums);
+        piv_analyzer_destroy(s.an);
+    }
+    delete pl;
+}
+
+int32_t piv_pipeline_submit(PivPipeline* pl, const void* frame_a, const void* frame_b, float* dx, float* dy,
+                            float* peak_ratio, uint8_t* flags, uint64_t* ticket) {
+    if (!pl || !frame_a || !frame_b || !ticket) return fail(PIV_ERR_ARGUMENT, "null argument");
+    CUDA_TRY(cudaSetDevice(pl->device));
+    PivPipeline::Slot& s = pl->slots[pl->next % pl->slots.size()];
+    if (s.ticket) {
+        int st = retire_slot(pl, s, nullptr);
+        if (st) return st;
+    }
+    int st = piv_frame_prepare(s.an, s.fa, frame_a, pl->dtype, &pl->pre, nullptr);
+    if (!st) st = piv_frame_prepare(s.an, s.fb, frame_b, pl->dtype, &pl->pre, nullptr);
+    if (!st) st = run_passes(s.an, s.fa, s.fb);
+    if (st) return st;
+    const PassBuf& last = s.an->pairs[0].back();
+    const size_t c = (size_t)last.cells;
+    cudaStream_t cs = s.an->cur;
+    if (dx) CUDA_TRY(cudaMemcpyAsync(dx, last.dx, 4 * c, cudaMemcpyDeviceToHost, cs));
+    if (dy) CUDA_TRY(cudaMemcpyAsync(dy, last.dy, 4 * c, cudaMemcpyDeviceToHost, cs));
+    if (peak_ratio) CUDA_TRY(cudaMemcpyAsync(peak_ratio, last.raw_ppr, 4 * c, cudaMemcpyDeviceToHost, cs));
+    if (flags) CUDA_TRY(cudaMemcpyAsync(flags, last.flags, c, cudaMemcpyDeviceToHost, cs));
+    CUDA_TRY(cudaMemcpyAsync(s.sums, s.an->d_counts, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, cs));
+    CUDA_TRY(cudaEventRecord(s.done, cs));
+    s.ticket = ++pl->tickets;
+    pl->next++;
+    *ticket = s.ticket;
+    return PIV_OK;
+}
+
+int32_t piv_pipeline_wait(PivPipeline* pl, uint64_t ticket, PivSummaryC* summary) {
+    if (!pl) return fail(PIV_ERR_ARGUMENT, "null pipeline");
+    CUDA_TRY(cudaSetDevice(pl->device));
+    auto it = pl->finished.find(ticket);
+    if (it != pl->finished.end()) {
+        if (summary) *summary = it->second;
+        pl->finished.erase(it);
+        return PIV_OK;
+    }
+    for (auto& s : pl->slots)
+        if (s.ticket == ticket) {
+            PivSummaryC r{};
+            int st = retire_slot(pl, s, &r);
+            if (st) return st;
+            if (summary) *summary = r;
+            return PIV_OK;
+        }
+    return fail(PIV_ERR_ARGUMENT, "unknown or already collected ticket %llu", (unsigned long long)ticket);
 }
 
 void* piv_batch_input_device(PivBatch* bt) { return bt ? bt->raw : nullptr; }

@@ -80,3 +80,30 @@ def test_batch_device_entry_matches():
         sl = slice(i * c, (i + 1) * c)
         assert np.array_equal(fl[sl].cpu().numpy().reshape(g.ny, g.nx), r.field.flags)
         assert same_floats(dx[sl].cpu().numpy().reshape(g.ny, g.nx), r.field.dx)
+
+
+@pytest.mark.parametrize("depth", [1, 2, 3])
+def test_pipeline_matches_per_pair_analysis(depth):
+    """Pipelined pairs equal PivAnalyzer.analyze bit for bit, also when more pairs are submitted
+    than there are slots (a slot is reused before its ticket is collected) and when tickets are
+    collected out of order."""
+    import piv_b200 as P
+    h, w, k = 200, 264, 5
+    an = P.PivAnalyzer(P.PivConfig(windows=[64, 32], overlap=0.5, final_iterations=2))
+    frames = _frames(2 * k, h, w, 17)
+    ref = _reference(an, frames, [(2 * i, 2 * i + 1) for i in range(k)])
+    pl = P.PivPipeline(an, h, w, depth=depth)
+    tickets = [pl.submit(frames[2 * i], frames[2 * i + 1]) for i in range(k)]
+    order = list(range(k))[::-1]
+    for i in order:
+        _same(pl.wait(tickets[i]), ref[i])
+    # steady state: wait for the oldest before each new submission
+    live = []
+    for i in range(2 * k):
+        if len(live) == depth:
+            j, t = live.pop(0)
+            _same(pl.wait(t), ref[j % k])
+        live.append((i, pl.submit(frames[2 * (i % k)], frames[2 * (i % k) + 1])))
+    for j, t in live:
+        _same(pl.wait(t), ref[j % k])
+    pl.close()
