@@ -68,11 +68,11 @@ __device__ __forceinline__ uint32_t mnmaj_chunk(int rows, int m, int k) {
 
 // Window sampling for the tensor-core tier (correlate.rs:182-202 semantics: integer copy when
 // both fractional parts are < 1e-4, bilinear otherwise), one lane per column streaming down the
-// rows: each pixel of the patch is loaded once, the right-hand neighbour comes from the next lane
-// and the row below is carried to the next iteration. The bilinear weights are applied as two
-// linear interpolations with FMA (rounding differs from the reference's weight sum by an ulp,
-// far below the split-BF16 precision); zero fractions make it an exact copy. The last column of
-// a window (and lane 31) loads its right neighbour itself.
+// rows. Each lane loads both taps of every row itself from one row pointer (the right-hand tap
+// is the next float, or the same one at the right image border), with no shuffles and no
+// conditional loads; the row below is carried to the next iteration. The bilinear weights are
+// applied as two linear interpolations with FMA (rounding differs from the reference's weight
+// sum by an ulp, far below the split-BF16 precision); zero fractions make it an exact copy.
 template <int N, bool IMAG>
 __device__ __forceinline__ void sample_rows(const float* __restrict__ img, int H, int W, float ox, float oy, int x,
                                             float2 (&z)[N]) {
@@ -80,19 +80,16 @@ __device__ __forceinline__ void sample_rows(const float* __restrict__ img, int H
     const int x0 = min(max((int)fx0, 0), W - 1), y0 = min(max((int)fy0, 0), H - 1);
     float tx = ox - fx0, ty = oy - fy0;
     if (tx < 1e-4f && ty < 1e-4f) tx = ty = 0.0f;
-    const int c0 = min(x0 + x, W - 1), c1 = min(x0 + x + 1, W - 1);
-    const bool edge = (threadIdx.x & 31) == 31 || x == N - 1;
-    int off = y0 * W;  // H * W < 2^31
-    float top = __ldg(img + off + c0);
-    float topr = __shfl_down_sync(0xffffffffu, top, 1);
-    if (edge) topr = __ldg(img + off + c1);
+    const int c0 = min(x0 + x, W - 1);
+    const int dc = min(x0 + x + 1, W - 1) - c0;  // 1, or 0 at the right border
+    const float* base = img + (size_t)y0 * W + c0;
+    const int last = H - 1 - y0;                  // rows below y0 that exist
+    float top = __ldg(base), topr = __ldg(base + dc);
     float ht = fmaf(tx, topr - top, top);
 #pragma unroll
     for (int p = 0; p < N; ++p) {
-        off = min(y0 + p + 1, H - 1) * W;
-        const float bot = __ldg(img + off + c0);
-        float botr = __shfl_down_sync(0xffffffffu, bot, 1);
-        if (edge) botr = __ldg(img + off + c1);
+        const float* row = base + (size_t)min(p + 1, last) * W;
+        const float bot = __ldg(row), botr = __ldg(row + dc);
         const float hb = fmaf(tx, botr - bot, bot);
         const float v = fmaf(ty, hb - ht, ht);
         if (IMAG) z[p].y = v; else z[p].x = v;

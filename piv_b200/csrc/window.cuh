@@ -32,7 +32,10 @@ __device__ __forceinline__ void sample_column_direct(const float* __restrict__ i
     const float fx0 = floorf(ox), fy0 = floorf(oy);
     const int x0 = min(max((int)fx0, 0), W - 1), y0 = min(max((int)fy0, 0), H - 1);
     const float tx = __fsub_rn(ox, fx0), ty = __fsub_rn(oy, fy0);
-    const int c0 = min(x0 + x, W - 1), c1 = min(x0 + x + 1, W - 1);
+    const int c0 = min(x0 + x, W - 1);
+    const int dc = min(x0 + x + 1, W - 1) - c0;  // right-hand tap: next float, or the same at the border
+    const int last = H - 1 - y0;                  // rows below y0 that exist (row clamp)
+    const float* base = img + (size_t)y0 * W + c0;
     if (tx < 1e-4f && ty < 1e-4f) {
 #pragma unroll
         for (int p = 0; p < P; ++p) {
@@ -42,15 +45,33 @@ __device__ __forceinline__ void sample_column_direct(const float* __restrict__ i
     } else {
         const float ux = __fsub_rn(1.0f, tx), uy = __fsub_rn(1.0f, ty);
         const float w00 = __fmul_rn(ux, uy), w01 = __fmul_rn(tx, uy), w10 = __fmul_rn(ux, ty), w11 = __fmul_rn(tx, ty);
+        if constexpr (T == 1) {
+            // one lane holds the whole column: stream down the rows, carrying the row below
+            float top = __ldg(base), topr = __ldg(base + dc);
 #pragma unroll
-        for (int p = 0; p < P; ++p) {
-            const float* top = img + (size_t)min(y0 + t + T * p, H - 1) * W;
-            const float* bot = img + (size_t)min(y0 + t + T * p + 1, H - 1) * W;
-            float s = __fmul_rn(w00, __ldg(top + c0));
-            s = __fadd_rn(s, __fmul_rn(w01, __ldg(top + c1)));
-            s = __fadd_rn(s, __fmul_rn(w10, __ldg(bot + c0)));
-            s = __fadd_rn(s, __fmul_rn(w11, __ldg(bot + c1)));
-            if (IMAG) z[p].y = s; else z[p].x = s;
+            for (int p = 0; p < P; ++p) {
+                const float* bot = base + (size_t)min(p + 1, last) * W;
+                const float b0 = __ldg(bot), b1 = __ldg(bot + dc);
+                float s = __fmul_rn(w00, top);
+                s = __fadd_rn(s, __fmul_rn(w01, topr));
+                s = __fadd_rn(s, __fmul_rn(w10, b0));
+                s = __fadd_rn(s, __fmul_rn(w11, b1));
+                if (IMAG) z[p].y = s; else z[p].x = s;
+                top = b0;
+                topr = b1;
+            }
+        } else {
+            const int c1 = c0 + dc;
+#pragma unroll
+            for (int p = 0; p < P; ++p) {
+                const float* top = img + (size_t)min(y0 + t + T * p, H - 1) * W;
+                const float* bot = img + (size_t)min(y0 + t + T * p + 1, H - 1) * W;
+                float s = __fmul_rn(w00, __ldg(top + c0));
+                s = __fadd_rn(s, __fmul_rn(w01, __ldg(top + c1)));
+                s = __fadd_rn(s, __fmul_rn(w10, __ldg(bot + c0)));
+                s = __fadd_rn(s, __fmul_rn(w11, __ldg(bot + c1)));
+                if (IMAG) z[p].y = s; else z[p].x = s;
+            }
         }
     }
 }
@@ -68,25 +89,28 @@ __device__ __forceinline__ void sample_column(const float* __restrict__ img, int
     const float fx0 = floorf(ox), fy0 = floorf(oy);
     const int x0 = min(max((int)fx0, 0), W - 1), y0 = min(max((int)fy0, 0), H - 1);
     const float tx = __fsub_rn(ox, fx0), ty = __fsub_rn(oy, fy0);
-    const int c0 = min(x0 + x, W - 1), c1 = min(x0 + x + 1, W - 1);
+    const int c0 = min(x0 + x, W - 1);
+    const int dc = min(x0 + x + 1, W - 1) - c0;  // right-hand tap: next float, or the same at the border
+    const int last = H - 1 - y0;                  // rows below y0 that exist (row clamp)
+    const float* base = img + (size_t)y0 * W + c0;
     const bool integer = tx < 1e-4f && ty < 1e-4f;
     float top[P];
 #pragma unroll
-    for (int p = 0; p < P; ++p) top[p] = __ldg(img + (size_t)min(y0 + t + T * p, H - 1) * W + c0);
+    for (int p = 0; p < P; ++p) top[p] = __ldg(base + (size_t)min(t + T * p, last) * W);
     // Every lane runs the shuffles below (a warp may hold windows of both kinds); an integer
     // window then keeps its copied values.
     // Row N of the patch (below the window), held by the last lane of each line.
-    const int rN = min(y0 + N, H - 1);
-    const float extra = __ldg(img + (size_t)rN * W + c0);
+    const float* rowN = base + (size_t)min(N, last) * W;
+    const float extra = __ldg(rowN);
     const bool edge = lane + T >= 32 || x == N - 1;  // right neighbour not reachable by a shuffle
     float right[P];
 #pragma unroll
     for (int p = 0; p < P; ++p) {
         right[p] = __shfl_down_sync(0xffffffffu, top[p], T);
-        if (edge) right[p] = __ldg(img + (size_t)min(y0 + t + T * p, H - 1) * W + c1);
+        if (edge) right[p] = __ldg(base + (size_t)min(t + T * p, last) * W + dc);
     }
     float extra_r = __shfl_down_sync(0xffffffffu, extra, T);
-    if (edge) extra_r = __ldg(img + (size_t)rN * W + c1);
+    if (edge) extra_r = __ldg(rowN + dc);
     const float ux = __fsub_rn(1.0f, tx), uy = __fsub_rn(1.0f, ty);
     const float w00 = __fmul_rn(ux, uy), w01 = __fmul_rn(tx, uy), w10 = __fmul_rn(ux, ty), w11 = __fmul_rn(tx, ty);
 #pragma unroll
