@@ -61,7 +61,8 @@ typedef enum { PIV_DTYPE_U8 = 0, PIV_DTYPE_U16 = 1, PIV_DTYPE_F32 = 2 } PivDtype
  * PIV_PRECISION_BF16X3 runs the 2-D DFTs as DFT-matrix products on the tensor cores with every
  * operand split into two BF16 halves and three products summed in FP32 (about 16 significant
  * bits) for window sizes 16 and 32 and uniform windows; other sizes and deformed windows keep
- * the FP32 kernel. */
+ * the FP32 kernel. piv_analyzer_autotune also times the tensor-core kernel and keeps the FP32
+ * kernel (higher precision) for a size where it is faster. */
 #define PIV_PRECISION_FP32 0
 #define PIV_PRECISION_BF16X3 1
 

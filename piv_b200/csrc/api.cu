@@ -128,6 +128,8 @@ struct PivAnalyzer {
 
     // correlation launch variant chosen per window size (0 until autotuned), uniform / deformed
     int variant[2][129] = {};
+    // with tensor cores allowed: window sizes where the autotuner found the FP32 kernel faster
+    bool fp32_faster[129] = {};
 
     bool mask_trivial() const { return min_mean <= 0.0f && min_std <= 0.0f; }
     std::vector<int32_t> pass_windows() const {
@@ -351,10 +353,12 @@ int run_passes(PivAnalyzer* an, const PivFrame* const* a, const PivFrame* const*
         }
         const int nwin = (int)an->pairs[0][i].grid.window;
         const int kind = cps[0].corners ? 1 : 0;
-        const bool tensor = kind == 0 && an->precision == PIV_PRECISION_BF16X3 && corr_tc_supported(nwin);
-        if (tune && !tensor) {
+        const bool tc_ok = kind == 0 && an->precision == PIV_PRECISION_BF16X3 && corr_tc_supported(nwin);
+        if (tune) {
             // Time every launch variant of this window size on this pass's data (all compute the
-            // same results) and keep the fastest for later calls.
+            // same results) and keep the fastest for later calls. With tensor cores allowed, the
+            // tensor-core kernel is timed too, and the FP32 kernel (higher precision) is kept
+            // for this size when it is faster.
             cudaEvent_t t0, t1;
             CUDA_TRY(cudaEventCreate(&t0));
             CUDA_TRY(cudaEventCreate(&t1));
@@ -373,10 +377,21 @@ int run_passes(PivAnalyzer* an, const PivFrame* const* a, const PivFrame* const*
                     best_v = v;
                 }
             }
+            an->variant[kind][nwin] = best_v;
+            if (tc_ok) {
+                CUDA_TRY(launch_correlate_tc_items(nwin, cps.data(), K, an->cur, &nl));
+                CUDA_TRY(cudaEventRecord(t0, an->cur));
+                for (int r = 0; r < 3; ++r) CUDA_TRY(launch_correlate_tc_items(nwin, cps.data(), K, an->cur, &nl));
+                CUDA_TRY(cudaEventRecord(t1, an->cur));
+                CUDA_TRY(cudaEventSynchronize(t1));
+                float ms = 0.0f;
+                CUDA_TRY(cudaEventElapsedTime(&ms, t0, t1));
+                an->fp32_faster[nwin] = best < ms;
+            }
             cudaEventDestroy(t0);
             cudaEventDestroy(t1);
-            an->variant[kind][nwin] = best_v;
         }
+        const bool tensor = tc_ok && !an->fp32_faster[nwin];
         if (tensor)
             CUDA_TRY(launch_correlate_tc_items(nwin, cps.data(), K, an->cur, &nl));
         else
@@ -622,7 +637,10 @@ int32_t piv_analyzer_variant(const PivAnalyzer* an, int32_t window, char* name, 
     if (!an || !name || capacity <= 0) return fail(PIV_ERR_ARGUMENT, "bad argument");
     if (!corr_supported(window)) return fail(PIV_ERR_UNSUPPORTED, "window size %d", window);
     const int kind = an->deform ? 1 : 0;
-    snprintf(name, (size_t)capacity, "%s", corr_variant_name(window, an->variant[kind][window], kind));
+    if (!an->deform && an->precision == PIV_PRECISION_BF16X3 && corr_tc_supported(window) && !an->fp32_faster[window])
+        snprintf(name, (size_t)capacity, "%d/tensor-core/bf16x3", window);
+    else
+        snprintf(name, (size_t)capacity, "%s", corr_variant_name(window, an->variant[kind][window], kind));
     return PIV_OK;
 }
 
@@ -1220,6 +1238,7 @@ PivAnalyzer* clone_config(const PivAnalyzer* parent) {
     an->device = parent->device;
     for (int k = 0; k < 2; ++k)
         for (int i = 0; i < 129; ++i) an->variant[k][i] = parent->variant[k][i];
+    for (int i = 0; i < 129; ++i) an->fp32_faster[i] = parent->fp32_faster[i];
     return an;
 }
 }  // namespace
