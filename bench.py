@@ -158,16 +158,35 @@ def run_stream(args, wl):
     # end to end: pinned host frames -> input slab -> graph -> results to host, every step
     pin = torch.from_numpy(frames.view(np.int16)).pin_memory().numpy().view(np.uint16)
     res = batch.run_host(pin)
-    ev2 = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
-    e2e_steps = max(3, args.steps // 4)
+    # two batches (each its own stream and graph) in turn: one's upload and download overlap
+    # the other's graph; host clock with the device synchronised at both ends
+    batch2 = P.PivBatch(an, h, w, k, sequential=True)
+    batch2.run_host(pin)
+    batch2.run_host(pin)
+    g = batch.grid
+    outs = [tuple(torch.empty(k * g.ny * g.nx, dtype=dt).pin_memory().numpy().reshape(k, g.ny, g.nx)
+                  for dt in (torch.float32, torch.float32, torch.float32, torch.uint8)) for _ in range(2)]
+    pair_of_batches = [batch, batch2]
+
+    def e2e_run(n):
+        last = None
+        for i in range(n):
+            b = pair_of_batches[i % 2]
+            if i >= 2:
+                last = b.wait_host()
+            b.submit_host(pin, out=outs[i % 2])
+        for i in range(max(0, n - 2), n):
+            last = pair_of_batches[i % 2].wait_host()
+        return last
+
+    e2e_run(4)
+    e2e_steps = max(8, args.steps // 2)
     ranks.barrier()
     torch.cuda.synchronize()
-    ev2[0].record(bstream)
-    for _ in range(e2e_steps):
-        res = batch.run_host(pin)
-    ev2[1].record(bstream)
-    ev2[1].synchronize()
-    e2e_ms = ranks.max(ev2[0].elapsed_time(ev2[1]))
+    t_e2e = time.perf_counter()
+    res = e2e_run(e2e_steps)
+    torch.cuda.synchronize()
+    e2e_ms = ranks.max(1e3 * (time.perf_counter() - t_e2e))
     line = {"metric": METRIC, "value": value, "unit": "vectors/s", "n_gpus": ranks.world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -176,14 +195,17 @@ def run_stream(args, wl):
                        "l2": "inputs > L2: 33 frames = 66 MiB of samples + 132 MiB prepared per step"},
             "e2e": {"value": ranks.world * e2e_steps * nvec / (e2e_ms * 1e-3), "unit": "vectors/s",
                     "h2d_bytes_per_step": int(pin.nbytes), "d2h_bytes_per_step": int(nvec * 13 + k * 40),
-                    "ms_per_step": e2e_ms / e2e_steps},
+                    "ms_per_step": e2e_ms / e2e_steps,
+                    "how": "two PivBatch objects in turn (submit_host / wait_host over pinned frames): upload of "
+                           "33 frames, one graph replay and download of 32 fields per step; host clock, device "
+                           "synchronised at both ends"},
             "gpu_launches": int(batch.kernels() * args.steps), "graph_launches": args.steps,
             "clocks": clocks, "autotuned_variants": tuned, "wall_ms_per_step": 1e3 * wall / args.steps,
             "valid_fraction_last_pair": float(np.mean((res[-1].field.flags & P.flags.INVALID) == 0)),
             "parallelism": f"replicas x{ranks.world}"}
     if ranks.rank == 0:
         print(json.dumps(line), flush=True)
-    del batch
+    del batch, batch2
     ranks.close()
     return 0
 

@@ -222,6 +222,13 @@ int32_t piv_batch_outputs_device(PivBatch* batch, float** dx, float** dy, float*
  * copies the results back; any output may be NULL. Blocking. */
 int32_t piv_batch_run_host(PivBatch* batch, const void* raw, float* dx, float* dy, float* peak_ratio, uint8_t* flags,
                            PivSummaryC* summaries);
+/* As piv_batch_run_host without waiting: the upload, the run and the downloads are queued on the
+ * batch's stream and the call returns; piv_batch_wait_host waits and fills the summaries. Two
+ * batches (each with its own stream) used in turn overlap one's copies with the other's kernels.
+ * `raw` and the outputs should be pinned and must stay valid until the wait returns; a batch
+ * takes a new submission only after the previous one was waited for. */
+int32_t piv_batch_submit_host(PivBatch* batch, const void* raw, float* dx, float* dy, float* peak_ratio, uint8_t* flags);
+int32_t piv_batch_wait_host(PivBatch* batch, PivSummaryC* summaries);
 /* Kernels executed per run (counted on the eager first run; the graph replays the same set). */
 int64_t piv_batch_kernels(const PivBatch* batch);
 

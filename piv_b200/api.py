@@ -561,6 +561,28 @@ class PivBatch:
         return [PairResult(VectorField(g, dx[k], dy[k], ppr[k], fl[k]), ValidationSummary._from_c(sums[k]))
                 for k in range(self.pairs)]
 
+    def submit_host(self, frames, out=None):
+        """run_host without waiting; collect with wait_host(). `frames` and the outputs should be
+        pinned; they are kept alive until the wait."""
+        frames = np.ascontiguousarray(frames, dtype=self.dtype)
+        if frames.shape != (self.nframes, self.height, self.width):
+            raise ShapeMismatchError(f"expected {(self.nframes, self.height, self.width)}, got {frames.shape}")
+        g = self.grid
+        sh = (self.pairs, g.ny, g.nx)
+        if out is None:
+            out = (np.empty(sh, np.float32), np.empty(sh, np.float32), np.empty(sh, np.float32), np.empty(sh, np.uint8))
+        _check(_lib.load().piv_batch_submit_host(self._h, _ptr(frames), *[_ptr(x) for x in out]))
+        self._inflight = (frames, out)
+
+    def wait_host(self):
+        frames, out = self._inflight
+        self._inflight = None
+        sums = (_lib.PivSummaryC * self.pairs)()
+        _check(_lib.load().piv_batch_wait_host(self._h, sums))
+        dx, dy, ppr, fl = out
+        return [PairResult(VectorField(self.grid, dx[k], dy[k], ppr[k], fl[k]), ValidationSummary._from_c(sums[k]))
+                for k in range(self.pairs)]
+
     def close(self):
         if getattr(self, "_h", None):
             _lib.load().piv_batch_destroy(self._h)

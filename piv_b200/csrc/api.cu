@@ -179,6 +179,10 @@ struct PivBatch {
     cudaGraphExec_t exec = nullptr;
     long long kernels = 0;  // kernel launches of the eager run
     int runs = 0;
+    // asynchronous host submission: pinned summary counters and completion event
+    unsigned long long* hsums = nullptr;
+    cudaEvent_t hdone = nullptr;
+    bool pending = false;
 };
 
 namespace {
@@ -1311,6 +1315,8 @@ void piv_batch_destroy(PivBatch* bt) {
     }
     if (bt->exec) cudaGraphExecDestroy(bt->exec);
     if (bt->graph) cudaGraphDestroy(bt->graph);
+    if (bt->hdone) cudaEventDestroy(bt->hdone);
+    if (bt->hsums) cudaFreeHost(bt->hsums);
     for (PivFrame* f : bt->frames) piv_frame_destroy(f);
     cudaFree(bt->raw);
     cudaFree(bt->out);
@@ -1539,6 +1545,48 @@ int32_t piv_batch_run_host(PivBatch* bt, const void* raw, float* dx, float* dy, 
             summaries[k].median_outliers = (int64_t)hs[8 * k + 2];
             summaries[k].out_of_range = (int64_t)hs[8 * k + 3];
             summaries[k].replaced = (int64_t)hs[8 * k + 4];
+        }
+    return PIV_OK;
+}
+
+int32_t piv_batch_submit_host(PivBatch* bt, const void* raw, float* dx, float* dy, float* peak_ratio, uint8_t* flags) {
+    if (!bt || !raw) return fail(PIV_ERR_ARGUMENT, "null argument");
+    if (bt->pending) return fail(PIV_ERR_ARGUMENT, "the previous submission of this batch has not been collected");
+    PivAnalyzer* an = bt->an;
+    int st = use_device(an);
+    if (st) return st;
+    if (!bt->hsums) {
+        CUDA_TRY(cudaHostAlloc((void**)&bt->hsums, sizeof(unsigned long long) * 8 * (size_t)bt->K, cudaHostAllocDefault));
+        CUDA_TRY(cudaEventCreateWithFlags(&bt->hdone, cudaEventDisableTiming));
+    }
+    CUDA_TRY(cudaMemcpyAsync(bt->raw, raw, bt->frame_bytes * bt->frames.size(), cudaMemcpyHostToDevice, an->cur));
+    st = piv_batch_run(bt);
+    if (st) return st;
+    const size_t c = (size_t)bt->cells * (size_t)bt->K;
+    if (dx) CUDA_TRY(cudaMemcpyAsync(dx, bt->dx, 4 * c, cudaMemcpyDeviceToHost, an->cur));
+    if (dy) CUDA_TRY(cudaMemcpyAsync(dy, bt->dy, 4 * c, cudaMemcpyDeviceToHost, an->cur));
+    if (peak_ratio) CUDA_TRY(cudaMemcpyAsync(peak_ratio, bt->ppr, 4 * c, cudaMemcpyDeviceToHost, an->cur));
+    if (flags) CUDA_TRY(cudaMemcpyAsync(flags, bt->flags, c, cudaMemcpyDeviceToHost, an->cur));
+    CUDA_TRY(cudaMemcpyAsync(bt->hsums, bt->sums, sizeof(unsigned long long) * 8 * (size_t)bt->K, cudaMemcpyDeviceToHost,
+                             an->cur));
+    CUDA_TRY(cudaEventRecord(bt->hdone, an->cur));
+    bt->pending = true;
+    return PIV_OK;
+}
+
+int32_t piv_batch_wait_host(PivBatch* bt, PivSummaryC* summaries) {
+    if (!bt) return fail(PIV_ERR_ARGUMENT, "null batch");
+    if (!bt->pending) return fail(PIV_ERR_ARGUMENT, "nothing submitted");
+    int st = use_device(bt->an);
+    if (st) return st;
+    CUDA_TRY(cudaEventSynchronize(bt->hdone));
+    bt->pending = false;
+    st = check_device_error(bt->an->device);
+    if (st) return st;
+    if (summaries)
+        for (int k = 0; k < bt->K; ++k) {
+            const unsigned long long* h = bt->hsums + 8 * (size_t)k;
+            summaries[k] = PivSummaryC{(int64_t)h[0], (int64_t)h[1], (int64_t)h[2], (int64_t)h[3], (int64_t)h[4]};
         }
     return PIV_OK;
 }

@@ -107,3 +107,19 @@ def test_pipeline_matches_per_pair_analysis(depth):
     for j, t in live:
         _same(pl.wait(t), ref[j % k])
     pl.close()
+
+
+def test_asynchronous_host_submission_alternating_batches():
+    """submit_host / wait_host on two batches in turn give the run_host results."""
+    import piv_b200 as P
+    h, w, k = 160, 192, 3
+    an = P.PivAnalyzer(P.PivConfig(windows=[32, 16], overlap=0.5, final_iterations=1))
+    frames = [_frames(k + 1, h, w, s) for s in (31, 32)]
+    ref = [_reference(an, f, [(i, i + 1) for i in range(k)]) for f in frames]
+    bs = [P.PivBatch(an, h, w, k, sequential=True) for _ in range(2)]
+    for rnd in range(3):
+        for b, f in zip(bs, frames):
+            b.submit_host(f)
+        for b, r in zip(bs, ref):
+            for x, y in zip(b.wait_host(), r):
+                _same(x, y)
