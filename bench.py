@@ -533,7 +533,7 @@ def main():
     ap.add_argument("--workload", default="c5", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
-    ap.add_argument("--precision", choices=["fp32", "bf16x3"], default=None,
+    ap.add_argument("--precision", choices=["fp32", "bf16x3", "fp16x3"], default=None,
                     help="correlation arithmetic: FP32 FFTs, or split-BF16 tensor-core DFTs (16 and 32 px windows)")
     ap.add_argument("--deform", type=int, choices=[0, 1], default=None,
                     help="window deformation from the second pass on (default: the workload's setting)")
@@ -552,7 +552,8 @@ def main():
     if args.precision is not None:
         wl["precision"] = args.precision
         if args.precision != "fp32":
-            wl["name"] = wl["name"].replace("FP32 plain", "BF16x3 tensor cores (16/32 px), FP32 elsewhere")
+            wl["name"] = wl["name"].replace("FP32 plain", f"{args.precision.upper()} tensor cores where the autotuner "
+                                            "finds them faster (16/32 px), FP32 elsewhere")
     if args.profile_case:
         return run_profile_case(args, wl)
     if args.impl == "reference":
@@ -735,7 +736,7 @@ def main():
 
     line = {"metric": METRIC, "value": value, "unit": "vectors/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32" if wl.get("precision", "fp32") == "fp32" else "bf16x3+f32", "data": "synthetic",
+            "vs_baseline": None, "dtype": "f32" if wl.get("precision", "fp32") == "fp32" else wl["precision"] + "+f32", "data": "synthetic",
             "config": {"workload": wl["name"], "image": f"{h}x{w} u16 ({wl['bits']}-bit)", "windows": pw,
                        "overlap": wl["overlap"], "final_pass_vectors": nvec, "parallelism": f"replicas x{world}",
                        "l2": "inputs > L2: 2 alternating pairs, 192 MiB of samples + prepared images per step"},

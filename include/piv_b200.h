@@ -65,6 +65,7 @@ typedef enum { PIV_DTYPE_U8 = 0, PIV_DTYPE_U16 = 1, PIV_DTYPE_F32 = 2 } PivDtype
  * kernel (higher precision) for a size where it is faster. */
 #define PIV_PRECISION_FP32 0
 #define PIV_PRECISION_BF16X3 1
+#define PIV_PRECISION_FP16X3 2  /* as BF16X3 with FP16 halves: about 22 significant bits */
 
 /* PivConfig + MaskConfig + ValidationConfig (multipass.rs:22-63, validate.rs:7-37).
  * Defaults of the reference: windows {96, 64}, overlap 0.5, final_iterations 2, mask 0/0,
@@ -84,7 +85,7 @@ typedef struct {
     int32_t deform;         /* 0: windows shift uniformly (the reference, multipass.rs:224-231);
                              * 1: from the second pass on, windows deform with the predictor
                              * (see piv_correlate_deform) */
-    int32_t precision;      /* PIV_PRECISION_FP32 (the reference) or PIV_PRECISION_BF16X3 */
+    int32_t precision;      /* PIV_PRECISION_FP32 (the reference), _BF16X3 or _FP16X3 */
 } PivConfigC;
 
 /* PreprocessConfig (preprocess.rs:5-29) plus the percentile clip of integer codes

@@ -85,7 +85,7 @@ class ValidationConfig:
     replace: bool = True
 
 
-_PRECISIONS = {"fp32": 0, "bf16x3": 1}
+_PRECISIONS = {"fp32": 0, "bf16x3": 1, "fp16x3": 2}
 
 
 @dataclass
@@ -98,8 +98,9 @@ class PivConfig:
     # False: windows shift uniformly (the reference). True: from the second pass on, each window
     # is deformed by the bilinear blend of the predictor at its four corner pixels.
     deform: bool = False
-    # "fp32": FFTs on the FP32 cores (the reference's precision). "bf16x3": DFTs on the tensor
-    # cores with operands split into two BF16 halves (window sizes 16 and 32, uniform windows).
+    # "fp32": FFTs on the FP32 cores (the reference's precision). "bf16x3" / "fp16x3": DFTs on the
+    # tensor cores with operands split into two BF16 / FP16 halves (window sizes 16 and 32,
+    # uniform windows).
     precision: str = "fp32"
 
     def passes(self):

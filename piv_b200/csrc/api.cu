@@ -187,6 +187,8 @@ struct PivBatch {
 
 namespace {
 
+bool split_precision(int32_t p) { return p == PIV_PRECISION_BF16X3 || p == PIV_PRECISION_FP16X3; }
+
 int check_cfg(const PivConfigC* c) {
     // multipass.rs:91-119
     if (!c) return fail(PIV_ERR_ARGUMENT, "null config");
@@ -197,8 +199,9 @@ int check_cfg(const PivConfigC* c) {
     if (!(c->overlap >= 0.0f && c->overlap < 1.0f)) return fail(PIV_ERR_CONFIG, "overlap %g must be in [0, 1)", c->overlap);
     if (c->final_iterations < 1) return fail(PIV_ERR_CONFIG, "final_iterations must be at least 1");
     if (c->deform != 0 && c->deform != 1) return fail(PIV_ERR_CONFIG, "deform must be 0 or 1");
-    if (c->precision != PIV_PRECISION_FP32 && c->precision != PIV_PRECISION_BF16X3)
-        return fail(PIV_ERR_CONFIG, "precision must be PIV_PRECISION_FP32 or PIV_PRECISION_BF16X3");
+    if (c->precision != PIV_PRECISION_FP32 && c->precision != PIV_PRECISION_BF16X3 &&
+        c->precision != PIV_PRECISION_FP16X3)
+        return fail(PIV_ERR_CONFIG, "precision must be PIV_PRECISION_FP32, _BF16X3 or _FP16X3");
     for (int i = 0; i < c->n_windows; ++i)
         if (!corr_supported(c->windows[i]))
             return fail(PIV_ERR_UNSUPPORTED, "window size %d is not supported on the GPU (8, 12, 16, 24, 32, 48, 64, 96, 128)",
@@ -357,7 +360,8 @@ int run_passes(PivAnalyzer* an, const PivFrame* const* a, const PivFrame* const*
         }
         const int nwin = (int)an->pairs[0][i].grid.window;
         const int kind = cps[0].corners ? 1 : 0;
-        const bool tc_ok = kind == 0 && an->precision == PIV_PRECISION_BF16X3 && corr_tc_supported(nwin);
+        const bool tc_ok = kind == 0 && split_precision(an->precision) && corr_tc_supported(nwin);
+        const bool f16 = an->precision == PIV_PRECISION_FP16X3;
         if (tune) {
             // Time every launch variant of this window size on this pass's data (all compute the
             // same results) and keep the fastest for later calls. With tensor cores allowed, the
@@ -383,9 +387,9 @@ int run_passes(PivAnalyzer* an, const PivFrame* const* a, const PivFrame* const*
             }
             an->variant[kind][nwin] = best_v;
             if (tc_ok) {
-                CUDA_TRY(launch_correlate_tc_items(nwin, cps.data(), K, an->cur, &nl));
+                CUDA_TRY(launch_correlate_tc_items(nwin, f16, cps.data(), K, an->cur, &nl));
                 CUDA_TRY(cudaEventRecord(t0, an->cur));
-                for (int r = 0; r < 3; ++r) CUDA_TRY(launch_correlate_tc_items(nwin, cps.data(), K, an->cur, &nl));
+                for (int r = 0; r < 3; ++r) CUDA_TRY(launch_correlate_tc_items(nwin, f16, cps.data(), K, an->cur, &nl));
                 CUDA_TRY(cudaEventRecord(t1, an->cur));
                 CUDA_TRY(cudaEventSynchronize(t1));
                 float ms = 0.0f;
@@ -397,7 +401,7 @@ int run_passes(PivAnalyzer* an, const PivFrame* const* a, const PivFrame* const*
         }
         const bool tensor = tc_ok && !an->fp32_faster[nwin];
         if (tensor)
-            CUDA_TRY(launch_correlate_tc_items(nwin, cps.data(), K, an->cur, &nl));
+            CUDA_TRY(launch_correlate_tc_items(nwin, f16, cps.data(), K, an->cur, &nl));
         else
             CUDA_TRY(launch_correlate_items(nwin, an->variant[kind][nwin], cps.data(), K, an->cur, &nl));
         if (an->profiling) {
@@ -641,8 +645,9 @@ int32_t piv_analyzer_variant(const PivAnalyzer* an, int32_t window, char* name, 
     if (!an || !name || capacity <= 0) return fail(PIV_ERR_ARGUMENT, "bad argument");
     if (!corr_supported(window)) return fail(PIV_ERR_UNSUPPORTED, "window size %d", window);
     const int kind = an->deform ? 1 : 0;
-    if (!an->deform && an->precision == PIV_PRECISION_BF16X3 && corr_tc_supported(window) && !an->fp32_faster[window])
-        snprintf(name, (size_t)capacity, "%d/tensor-core/bf16x3", window);
+    if (!an->deform && split_precision(an->precision) && corr_tc_supported(window) && !an->fp32_faster[window])
+        snprintf(name, (size_t)capacity, "%d/tensor-core/%s", window,
+                 an->precision == PIV_PRECISION_FP16X3 ? "fp16x3" : "bf16x3");
     else
         snprintf(name, (size_t)capacity, "%s", corr_variant_name(window, an->variant[kind][window], kind));
     return PIV_OK;
@@ -972,8 +977,8 @@ int32_t piv_correlate_origins(PivAnalyzer* an, const PivFrame* a, const PivFrame
     if (e == cudaSuccess) e = launch_mask(pp, d_org, (int)ncells, an->cur);
     CorrParams cp{a->image, b->image, (int)a->H, (int)a->W, d_org, d_st, (int)ncells, d_dx, d_dy, d_ppr, d_fl};
     if (e == cudaSuccess)
-        e = (an->precision == PIV_PRECISION_BF16X3 && corr_tc_supported((int)window))
-                ? launch_correlate_tc_items((int)window, &cp, 1, an->cur, nullptr)
+        e = (split_precision(an->precision) && corr_tc_supported((int)window))
+                ? launch_correlate_tc_items((int)window, an->precision == PIV_PRECISION_FP16X3, &cp, 1, an->cur, nullptr)
                 : launch_correlate((int)window, cp, an->cur);
     an->launches += 2;
     if (e == cudaSuccess && dx) e = cudaMemcpyAsync(dx, d_dx, 4 * c, cudaMemcpyDeviceToHost, an->cur);
@@ -1775,8 +1780,9 @@ void PivServer::launch_step(std::vector<Request*>& work) {
         pp.min_std = r->cfg.min_std;
         pps.push_back(pp);
         const int kind = pp.corners ? 1
-                         : (r->cfg.precision == PIV_PRECISION_BF16X3 && corr_tc_supported((int)pb.grid.window)) ? 2
-                                                                                                              : 0;
+                         : (split_precision(r->cfg.precision) && corr_tc_supported((int)pb.grid.window))
+                             ? (r->cfg.precision == PIV_PRECISION_FP16X3 ? 3 : 2)
+                             : 0;
         cps[{(int)pb.grid.window, kind}].push_back(
             CorrParams{r->fa.image, r->fb.image, (int)r->H, (int)r->W, pb.origins, pb.status, (int)pb.cells, pb.raw_dx,
                        pb.raw_dy, pb.raw_ppr, pb.raw_flags, pp.corners, (int)pb.grid.x0, (int)pb.grid.y0,
@@ -1789,8 +1795,9 @@ void PivServer::launch_step(std::vector<Request*>& work) {
     cudaError_t e = launch_place_items(pps.data(), (int)pps.size(), stream, &nl);
     for (auto& kv : cps)
         if (e == cudaSuccess)
-            e = kv.first.second == 2
-                    ? launch_correlate_tc_items(kv.first.first, kv.second.data(), (int)kv.second.size(), stream, &nl)
+            e = kv.first.second >= 2
+                    ? launch_correlate_tc_items(kv.first.first, kv.first.second == 3, kv.second.data(),
+                                                (int)kv.second.size(), stream, &nl)
                     : launch_correlate_items(kv.first.first, variant[kv.first.second][kv.first.first], kv.second.data(),
                                              (int)kv.second.size(), stream, &nl);
     if (e == cudaSuccess) e = launch_validate_items(vps.data(), (int)vps.size(), stream, &nl);

@@ -3,8 +3,15 @@
 //
 // The 2-D DFTs of CorrelationPlan::correlate become dense DFT-matrix products on the 5th-
 // generation tensor cores (tcgen05.mma kind::f16, BF16 operands in shared memory, FP32
-// accumulators in TMEM). Every operand x is split into hi = bf16(x) and lo = bf16(x - hi), and a
-// product A*B is evaluated as hi*hi + lo*hi + hi*lo (about 16 significant bits, FP32 sums).
+// accumulators in TMEM). Every operand x is split into hi = h(x) and lo = h(x - hi), h the
+// rounding to BF16 (about 16 significant bits for the pair) or FP16 (about 22), and a product
+// A*B is evaluated as hi*hi + lo*hi + hi*lo with FP32 sums.
+//
+// Operand ranges: each window is normalised to unit variance before F1 (x * N / sqrt(E)); by
+// Parseval every spectrum is then bounded by N^2 and every cross spectrum by N^4, so the fixed
+// power-of-two factors 2^(12 - 4 log2 N) on the cross spectrum and 1/N before I2 keep all
+// operands inside FP16's range. The correlation plane is rescaled by the exact inverse power of
+// two, which with the normalisation equals the reference's 1 / (n^2 sqrt(Ea Eb)).
 //
 // One warpgroup owns a 128-row tile of 128/N windows; thread i is row i of every operand and
 // TMEM lane i. Real input makes the transforms half-size, so every stage is a 128 x N x K GEMM
@@ -55,6 +62,11 @@ struct TcCfg {
     static constexpr size_t SMEM = ZST_OFF + sizeof(float) * NWG * WPT * 4 * N + 64;
     static_assert((size_t)128 * PLD * 4 <= 2 * A_BYTES, "plane fits in the operand buffers");
     static_assert(N % 16 == 0 && 128 % N == 0, "tile shape");
+    // fixed operand factors (see the top of the file) and the plane's exact rescale
+    static constexpr int LOG2N = N == 16 ? 4 : (N == 32 ? 5 : 6);
+    static constexpr float CROSS_SCALE = (4 * LOG2N > 12) ? 1.0f / (float)(1 << (4 * LOG2N - 12)) : 1.0f;
+    // plane = I2 / (CROSS_SCALE * (1/N)) / N^4, the unit-variance factors N/sqrt(E) included
+    static constexpr float PLANE_SCALE = (float)N / (CROSS_SCALE * (float)N * (float)N * (float)N * (float)N);
 };
 
 // K-major operand of `rows` rows: byte offset of the 16-byte chunk holding (row, k..k+7).
@@ -99,9 +111,10 @@ __device__ __forceinline__ void sample_rows(const float* __restrict__ img, int H
 
 __device__ __forceinline__ void wg_sync(int wg) { asm volatile("bar.sync %0, 128;" ::"r"(wg + 1) : "memory"); }
 
+template <bool F16>
 __device__ __forceinline__ void store_split(uint8_t* hi, uint8_t* lo, uint32_t off, const float (&v)[8]) {
     uint4 h, l;
-    tc::split8_bf16(v, h, l);
+    if constexpr (F16) tc::split8_f16(v, h, l); else tc::split8_bf16(v, h, l);
     *reinterpret_cast<uint4*>(hi + off) = h;
     *reinterpret_cast<uint4*>(lo + off) = l;
 }
@@ -122,7 +135,7 @@ __device__ __forceinline__ void mma_split(uint32_t d, uint32_t a_hi, uint32_t a_
         }
 }
 
-template <int N>
+template <int N, bool F16>
 __global__ void __launch_bounds__(TcCfg<N>::THREADS, 1)
     correlate_tc_kernel(const __grid_constant__ CorrBatch batch, const uint4* __restrict__ mats, int total_tiles,
                         unsigned int* err) {
@@ -218,7 +231,14 @@ __global__ void __launch_bounds__(TcCfg<N>::THREADS, 1)
             }
         }
         ok = ok && e.x > 1e-12f && e.y > 1e-12f;
-        const float scale = 1.0f / ((float)(N * N) * (sqrtf(e.x) * sqrtf(e.y)));
+        {  // unit-variance windows (a flat or masked window is zeroed: its result is discarded)
+            const float ka = ok ? (float)N / sqrtf(e.x) : 0.0f, kb = ok ? (float)N / sqrtf(e.y) : 0.0f;
+#pragma unroll
+            for (int p = 0; p < N; ++p) {
+                z[p].x *= ka;
+                z[p].y *= kb;
+            }
+        }
         // F1 operands, MN-major (m = c*N + r, k = column q); frame b after frame a.
 #pragma unroll
         for (int j = 0; j < N / 8; ++j) {
@@ -229,13 +249,13 @@ __global__ void __launch_bounds__(TcCfg<N>::THREADS, 1)
                 vb[t] = z[8 * j + t].y;
             }
             const uint32_t off = mnmaj_chunk(128, c * N + 8 * j, q);
-            store_split(a_hi, a_lo, off, va);
-            store_split(a_hi + 128 * N * 2, a_lo + 128 * N * 2, off, vb);
+            store_split<F16>(a_hi, a_lo, off, va);
+            store_split<F16>(a_hi + 128 * N * 2, a_lo + 128 * N * 2, off, vb);
         }
         sync_for_mma();
         if (i == 0) {
             tc::fence_after_sync();
-            constexpr uint32_t id = tc::idesc_f16(128, N, true, true);
+            constexpr uint32_t id = tc::idesc_f16(128, N, !F16, true);
             constexpr uint32_t lb = (N / 8) * 128;
             for (int f = 0; f < 2; ++f)
                 mma_split(tmem + f * N, ah + f * 128 * N * 2, al + f * 128 * N * 2, LBO_A, mh + C::R1_OFF * 2,
@@ -259,14 +279,14 @@ __global__ void __launch_bounds__(TcCfg<N>::THREADS, 1)
                     vr[t] = d[(t & 1) * N + 4 * j + (t >> 1)];
                     vi[t] = d[(t & 1) * N + H2 + 4 * j + (t >> 1)];
                 }
-                store_split(a_hi, a_lo, mnmaj_chunk(128, c * N + 8 * j, q), vr);
-                store_split(a_hi, a_lo, mnmaj_chunk(128, c * N + 8 * j, N + q), vi);
+                store_split<F16>(a_hi, a_lo, mnmaj_chunk(128, c * N + 8 * j, q), vr);
+                store_split<F16>(a_hi, a_lo, mnmaj_chunk(128, c * N + 8 * j, N + q), vi);
             }
         }
         sync_for_mma();
         if (i == 0) {
             tc::fence_after_sync();
-            constexpr uint32_t id = tc::idesc_f16(128, 2 * N, true, true);
+            constexpr uint32_t id = tc::idesc_f16(128, 2 * N, !F16, true);
             constexpr uint32_t lb = (2 * N / 8) * 128;
             mma_split(tmem, ah, al, LBO_A, mh + C::R2_OFF * 2, ml + C::R2_OFF * 2, lb, 2 * N / 16, id);
             tc::mma_commit(bar);
@@ -303,13 +323,13 @@ __global__ void __launch_bounds__(TcCfg<N>::THREADS, 1)
                     const float oai = __shfl_xor_sync(0xffffffffu, zi[ky], 1);
                     const float far_ = fr ? oar : zr[ky], fai = fr ? oai : zi[ky];
                     const float fbr = fr ? zr[ky] : oar, fbi = fr ? zi[ky] : oai;
-                    const float sg = (fr && (ky & 1)) ? -1.0f : 1.0f;  // frame-1 lane: (-1)^ky
+                    const float sg = (fr && (ky & 1)) ? -C::CROSS_SCALE : C::CROSS_SCALE;  // frame-1 lane: (-1)^ky
                     pr[t] = sg * (far_ * fbr + fai * fbi);
                     pi[t] = sg * (far_ * fbi - fai * fbr);
                 }
                 if (!dcrow) {
-                    store_split(a_hi, a_lo, kmaj_chunk(128, i, 8 * j), pr);
-                    store_split(a_hi, a_lo, kmaj_chunk(128, i, N + 8 * j), pi);
+                    store_split<F16>(a_hi, a_lo, kmaj_chunk(128, i, 8 * j), pr);
+                    store_split<F16>(a_hi, a_lo, kmaj_chunk(128, i, N + 8 * j), pi);
                 }
             }
         }
@@ -329,23 +349,30 @@ __global__ void __launch_bounds__(TcCfg<N>::THREADS, 1)
             if (ky == 0) a0r = a0i = b0r = b0i = 0.0f;
             const float c0r = a0r * b0r + a0i * b0i, c0i = a0r * b0i - a0i * b0r;
             const float cnr = anr * bnr + ani * bni, cni = anr * bni - ani * bnr;
-            const float prr = c0r - cni, pri = c0i + cnr;
+            const float prr = (c0r - cni) * C::CROSS_SCALE, pri = (c0i + cnr) * C::CROSS_SCALE;
             const float sg = (ky & 1) ? -1.0f : 1.0f;
             const float vals[4] = {prr, pri, sg * prr, sg * pri};
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 const int row = c * N + (u >> 1), k = (u & 1) * N + ky;
                 const uint32_t off = kmaj_chunk(128, row, k) + (k & 7) * 2;
-                const __nv_bfloat16 h = __float2bfloat16_rn(vals[u]);
-                const __nv_bfloat16 l = __float2bfloat16_rn(vals[u] - __bfloat162float(h));
-                *reinterpret_cast<__nv_bfloat16*>(a_hi + off) = h;
-                *reinterpret_cast<__nv_bfloat16*>(a_lo + off) = l;
+                if constexpr (F16) {
+                    const __half h = __float2half_rn(vals[u]);
+                    const __half l = __float2half_rn(vals[u] - __half2float(h));
+                    *reinterpret_cast<__half*>(a_hi + off) = h;
+                    *reinterpret_cast<__half*>(a_lo + off) = l;
+                } else {
+                    const __nv_bfloat16 h = __float2bfloat16_rn(vals[u]);
+                    const __nv_bfloat16 l = __float2bfloat16_rn(vals[u] - __bfloat162float(h));
+                    *reinterpret_cast<__nv_bfloat16*>(a_hi + off) = h;
+                    *reinterpret_cast<__nv_bfloat16*>(a_lo + off) = l;
+                }
             }
         }
         sync_for_mma();
         if (i == 0) {
             tc::fence_after_sync();
-            constexpr uint32_t id = tc::idesc_f16(128, N, true, false);
+            constexpr uint32_t id = tc::idesc_f16(128, N, !F16, false);
             constexpr uint32_t lb = (N / 8) * 128;
             mma_split(tmem, ah, al, LBO_A, mh + C::R3_OFF * 2, ml + C::R3_OFF * 2, lb, 2 * N / 16, id);
             tc::mma_commit(bar);
@@ -365,18 +392,18 @@ __global__ void __launch_bounds__(TcCfg<N>::THREADS, 1)
                 float vr[8], vi[8];
 #pragma unroll
                 for (int t = 0; t < 8; ++t) {
-                    vr[t] = g[8 * j + t];
-                    vi[t] = g[H2 + 8 * j + t];
+                    vr[t] = g[8 * j + t] * (1.0f / (float)N);
+                    vi[t] = g[H2 + 8 * j + t] * (1.0f / (float)N);
                 }
                 const int m = c * N + fr * H2 + 8 * j;
-                store_split(a_hi, a_lo, mnmaj_chunk(128, m, kxp), vr);
-                store_split(a_hi, a_lo, mnmaj_chunk(128, m, H2 + kxp), vi);
+                store_split<F16>(a_hi, a_lo, mnmaj_chunk(128, m, kxp), vr);
+                store_split<F16>(a_hi, a_lo, mnmaj_chunk(128, m, H2 + kxp), vi);
             }
         }
         sync_for_mma();
         if (i == 0) {
             tc::fence_after_sync();
-            constexpr uint32_t id = tc::idesc_f16(128, N, true, true);
+            constexpr uint32_t id = tc::idesc_f16(128, N, !F16, true);
             constexpr uint32_t lb = (N / 8) * 128;
             mma_split(tmem, ah, al, LBO_A, mh + C::R4_OFF * 2, ml + C::R4_OFF * 2, lb, N / 16, id);
             tc::mma_commit(bar);
@@ -393,10 +420,10 @@ __global__ void __launch_bounds__(TcCfg<N>::THREADS, 1)
         float* prow = plane + (size_t)(c * N) * C::PLD;  // window c's plane
 #pragma unroll
         for (int x = 0; x < N; x += 4) {
-            v[x] *= scale;
-            v[x + 1] *= scale;
-            v[x + 2] *= scale;
-            v[x + 3] *= scale;
+            v[x] *= C::PLANE_SCALE;
+            v[x + 1] *= C::PLANE_SCALE;
+            v[x + 2] *= C::PLANE_SCALE;
+            v[x + 3] *= C::PLANE_SCALE;
             *reinterpret_cast<float4*>(prow + y * C::PLD + x) = make_float4(v[x], v[x + 1], v[x + 2], v[x + 3]);
         }
         // argmax, lowest row-major index on ties
@@ -519,7 +546,19 @@ static double cs(long long k, int n, bool sine) {
     return sine ? std::sin(a) : std::cos(a);
 }
 
-template <int N>
+static uint16_t f16_rn(float f) {
+    const __half h = __float2half_rn(f);
+    uint16_t u;
+    std::memcpy(&u, &h, 2);
+    return u;
+}
+static float f16_f(uint16_t u) {
+    __half h;
+    std::memcpy(&h, &u, 2);
+    return __half2float(h);
+}
+
+template <int N, bool F16>
 static std::vector<uint16_t> build_mats() {
     using C = TcCfg<N>;
     constexpr int H2 = N / 2;
@@ -527,8 +566,8 @@ static std::vector<uint16_t> build_mats() {
     auto put = [&](int off, int rows, int row, int k, double val) {
         const size_t e = (size_t)off + (size_t)(k >> 3) * (rows >> 3) * 64 + (size_t)(row >> 3) * 64 + (row & 7) * 8 +
                          (k & 7);  // element index of the K-major layout (64 elements per core)
-        const uint16_t h = bf16_rne((float)val);
-        const uint16_t l = bf16_rne((float)(val - (double)bf16_f(h)));
+        const uint16_t h = F16 ? f16_rn((float)val) : bf16_rne((float)val);
+        const uint16_t l = F16 ? f16_rn((float)(val - (double)f16_f(h))) : bf16_rne((float)(val - (double)bf16_f(h)));
         img[e] = h;
         img[(size_t)C::RMAT + e] = l;
     };
@@ -572,15 +611,15 @@ static std::vector<uint16_t> build_mats() {
 
 namespace {
 constexpr int kMaxDevices = 64;
-const uint4* g_mats16[kMaxDevices] = {};
-const uint4* g_mats32[kMaxDevices] = {};
+// DFT matrix images per device: [size 16 | size 32][BF16 | FP16]
+const uint4* g_mats[kMaxDevices][2][2] = {};
 unsigned int* g_err_host[kMaxDevices] = {};
 unsigned int* g_err_dev[kMaxDevices] = {};
 
-template <int N>
+template <int N, bool F16>
 cudaError_t upload(const uint4** slot) {
     if (*slot) return cudaSuccess;
-    const std::vector<uint16_t> img = build_mats<N>();
+    const std::vector<uint16_t> img = build_mats<N, F16>();
     void* d = nullptr;
     cudaError_t e = cudaMalloc(&d, img.size() * 2);
     if (e != cudaSuccess) return e;
@@ -601,8 +640,10 @@ cudaError_t corr_tc_init_device() {
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-    e = upload<16>(&g_mats16[dev]);
-    if (e == cudaSuccess) e = upload<32>(&g_mats32[dev]);
+    e = upload<16, false>(&g_mats[dev][0][0]);
+    if (e == cudaSuccess) e = upload<16, true>(&g_mats[dev][0][1]);
+    if (e == cudaSuccess) e = upload<32, false>(&g_mats[dev][1][0]);
+    if (e == cudaSuccess) e = upload<32, true>(&g_mats[dev][1][1]);
     if (e == cudaSuccess && !g_err_host[dev]) {
         e = cudaHostAlloc(reinterpret_cast<void**>(&g_err_host[dev]), sizeof(unsigned int), cudaHostAllocMapped);
         if (e == cudaSuccess) {
@@ -617,7 +658,7 @@ unsigned int corr_tc_error(int device) {
     return (device >= 0 && device < kMaxDevices && g_err_host[device]) ? *(volatile unsigned int*)g_err_host[device] : 0u;
 }
 
-template <int N>
+template <int N, bool F16>
 static cudaError_t launch_tc(CorrBatch b, cudaStream_t s, const uint4* mats, unsigned int* err) {
     using C = TcCfg<N>;
     long long total = 0;
@@ -632,7 +673,7 @@ static cudaError_t launch_tc(CorrBatch b, cudaStream_t s, const uint4* mats, uns
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
-    auto kern = correlate_tc_kernel<N>;
+    auto kern = correlate_tc_kernel<N, F16>;
     e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
     if (e != cudaSuccess) return e;
     const long long ctas = std::min<long long>((total + C::NWG - 1) / C::NWG, (long long)sms);
@@ -640,7 +681,8 @@ static cudaError_t launch_tc(CorrBatch b, cudaStream_t s, const uint4* mats, uns
     return cudaGetLastError();
 }
 
-cudaError_t launch_correlate_tc_items(int n, const CorrParams* items, int count, cudaStream_t s, int* launches) {
+cudaError_t launch_correlate_tc_items(int n, bool f16, const CorrParams* items, int count, cudaStream_t s,
+                                      int* launches) {
     if (count <= 0) return cudaSuccess;
     if (!corr_tc_supported(n)) return cudaErrorInvalidValue;
     for (int i = 0; i < count; ++i)
@@ -653,7 +695,11 @@ cudaError_t launch_correlate_tc_items(int n, const CorrParams* items, int count,
         CorrBatch b;
         b.n = count - off < kMaxBatch ? count - off : kMaxBatch;
         for (int i = 0; i < b.n; ++i) b.item[i] = items[off + i];
-        e = n == 16 ? launch_tc<16>(b, s, g_mats16[dev], g_err_dev[dev]) : launch_tc<32>(b, s, g_mats32[dev], g_err_dev[dev]);
+        const uint4* m = g_mats[dev][n == 16 ? 0 : 1][f16 ? 1 : 0];
+        if (n == 16)
+            e = f16 ? launch_tc<16, true>(b, s, m, g_err_dev[dev]) : launch_tc<16, false>(b, s, m, g_err_dev[dev]);
+        else
+            e = f16 ? launch_tc<32, true>(b, s, m, g_err_dev[dev]) : launch_tc<32, false>(b, s, m, g_err_dev[dev]);
         if (e != cudaSuccess) return e;
         if (launches) ++*launches;
     }

@@ -61,13 +61,15 @@ cudaError_t launch_correlate_variant(int n, int v, const CorrParams& p, cudaStre
 // All items share window size n and either all have corners (deformed windows) or none; v
 // indexes the variants of that kind. Returns the number of launches issued in *launches.
 cudaError_t launch_correlate_items(int n, int v, const CorrParams* items, int count, cudaStream_t s, int* launches);
-// Split-precision (BF16 hi/lo, three products) tensor-core correlation, window sizes 16 and 32;
+// Split-precision (BF16 or FP16 hi/lo, three products) tensor-core correlation, window sizes 16
+// and 32;
 // uniform windows only. corr_tc_init_device uploads its DFT matrices to the current device;
 // corr_tc_error reads the device's error word (non-zero after a tensor-core wait ran out).
 bool corr_tc_supported(int n);
 cudaError_t corr_tc_init_device();
 unsigned int corr_tc_error(int device);
-cudaError_t launch_correlate_tc_items(int n, const CorrParams* items, int count, cudaStream_t s, int* launches);
+cudaError_t launch_correlate_tc_items(int n, bool f16, const CorrParams* items, int count, cudaStream_t s,
+                                      int* launches);
 // D (128 x n) = A (128 x k) * B (n x k)^T on the tensor cores, BF16 operands (device pointers).
 cudaError_t tc_selftest(int a_mn, int n, int k, const float* a, const float* b, float* d);
 // Number of kernel launches launch_correlate issues (for launch accounting).

@@ -15,6 +15,7 @@
 
 #include <cstdint>
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 namespace pivb200 {
 namespace tc {
@@ -149,6 +150,21 @@ __device__ __forceinline__ void split8_bf16(const float (&x)[8], uint4& hi, uint
         const __nv_bfloat162 hp = __floats2bfloat162_rn(x[2 * i], x[2 * i + 1]);
         const float2 hf = __bfloat1622float2(hp);
         const __nv_bfloat162 lp = __floats2bfloat162_rn(x[2 * i] - hf.x, x[2 * i + 1] - hf.y);
+        h[i] = *reinterpret_cast<const uint32_t*>(&hp);
+        l[i] = *reinterpret_cast<const uint32_t*>(&lp);
+    }
+    hi = make_uint4(h[0], h[1], h[2], h[3]);
+    lo = make_uint4(l[0], l[1], l[2], l[3]);
+}
+
+// The same with FP16 halves (about 22 significant bits; operands must lie within FP16's range).
+__device__ __forceinline__ void split8_f16(const float (&x)[8], uint4& hi, uint4& lo) {
+    uint32_t h[4], l[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const __half2 hp = __floats2half2_rn(x[2 * i], x[2 * i + 1]);
+        const float2 hf = __half22float2(hp);
+        const __half2 lp = __floats2half2_rn(x[2 * i] - hf.x, x[2 * i + 1] - hf.y);
         h[i] = *reinterpret_cast<const uint32_t*>(&hp);
         l[i] = *reinterpret_cast<const uint32_t*>(&lp);
     }

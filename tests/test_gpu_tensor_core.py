@@ -1,4 +1,4 @@
-"""The split-precision tensor-core correlation (precision "bf16x3").
+"""The split-precision tensor-core correlation (precisions "bf16x3" and "fp16x3").
 
 1. The tcgen05 building blocks: a 128 x n x k GEMM with the operand layouts the correlation uses
    (A K-major and MN-major, B K-major, FP32 accumulators read back from TMEM), exact on small
@@ -44,12 +44,11 @@ def _pair(h, seed=4, vmax=6.0):
     return S.baseline_pair(h, h, seed, f, ppp=0.05, dmin=2.0, dmax=4.0, bits=12)
 
 
-@pytest.mark.parametrize("n", [32, 16])
-def test_one_pass_against_fp64_oracle(n):
+def _one_pass_errors(n, precision):
     import piv_b200 as P
     h = 320
     a, b = _pair(h)
-    an = P.PivAnalyzer(P.PivConfig(windows=[n], overlap=0.5, final_iterations=1, precision="bf16x3"))
+    an = P.PivAnalyzer(P.PivConfig(windows=[n], overlap=0.5, final_iterations=1, precision=precision))
     fa, fb = an.prepare(a, P.RAW), an.prepare(b, P.RAW)
     g = an.output_grid(h, h)
     # shifted, fractional origins exercise the bilinear sampler
@@ -68,19 +67,33 @@ def test_one_pass_against_fp64_oracle(n):
     # peaks whose sub-pixel offset sits at +-0.5 may round either way
     ambiguous = np.abs(np.abs(od - oo - np.round(od - oo)) - 0.5) < 1e-3
     assert np.mean((np.round(gd - oo) == np.round(od - oo)) | ambiguous) == 1.0
-    err = np.abs(gd - od)
+    return np.abs(gd - od)
+
+
+@pytest.mark.parametrize("precision", ["bf16x3", "fp16x3"])
+@pytest.mark.parametrize("n", [32, 16])
+def test_one_pass_against_fp64_oracle(n, precision):
+    err = _one_pass_errors(n, precision)
     assert np.sqrt(np.mean(err ** 2)) < 1e-3, np.sqrt(np.mean(err ** 2))
     assert np.quantile(err, 0.999) < 0.01
 
 
+@pytest.mark.parametrize("n", [32, 16])
+def test_fp16_halves_are_more_accurate_than_bf16(n):
+    e16 = _one_pass_errors(n, "fp16x3")
+    eb = _one_pass_errors(n, "bf16x3")
+    assert np.sqrt(np.mean(e16 ** 2)) < 0.5 * np.sqrt(np.mean(eb ** 2))
+
+
+@pytest.mark.parametrize("precision", ["bf16x3", "fp16x3"])
 @pytest.mark.parametrize("windows,overlap", [([64, 32, 16], 0.5), ([128, 64, 32, 16], 0.75), ([32, 16], 0.5)])
-def test_pipeline_within_0p01_px_rms_of_fp64(windows, overlap):
+def test_pipeline_within_0p01_px_rms_of_fp64(windows, overlap, precision):
     import piv_b200 as P
     from piv_b200 import synthetic as S
     h = 512
     f = S.vortex_shear_field(h, h, vmax=8.0, shear=0.01)
     a, b = S.baseline_pair(h, h, 9, f, ppp=0.05, dmin=2.0, dmax=4.0, bits=12)
-    an = P.PivAnalyzer(P.PivConfig(windows=windows, overlap=overlap, final_iterations=1, precision="bf16x3"))
+    an = P.PivAnalyzer(P.PivConfig(windows=windows, overlap=overlap, final_iterations=1, precision=precision))
     r = an.analyze(an.prepare(a, P.RAW), an.prepare(b, P.RAW))
     ref, _, _ = O.analyze(O.OracleConfig(windows, overlap, 1), O.u16_to_f32(a), O.u16_to_f32(b), mode=O.FP64)
     ok = (ref["flags"] == 0) & (r.field.flags == 0)
@@ -90,11 +103,12 @@ def test_pipeline_within_0p01_px_rms_of_fp64(windows, overlap):
     assert np.mean(ref["flags"] == r.field.flags) > 0.99
 
 
-def test_batch_and_server_forms_match_the_analyzer():
+@pytest.mark.parametrize("precision", ["bf16x3", "fp16x3"])
+def test_batch_and_server_forms_match_the_analyzer(precision):
     import piv_b200 as P
     h = w = 256
     frames = np.stack([x for s in range(3) for x in _pair(h, seed=20 + s)])
-    cfg = P.PivConfig(windows=[64, 32, 16], overlap=0.5, final_iterations=1, precision="bf16x3")
+    cfg = P.PivConfig(windows=[64, 32, 16], overlap=0.5, final_iterations=1, precision=precision)
     an = P.PivAnalyzer(cfg)
     ref = [an.analyze(an.prepare(frames[2 * k], P.RAW), an.prepare(frames[2 * k + 1], P.RAW)) for k in range(3)]
     batch = P.PivBatch(an, h, w, 3, sequential=False)
