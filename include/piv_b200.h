@@ -143,6 +143,10 @@ int64_t piv_analyzer_launches(const PivAnalyzer* an);
  * size for this analyzer. Variants of one size differ only in threads per block, register cap
  * and sampler, never in arithmetic: results are bit-identical whichever is chosen. Blocking. */
 int32_t piv_analyzer_autotune(PivAnalyzer* an, const PivFrame* a, const PivFrame* b);
+/* Launch variants of the FP32 kernel for `window` (uniform windows), and pinning one of them for
+ * this analyzer (for tests and external tuning; results are identical whichever is used). */
+int32_t piv_num_variants(int32_t window);
+int32_t piv_analyzer_set_variant(PivAnalyzer* an, int32_t window, int32_t variant);
 /* Name of the variant in use for `window` ("<n>/T<lanes per line>/G<groups>/B<min blocks>/<sampler>"). */
 int32_t piv_analyzer_variant(const PivAnalyzer* an, int32_t window, char* name, int32_t capacity);
 /* Stage timing (no counterpart in the reference, which has only wall-clock splits,

@@ -18,7 +18,8 @@ EXPORTS = [
     "piv_abi_version", "piv_last_error", "piv_grid", "piv_check_config",
     "piv_analyzer_create", "piv_analyzer_destroy", "piv_num_passes", "piv_output_grid", "piv_pass_grid",
     "piv_analyzer_set_stream", "piv_analyzer_sync", "piv_analyzer_launches", "piv_analyzer_set_profiling",
-    "piv_analyzer_profile", "piv_analyzer_autotune", "piv_analyzer_variant",
+    "piv_analyzer_profile", "piv_analyzer_autotune", "piv_analyzer_variant", "piv_num_variants",
+    "piv_analyzer_set_variant",
     "piv_frame_create", "piv_frame_destroy", "piv_frame_prepare", "piv_frame_prepare_device",
     "piv_frame_set_prepared", "piv_frame_download", "piv_frame_image_device", "piv_background_device",
     "piv_analyze", "piv_analyze_device", "piv_analyze_traced", "piv_analyze_batch_device",
@@ -130,6 +131,8 @@ def load():
         "piv_analyzer_profile": ([vp, i32, P(ctypes.c_double), P(i64)], i32),
         "piv_analyzer_autotune": ([vp, vp, vp], i32),
         "piv_analyzer_variant": ([vp, i32, ctypes.c_char_p, i32], i32),
+        "piv_num_variants": ([i32], i32),
+        "piv_analyzer_set_variant": ([vp, i32, i32], i32),
         "piv_frame_create": ([vp, i64, i64, P(vp)], i32),
         "piv_frame_destroy": ([vp], None),
         "piv_frame_prepare": ([vp, vp, vp, i32, P(PivPreprocessC), vp], i32),

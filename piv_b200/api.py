@@ -500,10 +500,19 @@ def _profile_methods():
         _check(_lib.load().piv_analyzer_variant(self._h, int(window), buf, 64))
         return buf.value.decode()
 
+    def set_variant(self, window, v):
+        """Pins FP32 launch variant `v` (0 .. num_variants(window) - 1) for `window`."""
+        _check(_lib.load().piv_analyzer_set_variant(self._h, int(window), int(v)))
+
+    def num_variants(window):
+        return int(_lib.load().piv_num_variants(int(window)))
+
     PivAnalyzer.set_profiling = set_profiling
     PivAnalyzer.profile = profile
     PivAnalyzer.autotune = autotune
     PivAnalyzer.variant = variant
+    PivAnalyzer.set_variant = set_variant
+    PivAnalyzer.num_variants = staticmethod(num_variants)
 
 
 _profile_methods()

@@ -653,6 +653,19 @@ int32_t piv_analyzer_variant(const PivAnalyzer* an, int32_t window, char* name, 
     return PIV_OK;
 }
 
+int32_t piv_num_variants(int32_t window) { return corr_supported(window) ? corr_num_variants(window, false) : 0; }
+
+int32_t piv_analyzer_set_variant(PivAnalyzer* an, int32_t window, int32_t v) {
+    if (!an) return fail(PIV_ERR_ARGUMENT, "null analyzer");
+    if (!corr_supported(window)) return fail(PIV_ERR_UNSUPPORTED, "window size %d", window);
+    const int kind = an->deform ? 1 : 0;
+    if (v < 0 || v >= corr_num_variants(window, kind))
+        return fail(PIV_ERR_ARGUMENT, "variant %d out of range for window %d", v, window);
+    an->variant[kind][window] = v;
+    an->fp32_faster[window] = true;  // an explicit FP32 launch variant
+    return PIV_OK;
+}
+
 int32_t piv_analyzer_set_profiling(PivAnalyzer* an, int32_t enable) {
     if (!an) return fail(PIV_ERR_ARGUMENT, "null analyzer");
     an->profiling = enable != 0;

@@ -505,16 +505,18 @@ struct CorrVariant {
 
 #define PIV_V(N, T, PR, G, MB, SH) {#N "/T" #T "/G" #G "/B" #MB "/" #SH, &launch_t<CorrCfg<N, T, PR, G, MB, SH>>}
 static const CorrVariant kV8[] = {PIV_V(8, 1, true, 32, 1, false), PIV_V(8, 1, true, 16, 2, false),
-                                  PIV_V(8, 1, true, 32, 2, true)};
+                                  PIV_V(8, 1, true, 32, 2, true), PIV_V(8, 1, true, 4, 16, false)};
 static const CorrVariant kV12[] = {PIV_V(12, 1, true, 16, 1, false), PIV_V(12, 1, true, 8, 3, false),
                                    PIV_V(12, 1, true, 16, 2, true)};
 static const CorrVariant kV16[] = {PIV_V(16, 1, true, 16, 2, false), PIV_V(16, 1, true, 8, 4, false),
                                    PIV_V(16, 1, true, 8, 3, false), PIV_V(16, 1, true, 16, 2, true),
-                                   PIV_V(16, 1, true, 8, 4, true)};
+                                   PIV_V(16, 1, true, 8, 4, true), PIV_V(16, 1, true, 2, 16, false),
+                                   PIV_V(16, 1, true, 4, 8, false), PIV_V(16, 1, true, 2, 16, true)};
 static const CorrVariant kV24[] = {PIV_V(24, 2, true, 4, 2, true), PIV_V(24, 2, true, 4, 2, false),
                                    PIV_V(24, 2, true, 2, 4, true)};
 static const CorrVariant kV32[] = {PIV_V(32, 2, true, 4, 2, true), PIV_V(32, 2, true, 4, 2, false),
-                                   PIV_V(32, 2, true, 2, 4, true), PIV_V(32, 2, true, 2, 3, true)};
+                                   PIV_V(32, 2, true, 2, 4, true), PIV_V(32, 2, true, 2, 3, true),
+                                   PIV_V(32, 2, true, 1, 8, true), PIV_V(32, 2, true, 1, 8, false)};
 static const CorrVariant kV48[] = {PIV_V(48, 4, true, 1, 2, true), PIV_V(48, 4, true, 1, 2, false),
                                    PIV_V(48, 4, true, 1, 1, true)};
 static const CorrVariant kV64[] = {PIV_V(64, 4, true, 1, 2, true), PIV_V(64, 4, true, 1, 2, false),

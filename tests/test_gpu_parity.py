@@ -189,3 +189,24 @@ def test_autotuned_variants_give_identical_results():
             assert np.array_equal(x.raw.flags, y.raw.flags)
             assert same_floats(x.raw.dx, y.raw.dx) and same_floats(x.raw.dy, y.raw.dy)
             assert same_floats(x.raw.peak_ratio, y.raw.peak_ratio)
+
+
+def test_every_launch_variant_gives_identical_results():
+    """Each FP32 launch variant of each window size (groups per CTA, register cap, sampler) gives
+    the bit-identical field: the variants share the FFT decomposition and every rounding."""
+    import piv_b200 as P
+    from piv_b200 import synthetic as S
+    a, b = S.particle_pair(288, 288, 23, 0.05, 0.75, lambda x, y: (3.1 + 0.01 * y, -2.2 + 0.003 * x))
+    for windows in ([128, 64, 32, 16], [96, 48, 24, 12], [64, 32, 16, 8]):
+        an = P.PivAnalyzer(P.PivConfig(windows=windows, overlap=0.75, final_iterations=1))
+        fa, fb = an.prepare(a, P.RAW), an.prepare(b, P.RAW)
+        _, ref = an.analyze_traced(fa, fb)
+        counts = {n: P.PivAnalyzer.num_variants(n) for n in windows}
+        for k in range(1, max(counts.values())):
+            for n in windows:
+                an.set_variant(n, min(k, counts[n] - 1))
+            _, got = an.analyze_traced(fa, fb)
+            for x, y in zip(ref, got):
+                assert np.array_equal(x.raw.flags, y.raw.flags), (windows, k)
+                assert same_floats(x.raw.dx, y.raw.dx) and same_floats(x.raw.dy, y.raw.dy), (windows, k)
+                assert same_floats(x.raw.peak_ratio, y.raw.peak_ratio), (windows, k)
