@@ -239,8 +239,10 @@ int64_t piv_batch_kernels(const PivBatch* batch);
 
 /* Pipelined pairs (no counterpart in the reference, which analyses pairs one after another,
  * analyze.rs:441): pairs of HOST frames are submitted without waiting; `depth` slots, each with
- * its own stream, prepared frames and workspace, let the uploads and downloads of one pair overlap
- * the kernels of the others. Each result equals piv_analyze of that pair. Host buffers should be
+ * its own prepared frames and workspace, let the uploads and downloads of one pair overlap the
+ * kernels of the others. Uploads, kernels and downloads go on three streams shared by the slots,
+ * so the kernels of successive pairs run in submission order. Each result equals piv_analyze of
+ * that pair. Host buffers should be
  * pinned (cudaHostAlloc) for the copies to be asynchronous, and must stay valid (outputs
  * untouched) until piv_pipeline_wait returns for that ticket. Submitting blocks only when the
  * next slot still holds an unfinished pair. */

@@ -1343,9 +1343,12 @@ void piv_batch_destroy(PivBatch* bt) {
 }
 
 // ---------------------------------------------------------------------------------------------
-// Pipelined pairs: `depth` slots, each a private analyzer with its own stream and frames. A
-// submitted pair's uploads, preparation, passes and downloads are queued on its slot's stream,
-// so the copies of one pair overlap the kernels of the others.
+// Pipelined pairs: `depth` slots, each a private analyzer (workspace) with its own frames, and
+// three streams shared by the slots. A submitted pair's uploads go on the upload stream, its
+// preparation and passes on the compute stream (after the uploads), its downloads on the
+// download stream (after the passes). The copies of one pair overlap the kernels of the others,
+// while the kernels of different pairs run one after another as in a single analyzer, so they
+// never compete for the SMs. A slot is reused only after its previous pair fully completed.
 // ---------------------------------------------------------------------------------------------
 struct PivPipeline {
     struct Slot {
@@ -1353,9 +1356,12 @@ struct PivPipeline {
         PivFrame* fa = nullptr;
         PivFrame* fb = nullptr;
         unsigned long long* sums = nullptr;  // pinned: 5 counters of the slot's last pair
-        cudaEvent_t done = nullptr;
+        cudaEvent_t uploaded = nullptr;       // on the upload stream
+        cudaEvent_t computed = nullptr;       // on the compute stream
+        cudaEvent_t done = nullptr;           // on the download stream
         uint64_t ticket = 0;  // 0: idle
     };
+    cudaStream_t up = nullptr, comp = nullptr, down = nullptr;
     int device = 0;
     int64_t H = 0, W = 0;
     int32_t dtype = PIV_DTYPE_U16;
@@ -1398,15 +1404,28 @@ int32_t piv_pipeline_create(const PivAnalyzer* parent, int64_t height, int64_t w
     pl->dtype = dtype;
     pl->pre = pre ? *pre : PivPreprocessC{1.0f, 4, 0.02f, 0.0};
     pl->slots.resize((size_t)depth);
+    {
+        cudaError_t e = cudaStreamCreateWithFlags(&pl->up, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&pl->comp, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&pl->down, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            piv_pipeline_destroy(pl);
+            return fail(PIV_ERR_CUDA, "pipeline streams: %s", cudaGetErrorString(e));
+        }
+    }
+    const size_t raw_bytes = dtype_size(dtype) * (size_t)height * (size_t)width;
     for (auto& s : pl->slots) {
         s.an = clone_config(parent);
-        cudaError_t e = cudaStreamCreateWithFlags(&s.an->own, cudaStreamNonBlocking);
-        s.an->cur = s.an->own;
+        s.an->cur = pl->comp;
+        cudaError_t e = cudaEventCreateWithFlags(&s.uploaded, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.computed, cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.sums, 8 * sizeof(unsigned long long), cudaHostAllocDefault);
         int st = e == cudaSuccess ? PIV_OK : fail(PIV_ERR_CUDA, "pipeline slot: %s", cudaGetErrorString(e));
         if (!st) st = piv_frame_create(s.an, height, width, &s.fa);
         if (!st) st = piv_frame_create(s.an, height, width, &s.fb);
+        if (!st) st = stage_raw(s.fa, raw_bytes);
+        if (!st) st = stage_raw(s.fb, raw_bytes);
         if (st) {
             piv_pipeline_destroy(pl);
             return st;
@@ -1419,14 +1438,18 @@ int32_t piv_pipeline_create(const PivAnalyzer* parent, int64_t height, int64_t w
 void piv_pipeline_destroy(PivPipeline* pl) {
     if (!pl) return;
     cudaSetDevice(pl->device);
+    for (cudaStream_t st : {pl->up, pl->comp, pl->down})
+        if (st) cudaStreamSynchronize(st);
     for (auto& s : pl->slots) {
-        if (s.an && s.an->own) cudaStreamSynchronize(s.an->own);
         if (s.fa) piv_frame_destroy(s.fa);
         if (s.fb) piv_frame_destroy(s.fb);
-        if (s.done) cudaEventDestroy(s.done);
+        for (cudaEvent_t ev : {s.uploaded, s.computed, s.done})
+            if (ev) cudaEventDestroy(ev);
         if (s.sums) cudaFreeHost(s.sums);
         piv_analyzer_destroy(s.an);
     }
+    for (cudaStream_t st : {pl->up, pl->comp, pl->down})
+        if (st) cudaStreamDestroy(st);
     delete pl;
 }
 
@@ -1439,13 +1462,20 @@ int32_t piv_pipeline_submit(PivPipeline* pl, const void* frame_a, const void* fr
         int st = retire_slot(pl, s, nullptr);
         if (st) return st;
     }
-    int st = piv_frame_prepare(s.an, s.fa, frame_a, pl->dtype, &pl->pre, nullptr);
-    if (!st) st = piv_frame_prepare(s.an, s.fb, frame_b, pl->dtype, &pl->pre, nullptr);
+    const size_t raw_bytes = dtype_size(pl->dtype) * (size_t)pl->H * (size_t)pl->W;
+    CUDA_TRY(cudaMemcpyAsync(s.fa->d_raw, frame_a, raw_bytes, cudaMemcpyHostToDevice, pl->up));
+    CUDA_TRY(cudaMemcpyAsync(s.fb->d_raw, frame_b, raw_bytes, cudaMemcpyHostToDevice, pl->up));
+    CUDA_TRY(cudaEventRecord(s.uploaded, pl->up));
+    CUDA_TRY(cudaStreamWaitEvent(pl->comp, s.uploaded, 0));
+    int st = prepare_common(s.an, s.fa, s.fa->d_raw, pl->dtype, &pl->pre, nullptr);
+    if (!st) st = prepare_common(s.an, s.fb, s.fb->d_raw, pl->dtype, &pl->pre, nullptr);
     if (!st) st = run_passes(s.an, s.fa, s.fb);
     if (st) return st;
+    CUDA_TRY(cudaEventRecord(s.computed, pl->comp));
+    CUDA_TRY(cudaStreamWaitEvent(pl->down, s.computed, 0));
     const PassBuf& last = s.an->pairs[0].back();
     const size_t c = (size_t)last.cells;
-    cudaStream_t cs = s.an->cur;
+    cudaStream_t cs = pl->down;
     if (dx) CUDA_TRY(cudaMemcpyAsync(dx, last.dx, 4 * c, cudaMemcpyDeviceToHost, cs));
     if (dy) CUDA_TRY(cudaMemcpyAsync(dy, last.dy, 4 * c, cudaMemcpyDeviceToHost, cs));
     if (peak_ratio) CUDA_TRY(cudaMemcpyAsync(peak_ratio, last.raw_ppr, 4 * c, cudaMemcpyDeviceToHost, cs));
