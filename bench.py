@@ -158,9 +158,11 @@ def run_stream(args, wl):
     # end to end: pinned host frames -> input slab -> graph -> results to host, every step
     pin = torch.from_numpy(frames.view(np.int16)).pin_memory().numpy().view(np.uint16)
     res = batch.run_host(pin)
-    # two batches (each its own stream and graph) in turn: one's upload and download overlap
-    # the other's graph; host clock with the device synchronised at both ends
+    # two batches (each its own graph and copy streams, one shared compute stream) in turn: one's
+    # upload and download overlap the other's graph; host clock with the device synchronised at
+    # both ends
     batch2 = P.PivBatch(an, h, w, k, sequential=True)
+    batch2.set_stream(batch.stream())
     batch2.run_host(pin)
     batch2.run_host(pin)
     g = batch.grid
@@ -196,9 +198,9 @@ def run_stream(args, wl):
             "e2e": {"value": ranks.world * e2e_steps * nvec / (e2e_ms * 1e-3), "unit": "vectors/s",
                     "h2d_bytes_per_step": int(pin.nbytes), "d2h_bytes_per_step": int(nvec * 13 + k * 40),
                     "ms_per_step": e2e_ms / e2e_steps,
-                    "how": "two PivBatch objects in turn (submit_host / wait_host over pinned frames): upload of "
-                           "33 frames, one graph replay and download of 32 fields per step; host clock, device "
-                           "synchronised at both ends"},
+                    "how": "two PivBatch objects in turn sharing one compute stream (submit_host / wait_host "
+                           "over pinned frames): upload of 33 frames, one graph replay and download of 32 fields "
+                           "per step; host clock, device synchronised at both ends"},
             "gpu_launches": int(batch.kernels() * args.steps), "graph_launches": args.steps,
             "clocks": clocks, "autotuned_variants": tuned, "wall_ms_per_step": 1e3 * wall / args.steps,
             "valid_fraction_last_pair": float(np.mean((res[-1].field.flags & P.flags.INVALID) == 0)),

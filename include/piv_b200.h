@@ -218,6 +218,10 @@ int64_t piv_batch_input_bytes(const PivBatch* batch);
 int32_t piv_batch_run(PivBatch* batch);
 /* The batch's CUDA stream (a cudaStream_t), for callers that order their own work after it. */
 void* piv_batch_stream(PivBatch* batch);
+/* Runs the batch's kernels on `stream` from now on (NULL: its own stream again). Batches that
+ * share one stream replay their graphs one after another while their host copies (which go on
+ * private copy streams, see piv_batch_submit_host) overlap. Not while a submission is pending. */
+int32_t piv_batch_set_stream(PivBatch* batch, void* stream);
 int32_t piv_batch_sync(PivBatch* batch);
 /* Device output slabs: dx, dy, peak ratio (f32) and flags (u8), pairs*nx*ny each; 8 uint64
  * summary counters per pair; nx*ny is piv_output_grid's. */
@@ -227,9 +231,11 @@ int32_t piv_batch_outputs_device(PivBatch* batch, float** dx, float** dy, float*
  * copies the results back; any output may be NULL. Blocking. */
 int32_t piv_batch_run_host(PivBatch* batch, const void* raw, float* dx, float* dy, float* peak_ratio, uint8_t* flags,
                            PivSummaryC* summaries);
-/* As piv_batch_run_host without waiting: the upload, the run and the downloads are queued on the
- * batch's stream and the call returns; piv_batch_wait_host waits and fills the summaries. Two
- * batches (each with its own stream) used in turn overlap one's copies with the other's kernels.
+/* As piv_batch_run_host without waiting: the upload (on a private upload stream), the run (on the
+ * batch's stream, after the upload) and the downloads (on a private download stream, after the
+ * run) are queued and the call returns; piv_batch_wait_host waits and fills the summaries. Two
+ * batches used in turn overlap one's copies with the other's kernels; sharing one stream
+ * (piv_batch_set_stream) keeps their kernels from running at the same time.
  * `raw` and the outputs should be pinned and must stay valid until the wait returns; a batch
  * takes a new submission only after the previous one was waited for. */
 int32_t piv_batch_submit_host(PivBatch* batch, const void* raw, float* dx, float* dy, float* peak_ratio, uint8_t* flags);

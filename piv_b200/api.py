@@ -552,6 +552,11 @@ class PivBatch:
         """The batch's CUDA stream handle (for torch.cuda.ExternalStream)."""
         return int(_lib.load().piv_batch_stream(self._h))
 
+    def set_stream(self, stream):
+        """Run this batch's kernels on `stream` (a cudaStream_t handle; None: its own stream).
+        Batches sharing a stream replay one after another while their host copies overlap."""
+        _check(_lib.load().piv_batch_set_stream(self._h, ctypes.c_void_p(stream) if stream else None))
+
     def outputs_device(self):
         ptrs = [ctypes.c_void_p() for _ in range(5)]
         _check(_lib.load().piv_batch_outputs_device(self._h, *[ctypes.byref(p) for p in ptrs]))

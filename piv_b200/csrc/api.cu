@@ -179,9 +179,11 @@ struct PivBatch {
     cudaGraphExec_t exec = nullptr;
     long long kernels = 0;  // kernel launches of the eager run
     int runs = 0;
-    // asynchronous host submission: pinned summary counters and completion event
+    // asynchronous host submission: pinned summary counters, the copy streams (uploads and
+    // downloads overlap graph replays on the compute stream) and their ordering events
     unsigned long long* hsums = nullptr;
-    cudaEvent_t hdone = nullptr;
+    cudaStream_t up = nullptr, down = nullptr;
+    cudaEvent_t uploaded = nullptr, computed = nullptr, hdone = nullptr;
     bool pending = false;
 };
 
@@ -1329,11 +1331,18 @@ void piv_batch_destroy(PivBatch* bt) {
     if (!bt) return;
     if (bt->an) {
         cudaSetDevice(bt->an->device);
+        cudaStreamSynchronize(bt->an->cur);
         if (bt->an->own) cudaStreamSynchronize(bt->an->own);
     }
+    for (cudaStream_t st : {bt->up, bt->down})
+        if (st) {
+            cudaStreamSynchronize(st);
+            cudaStreamDestroy(st);
+        }
     if (bt->exec) cudaGraphExecDestroy(bt->exec);
     if (bt->graph) cudaGraphDestroy(bt->graph);
-    if (bt->hdone) cudaEventDestroy(bt->hdone);
+    for (cudaEvent_t ev : {bt->uploaded, bt->computed, bt->hdone})
+        if (ev) cudaEventDestroy(ev);
     if (bt->hsums) cudaFreeHost(bt->hsums);
     for (PivFrame* f : bt->frames) piv_frame_destroy(f);
     cudaFree(bt->raw);
@@ -1547,6 +1556,13 @@ int32_t piv_batch_run(PivBatch* bt) {
 
 void* piv_batch_stream(PivBatch* bt) { return bt ? (void*)bt->an->cur : nullptr; }
 
+int32_t piv_batch_set_stream(PivBatch* bt, void* stream) {
+    if (!bt) return fail(PIV_ERR_ARGUMENT, "null batch");
+    if (bt->pending) return fail(PIV_ERR_ARGUMENT, "the batch has a submission that has not been collected");
+    bt->an->cur = stream ? (cudaStream_t)stream : bt->an->own;
+    return PIV_OK;
+}
+
 int32_t piv_batch_sync(PivBatch* bt) {
     if (!bt) return fail(PIV_ERR_ARGUMENT, "null batch");
     CUDA_TRY(cudaSetDevice(bt->an->device));
@@ -1605,19 +1621,30 @@ int32_t piv_batch_submit_host(PivBatch* bt, const void* raw, float* dx, float* d
     if (st) return st;
     if (!bt->hsums) {
         CUDA_TRY(cudaHostAlloc((void**)&bt->hsums, sizeof(unsigned long long) * 8 * (size_t)bt->K, cudaHostAllocDefault));
+        CUDA_TRY(cudaStreamCreateWithFlags(&bt->up, cudaStreamNonBlocking));
+        CUDA_TRY(cudaStreamCreateWithFlags(&bt->down, cudaStreamNonBlocking));
+        CUDA_TRY(cudaEventCreateWithFlags(&bt->uploaded, cudaEventDisableTiming));
+        CUDA_TRY(cudaEventCreateWithFlags(&bt->computed, cudaEventDisableTiming));
         CUDA_TRY(cudaEventCreateWithFlags(&bt->hdone, cudaEventDisableTiming));
     }
-    CUDA_TRY(cudaMemcpyAsync(bt->raw, raw, bt->frame_bytes * bt->frames.size(), cudaMemcpyHostToDevice, an->cur));
+    // upload stream -> compute stream (graph replay) -> download stream; the previous submission
+    // was collected, so the input slab and the outputs are free
+    CUDA_TRY(cudaMemcpyAsync(bt->raw, raw, bt->frame_bytes * bt->frames.size(), cudaMemcpyHostToDevice, bt->up));
+    CUDA_TRY(cudaEventRecord(bt->uploaded, bt->up));
+    CUDA_TRY(cudaStreamWaitEvent(an->cur, bt->uploaded, 0));
     st = piv_batch_run(bt);
     if (st) return st;
+    CUDA_TRY(cudaEventRecord(bt->computed, an->cur));
+    CUDA_TRY(cudaStreamWaitEvent(bt->down, bt->computed, 0));
     const size_t c = (size_t)bt->cells * (size_t)bt->K;
-    if (dx) CUDA_TRY(cudaMemcpyAsync(dx, bt->dx, 4 * c, cudaMemcpyDeviceToHost, an->cur));
-    if (dy) CUDA_TRY(cudaMemcpyAsync(dy, bt->dy, 4 * c, cudaMemcpyDeviceToHost, an->cur));
-    if (peak_ratio) CUDA_TRY(cudaMemcpyAsync(peak_ratio, bt->ppr, 4 * c, cudaMemcpyDeviceToHost, an->cur));
-    if (flags) CUDA_TRY(cudaMemcpyAsync(flags, bt->flags, c, cudaMemcpyDeviceToHost, an->cur));
+    cudaStream_t ds = bt->down;
+    if (dx) CUDA_TRY(cudaMemcpyAsync(dx, bt->dx, 4 * c, cudaMemcpyDeviceToHost, ds));
+    if (dy) CUDA_TRY(cudaMemcpyAsync(dy, bt->dy, 4 * c, cudaMemcpyDeviceToHost, ds));
+    if (peak_ratio) CUDA_TRY(cudaMemcpyAsync(peak_ratio, bt->ppr, 4 * c, cudaMemcpyDeviceToHost, ds));
+    if (flags) CUDA_TRY(cudaMemcpyAsync(flags, bt->flags, c, cudaMemcpyDeviceToHost, ds));
     CUDA_TRY(cudaMemcpyAsync(bt->hsums, bt->sums, sizeof(unsigned long long) * 8 * (size_t)bt->K, cudaMemcpyDeviceToHost,
-                             an->cur));
-    CUDA_TRY(cudaEventRecord(bt->hdone, an->cur));
+                             ds));
+    CUDA_TRY(cudaEventRecord(bt->hdone, ds));
     bt->pending = true;
     return PIV_OK;
 }

@@ -123,3 +123,28 @@ def test_asynchronous_host_submission_alternating_batches():
         for b, r in zip(bs, ref):
             for x, y in zip(b.wait_host(), r):
                 _same(x, y)
+
+
+def test_batches_sharing_one_compute_stream():
+    """Two batches replaying on one shared stream (their copies on private streams) give the
+    run_host results, submitted back to back and alternating."""
+    import piv_b200 as P
+    h, w, k = 160, 192, 3
+    an = P.PivAnalyzer(P.PivConfig(windows=[32, 16], overlap=0.5, final_iterations=1))
+    frames = [_frames(k + 1, h, w, s) for s in (41, 42)]
+    ref = [_reference(an, f, [(i, i + 1) for i in range(k)]) for f in frames]
+    bs = [P.PivBatch(an, h, w, k, sequential=True) for _ in range(2)]
+    bs[1].set_stream(bs[0].stream())
+    assert bs[1].stream() == bs[0].stream()
+    for rnd in range(3):
+        for b, f in zip(bs, frames):
+            b.submit_host(f)
+        with pytest.raises(P.PivError):
+            bs[0].set_stream(None)  # a submission is pending
+        for b, r in zip(bs, ref):
+            for x, y in zip(b.wait_host(), r):
+                _same(x, y)
+    bs[1].set_stream(None)
+    assert bs[1].stream() != bs[0].stream()
+    for b in bs:
+        b.close()
