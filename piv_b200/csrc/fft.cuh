@@ -141,36 +141,59 @@ __device__ __forceinline__ int bitrev(int t) {
 }
 
 // T-point DFT across the T lanes of a line, natural lane order in, bit-reversed out (DIF).
+// Radix-2 step over lane pairs (t, t ^ h): the lower lane keeps x + o, the upper (o - x) * w.
+// Both are written as one signed add fma(s, x, o) (s = +1 or -1, an exact single rounding like a
+// plain add) and one complex multiply by w, with w = 1 on the lower lane (exact up to the sign of
+// a zero), so a lane issues no instructions for the other lane's formula.
 template <int N, int T, int P, int DIR>
 __device__ __forceinline__ void xlane_dif(float2 (&x)[P], int t, const float2* s_roots) {
 #pragma unroll
     for (int h = T / 2; h >= 1; h >>= 1) {
         const bool upper = (t & h) != 0;
-        const float2 w = s_roots[(t & (h - 1)) * (N / (2 * h))];
+        const float sg = upper ? -1.0f : 1.0f;
+        const float2 w = upper ? s_roots[(t & (h - 1)) * (N / (2 * h))] : make_float2(1.0f, 0.0f);
 #pragma unroll
         for (int i = 0; i < P; ++i) {
             float2 o;
             o.x = __shfl_xor_sync(0xffffffffu, x[i].x, h);
             o.y = __shfl_xor_sync(0xffffffffu, x[i].y, h);
-            x[i] = upper ? cmulw<DIR>(csub(o, x[i]), w) : cadd(x[i], o);
+            x[i] = cmulw<DIR>(make_float2(fmaf(sg, x[i].x, o.x), fmaf(sg, x[i].y, o.y)), w);
         }
     }
 }
 
 // T-point DFT across the T lanes of a line, bit-reversed lane order in, natural out (DIT).
-template <int N, int T, int P, int DIR>
+// SIGNED: the upper lane of each pair first multiplies by w (w = 1 on the lower lane), then the
+// lower keeps v + o and the upper o - v, again as one signed add. Otherwise each lane selects
+// between the two formulas. Both give the same values (up to the sign of a zero); which one
+// schedules better depends on the window size (measured: the select form for 32 and 64 points,
+// the signed form elsewhere).
+template <int N, int T, int P, int DIR, bool SIGNED>
 __device__ __forceinline__ void xlane_dit(float2 (&x)[P], int t, const float2* s_roots) {
 #pragma unroll
     for (int h = 1; h < T; h <<= 1) {
         const bool upper = (t & h) != 0;
-        const float2 w = s_roots[(t & (h - 1)) * (N / (2 * h))];
+        if constexpr (SIGNED) {
+            const float sg = upper ? -1.0f : 1.0f;
+            const float2 w = upper ? s_roots[(t & (h - 1)) * (N / (2 * h))] : make_float2(1.0f, 0.0f);
 #pragma unroll
-        for (int i = 0; i < P; ++i) {
-            float2 v = upper ? cmulw<DIR>(x[i], w) : x[i];
-            float2 o;
-            o.x = __shfl_xor_sync(0xffffffffu, v.x, h);
-            o.y = __shfl_xor_sync(0xffffffffu, v.y, h);
-            x[i] = upper ? csub(o, v) : cadd(v, o);
+            for (int i = 0; i < P; ++i) {
+                const float2 v = cmulw<DIR>(x[i], w);
+                float2 o;
+                o.x = __shfl_xor_sync(0xffffffffu, v.x, h);
+                o.y = __shfl_xor_sync(0xffffffffu, v.y, h);
+                x[i] = make_float2(fmaf(sg, v.x, o.x), fmaf(sg, v.y, o.y));
+            }
+        } else {
+            const float2 w = s_roots[(t & (h - 1)) * (N / (2 * h))];
+#pragma unroll
+            for (int i = 0; i < P; ++i) {
+                float2 v = upper ? cmulw<DIR>(x[i], w) : x[i];
+                float2 o;
+                o.x = __shfl_xor_sync(0xffffffffu, v.x, h);
+                o.y = __shfl_xor_sync(0xffffffffu, v.y, h);
+                x[i] = upper ? csub(o, v) : cadd(v, o);
+            }
         }
     }
 }
@@ -192,7 +215,7 @@ template <int N, int T, int DIR>
 __device__ __forceinline__ void fft_line_blocked(float2 (&x)[N / T], int t, const float2* s_roots) {
     constexpr int P = N / T;
     if constexpr (T > 1) {
-        xlane_dit<N, T, P, DIR>(x, t, s_roots);
+        xlane_dit<N, T, P, DIR, !(N == 32 || N == 64)>(x, t, s_roots);
 #pragma unroll
         for (int p = 1; p < P; ++p) x[p] = cmulw<DIR>(x[p], s_roots[p * t]);
     }
