@@ -149,6 +149,38 @@ __device__ __forceinline__ void group_argmax(float& v, int& idx, float* s_red, i
     }
 }
 
+// Rows of the lane with block rt (rows P*rt .. P*rt + P - 1) that lie outside the primary
+// peak's footprint: row y qualifies when its circular distance from `by` exceeds `ex`, or every
+// row does when the lane's column distance `cx` exceeds `ex`. Bit k of the result is row
+// P*rt + k. The rows within `ex` of `by` form one circular interval, at most two linear ones.
+template <int N, int P>
+__device__ __forceinline__ unsigned eligible_rows(int by, int ex, int cx, int rt) {
+    static_assert(P <= 32, "row mask");
+    constexpr unsigned all = (unsigned)((1ull << P) - 1ull);
+    if constexpr (N <= 32) {
+        // the whole column in one word: rotate a band of 2 ex + 1 bits to start at by - ex
+        constexpr unsigned long long full = (1ull << N) - 1ull;
+        unsigned long long near = full;
+        if (2 * ex + 1 < N) {
+            const unsigned long long x = ((1ull << (2 * ex + 1)) - 1ull) << ((by - ex + N) % N);
+            near = (x | (x >> N)) & full;
+        }
+        const unsigned long long el = cx > ex ? full : (~near & full);
+        return (unsigned)(el >> (P * rt)) & all;
+    }
+    if (cx > ex) return all;
+    if (2 * ex + 1 >= N) return 0u;  // the footprint covers the whole column
+    const int r0 = P * rt;
+    auto span = [&](int lo, int hi) -> unsigned {  // lane bits of the rows lo..hi
+        const int a = max(lo - r0, 0), b = min(hi - r0, P - 1);
+        return a > b ? 0u : (unsigned)(((1ull << (b - a + 1)) - 1ull) << a);
+    };
+    const int lo = by - ex, hi = by + ex;  // not both outside [0, N): 2 ex + 1 < N
+    const unsigned near = lo < 0 ? (span(0, hi) | span(lo + N, N - 1))
+                                 : (hi >= N ? (span(0, hi - N) | span(lo, N - 1)) : span(lo, hi));
+    return ~near & all;
+}
+
 // Separates Z and its Hermitian partner M = Z[-k] into the cross spectrum (times 4):
 //   2FA = Z + conj(M), 2FB = -i (Z - conj(M)), C = conj(2FA) * 2FB.
 __device__ __forceinline__ float2 cross4(float2 z, float2 m) {
@@ -332,14 +364,21 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB) correlate_kernel(const __
     }
 
     // ------------------------------------------------------------------ find_peak
-    // Argmax of both planes (lowest row-major index among equal maxima).
+    // Argmax of both planes (lowest row-major index among equal maxima). A lane's indices grow
+    // with k, so inside the lane a strictly larger value is the only one that replaces the best.
     float2 best = make_float2(-INFINITY, -INFINITY);
     int bi0 = 0x7fffffff, bi1 = 0x7fffffff;
 #pragma unroll
     for (int k = 0; k < P; ++k) {
         const int idx = (k + P * rt) * N + line;
-        if (z0[k].x > -INFINITY) amax_combine(best.x, bi0, z0[k].x, idx);
-        if (PAIR && z0[k].y > -INFINITY) amax_combine(best.y, bi1, z0[k].y, idx);
+        if (z0[k].x > best.x) {
+            best.x = z0[k].x;
+            bi0 = idx;
+        }
+        if (PAIR && z0[k].y > best.y) {
+            best.y = z0[k].y;
+            bi1 = idx;
+        }
     }
     group_argmax<C>(best.x, bi0, s_red, g, gt);
     if constexpr (PAIR) group_argmax<C>(best.y, bi1, s_red, g, gt);
@@ -411,6 +450,15 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB) correlate_kernel(const __
             return min(d, N - d);
         };
         const int cx0 = circ(line, bx0), cx1 = circ(line, bx1);
+        // A cell is outside the footprint when max(circular row distance, column distance) > ex:
+        // one bit of a per-lane mask of eligible rows (the direct test at 128 rows, where the
+        // mask measured slower).
+        constexpr bool MASK = N < 128;
+        const unsigned el0 = MASK ? eligible_rows<N, P>(by0, ex0, cx0, rt) : 0u;
+        const unsigned el1 = MASK && PAIR ? eligible_rows<N, P>(by1, ex1, cx1, rt) : 0u;
+        auto outside = [&](int k, int y, unsigned el, int by, int cx, int ex) {
+            return MASK ? ((el >> k) & 1u) != 0u : max(circ(y, by), cx) > ex;
+        };
 #pragma unroll
         for (int k = 0; k < P; ++k) {
             const int y = k + P * rt;
@@ -418,11 +466,11 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB) correlate_kernel(const __
                 const float2* v2 = reinterpret_cast<const float2*>(vm);
                 const float2 l = v2[C::A(y, xl)], c = v2[C::A(y, line)], r = v2[C::A(y, xr)];
                 const float h0 = fmaxf(fmaxf(l.x, r.x), c.x), h1 = fmaxf(fmaxf(l.y, r.y), c.y);
-                if (z0[k].x == h0 && max(circ(y, by0), cx0) > ex0) second.x = fmaxf(second.x, z0[k].x);
-                if (z0[k].y == h1 && max(circ(y, by1), cx1) > ex1) second.y = fmaxf(second.y, z0[k].y);
+                if (z0[k].x == h0 && outside(k, y, el0, by0, cx0, ex0)) second.x = fmaxf(second.x, z0[k].x);
+                if (z0[k].y == h1 && outside(k, y, el1, by1, cx1, ex1)) second.y = fmaxf(second.y, z0[k].y);
             } else {
                 const float h0 = fmaxf(fmaxf(vm[C::A(y, xl)], vm[C::A(y, xr)]), vm[C::A(y, line)]);
-                if (z0[k].x == h0 && max(circ(y, by0), cx0) > ex0) second.x = fmaxf(second.x, z0[k].x);
+                if (z0[k].x == h0 && outside(k, y, el0, by0, cx0, ex0)) second.x = fmaxf(second.x, z0[k].x);
             }
         }
     }
