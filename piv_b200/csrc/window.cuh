@@ -46,19 +46,39 @@ __device__ __forceinline__ void sample_column_direct(const float* __restrict__ i
         const float ux = __fsub_rn(1.0f, tx), uy = __fsub_rn(1.0f, ty);
         const float w00 = __fmul_rn(ux, uy), w01 = __fmul_rn(tx, uy), w10 = __fmul_rn(ux, ty), w11 = __fmul_rn(tx, ty);
         if constexpr (T == 1) {
-            // one lane holds the whole column: stream down the rows, carrying the row below
-            float top = __ldg(base), topr = __ldg(base + dc);
-#pragma unroll
-            for (int p = 0; p < P; ++p) {
-                const float* bot = base + (size_t)min(p + 1, last) * W;
-                const float b0 = __ldg(bot), b1 = __ldg(bot + dc);
-                float s = __fmul_rn(w00, top);
-                s = __fadd_rn(s, __fmul_rn(w01, topr));
-                s = __fadd_rn(s, __fmul_rn(w10, b0));
-                s = __fadd_rn(s, __fmul_rn(w11, b1));
+            // One lane holds the whole column: stream down the rows, carrying the row below. The
+            // right-hand tap is the next float (an immediate offset), or the same value at the
+            // right border (dc == 0), where that load is skipped.
+            auto blend = [&](int p, float tl, float tr, float bl, float br) {
+                float s = __fmul_rn(w00, tl);
+                s = __fadd_rn(s, __fmul_rn(w01, tr));
+                s = __fadd_rn(s, __fmul_rn(w10, bl));
+                s = __fadd_rn(s, __fmul_rn(w11, br));
                 if (IMAG) z[p].y = s; else z[p].x = s;
-                top = b0;
-                topr = b1;
+            };
+            float top = __ldg(base);
+            float topr = dc ? __ldg(base + 1) : top;
+            if (last >= P) {  // rows y0 .. y0 + P all exist: no row clamp, the row pointer steps by W
+                const float* bot = base;
+#pragma unroll
+                for (int p = 0; p < P; ++p) {
+                    bot += W;
+                    const float b0 = __ldg(bot);
+                    const float b1 = dc ? __ldg(bot + 1) : b0;
+                    blend(p, top, topr, b0, b1);
+                    top = b0;
+                    topr = b1;
+                }
+            } else {
+#pragma unroll
+                for (int p = 0; p < P; ++p) {
+                    const float* bot = base + (size_t)min(p + 1, last) * W;
+                    const float b0 = __ldg(bot);
+                    const float b1 = dc ? __ldg(bot + 1) : b0;
+                    blend(p, top, topr, b0, b1);
+                    top = b0;
+                    topr = b1;
+                }
             }
         } else {
             const int c1 = c0 + dc;
