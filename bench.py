@@ -498,6 +498,9 @@ def run_profile_case(args, wl):
     return 0
 
 
+REF_TOTAL_S = 150.0
+
+
 def run_reference(args, wl):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -510,8 +513,10 @@ def run_reference(args, wl):
         pass  # the oracle has no warm-up state; warm-up steps run no work
     base = None
     samples = []
+    # each step is a bounded sample of the workload; the whole run stays near REF_TOTAL_S seconds
+    step_s = max(0.5, min(args.ref_step_s, REF_TOTAL_S / max(args.steps, 1)))
     for _ in range(args.steps):
-        r = cpu_baseline(wl, a, b, budget_s=max(1.0, args.ref_step_s), crop=args.ref_crop)
+        r = cpu_baseline(wl, a, b, budget_s=step_s, crop=args.ref_crop)
         samples.append(r["value"])
         base = r
     v = float(np.median(samples))
