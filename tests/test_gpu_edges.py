@@ -61,3 +61,27 @@ def test_u8_frames_are_scaled_as_the_reference_decodes_them():
     # one 32 px pass on 8-bit particles: peak locking leaves a bias of a few hundredths of a pixel
     err = np.hypot(r8.field.dx[ok] - 2.3, r8.field.dy[ok] + 1.7)
     assert np.sqrt(np.mean(err ** 2)) < 0.1 and err.max() < 0.3
+
+
+@pytest.mark.parametrize("dtype", [np.uint8, np.uint16])
+def test_every_code_decodes_as_the_reference_divides(dtype):
+    """Every u8 / u16 code becomes exactly f32(code) / 255 or / 65535, correctly rounded as
+    decode.rs:227-234 divides, through the vectorised path (aligned buffers) and the per-code path
+    (a device pointer one code past an aligned address, and a ragged frame size)."""
+    import torch
+
+    import piv_b200 as P
+    top = np.iinfo(dtype).max
+    h, w = 257, 259  # 66,563 samples: every code, then the sequence again, ragged against 16 bytes
+    frame = np.resize(np.arange(top + 1, dtype=np.uint32).astype(dtype), (h, w))
+    ref = (frame.astype(np.float32) / np.float32(top)).astype(np.float32)
+    an = P.PivAnalyzer(P.PivConfig(windows=[32], final_iterations=1))
+    img = an.prepare(frame, P.RAW).image
+    assert np.array_equal(img.view(np.uint32), ref.view(np.uint32))
+    # the same codes from a device buffer that starts one code past a 16-byte boundary
+    flat = np.concatenate([np.zeros(1, dtype), frame.ravel()])
+    dev = torch.from_numpy(flat.view(np.int8 if dtype == np.uint8 else np.int16)).to("cuda:0")
+    f = an.frame(h, w)
+    f.prepare_device(dev.data_ptr() + flat.itemsize, P.api._dtype_code(frame), P.RAW)
+    torch.cuda.synchronize()
+    assert np.array_equal(f.image.view(np.uint32), ref.view(np.uint32))
