@@ -390,8 +390,16 @@ struct Integral {
 // ---------------------------------------------------------------------------------------------
 // Validation helpers (validate.rs:133-170)
 // ---------------------------------------------------------------------------------------------
+// f32::total_cmp for non-NaN values (validate.rs:164): ascending, -0.0 before +0.0. The signed
+// integer key of the bit pattern orders exactly so.
+int32_t total_key(float f) {
+    int32_t b;
+    std::memcpy(&b, &f, sizeof b);
+    return b ^ ((b >> 31) & 0x7fffffff);
+}
+
 float median(float* v, int n) {
-    std::sort(v, v + n);  // usable neighbours are never NaN: ascending sort == total_cmp
+    std::sort(v, v + n, [](float a, float b) { return total_key(a) < total_key(b); });
     if (n % 2 == 1) return v[n / 2];
     return 0.5f * (v[n / 2 - 1] + v[n / 2]);
 }

@@ -172,13 +172,22 @@ cudaError_t launch_mask(const PlaceParams& p, const float4* origins, int ncells,
 // ---------------------------------------------------------------------------------------------
 // Validation
 // ---------------------------------------------------------------------------------------------
-// Sorts v[0..n) ascending (insertion sort; usable neighbours are never NaN, so this orders them
-// as f32::total_cmp does) and returns the median, the mean of the middle two when n is even.
+// Total-order key of a non-NaN float: signed integer order of the keys is f32::total_cmp order
+// (-0.0 before +0.0), which validate.rs:164 sorts by. The map is its own inverse.
+__device__ __forceinline__ int tkey(float f) {
+    const int b = __float_as_int(f);
+    return b ^ ((b >> 31) & 0x7fffffff);
+}
+__device__ __forceinline__ float tval(int k) { return __int_as_float(k ^ ((k >> 31) & 0x7fffffff)); }
+
+// Sorts v[0..n) ascending by total order (insertion sort) and returns the median, the mean of
+// the middle two when n is even (validate.rs:163-170).
 __device__ float median_sorted(float* v, int n) {
     for (int i = 1; i < n; ++i) {
         const float x = v[i];
+        const int kx = tkey(x);
         int j = i;
-        while (j > 0 && v[j - 1] > x) {
+        while (j > 0 && tkey(v[j - 1]) > kx) {
             v[j] = v[j - 1];
             --j;
         }
@@ -186,6 +195,44 @@ __device__ float median_sorted(float* v, int n) {
     }
     if (n % 2 == 1) return v[n / 2];
     return __fmul_rn(0.5f, __fadd_rn(v[n / 2 - 1], v[n / 2]));
+}
+
+// Radius-1 neighbourhoods in registers: eight key slots, absent or unusable neighbours padded with
+// INT_MAX (above every finite key), sorted by Batcher's odd-even merge network (19 exchanges), so
+// the c usable keys come first in order.
+__device__ __forceinline__ void kx_swap(int& a, int& b) {
+    const int lo = min(a, b), hi = max(a, b);
+    a = lo;
+    b = hi;
+}
+__device__ __forceinline__ void sort8(int (&k)[8]) {
+    kx_swap(k[0], k[1]); kx_swap(k[2], k[3]); kx_swap(k[4], k[5]); kx_swap(k[6], k[7]);
+    kx_swap(k[0], k[2]); kx_swap(k[1], k[3]); kx_swap(k[4], k[6]); kx_swap(k[5], k[7]);
+    kx_swap(k[1], k[2]); kx_swap(k[5], k[6]);
+    kx_swap(k[0], k[4]); kx_swap(k[1], k[5]); kx_swap(k[2], k[6]); kx_swap(k[3], k[7]);
+    kx_swap(k[2], k[4]); kx_swap(k[3], k[5]);
+    kx_swap(k[1], k[2]); kx_swap(k[3], k[4]); kx_swap(k[5], k[6]);
+}
+// Median of the first c (1..8) of eight sorted keys, as median_sorted computes it.
+__device__ __forceinline__ float median8(const int (&k)[8], int c) {
+    int lo = k[0], hi = k[0];
+#pragma unroll
+    for (int i = 1; i < 8; ++i) {
+        if (i == (c - 1) / 2) lo = k[i];
+        if (i == c / 2) hi = k[i];
+    }
+    if (c % 2 == 1) return tval(hi);
+    return __fmul_rn(0.5f, __fadd_rn(tval(lo), tval(hi)));
+}
+// Normalised residual |value - med| / (median |nb - med| + eps) over the first c sorted keys
+// (validate.rs:157-161).
+__device__ __forceinline__ float residual8(float value, const int (&k)[8], int c, float eps) {
+    const float med = median8(k, c);
+    int dev[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) dev[i] = i < c ? tkey(fabsf(__fsub_rn(tval(k[i]), med))) : 0x7fffffff;
+    sort8(dev);
+    return __fdiv_rn(fabsf(__fsub_rn(value, med)), __fadd_rn(median8(dev, c), eps));
 }
 
 __device__ int collect_neighbours(const float* dx, const float* dy, const uint8_t* snap, int nx, int ny, int ix, int iy,
@@ -203,13 +250,6 @@ __device__ int collect_neighbours(const float* dx, const float* dy, const uint8_
     return c;
 }
 
-__device__ float residual(float value, float* nb, int n, float eps) {
-    const float med = median_sorted(nb, n);
-    float dev[8];
-    for (int i = 0; i < n; ++i) dev[i] = fabsf(__fsub_rn(nb[i], med));
-    return __fdiv_rn(fabsf(__fsub_rn(value, med)), __fadd_rn(median_sorted(dev, n), eps));
-}
-
 // Per-vector tests (validate.rs:59-78).
 __device__ __forceinline__ void validate_vector(const ValidateParams& p, int k) {
     uint8_t f = p.flags0[k];
@@ -225,11 +265,29 @@ __device__ __forceinline__ void validate_median(const ValidateParams& p, int k) 
     const int ix = k % p.nx, iy = k / p.nx;
     uint8_t f = p.flags1[k];
     if ((f & F_INVALID) == 0) {
-        float nu[8], nv[8];
-        const int c = collect_neighbours(p.dx, p.dy, p.flags1, p.nx, p.ny, ix, iy, 1, nu, nv);
+        // usable 3x3 neighbours (validate.rs:133-155), padded slots for the others
+        int ku[8], kv[8];
+        int c = 0;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int dxo = (j < 3) ? j - 1 : (j < 5 ? (j == 3 ? -1 : 1) : j - 6);
+            const int dyo = (j < 3) ? -1 : (j < 5 ? 0 : 1);
+            const int x = ix + dxo, y = iy + dyo;
+            ku[j] = kv[j] = 0x7fffffff;
+            if (x >= 0 && x < p.nx && y >= 0 && y < p.ny) {
+                const int o = y * p.nx + x;
+                if ((p.flags1[o] & F_INVALID) == 0) {
+                    ku[j] = tkey(p.dx[o]);
+                    kv[j] = tkey(p.dy[o]);
+                    ++c;
+                }
+            }
+        }
         if (c >= 2) {
-            const float ru = residual(p.dx[k], nu, c, p.median_eps);
-            const float rv = residual(p.dy[k], nv, c, p.median_eps);
+            sort8(ku);
+            sort8(kv);
+            const float ru = residual8(p.dx[k], ku, c, p.median_eps);
+            const float rv = residual8(p.dy[k], kv, c, p.median_eps);
             if (__fsqrt_rn(__fadd_rn(__fmul_rn(ru, ru), __fmul_rn(rv, rv))) > p.median_threshold) f |= F_MEDIAN_OUTLIER;
         }
     }

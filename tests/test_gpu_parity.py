@@ -210,3 +210,29 @@ def test_every_launch_variant_gives_identical_results():
                 assert np.array_equal(x.raw.flags, y.raw.flags), (windows, k)
                 assert same_floats(x.raw.dx, y.raw.dx) and same_floats(x.raw.dy, y.raw.dy), (windows, k)
                 assert same_floats(x.raw.peak_ratio, y.raw.peak_ratio), (windows, k)
+
+
+def test_validation_with_signed_zero_and_repeated_values_matches_oracle():
+    """Median test and replacement on fields full of ties (values drawn from a few, with -0.0
+    and +0.0 both present) agree with the oracle bit for bit: the GPU's register sorting network
+    and the oracle's sort both order as f32::total_cmp."""
+    import piv_b200 as P
+    from oracle import oracle as O
+    rng = np.random.default_rng(3)
+    pool = np.array([-0.0, 0.0, 0.5, -0.5, 1.0, 3.0, -7.0], np.float32)
+    an = P.PivAnalyzer(P.PivConfig(windows=[64, 32]))
+    for trial in range(4):
+        ny, nx = 37, 53
+        dx = rng.choice(pool, (ny, nx)).astype(np.float32)
+        dy = rng.choice(pool, (ny, nx)).astype(np.float32)
+        ppr = rng.choice(np.array([1.0, 2.0, 9.0], np.float32), (ny, nx)).astype(np.float32)
+        fl = (rng.random((ny, nx)) < 0.05).astype(np.uint8)  # a few NO_SIGNAL cells
+        dx[fl == 1] = np.nan
+        dy[fl == 1] = np.nan
+        gx, gy, gf, _ = an.validate_field(dx, dy, ppr, fl)
+        ox, oy, of, _ = O.validate(dx, dy, ppr, fl, max_displacement=32.0)
+        def same_bits(a, b):  # bit patterns, with any NaN equal to any NaN
+            return bool(np.all((a.view(np.uint32) == b.view(np.uint32)) | (np.isnan(a) & np.isnan(b))))
+        assert np.array_equal(gf, of), trial
+        assert np.any(np.signbit(ox[ox == 0])) and np.any(~np.signbit(ox[ox == 0]))
+        assert same_bits(gx, ox) and same_bits(gy, oy), trial

@@ -264,3 +264,28 @@ def test_percentile_clip_definition():
     assert clip == 99 and c.max() == 99
     c, clip = O.percentile_clip_u16(codes, 100.0)
     assert clip == 100
+
+
+def test_replacement_median_orders_signed_zeros_as_total_cmp():
+    """validate.rs:164 sorts neighbours with f32::total_cmp, which puts -0.0 before +0.0. Seven
+    usable neighbours [+0, -0, +0, -0, -0, 1, 2] sort to [-0, -0, -0, +0, +0, 1, 2]: the
+    replacement of the centre is the fourth, +0.0 (a stable sort that treats the zeros as equal
+    would keep the input order and give -0.0)."""
+    from oracle import oracle as O
+    dx = np.zeros((3, 3), np.float32)
+    nb = [0.0, -0.0, 0.0, -0.0, -0.0, 1.0, 2.0, 7.0]
+    k = 0
+    for y in range(3):
+        for x in range(3):
+            if (x, y) != (1, 1):
+                dx[y, x] = nb[k]
+                k += 1
+    dx[1, 1] = 50.0
+    dy = np.zeros_like(dx)
+    ppr = np.full_like(dx, 5.0)
+    ppr[1, 1] = 1.0   # LOW_PPR: the centre is replaced
+    ppr[2, 2] = 1.0   # the neighbour holding 7.0 is not usable either
+    fl = np.zeros((3, 3), np.uint8)
+    odx, _, ofl, _ = O.validate(dx, dy, ppr, fl)
+    assert ofl[1, 1] & 8  # REPLACED
+    assert odx[1, 1] == 0.0 and not np.signbit(odx[1, 1])
