@@ -68,6 +68,23 @@ struct CorrCfg {
 };
 
 // ---------------------------------------------------------------------------------------------
+// Barrier of one group (the N*T threads of a window pair). Groups share nothing in shared memory
+// but the read-only twiddles, so they need not wait for each other: a named barrier per group
+// when a group is whole warps, a warp barrier when groups tile a warp (a warp's groups then wait
+// together), the CTA barrier otherwise.
+// ---------------------------------------------------------------------------------------------
+template <class C>
+__device__ __forceinline__ void group_sync(int g) {
+    if constexpr (C::G > 1 && C::G <= 15 && C::NT % 32 == 0) {
+        asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "r"(C::NT) : "memory");
+    } else if constexpr (C::G > 1 && C::NT <= 32 && 32 % C::NT == 0) {
+        __syncwarp();
+    } else {
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
 // Group reductions (segments of SW lanes by shuffles, then NSEG partials through shared memory).
 // Every thread of the group returns the same value; the combination order is fixed.
 // ---------------------------------------------------------------------------------------------
@@ -86,7 +103,7 @@ __device__ __forceinline__ float4 group_sum4(float4 v, float* s_red, int g, int 
     } else {
         float4* r = reinterpret_cast<float4*>(s_red) + g * NSEG;
         if (gt % SW == 0) r[gt / SW] = v;
-        __syncthreads();
+        group_sync<C>(g);
         float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
         for (int i = 0; i < NSEG; ++i) {
@@ -96,7 +113,7 @@ __device__ __forceinline__ float4 group_sum4(float4 v, float* s_red, int g, int 
             s.z += q.z;
             s.w += q.w;
         }
-        __syncthreads();
+        group_sync<C>(g);
         return s;
     }
 }
@@ -114,14 +131,14 @@ __device__ __forceinline__ float2 group_max2(float2 v, float* s_red, int g, int 
     } else {
         float2* r = reinterpret_cast<float2*>(s_red) + g * NSEG * 2;
         if (gt % SW == 0) r[gt / SW] = v;
-        __syncthreads();
+        group_sync<C>(g);
         float2 s = make_float2(-INFINITY, -INFINITY);
 #pragma unroll
         for (int i = 0; i < NSEG; ++i) {
             s.x = fmaxf(s.x, r[i].x);
             s.y = fmaxf(s.y, r[i].y);
         }
-        __syncthreads();
+        group_sync<C>(g);
         return s;
     }
 }
@@ -138,12 +155,12 @@ __device__ __forceinline__ void group_argmax(float& v, int& idx, float* s_red, i
     if constexpr (NSEG > 1) {
         float2* r = reinterpret_cast<float2*>(s_red) + g * NSEG * 2;
         if (gt % SW == 0) r[gt / SW] = make_float2(v, __int_as_float(idx));
-        __syncthreads();
+        group_sync<C>(g);
         float bv = -INFINITY;
         int bi = 0x7fffffff;
 #pragma unroll
         for (int i = 0; i < NSEG; ++i) amax_combine(bv, bi, r[i].x, __float_as_int(r[i].y));
-        __syncthreads();
+        group_sync<C>(g);
         v = bv;
         idx = bi;
     }
@@ -314,13 +331,13 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB) correlate_kernel(const __
         plane0[C::A(k + P * rt, line)] = z0[k];
         if constexpr (PAIR) plane1[C::A(k + P * rt, line)] = z1[k];
     }
-    __syncthreads();
+    group_sync<C>(g);
 #pragma unroll
     for (int q = 0; q < P; ++q) {
         z0[q] = plane0[C::A(line, t + T * q)];
         if constexpr (PAIR) z1[q] = plane1[C::A(line, t + T * q)];
     }
-    __syncthreads();
+    group_sync<C>(g);
     fft_line_interleaved<N, T, 1>(z0, t, s_roots);
     if constexpr (PAIR) fft_line_interleaved<N, T, 1>(z1, t, s_roots);
     // ------------------------------------------------------------------ cross spectra
@@ -329,7 +346,7 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB) correlate_kernel(const __
         plane0[C::B(line, k + P * rt)] = z0[k];
         if constexpr (PAIR) plane1[C::B(line, k + P * rt)] = z1[k];
     }
-    __syncthreads();
+    group_sync<C>(g);
     {
         const int my = (N - line) % N;
 #pragma unroll
@@ -344,16 +361,16 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB) correlate_kernel(const __
             }
         }
     }
-    __syncthreads();
+    group_sync<C>(g);
 
     // ------------------------------------------------------------------ inverse 2-D FFT
     fft_line_blocked<N, T, -1>(z0, t, s_roots);
 #pragma unroll
     for (int k = 0; k < P; ++k) plane0[C::A(line, t + T * k)] = z0[k];
-    __syncthreads();
+    group_sync<C>(g);
 #pragma unroll
     for (int q = 0; q < P; ++q) z0[q] = plane0[C::A(t + T * q, line)];
-    __syncthreads();
+    group_sync<C>(g);
     fft_line_interleaved<N, T, -1>(z0, t, s_roots);
     // Lane now holds corr[y = k + P*rt][x = line]; scale as the reference does (c *= scale).
 #pragma unroll
@@ -384,7 +401,7 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB) correlate_kernel(const __
     if constexpr (PAIR) group_argmax<C>(best.y, bi1, s_red, g, gt);
     if (!(best.x > -INFINITY)) bi0 = 0;
     if (!(best.y > -INFINITY)) bi1 = 0;
-    __syncthreads();  // the scaled planes are complete in shared memory
+    group_sync<C>(g);  // the scaled planes are complete in shared memory
     auto at = [&](int ch, int y, int x) -> float {
         const float2 v = plane0[C::A(y % N, x % N)];
         return ch == 0 ? v.x : v.y;
@@ -431,7 +448,7 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB) correlate_kernel(const __
             }
         }
     }
-    __syncthreads();
+    group_sync<C>(g);
     const int hw0 = max(max(s_hw[g][0], s_hw[g][1]), max(s_hw[g][2], s_hw[g][3]));
     const int ex0 = max((int)ceilf(1.5f * (float)hw0), 2);
     int ex1 = 0;
