@@ -620,10 +620,8 @@ def main():
     stream.synchronize()
 
     # ---------------------------------------------------------------- timed: device-resident
+    # (repeated calls on the same frames replay the analyzer's captured pass graph)
     npass = len(pass_windows(wl))
-    an.set_profiling(True)
-    for p in range(npass):
-        an.profile(p)  # reset
     ranks.barrier()
     torch.cuda.synchronize()
     gpu_uuid = str(torch.cuda.get_device_properties(local).uuid)
@@ -641,9 +639,17 @@ def main():
     launches = an.launches() - l0
     clocks = sampler.stop()
     ms = e0.elapsed_time(e1)
+    ms_max = ranks.max(ms)
+    # the same steps again with CUDA events around every correlation launch (eager launches):
+    # per-pass kernel times for the roofline
+    an.set_profiling(True)
+    for p in range(npass):
+        an.profile(p)  # reset
+    for i in range(args.steps):
+        step(i)
+    stream.synchronize()
     corr = [an.profile(p) for p in range(npass)]
     an.set_profiling(False)
-    ms_max = ranks.max(ms)
     value = world * args.steps * nvec / (ms_max * 1e-3)
 
     # ---------------------------------------------------------------- timed: end to end (host buffers)
@@ -737,6 +743,8 @@ def main():
             "frac": (achieved / sgemm) if sgemm else None,
             "traffic": (traffic or {}).get("bytes_per_pair"),
             "kernel": "correlate_kernel (all passes of one pair)",
+            "source": "CUDA events around each correlation launch on the analyzer's stream, over a second "
+                      "loop of the same steps (the timed loop replays the pass graph)",
             "peak_source": "measured cuBLAS SGEMM (FP32 CUDA cores, TF32 off), 8192^3, in this run",
             "per_pass": per_pass,
             "hbm_peak_gbs": peaks.get("hbm_gbs")}

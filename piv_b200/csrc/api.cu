@@ -130,6 +130,12 @@ struct PivAnalyzer {
     int variant[2][129] = {};
     // with tensor cores allowed: window sizes where the autotuner found the FP32 kernel faster
     bool fp32_faster[129] = {};
+    // launch choices change (autotune, variant pinning): cached pass graphs are stale
+    uint64_t epoch = 0;
+    // the passes of the last repeated call, as a CUDA graph replayed while its key holds
+    cudaGraphExec_t gexec = nullptr;
+    std::vector<uintptr_t> gkey, pending_key;
+    long long gnl = 0;  // kernels in the graph
 
     bool mask_trivial() const { return min_mean <= 0.0f && min_std <= 0.0f; }
     std::vector<int32_t> pass_windows() const {
@@ -289,7 +295,7 @@ int alloc_stats(PivFrame* f) {
 // The multipass loop (multipass.rs:152-192) for K pairs of equal size at once: every pass is
 // placement -> correlation -> validation, each stage ONE launch covering all K pairs, on the
 // analyzer's stream; the predictor of pair k is its own previous pass's validated field.
-int run_passes(PivAnalyzer* an, const PivFrame* const* a, const PivFrame* const* b, int K, bool tune = false) {
+int run_passes_eager(PivAnalyzer* an, const PivFrame* const* a, const PivFrame* const* b, int K, bool tune) {
     if (K <= 0) return fail(PIV_ERR_ARGUMENT, "no pairs");
     for (int k = 0; k < K; ++k) {
         if (!a[k] || !b[k]) return fail(PIV_ERR_ARGUMENT, "null frame");
@@ -388,6 +394,7 @@ int run_passes(PivAnalyzer* an, const PivFrame* const* a, const PivFrame* const*
                 }
             }
             an->variant[kind][nwin] = best_v;
+            ++an->epoch;
             if (tc_ok) {
                 CUDA_TRY(launch_correlate_tc_items(nwin, f16, cps.data(), K, an->cur, &nl));
                 CUDA_TRY(cudaEventRecord(t0, an->cur));
@@ -421,6 +428,69 @@ int run_passes(PivAnalyzer* an, const PivFrame* const* a, const PivFrame* const*
     }
     int nl = 0;
     CUDA_TRY(launch_summary_items(sums.data(), K, an->cur, &nl));
+    an->launches += nl;
+    return PIV_OK;
+}
+
+// All passes of K pairs on the analyzer's stream. A call that repeats the previous call's launch
+// sequence exactly (same frames and their buffers, sizes, workspace and launch choices: the key)
+// is captured once as a CUDA graph, and later calls with that key replay it, which removes the
+// per-kernel launch cost that dominates small frames. The graph reads the frames' current
+// contents, so new samples in the same frames need no new capture. Tuning, profiling and a
+// stream that the caller is capturing run eagerly.
+int run_passes(PivAnalyzer* an, const PivFrame* const* a, const PivFrame* const* b, int K, bool tune = false) {
+    if (tune || an->profiling || K <= 0) {
+        an->pending_key.clear();
+        return run_passes_eager(an, a, b, K, tune);
+    }
+    for (int k = 0; k < K; ++k)
+        if (!a[k] || !b[k] || a[k]->H != a[0]->H || a[k]->W != a[0]->W || b[k]->H != a[0]->H || b[k]->W != a[0]->W)
+            return run_passes_eager(an, a, b, K, tune);  // reports the error
+    int st = use_device(an);
+    if (st) return st;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    CUDA_TRY(cudaStreamIsCapturing(an->cur, &cap));
+    if (cap != cudaStreamCaptureStatusNone) return run_passes_eager(an, a, b, K, tune);
+    st = ensure_workspace(an, a[0]->H, a[0]->W, K);
+    if (st) return st;
+    std::vector<uintptr_t> key = {(uintptr_t)K, (uintptr_t)a[0]->H, (uintptr_t)a[0]->W, (uintptr_t)an->arena,
+                                  (uintptr_t)an->epoch};
+    for (int k = 0; k < K; ++k)
+        for (const PivFrame* f : {a[k], b[k]})
+            for (uintptr_t v : {(uintptr_t)f, (uintptr_t)f->image, (uintptr_t)f->sum, (uintptr_t)f->sumsq,
+                                (uintptr_t)f->scales, (uintptr_t)needs_stats(an, f), (uintptr_t)f->stats_valid})
+                key.push_back(v);
+    if (an->gexec && key == an->gkey) {
+        CUDA_TRY(cudaGraphLaunch(an->gexec, an->cur));
+        an->launches += an->gnl;
+        return PIV_OK;
+    }
+    if (key != an->pending_key) {  // first call with this key: eager
+        an->pending_key = key;
+        return run_passes_eager(an, a, b, K, tune);
+    }
+    // second call with the same key: capture, then replay
+    CUDA_TRY(cudaStreamBeginCapture(an->cur, cudaStreamCaptureModeRelaxed));
+    const long long l0 = an->launches;
+    st = run_passes_eager(an, a, b, K, tune);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(an->cur, &graph);
+    const long long nl = an->launches - l0;
+    an->launches = l0;
+    if (st) {
+        if (graph) cudaGraphDestroy(graph);
+        return st;
+    }
+    if (ce != cudaSuccess) return fail(PIV_ERR_CUDA, "pass graph capture: %s", cudaGetErrorString(ce));
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ie != cudaSuccess) return fail(PIV_ERR_CUDA, "pass graph instantiation: %s", cudaGetErrorString(ie));
+    if (an->gexec) cudaGraphExecDestroy(an->gexec);
+    an->gexec = exec;
+    an->gkey = key;
+    an->gnl = nl;
+    CUDA_TRY(cudaGraphLaunch(exec, an->cur));
     an->launches += nl;
     return PIV_OK;
 }
@@ -597,6 +667,7 @@ void piv_analyzer_destroy(PivAnalyzer* an) {
             cudaEventDestroy(pr.second);
         }
     for (cudaEvent_t e : an->spare) cudaEventDestroy(e);
+    if (an->gexec) cudaGraphExecDestroy(an->gexec);
     if (an->arena) cudaFree(an->arena);
     if (an->own) cudaStreamDestroy(an->own);
     delete an;
@@ -665,6 +736,7 @@ int32_t piv_analyzer_set_variant(PivAnalyzer* an, int32_t window, int32_t v) {
         return fail(PIV_ERR_ARGUMENT, "variant %d out of range for window %d", v, window);
     an->variant[kind][window] = v;
     an->fp32_faster[window] = true;  // an explicit FP32 launch variant
+    ++an->epoch;
     return PIV_OK;
 }
 
