@@ -51,9 +51,11 @@ WORKLOADS = {
         schedules=[[32], [64, 32], [64, 32, 16]], pool=3, budget=60 << 30, max_in_flight=256, seed=4,
         serving=True, windows=[32], overlap=0.5, final_iterations=1, h=512, w=512, outlier_frac=0.0),
     "c2": dict(
-        name="1024x1024 u16 12-bit Lamb-Oseen pair, 64->32->16 px at 50% overlap, FP32 plain",
+        name="1024x1024 u16 12-bit Lamb-Oseen pair, min-background subtraction and 99th-percentile clip, "
+             "64->32->16 px at 50% overlap, FP32 plain",
         h=1024, w=1024, bits=12, windows=[64, 32, 16], overlap=0.5, final_iterations=1, ppp=0.03,
-        dmin=3.0, dmax=3.0, vmax=8.0, shear=0.0, outlier_frac=0.0, seed=2, core=80.0),
+        dmin=3.0, dmax=3.0, vmax=8.0, shear=0.0, outlier_frac=0.0, seed=2, core=80.0,
+        clip_percentile=99.0, background="min", deform=True),
 }
 
 
@@ -421,14 +423,39 @@ def load_traffic(workload):
         return None
 
 
+def _crop_background(wl, a, b, ch, cw):
+    """The workload's background over the cropped pair (per-pixel minimum, decoded), or None."""
+    if wl.get("background") != "min":
+        return None
+    top = np.float32(np.iinfo(a.dtype).max)
+    return (np.minimum(a[:ch, :cw], b[:ch, :cw]).astype(np.float32) / top).astype(np.float32)
+
+
 def _oracle_inputs(wl, a, b, crop):
+    """The oracle's prepared images of a crop of the pair, with the workload's preprocessing: the
+    percentile clip of each frame's codes (a3), then decoding and the background subtraction
+    base = max(raw - background, 0) (preprocess.rs:138-145)."""
     from oracle import oracle as O
     ch, cw = min(crop, wl["h"]), min(crop, wl["w"])
-    fa = O.u16_to_f32(np.ascontiguousarray(a[:ch, :cw])) if a.dtype == np.uint16 else O.u8_to_f32(a[:ch, :cw])
-    fb = O.u16_to_f32(np.ascontiguousarray(b[:ch, :cw])) if b.dtype == np.uint16 else O.u8_to_f32(b[:ch, :cw])
+    dec = O.u16_to_f32 if a.dtype == np.uint16 else O.u8_to_f32
+    ca, cb = np.ascontiguousarray(a[:ch, :cw]), np.ascontiguousarray(b[:ch, :cw])
+    if wl.get("clip_percentile"):
+        ca, _ = O.percentile_clip_u16(ca, wl["clip_percentile"])
+        cb, _ = O.percentile_clip_u16(cb, wl["clip_percentile"])
+    fa, fb = dec(ca), dec(cb)
+    bg = _crop_background(wl, a, b, ch, cw)
+    if bg is not None:
+        fa = O.prepare(fa, 0.0, 0, 0.0, background=bg)[0]
+        fb = O.prepare(fb, 0.0, 0, 0.0, background=bg)[0]
     cfg = O.OracleConfig(tuple(wl["windows"]), wl["overlap"], wl["final_iterations"],
                          deform=int(bool(wl.get("deform", False))))
     return O, fa, fb, cfg, ch, cw
+
+
+def preprocess_config(wl):
+    import piv_b200 as P
+    return P.PreprocessConfig(smooth_sigma=0.0, normalize_radius=0, normalize_eps=0.0,
+                              clip_percentile=float(wl.get("clip_percentile", 0.0)))
 
 
 def cpu_baseline(wl, a, b, budget_s=12.0, crop=1024, single_s=0.0):
@@ -466,7 +493,9 @@ def accuracy_vs_fp64(wl, a, b, an, crop=1024):
     import piv_b200 as P
     O, fa, fb, cfg, ch, cw = _oracle_inputs(wl, a, b, crop)
     ref, _, _ = O.analyze(cfg, fa, fb, mode=O.FP64)
-    r = an.analyze(an.prepare(np.ascontiguousarray(a[:ch, :cw]), P.RAW), an.prepare(np.ascontiguousarray(b[:ch, :cw]), P.RAW))
+    pre, bg = preprocess_config(wl), _crop_background(wl, a, b, ch, cw)
+    r = an.analyze(an.prepare(np.ascontiguousarray(a[:ch, :cw]), pre, background=bg),
+                   an.prepare(np.ascontiguousarray(b[:ch, :cw]), pre, background=bg))
     ok = (ref["flags"] == 0) & (r.field.flags == 0)
     d = np.hypot(r.field.dx[ok] - ref["dx"][ok], r.field.dy[ok] - ref["dy"][ok])
     return {"rms_px_vs_fp64": float(np.sqrt(np.mean(d * d))) if d.size else None,
@@ -555,7 +584,8 @@ def main():
     wl = dict(WORKLOADS[args.workload])
     if args.deform is not None:
         wl["deform"] = bool(args.deform)
-        wl["name"] = wl["name"] + (", deformed windows" if args.deform else ", uniform windows")
+    if args.deform is not None or "deform" in WORKLOADS[args.workload]:
+        wl["name"] = wl["name"] + (", deformed windows" if wl.get("deform") else ", uniform windows")
     if args.precision is not None:
         wl["precision"] = args.precision
         if args.precision != "fp32":
@@ -583,8 +613,12 @@ def main():
 
     # ---------------------------------------------------------------- inputs (host, then device)
     a0, b0 = make_inputs(wl, seed_offset=rank)
-    pairs_host = [(a0, b0), (np.ascontiguousarray(np.roll(a0, (37, 53), (0, 1))),
-                            np.ascontiguousarray(np.roll(b0, (37, 53), (0, 1))))]
+    # a ring of shifted copies of the pair, at least 256 MiB of samples, so that the steps read
+    # their inputs from HBM rather than from the 126 MB L2
+    pair_bytes = a0.nbytes + b0.nbytes
+    n_ring = max(2, -(-(256 << 20) // pair_bytes))
+    pairs_host = [(a0, b0)] + [(np.ascontiguousarray(np.roll(a0, (37 * k, 53 * k), (0, 1))),
+                                np.ascontiguousarray(np.roll(b0, (37 * k, 53 * k), (0, 1)))) for k in range(1, n_ring)]
     dtype_code = P.api._dtype_code(a0)
     h, w = a0.shape
     # raw u16 samples on the device (held as int16 tensors: same bytes)
@@ -602,18 +636,36 @@ def main():
     out_ppr = torch.empty_like(out_dx)
     out_fl = torch.empty(nvec, device=dev, dtype=torch.uint8)
     out_sum = torch.empty(8, device=dev, dtype=torch.int64)
-    pre = P.RAW
+    pre = preprocess_config(wl)
+    lib = P.load_library()
+    import ctypes
+    bg_devs, bg_ptrs, bg_hosts = [], [None] * n_ring, [None] * n_ring
+    if wl.get("background") == "min":
+        # the background of each pair, the per-pixel minimum over its two frames
+        # (BackgroundEstimator, preprocess.rs:47-72), estimated before the timed steps as the
+        # reference estimates it before its pair loop
+        for k, (ta, tb) in enumerate(pairs_dev):
+            stack = torch.stack([ta, tb])
+            bgk = torch.empty((h, w), dtype=torch.float32, device=dev)
+            P.api._check(lib.piv_background_device(an._h, ctypes.c_void_p(stack.data_ptr()), dtype_code, 2, h, w, 0,
+                                                   ctypes.c_void_p(bgk.data_ptr())))
+            bg_devs.append(bgk)
+            bg_ptrs[k] = bgk.data_ptr()
+        torch.cuda.synchronize()
+        bg_hosts = [b.cpu().numpy() for b in bg_devs[:2]] + [None] * (n_ring - 2)
+    bg_ptr = bg_ptrs[0]
 
     def step(i):
-        ta, tb = pairs_dev[i % len(pairs_dev)]
-        fa.prepare_device(ta.data_ptr(), dtype_code, pre)
-        fb.prepare_device(tb.data_ptr(), dtype_code, pre)
+        k = i % n_ring
+        ta, tb = pairs_dev[k]
+        fa.prepare_device(ta.data_ptr(), dtype_code, pre, bg_ptrs[k])
+        fb.prepare_device(tb.data_ptr(), dtype_code, pre, bg_ptrs[k])
         an.analyze_device(fa, fb, out_dx.data_ptr(), out_dy.data_ptr(), out_ppr.data_ptr(), out_fl.data_ptr(),
                           out_sum.data_ptr())
 
     # launch-geometry autotuning on the first pair (results are identical across variants)
-    fa.prepare_device(pairs_dev[0][0].data_ptr(), dtype_code, pre)
-    fb.prepare_device(pairs_dev[0][1].data_ptr(), dtype_code, pre)
+    fa.prepare_device(pairs_dev[0][0].data_ptr(), dtype_code, pre, bg_ptr)
+    fb.prepare_device(pairs_dev[0][1].data_ptr(), dtype_code, pre, bg_ptr)
     tuned = an.autotune(fa, fb) if not args.no_autotune else {}
     for i in range(args.warmup):
         step(i)
@@ -654,21 +706,20 @@ def main():
 
     # ---------------------------------------------------------------- timed: end to end (host buffers)
     pin = [(torch.from_numpy(a.view(np.int16)).pin_memory().numpy().view(np.uint16),
-            torch.from_numpy(b.view(np.int16)).pin_memory().numpy().view(np.uint16)) for a, b in pairs_host]
+            torch.from_numpy(b.view(np.int16)).pin_memory().numpy().view(np.uint16)) for a, b in pairs_host[:2]]
     hdx = torch.empty(nvec, dtype=torch.float32).pin_memory().numpy().reshape(g.ny, g.nx)
     hdy = torch.empty(nvec, dtype=torch.float32).pin_memory().numpy().reshape(g.ny, g.nx)
     hppr = torch.empty(nvec, dtype=torch.float32).pin_memory().numpy().reshape(g.ny, g.nx)
     hfl = torch.empty(nvec, dtype=torch.uint8).pin_memory().numpy().reshape(g.ny, g.nx)
-    lib = P.load_library()
-    import ctypes
     summ = P._lib.PivSummaryC()
     pc = pre._c()
+    bg_args = [None if x is None else ctypes.c_void_p(x.ctypes.data) for x in bg_hosts[:2]]
 
     def e2e_step(i):
         ha, hb = pin[i % len(pin)]
         for fr, hx in ((fa, ha), (fb, hb)):
             P.api._check(lib.piv_frame_prepare(an._h, fr._h, ctypes.c_void_p(hx.ctypes.data), dtype_code,
-                                               ctypes.byref(pc), None))
+                                               ctypes.byref(pc), bg_args[i % len(pin)]))
         P.api._check(lib.piv_analyze(an._h, fa._h, fb._h, ctypes.c_void_p(hdx.ctypes.data),
                                      ctypes.c_void_p(hdy.ctypes.data), ctypes.c_void_p(hppr.ctypes.data),
                                      ctypes.c_void_p(hfl.ctypes.data), ctypes.byref(summ)))
@@ -693,6 +744,7 @@ def main():
     # overlap the others' kernels; host clock with the device synchronised at both ends
     depth = 3
     pl = P.PivPipeline(an, h, w, dtype=np.uint16, cfg=pre, depth=depth)
+    pl.set_background(bg_ptr)  # one background image for the pipelined run (that of the first pair)
     outs = [tuple(torch.empty(nvec, dtype=dt).pin_memory().numpy().reshape(g.ny, g.nx)
                   for dt in (torch.float32, torch.float32, torch.float32, torch.uint8)) for _ in range(depth)]
 
@@ -754,7 +806,9 @@ def main():
             "vs_baseline": None, "dtype": "f32" if wl.get("precision", "fp32") == "fp32" else wl["precision"] + "+f32", "data": "synthetic",
             "config": {"workload": wl["name"], "image": f"{h}x{w} u16 ({wl['bits']}-bit)", "windows": pw,
                        "overlap": wl["overlap"], "final_pass_vectors": nvec, "parallelism": f"replicas x{world}",
-                       "l2": "inputs > L2: 2 alternating pairs, 192 MiB of samples + prepared images per step"},
+                       "l2": f"inputs > L2: {n_ring} shifted copies of the pair in turn, "
+                             f"{n_ring * pair_bytes / 2**20:.0f} MiB of samples"
+                             + (" (+ one background image per pair)" if wl.get("background") else "")},
             "e2e": {"value": e2e_value, "unit": "vectors/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "steps": pipe_steps,
                     "ms_per_step": ms2 / pipe_steps,

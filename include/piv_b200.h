@@ -261,6 +261,11 @@ int32_t piv_pipeline_submit(PivPipeline* pipeline, const void* frame_a, const vo
                             float* peak_ratio, uint8_t* flags, uint64_t* ticket);
 /* Waits for the pair of `ticket`; every ticket is waited for exactly once. */
 int32_t piv_pipeline_wait(PivPipeline* pipeline, uint64_t ticket, PivSummaryC* summary);
+/* Background image (DEVICE, height*width f32, e.g. from piv_background_device) subtracted from
+ * every frame submitted from now on, as piv_frame_prepare's `background` (preprocess.rs:138-145:
+ * base = max(raw - background, 0)); NULL = none. The reference estimates one background per run
+ * and uses it for every frame. Not while pairs are in flight; the image must outlive them. */
+int32_t piv_pipeline_set_background(PivPipeline* pipeline, const float* background_dev);
 
 /* ----------------------------------------------------------------------------- serving form
  * No counterpart in the reference. A request loop on one GPU with continuous batching: frame

@@ -25,7 +25,7 @@ EXPORTS = [
     "piv_analyze", "piv_analyze_device", "piv_analyze_traced", "piv_analyze_batch_device",
     "piv_batch_create", "piv_batch_destroy", "piv_batch_input_device", "piv_batch_input_bytes", "piv_batch_run",
     "piv_batch_sync", "piv_batch_outputs_device", "piv_batch_run_host", "piv_batch_kernels", "piv_batch_stream",
-    "piv_batch_submit_host", "piv_batch_wait_host", "piv_batch_set_stream",
+    "piv_batch_submit_host", "piv_batch_wait_host", "piv_batch_set_stream", "piv_pipeline_set_background",
     "piv_pipeline_create", "piv_pipeline_destroy", "piv_pipeline_submit", "piv_pipeline_wait",
     "piv_place_windows", "piv_correlate_origins", "piv_place_windows_deform", "piv_correlate_deform",
     "piv_validate_field", "piv_flow_stats_device", "piv_temporal_smooth_device", "piv_spatial_smooth_device",
@@ -167,6 +167,7 @@ def load():
         "piv_pipeline_destroy": ([vp], None),
         "piv_pipeline_submit": ([vp, vp, vp, vp, vp, vp, vp, P(ctypes.c_uint64)], i32),
         "piv_pipeline_wait": ([vp, ctypes.c_uint64, P(PivSummaryC)], i32),
+        "piv_pipeline_set_background": ([vp, vp], i32),
         "piv_flow_stats_device": ([i64, i64, i64, ctypes.c_double, vp, vp, vp, vp, P(PivFlowStatsC), vp], i32),
         "piv_temporal_smooth_device": ([i64, i64, i64, vp, vp, vp, vp, i32, i32, i32, vp, i32, vp, vp, vp, vp], i32),
         "piv_spatial_smooth_device": ([i64, i64, i64, vp, vp, vp, ctypes.c_float, ctypes.c_float, i32, vp, vp, vp, vp],

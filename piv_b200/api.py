@@ -612,8 +612,8 @@ class PivBatch:
 
 class PivPipeline:
     """Pipelined pairs of one size: submit() queues a pair of host frames and returns a ticket at
-    once; `depth` slots (each with its own stream and workspace) overlap one pair's copies with the
-    others' kernels. wait(ticket) returns the PairResult, equal to PivAnalyzer.analyze of that pair.
+    once; `depth` slots (each with its own workspace; uploads, kernels and downloads on three
+    shared streams) overlap one pair's copies with the others' kernels. wait(ticket) returns the PairResult, equal to PivAnalyzer.analyze of that pair.
     Frames should be pinned host memory for the uploads to be asynchronous."""
 
     def __init__(self, analyzer: PivAnalyzer, height, width, dtype=np.uint16, cfg: PreprocessConfig = None, depth=2):
@@ -640,6 +640,12 @@ class PivPipeline:
         _check(_lib.load().piv_pipeline_submit(self._h, _ptr(a), _ptr(b), *[_ptr(x) for x in out], ctypes.byref(t)))
         self._pending[t.value] = (a, b, out)  # keep the buffers alive until the pair is collected
         return t.value
+
+    def set_background(self, background_ptr: Optional[int]):
+        """Device background image (height*width f32, e.g. a torch CUDA tensor's data_ptr())
+        subtracted from every frame submitted from now on; None for none. It must stay alive
+        while pairs use it."""
+        _check(_lib.load().piv_pipeline_set_background(self._h, ctypes.c_void_p(background_ptr) if background_ptr else None))
 
     def wait(self, ticket):
         a, b, out = self._pending.pop(ticket)

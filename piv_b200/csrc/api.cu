@@ -1443,6 +1443,7 @@ struct PivPipeline {
         uint64_t ticket = 0;  // 0: idle
     };
     cudaStream_t up = nullptr, comp = nullptr, down = nullptr;
+    const float* background = nullptr;  // device image subtracted from every frame (caller-owned)
     int device = 0;
     int64_t H = 0, W = 0;
     int32_t dtype = PIV_DTYPE_U16;
@@ -1548,8 +1549,8 @@ int32_t piv_pipeline_submit(PivPipeline* pl, const void* frame_a, const void* fr
     CUDA_TRY(cudaMemcpyAsync(s.fb->d_raw, frame_b, raw_bytes, cudaMemcpyHostToDevice, pl->up));
     CUDA_TRY(cudaEventRecord(s.uploaded, pl->up));
     CUDA_TRY(cudaStreamWaitEvent(pl->comp, s.uploaded, 0));
-    int st = prepare_common(s.an, s.fa, s.fa->d_raw, pl->dtype, &pl->pre, nullptr);
-    if (!st) st = prepare_common(s.an, s.fb, s.fb->d_raw, pl->dtype, &pl->pre, nullptr);
+    int st = prepare_common(s.an, s.fa, s.fa->d_raw, pl->dtype, &pl->pre, pl->background);
+    if (!st) st = prepare_common(s.an, s.fb, s.fb->d_raw, pl->dtype, &pl->pre, pl->background);
     if (!st) st = run_passes(s.an, s.fa, s.fb);
     if (st) return st;
     CUDA_TRY(cudaEventRecord(s.computed, pl->comp));
@@ -1566,6 +1567,14 @@ int32_t piv_pipeline_submit(PivPipeline* pl, const void* frame_a, const void* fr
     s.ticket = ++pl->tickets;
     pl->next++;
     *ticket = s.ticket;
+    return PIV_OK;
+}
+
+int32_t piv_pipeline_set_background(PivPipeline* pl, const float* background_dev) {
+    if (!pl) return fail(PIV_ERR_ARGUMENT, "null pipeline");
+    for (const auto& s : pl->slots)
+        if (s.ticket) return fail(PIV_ERR_ARGUMENT, "pairs are in flight: wait for them before changing the background");
+    pl->background = background_dev;
     return PIV_OK;
 }
 

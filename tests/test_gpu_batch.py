@@ -1,6 +1,8 @@
 """The batching form (one launch per stage for many pairs, replayed from a CUDA graph) against
 the per-pair analysis: results must be bit-identical, on the eager first run, on graph replays
 and on new data written into the same input slab."""
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -195,3 +197,33 @@ def test_repeated_single_pair_calls_replay_the_pass_graph_on_current_data():
     for _ in range(3):
         same(an.analyze(fa, fb), refs[1])
     an.close()
+
+
+def test_pipeline_background_and_clip_match_piv_analyze():
+    """A pipeline-wide background (the per-pixel minimum of the run's frames) and a percentile
+    clip give each pair exactly what piv_analyze gives with the same background and settings."""
+    import torch
+
+    import piv_b200 as P
+    h, w, k = 192, 256, 3
+    frames = _frames(k + 1, h, w, 77)
+    cfg = P.PivConfig(windows=[32, 16], overlap=0.5, final_iterations=1)
+    pre = P.PreprocessConfig(smooth_sigma=0.0, normalize_radius=0, normalize_eps=0.0, clip_percentile=99.0)
+    an = P.PivAnalyzer(cfg)
+    # background over all frames on the device (BackgroundEstimator, min mode)
+    dev = torch.from_numpy(frames.view(np.int16)).to("cuda:0")
+    bg = torch.empty((h, w), dtype=torch.float32, device="cuda:0")
+    st = P.load_library().piv_background_device(an._h, ctypes.c_void_p(dev.data_ptr()), P.api._dtype_code(frames[0]),
+                                                k + 1, h, w, 0, ctypes.c_void_p(bg.data_ptr()))
+    assert st == 0
+    torch.cuda.synchronize()
+    bg_host = bg.cpu().numpy()
+    assert np.array_equal(bg_host, (frames.min(axis=0).astype(np.float32) / np.float32(65535)).astype(np.float32))
+    ref = [an.analyze(an.prepare(frames[i], pre, background=bg_host), an.prepare(frames[i + 1], pre, background=bg_host))
+           for i in range(k)]
+    pl = P.PivPipeline(an, h, w, dtype=np.uint16, cfg=pre, depth=2)
+    pl.set_background(bg.data_ptr())
+    tickets = [pl.submit(frames[i], frames[i + 1]) for i in range(k)]
+    for t, r in zip(tickets, ref):
+        _same(pl.wait(t), r)
+    pl.close()
