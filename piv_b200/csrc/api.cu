@@ -129,7 +129,7 @@ struct PivAnalyzer {
     // correlation launch variant chosen per window size (0 until autotuned), uniform / deformed
     int variant[2][129] = {};
     // with tensor cores allowed: window sizes where the autotuner found the FP32 kernel faster
-    bool fp32_faster[129] = {};
+    bool fp32_faster[2][129] = {};  // [uniform / deformed windows][window]
     // launch choices change (autotune, variant pinning): cached pass graphs are stale
     uint64_t epoch = 0;
     // the passes of the last repeated call, as a CUDA graph replayed while its key holds
@@ -368,7 +368,7 @@ int run_passes_eager(PivAnalyzer* an, const PivFrame* const* a, const PivFrame* 
         }
         const int nwin = (int)an->pairs[0][i].grid.window;
         const int kind = cps[0].corners ? 1 : 0;
-        const bool tc_ok = kind == 0 && split_precision(an->precision) && corr_tc_supported(nwin);
+        const bool tc_ok = split_precision(an->precision) && corr_tc_supported(nwin);
         const bool f16 = an->precision == PIV_PRECISION_FP16X3;
         if (tune) {
             // Time every launch variant of this window size on this pass's data (all compute the
@@ -403,12 +403,12 @@ int run_passes_eager(PivAnalyzer* an, const PivFrame* const* a, const PivFrame* 
                 CUDA_TRY(cudaEventSynchronize(t1));
                 float ms = 0.0f;
                 CUDA_TRY(cudaEventElapsedTime(&ms, t0, t1));
-                an->fp32_faster[nwin] = best < ms;
+                an->fp32_faster[kind][nwin] = best < ms;
             }
             cudaEventDestroy(t0);
             cudaEventDestroy(t1);
         }
-        const bool tensor = tc_ok && !an->fp32_faster[nwin];
+        const bool tensor = tc_ok && !an->fp32_faster[kind][nwin];
         if (tensor)
             CUDA_TRY(launch_correlate_tc_items(nwin, f16, cps.data(), K, an->cur, &nl));
         else
@@ -718,7 +718,7 @@ int32_t piv_analyzer_variant(const PivAnalyzer* an, int32_t window, char* name, 
     if (!an || !name || capacity <= 0) return fail(PIV_ERR_ARGUMENT, "bad argument");
     if (!corr_supported(window)) return fail(PIV_ERR_UNSUPPORTED, "window size %d", window);
     const int kind = an->deform ? 1 : 0;
-    if (!an->deform && split_precision(an->precision) && corr_tc_supported(window) && !an->fp32_faster[window])
+    if (split_precision(an->precision) && corr_tc_supported(window) && !an->fp32_faster[kind][window])
         snprintf(name, (size_t)capacity, "%d/tensor-core/%s", window,
                  an->precision == PIV_PRECISION_FP16X3 ? "fp16x3" : "bf16x3");
     else
@@ -735,7 +735,7 @@ int32_t piv_analyzer_set_variant(PivAnalyzer* an, int32_t window, int32_t v) {
     if (v < 0 || v >= corr_num_variants(window, kind))
         return fail(PIV_ERR_ARGUMENT, "variant %d out of range for window %d", v, window);
     an->variant[kind][window] = v;
-    an->fp32_faster[window] = true;  // an explicit FP32 launch variant
+    an->fp32_faster[kind][window] = true;  // an explicit FP32 launch variant
     ++an->epoch;
     return PIV_OK;
 }
@@ -1334,7 +1334,8 @@ PivAnalyzer* clone_config(const PivAnalyzer* parent) {
     an->device = parent->device;
     for (int k = 0; k < 2; ++k)
         for (int i = 0; i < 129; ++i) an->variant[k][i] = parent->variant[k][i];
-    for (int i = 0; i < 129; ++i) an->fp32_faster[i] = parent->fp32_faster[i];
+    for (int k = 0; k < 2; ++k)
+        for (int i = 0; i < 129; ++i) an->fp32_faster[k][i] = parent->fp32_faster[k][i];
     return an;
 }
 }  // namespace
@@ -1930,10 +1931,11 @@ void PivServer::launch_step(std::vector<Request*>& work) {
         pp.min_mean = r->cfg.min_mean;
         pp.min_std = r->cfg.min_std;
         pps.push_back(pp);
-        const int kind = pp.corners ? 1
-                         : (split_precision(r->cfg.precision) && corr_tc_supported((int)pb.grid.window))
-                             ? (r->cfg.precision == PIV_PRECISION_FP16X3 ? 3 : 2)
-                             : 0;
+        // 0 / 1: FP32 uniform / deformed windows; 2 / 3: tensor cores, BF16 / FP16 split, uniform;
+        // 4 / 5: the same with deformed windows
+        const bool tc = split_precision(r->cfg.precision) && corr_tc_supported((int)pb.grid.window);
+        const int kind = tc ? (r->cfg.precision == PIV_PRECISION_FP16X3 ? 3 : 2) + (pp.corners ? 2 : 0)
+                            : (pp.corners ? 1 : 0);
         cps[{(int)pb.grid.window, kind}].push_back(
             CorrParams{r->fa.image, r->fb.image, (int)r->H, (int)r->W, pb.origins, pb.status, (int)pb.cells, pb.raw_dx,
                        pb.raw_dy, pb.raw_ppr, pb.raw_flags, pp.corners, (int)pb.grid.x0, (int)pb.grid.y0,
@@ -1947,8 +1949,8 @@ void PivServer::launch_step(std::vector<Request*>& work) {
     for (auto& kv : cps)
         if (e == cudaSuccess)
             e = kv.first.second >= 2
-                    ? launch_correlate_tc_items(kv.first.first, kv.first.second == 3, kv.second.data(),
-                                                (int)kv.second.size(), stream, &nl)
+                    ? launch_correlate_tc_items(kv.first.first, kv.first.second == 3 || kv.first.second == 5,
+                                                kv.second.data(), (int)kv.second.size(), stream, &nl)
                     : launch_correlate_items(kv.first.first, variant[kv.first.second][kv.first.first], kv.second.data(),
                                              (int)kv.second.size(), stream, &nl);
     if (e == cudaSuccess) e = launch_validate_items(vps.data(), (int)vps.size(), stream, &nl);

@@ -39,6 +39,16 @@
 
 namespace pivb200 {
 
+// c / (N - 1) for c < N, the deformation ramps (correctly rounded, as the FP32 kernel computes
+// them), set by corr_tc_init_device.
+__constant__ float c_ramp16[16];
+__constant__ float c_ramp32[32];
+template <int N>
+__device__ __forceinline__ const float* c_ramp() {
+    if constexpr (N == 16) return c_ramp16;
+    else return c_ramp32;
+}
+
 template <int N_>
 struct TcCfg {
     static constexpr int N = N_, H2 = N / 2;
@@ -135,7 +145,7 @@ __device__ __forceinline__ void mma_split(uint32_t d, uint32_t a_hi, uint32_t a_
         }
 }
 
-template <int N, bool F16>
+template <int N, bool F16, bool DEFORM>
 __global__ void __launch_bounds__(TcCfg<N>::THREADS, 1)
     correlate_tc_kernel(const __grid_constant__ CorrBatch batch, const uint4* __restrict__ mats, int total_tiles,
                         unsigned int* err) {
@@ -194,13 +204,29 @@ __global__ void __launch_bounds__(TcCfg<N>::THREADS, 1)
         const CorrParams& prm = batch.item[item];
         const long long cell = (long long)(tile - batch.block_start[item]) * C::WPT + c;
         const bool active = cell < prm.ncells;
-        const float4 org = active ? prm.origins[cell] : make_float4(0.f, 0.f, 0.f, 0.f);
+        float4 org = make_float4(0.f, 0.f, 0.f, 0.f);  // deformed: (D(centre).x, D(centre).y, -, -)
+        if constexpr (!DEFORM) {
+            if (active) org = prm.origins[cell];
+        }
         bool ok = active && prm.status[cell] != 0;
 
         // ------------------------------------------------ sampling (lane = column q of window c)
         float2 z[N];
-        sample_rows<N, false>(prm.img_a, prm.H, prm.W, org.x, org.y, q, z);
-        sample_rows<N, true>(prm.img_b, prm.H, prm.W, org.z, org.w, q, z);
+        if constexpr (DEFORM) {
+            // Deformed windows (the FP32 kernel's sampling): the predictor's bilinear blend D of
+            // the four window corners, frame A at -D/2 and frame B at +D/2 from the base position.
+            const int ci = active ? (int)cell : 0;
+            const float4 k0 = active ? prm.corners[2 * (size_t)ci] : make_float4(0.f, 0.f, 0.f, 0.f);
+            const float4 k1 = active ? prm.corners[2 * (size_t)ci + 1] : make_float4(0.f, 0.f, 0.f, 0.f);
+            const int gx = min(prm.gx0 + (ci % prm.gnx) * prm.gstep, max(prm.W - N - 1, 0));
+            const int gy = min(prm.gy0 + (ci / prm.gnx) * prm.gstep, max(prm.H - N - 1, 0));
+            org = make_float4(corner_blend(k0.x, k0.z, k1.x, k1.z, 0.5f, 0.5f),
+                              corner_blend(k0.y, k0.w, k1.y, k1.w, 0.5f, 0.5f), 0.f, 0.f);
+            sample_deformed<N, 1>(prm.img_a, prm.img_b, prm.H, prm.W, gx, gy, k0, k1, q, 0, c_ramp<N>(), z);
+        } else {
+            sample_rows<N, false>(prm.img_a, prm.H, prm.W, org.x, org.y, q, z);
+            sample_rows<N, true>(prm.img_b, prm.H, prm.W, org.z, org.w, q, z);
+        }
         float2 e;
         {
             float2 s = make_float2(0.f, 0.f);
@@ -501,8 +527,13 @@ __global__ void __launch_bounds__(TcCfg<N>::THREADS, 1)
                 const float wx = bx >= N / 2 ? (float)bx - (float)N : (float)bx;
                 const float wy = by >= N / 2 ? (float)by - (float)N : (float)by;
                 const float pdx = __fadd_rn(wx, sx), pdy = __fadd_rn(wy, sy);
-                prm.raw_dx[cell] = __fadd_rn(__fsub_rn(org.z, org.x), pdx);
-                prm.raw_dy[cell] = __fadd_rn(__fsub_rn(org.w, org.y), pdy);
+                if constexpr (DEFORM) {
+                    prm.raw_dx[cell] = __fadd_rn(org.x, pdx);  // D(centre) + peak
+                    prm.raw_dy[cell] = __fadd_rn(org.y, pdy);
+                } else {
+                    prm.raw_dx[cell] = __fadd_rn(__fsub_rn(org.z, org.x), pdx);
+                    prm.raw_dy[cell] = __fadd_rn(__fsub_rn(org.w, org.y), pdy);
+                }
                 prm.raw_ppr[cell] = second > 0.0f ? fminf(__fdiv_rn(best, second), MAX_PPR) : MAX_PPR;
                 prm.raw_flags[cell] = 0;
             } else {
@@ -644,6 +675,13 @@ cudaError_t corr_tc_init_device() {
     if (e == cudaSuccess) e = upload<16, true>(&g_mats[dev][0][1]);
     if (e == cudaSuccess) e = upload<32, false>(&g_mats[dev][1][0]);
     if (e == cudaSuccess) e = upload<32, true>(&g_mats[dev][1][1]);
+    if (e == cudaSuccess) {
+        float r16[16], r32[32];
+        for (int i = 0; i < 16; ++i) r16[i] = (float)i / 15.0f;
+        for (int i = 0; i < 32; ++i) r32[i] = (float)i / 31.0f;
+        e = cudaMemcpyToSymbol(c_ramp16, r16, sizeof(r16));
+        if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_ramp32, r32, sizeof(r32));
+    }
     if (e == cudaSuccess && !g_err_host[dev]) {
         e = cudaHostAlloc(reinterpret_cast<void**>(&g_err_host[dev]), sizeof(unsigned int), cudaHostAllocMapped);
         if (e == cudaSuccess) {
@@ -658,7 +696,7 @@ unsigned int corr_tc_error(int device) {
     return (device >= 0 && device < kMaxDevices && g_err_host[device]) ? *(volatile unsigned int*)g_err_host[device] : 0u;
 }
 
-template <int N, bool F16>
+template <int N, bool F16, bool DEFORM>
 static cudaError_t launch_tc(CorrBatch b, cudaStream_t s, const uint4* mats, unsigned int* err) {
     using C = TcCfg<N>;
     long long total = 0;
@@ -673,7 +711,7 @@ static cudaError_t launch_tc(CorrBatch b, cudaStream_t s, const uint4* mats, uns
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
-    auto kern = correlate_tc_kernel<N, F16>;
+    auto kern = correlate_tc_kernel<N, F16, DEFORM>;
     e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
     if (e != cudaSuccess) return e;
     const long long ctas = std::min<long long>((total + C::NWG - 1) / C::NWG, (long long)sms);
@@ -685,8 +723,9 @@ cudaError_t launch_correlate_tc_items(int n, bool f16, const CorrParams* items, 
                                       int* launches) {
     if (count <= 0) return cudaSuccess;
     if (!corr_tc_supported(n)) return cudaErrorInvalidValue;
+    const bool deform = items[0].corners != nullptr;
     for (int i = 0; i < count; ++i)
-        if (items[i].corners) return cudaErrorInvalidValue;  // deformed windows: FP32 kernel only
+        if ((items[i].corners != nullptr) != deform) return cudaErrorInvalidValue;  // one kind per launch
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
@@ -696,10 +735,14 @@ cudaError_t launch_correlate_tc_items(int n, bool f16, const CorrParams* items, 
         b.n = count - off < kMaxBatch ? count - off : kMaxBatch;
         for (int i = 0; i < b.n; ++i) b.item[i] = items[off + i];
         const uint4* m = g_mats[dev][n == 16 ? 0 : 1][f16 ? 1 : 0];
-        if (n == 16)
-            e = f16 ? launch_tc<16, true>(b, s, m, g_err_dev[dev]) : launch_tc<16, false>(b, s, m, g_err_dev[dev]);
-        else
-            e = f16 ? launch_tc<32, true>(b, s, m, g_err_dev[dev]) : launch_tc<32, false>(b, s, m, g_err_dev[dev]);
+        unsigned int* err = g_err_dev[dev];
+        if (n == 16) {
+            if (deform) e = f16 ? launch_tc<16, true, true>(b, s, m, err) : launch_tc<16, false, true>(b, s, m, err);
+            else e = f16 ? launch_tc<16, true, false>(b, s, m, err) : launch_tc<16, false, false>(b, s, m, err);
+        } else {
+            if (deform) e = f16 ? launch_tc<32, true, true>(b, s, m, err) : launch_tc<32, false, true>(b, s, m, err);
+            else e = f16 ? launch_tc<32, true, false>(b, s, m, err) : launch_tc<32, false, false>(b, s, m, err);
+        }
         if (e != cudaSuccess) return e;
         if (launches) ++*launches;
     }

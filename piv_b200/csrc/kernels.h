@@ -62,8 +62,8 @@ cudaError_t launch_correlate_variant(int n, int v, const CorrParams& p, cudaStre
 // indexes the variants of that kind. Returns the number of launches issued in *launches.
 cudaError_t launch_correlate_items(int n, int v, const CorrParams* items, int count, cudaStream_t s, int* launches);
 // Split-precision (BF16 or FP16 hi/lo, three products) tensor-core correlation, window sizes 16
-// and 32;
-// uniform windows only. corr_tc_init_device uploads its DFT matrices to the current device;
+// and 32; all items of a call are uniform windows or all deformed (corners set).
+// corr_tc_init_device uploads its DFT matrices and deformation ramps to the current device;
 // corr_tc_error reads the device's error word (non-zero after a tensor-core wait ran out).
 bool corr_tc_supported(int n);
 cudaError_t corr_tc_init_device();

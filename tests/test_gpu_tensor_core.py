@@ -126,3 +126,29 @@ def test_batch_and_server_forms_match_the_analyzer(precision):
         assert np.array_equal(r.field.flags, q.field.flags)
         assert same_floats(r.field.dx, q.field.dx) and same_floats(r.field.dy, q.field.dy)
     sv.close()
+
+
+@pytest.mark.parametrize("precision", ["bf16x3", "fp16x3"])
+def test_deformed_windows_on_tensor_cores_within_0p01_px_of_fp64(precision):
+    """Window deformation (the predictor's bilinear blend over each window) with the 32 and 16 px
+    passes on the tensor cores: the final field within 0.01 px RMS of the FP64 oracle's deformed
+    analysis, and close to the FP32 kernel's."""
+    import piv_b200 as P
+    h = 384
+    a, b = _pair(h, seed=6, vmax=7.0)
+    cfg = dict(windows=[64, 32, 16], overlap=0.5, final_iterations=1, deform=True)
+    an = P.PivAnalyzer(P.PivConfig(precision=precision, **cfg))
+    assert "tensor-core" in an.variant(32) and "tensor-core" in an.variant(16)
+    r = an.analyze(an.prepare(a, P.RAW), an.prepare(b, P.RAW))
+    an32 = P.PivAnalyzer(P.PivConfig(**cfg))
+    r32 = an32.analyze(an32.prepare(a, P.RAW), an32.prepare(b, P.RAW))
+    ref, _, _ = O.analyze(O.OracleConfig((64, 32, 16), 0.5, 1, deform=1), O.u16_to_f32(a), O.u16_to_f32(b),
+                          mode=O.FP64)
+    ok = (ref["flags"] == 0) & (r.field.flags == 0)
+    assert ok.mean() > 0.9
+    d = np.hypot(r.field.dx[ok] - ref["dx"][ok], r.field.dy[ok] - ref["dy"][ok])
+    assert np.sqrt(np.mean(d * d)) <= 0.01
+    assert np.mean(ref["flags"] == r.field.flags) > 0.99
+    both = ok & (r32.field.flags == 0)
+    d32 = np.hypot(r.field.dx[both] - r32.field.dx[both], r.field.dy[both] - r32.field.dy[both])
+    assert np.sqrt(np.mean(d32 * d32)) <= 1e-3
