@@ -41,9 +41,9 @@ WORKLOADS = {
         h=4096, w=4096, bits=12, windows=[128, 64, 32, 16], overlap=0.75, final_iterations=1, ppp=0.05,
         dmin=2.0, dmax=4.0, vmax=10.0, shear=0.01, outlier_frac=0.02, seed=5),
     "c3": dict(
-        name="1280x800 u16 video stream, sequential pairs, 64->32 px at 50% overlap, 32 pairs per CUDA-graph replay",
+        name="1280x800 u16 video stream, sequential pairs, 64->32 px at 50% overlap, 64 pairs per CUDA-graph replay",
         h=800, w=1280, bits=12, windows=[64, 32], overlap=0.5, final_iterations=1, ppp=0.04, dmin=2.0, dmax=5.0,
-        amplitude=6.0, wavelength=320.0, phase_step=0.02, frames=33, stream=True, seed=3, outlier_frac=0.0),
+        amplitude=6.0, wavelength=320.0, phase_step=0.02, frames=65, stream=True, seed=3, outlier_frac=0.0),
     "c4": dict(
         name="serving: Poisson arrivals 400 pairs/s, u16 pairs of 512x512 / 1024x768 / 2048x2048, schedules "
              "[32] / [64,32] / [64,32,16] at 50% overlap, 60 GB admission budget, continuous batching",
@@ -196,13 +196,14 @@ def run_stream(args, wl):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": wl["name"], "frames_per_step": nf, "pairs_per_step": k,
                        "final_pass_vectors_per_pair": final_vectors(wl), "windows": pass_windows(wl),
-                       "l2": "inputs > L2: 33 frames = 66 MiB of samples + 132 MiB prepared per step"},
+                       "l2": f"inputs > L2: {nf} frames = {frames.nbytes / 2**20:.0f} MiB of samples + "
+                             f"{nf * h * w * 4 / 2**20:.0f} MiB prepared per step"},
             "e2e": {"value": ranks.world * e2e_steps * nvec / (e2e_ms * 1e-3), "unit": "vectors/s",
                     "h2d_bytes_per_step": int(pin.nbytes), "d2h_bytes_per_step": int(nvec * 13 + k * 40),
                     "ms_per_step": e2e_ms / e2e_steps,
-                    "how": "two PivBatch objects in turn sharing one compute stream (submit_host / wait_host "
-                           "over pinned frames): upload of 33 frames, one graph replay and download of 32 fields "
-                           "per step; host clock, device synchronised at both ends"},
+                    "how": f"two PivBatch objects in turn sharing one compute stream (submit_host / wait_host "
+                           f"over pinned frames): upload of {nf} frames, one graph replay and download of {k} "
+                           f"fields per step; host clock, device synchronised at both ends"},
             "gpu_launches": int(batch.kernels() * args.steps), "graph_launches": args.steps,
             "clocks": clocks, "autotuned_variants": tuned, "wall_ms_per_step": 1e3 * wall / args.steps,
             "valid_fraction_last_pair": float(np.mean((res[-1].field.flags & P.flags.INVALID) == 0)),

@@ -236,3 +236,23 @@ def test_validation_with_signed_zero_and_repeated_values_matches_oracle():
         assert np.array_equal(gf, of), trial
         assert np.any(np.signbit(ox[ox == 0])) and np.any(~np.signbit(ox[ox == 0]))
         assert same_bits(gx, ox) and same_bits(gy, oy), trial
+
+
+def test_single_pass_u8_pair_of_the_cpu_case():
+    """The reference's CPU-runnable case: a 512 x 512 u8 particle pair (0.05 ppp, diameters 2-4 px,
+    peaks 120-255, noise sigma 4), uniform displacement (2.3, -1.7), one 32 px pass at 50 %
+    overlap, no preprocessing, median test threshold 2 / eps 0.1, ppr 1.3. Stage by stage against
+    the oracle, and the known displacement recovered."""
+    import piv_b200 as P
+    from piv_b200 import synthetic as S
+    a, b = S.baseline_pair(512, 512, 1, lambda x, y: (2.3, -1.7), ppp=0.05, dmin=2.0, dmax=4.0, bits=8)
+    assert a.dtype == np.uint8
+    an = P.PivAnalyzer(P.PivConfig(windows=[32], overlap=0.5, final_iterations=1))
+    fa, fb = an.prepare(a, P.RAW), an.prepare(b, P.RAW)
+    res, traces = an.analyze_traced(fa, fb)
+    assert len(res.field.dx.ravel()) == 961
+    _stage_check(an, traces, O.u8_to_f32(a), O.u8_to_f32(b), [32], overlap=0.5)  # decoded as the GPU decodes
+    ok = res.field.flags == 0
+    assert ok.mean() > 0.95
+    err = np.hypot(res.field.dx[ok] - 2.3, res.field.dy[ok] + 1.7)
+    assert np.sqrt(np.mean(err ** 2)) < 0.1
