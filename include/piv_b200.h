@@ -398,6 +398,12 @@ int32_t piv_spatial_smooth_device(int64_t nt, int64_t ny, int64_t nx, const floa
  * stored K-major (a_mn = 0) or MN-major (a_mn = 1) as the tensor-core correlation stores its
  * operands. a, b, d are row-major DEVICE arrays; n, k multiples of 16 in [16, 256]. Blocking. */
 int32_t piv_tc_selftest(int32_t device, int32_t a_mn, int32_t n, int32_t k, const float* a, const float* b, float* d);
+/* Diagnostics (no counterpart in the reference): runs the tensor-core kernel's bounded mbarrier
+ * wait on a barrier that nothing completes, with 2^log2_iters try_wait rounds (18 is the kernel's
+ * own bound, about a second; at most 18). The wait gives up, and *timed_out is set to 1; *ms is the probe
+ * kernel's duration. Uses a private status word: the device's tensor-core error status read by
+ * piv_analyze is not touched. Blocking. */
+int32_t piv_tc_wait_probe(int32_t device, int32_t log2_iters, int32_t* timed_out, float* ms);
 
 /* ----------------------------------------------------------------------------- no allocation
  * No counterpart in the reference. Validation of a raw field (the same rules as

@@ -26,6 +26,7 @@ EXPORTS = [
     "piv_batch_create", "piv_batch_destroy", "piv_batch_input_device", "piv_batch_input_bytes", "piv_batch_run",
     "piv_batch_sync", "piv_batch_outputs_device", "piv_batch_run_host", "piv_batch_kernels", "piv_batch_stream",
     "piv_batch_submit_host", "piv_batch_wait_host", "piv_batch_set_stream", "piv_pipeline_set_background",
+    "piv_tc_wait_probe",
     "piv_pipeline_create", "piv_pipeline_destroy", "piv_pipeline_submit", "piv_pipeline_wait",
     "piv_place_windows", "piv_correlate_origins", "piv_place_windows_deform", "piv_correlate_deform",
     "piv_validate_field", "piv_flow_stats_device", "piv_temporal_smooth_device", "piv_spatial_smooth_device",
@@ -161,6 +162,7 @@ def load():
         "piv_place_windows_deform": ([vp, i64, i64, P(PivGridC), P(PivGridC), vp, vp, vp, vp], i32),
         "piv_correlate_deform": ([vp, vp, vp, P(PivGridC), vp, vp, vp, vp, vp, vp], i32),
         "piv_tc_selftest": ([i32, i32, i32, i32, vp, vp, vp], i32),
+        "piv_tc_wait_probe": ([i32, i32, P(i32), P(ctypes.c_float)], i32),
         "piv_batch_submit_host": ([vp, vp, vp, vp, vp, vp], i32),
         "piv_batch_wait_host": ([vp, vp], i32),
         "piv_pipeline_create": ([vp, i64, i64, i32, P(PivPreprocessC), i32, P(vp)], i32),

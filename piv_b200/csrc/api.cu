@@ -1221,6 +1221,18 @@ int32_t piv_tc_selftest(int32_t device, int32_t a_mn, int32_t n, int32_t k, cons
     return check_device_error(dev);
 }
 
+int32_t piv_tc_wait_probe(int32_t device, int32_t log2_iters, int32_t* timed_out, float* ms) {
+    if (!timed_out || !ms) return fail(PIV_ERR_ARGUMENT, "null pointer");
+    if (log2_iters < 0 || log2_iters > 18) return fail(PIV_ERR_ARGUMENT, "log2_iters must be in [0, 18]");
+    int dev = device;
+    if (dev < 0) CUDA_TRY(cudaGetDevice(&dev));
+    CUDA_TRY(cudaSetDevice(dev));
+    unsigned int t = 0;
+    CUDA_TRY(tc_wait_probe(log2_iters, &t, ms));
+    *timed_out = t != 0;
+    return PIV_OK;
+}
+
 int32_t piv_validate_field(PivAnalyzer* an, int64_t ny, int64_t nx, const float* dx, const float* dy,
                            const float* peak_ratio, const uint8_t* flags, float* out_dx, float* out_dy,
                            uint8_t* out_flags, PivSummaryC* summary) {

@@ -812,6 +812,44 @@ __global__ void __launch_bounds__(128, 1)
     }
 }
 
+// The bounded wait of the correlation kernel on an mbarrier that nothing arrives on: the wait
+// runs out after 2^log2_iters try_wait rounds and records that in `err`.
+__global__ void tc_wait_probe_kernel(unsigned int* err, int log2_iters) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        tc::mbar_init(&bar, 1);
+        tc::fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) tc::mbar_wait(&bar, 0, err, log2_iters);
+}
+
+cudaError_t tc_wait_probe(int log2_iters, unsigned int* timed_out, float* ms) {
+    if (log2_iters < 0 || log2_iters > tc::kWaitLog2Iters) return cudaErrorInvalidValue;
+    unsigned int* word = nullptr;  // host-mapped, private to the probe
+    cudaError_t e = cudaHostAlloc(reinterpret_cast<void**>(&word), sizeof(unsigned int), cudaHostAllocMapped);
+    if (e != cudaSuccess) return e;
+    *word = 0;
+    unsigned int* dword = nullptr;
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    e = cudaHostGetDevicePointer(reinterpret_cast<void**>(&dword), word, 0);
+    if (e == cudaSuccess) e = cudaEventCreate(&t0);
+    if (e == cudaSuccess) e = cudaEventCreate(&t1);
+    if (e == cudaSuccess) e = cudaEventRecord(t0, 0);
+    if (e == cudaSuccess) {
+        tc_wait_probe_kernel<<<1, 32>>>(dword, log2_iters);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(t1, 0);
+    if (e == cudaSuccess) e = cudaEventSynchronize(t1);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(ms, t0, t1);
+    if (e == cudaSuccess) *timed_out = *(volatile unsigned int*)word;
+    if (t0) cudaEventDestroy(t0);
+    if (t1) cudaEventDestroy(t1);
+    cudaFreeHost(word);
+    return e;
+}
+
 cudaError_t tc_selftest(int a_mn, int n, int k, const float* a, const float* b, float* d) {
     if (n < 16 || n > 256 || n % 16 || k < 16 || k > 256 || k % 16) return cudaErrorInvalidValue;
     int dev = 0;

@@ -72,6 +72,9 @@ cudaError_t launch_correlate_tc_items(int n, bool f16, const CorrParams* items, 
                                       int* launches);
 // D (128 x n) = A (128 x k) * B (n x k)^T on the tensor cores, BF16 operands (device pointers).
 cudaError_t tc_selftest(int a_mn, int n, int k, const float* a, const float* b, float* d);
+// The correlation kernel's bounded mbarrier wait on a barrier that nothing completes; reports
+// whether the wait recorded a timeout and how long the probe kernel took.
+cudaError_t tc_wait_probe(int log2_iters, unsigned int* timed_out, float* ms);
 // Number of kernel launches launch_correlate issues (for launch accounting).
 constexpr int kCorrLaunches = 1;
 

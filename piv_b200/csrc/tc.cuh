@@ -108,9 +108,12 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 // Bounded wait for the phase with the given parity to complete. try_wait itself suspends for a
-// hardware-defined window, so the bound is a time of the order of seconds.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsigned int* err) {
-    for (int i = 0; i < (1 << 22); ++i)
+// hardware-defined window (about 4 us a round on B200), so 2^18 rounds give up after about a
+// second; a stage's MMAs complete in microseconds.
+constexpr int kWaitLog2Iters = 18;  // try_wait rounds before a wait gives up
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsigned int* err,
+                                          int log2_iters = kWaitLog2Iters) {
+    for (int i = 0; i < (1 << log2_iters); ++i)
         if (mbar_try_wait(bar, parity)) return true;
     if (err) atomicOr(err, 1u);
     return false;

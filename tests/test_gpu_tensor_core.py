@@ -152,3 +152,24 @@ def test_deformed_windows_on_tensor_cores_within_0p01_px_of_fp64(precision):
     both = ok & (r32.field.flags == 0)
     d32 = np.hypot(r.field.dx[both] - r32.field.dx[both], r.field.dy[both] - r32.field.dy[both])
     assert np.sqrt(np.mean(d32 * d32)) <= 1e-3
+
+
+def test_bounded_wait_runs_out_reports_and_leaves_the_device_usable():
+    """The tensor-core kernel's mbarrier waits are bounded. On a barrier that nothing completes,
+    the wait gives up after the kernel's own bound (about a second), records the timeout in its
+    status word and returns; tensor-core work on the same context then runs normally."""
+    import piv_b200 as P
+    lib = P.load_library()
+    timings = {}
+    for log2_iters in (10, 18):
+        t, ms = ctypes.c_int32(-1), ctypes.c_float(-1.0)
+        assert lib.piv_tc_wait_probe(0, log2_iters, ctypes.byref(t), ctypes.byref(ms)) == 0, P._lib.last_error()
+        assert t.value == 1
+        timings[log2_iters] = ms.value
+    assert 0.0 < timings[10] < timings[18] < 5000.0
+    t = ctypes.c_int32()
+    ms = ctypes.c_float()
+    assert lib.piv_tc_wait_probe(0, 19, ctypes.byref(t), ctypes.byref(ms)) != 0  # beyond the kernel's bound
+    test_tensor_core_gemm_layouts(0, 32, 32)
+    err = _one_pass_errors(32, "bf16x3")  # a correlation pass, whose status checks read the error word
+    assert np.sqrt(np.mean(err ** 2)) < 1e-3
