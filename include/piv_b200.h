@@ -220,7 +220,9 @@ int32_t piv_batch_run(PivBatch* batch);
 void* piv_batch_stream(PivBatch* batch);
 /* Runs the batch's kernels on `stream` from now on (NULL: its own stream again). Batches that
  * share one stream replay their graphs one after another while their host copies (which go on
- * private copy streams, see piv_batch_submit_host) overlap. Not while a submission is pending. */
+ * private copy streams, see piv_batch_submit_host) overlap. Not while a submission is pending.
+ * The stream must stay valid while the batch runs on it; piv_batch_destroy itself needs no
+ * stream (it waits for the device). */
 int32_t piv_batch_set_stream(PivBatch* batch, void* stream);
 int32_t piv_batch_sync(PivBatch* batch);
 /* Device output slabs: dx, dy, peak ratio (f32) and flags (u8), pairs*nx*ny each; 8 uint64

@@ -1416,8 +1416,10 @@ void piv_batch_destroy(PivBatch* bt) {
     if (!bt) return;
     if (bt->an) {
         cudaSetDevice(bt->an->device);
-        cudaStreamSynchronize(bt->an->cur);
-        if (bt->an->own) cudaStreamSynchronize(bt->an->own);
+        // The batch's kernels may run on a stream it borrowed (piv_batch_set_stream), which may
+        // already be gone; waiting for the device needs no stream handle.
+        cudaDeviceSynchronize();
+        bt->an->cur = bt->an->own;
     }
     for (cudaStream_t st : {bt->up, bt->down})
         if (st) {
