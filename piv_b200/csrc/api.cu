@@ -667,7 +667,10 @@ void piv_analyzer_destroy(PivAnalyzer* an) {
             cudaEventDestroy(pr.second);
         }
     for (cudaEvent_t e : an->spare) cudaEventDestroy(e);
-    if (an->gexec) cudaGraphExecDestroy(an->gexec);
+    if (an->gexec) {
+        cudaDeviceSynchronize();  // a replay may still run on a caller's stream
+        cudaGraphExecDestroy(an->gexec);
+    }
     if (an->arena) cudaFree(an->arena);
     if (an->own) cudaStreamDestroy(an->own);
     delete an;
