@@ -760,7 +760,8 @@ def main():
             pl.wait(t)
 
     e2e_run(max(args.warmup, depth))
-    pipe_steps = max(12, args.steps // 2)
+    # host-clocked: enough pairs for about half a second, so that clock jitter stays small
+    pipe_steps = int(min(20000, max(12, args.steps // 2, 500.0 / max(ms_max / args.steps, 1e-3))))
     ranks.barrier()
     torch.cuda.synchronize()
     t_pipe = time.perf_counter()
