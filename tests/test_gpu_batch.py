@@ -227,3 +227,37 @@ def test_pipeline_background_and_clip_match_piv_analyze():
     for t, r in zip(tickets, ref):
         _same(pl.wait(t), r)
     pl.close()
+
+
+def test_batch_device_calls_replay_their_graph_on_new_frame_contents():
+    """piv_analyze_batch_device over K pairs, called repeatedly (eager, captured, replayed), and
+    again after new samples were prepared into the same frames: every call equals per-pair
+    analysis of the frames' current contents."""
+    import torch
+
+    import piv_b200 as P
+    h, w, k = 160, 192, 3
+    an = P.PivAnalyzer(P.PivConfig(windows=[32, 16], overlap=0.5, final_iterations=1))
+    sets = [_frames(2 * k, h, w, 51), _frames(2 * k, h, w, 52)]
+    refs = [_reference(an, f, [(2 * i, 2 * i + 1) for i in range(k)]) for f in sets]
+    fr = [an.frame(h, w) for _ in range(2 * k)]
+    g = an.output_grid(h, w)
+    c = g.nx * g.ny
+    dev = torch.device("cuda", 0)
+    dx, dy, ppr = (torch.empty(k * c, device=dev) for _ in range(3))
+    fl = torch.empty(k * c, device=dev, dtype=torch.uint8)
+    arr = ctypes.c_void_p * k
+    a = arr(*[f._h.value for f in fr[0::2]])
+    b = arr(*[f._h.value for f in fr[1::2]])
+    lib = P.load_library()
+    for s in (0, 0, 0, 1, 1, 0):
+        for f, raw in zip(fr, sets[s]):
+            f.prepare(raw, P.RAW)
+        assert lib.piv_analyze_batch_device(an._h, a, b, k, dx.data_ptr(), dy.data_ptr(), ppr.data_ptr(),
+                                            fl.data_ptr(), None) == 0
+        an.sync()
+        for i, r in enumerate(refs[s]):
+            sl = slice(i * c, (i + 1) * c)
+            assert np.array_equal(fl[sl].cpu().numpy().reshape(g.ny, g.nx), r.field.flags)
+            assert same_floats(dx[sl].cpu().numpy().reshape(g.ny, g.nx), r.field.dx)
+            assert same_floats(dy[sl].cpu().numpy().reshape(g.ny, g.nx), r.field.dy)
