@@ -56,6 +56,13 @@ WORKLOADS = {
         h=1024, w=1024, bits=12, windows=[64, 32, 16], overlap=0.5, final_iterations=1, ppp=0.03,
         dmin=3.0, dmax=3.0, vmax=8.0, shear=0.0, outlier_frac=0.0, seed=2, core=80.0,
         clip_percentile=99.0, background="min", deform=True),
+    # the reference's default analysis (PivConfig / PreprocessConfig defaults, preprocess.rs:5-29,
+    # multipass.rs:52-78) on a 1080p 8-bit pair: the frame shape its published timings use
+    "r1080": dict(
+        name="1920x1080 u8 particle pair, the reference's default analysis: blur 1 + local normalisation 4, "
+             "96->64->64 px at 50% overlap, FP32 plain",
+        h=1080, w=1920, bits=8, windows=[96, 64], overlap=0.5, final_iterations=2, ppp=0.03, dmin=2.0, dmax=4.0,
+        vmax=6.0, shear=0.005, outlier_frac=0.0, seed=12, preprocess="default"),
 }
 
 
@@ -444,26 +451,35 @@ def _oracle_inputs(wl, a, b, crop):
         ca, _ = O.percentile_clip_u16(ca, wl["clip_percentile"])
         cb, _ = O.percentile_clip_u16(cb, wl["clip_percentile"])
     fa, fb = dec(ca), dec(cb)
+    ba, bb = fa, fb  # the signal mask's intensity (preprocess.rs:138-158: base = max(raw - bg, 0))
     bg = _crop_background(wl, a, b, ch, cw)
-    if bg is not None:
-        fa = O.prepare(fa, 0.0, 0, 0.0, background=bg)[0]
-        fb = O.prepare(fb, 0.0, 0, 0.0, background=bg)[0]
+    blur, radius, eps = (1.0, 4, 0.02) if wl.get("preprocess") == "default" else (0.0, 0, 0.0)
+    if bg is not None or radius:
+        fa, ba = O.prepare(fa, blur, radius, eps, background=bg)
+        fb, bb = O.prepare(fb, blur, radius, eps, background=bg)
     cfg = O.OracleConfig(tuple(wl["windows"]), wl["overlap"], wl["final_iterations"],
                          deform=int(bool(wl.get("deform", False))))
-    return O, fa, fb, cfg, ch, cw
+    return O, fa, fb, cfg, ch, cw, ba, bb
 
 
 def preprocess_config(wl):
     import piv_b200 as P
-    return P.PreprocessConfig(smooth_sigma=0.0, normalize_radius=0, normalize_eps=0.0,
-                              clip_percentile=float(wl.get("clip_percentile", 0.0)))
+    clip = float(wl.get("clip_percentile", 0.0))
+    if wl.get("preprocess") == "default":  # blur sigma 1, local normalisation radius 4, eps 0.02
+        return P.PreprocessConfig(clip_percentile=clip)
+    return P.PreprocessConfig(smooth_sigma=0.0, normalize_radius=0, normalize_eps=0.0, clip_percentile=clip)
+
+
+def _torch_view(x):
+    """A numpy frame as a torch-compatible array of the same bytes (torch has no uint16)."""
+    return x.view(np.int16) if x.dtype == np.uint16 else x
 
 
 def cpu_baseline(wl, a, b, budget_s=12.0, crop=1024, single_s=0.0):
     """Times the oracle port (reference operation order, OpenMP over windows) on a crop of the
     workload with the same pass schedule; returns final-pass vectors/s and the sample used, plus a
     single-thread figure when single_s > 0."""
-    O, fa, fb, cfg, ch, cw = _oracle_inputs(wl, a, b, crop)
+    O, fa, fb, cfg, ch, cw, ba, bb = _oracle_inputs(wl, a, b, crop)
     nthreads = os.cpu_count() or 1
     vec = final_vectors(wl, ch, cw)
 
@@ -471,7 +487,7 @@ def cpu_baseline(wl, a, b, budget_s=12.0, crop=1024, single_s=0.0):
         t0 = time.perf_counter()
         reps = 0
         while True:
-            O.analyze(cfg, fa, fb, nthreads=nt)
+            O.analyze(cfg, fa, fb, ba, bb, nthreads=nt)
             reps += 1
             if time.perf_counter() - t0 >= budget:
                 break
@@ -492,8 +508,8 @@ def accuracy_vs_fp64(wl, a, b, an, crop=1024):
     """The GPU's final field on a crop of the pair against the FP64 oracle's (every correlation
     step in f64): RMS and max |d| over cells both mark valid, and the share of equal flags."""
     import piv_b200 as P
-    O, fa, fb, cfg, ch, cw = _oracle_inputs(wl, a, b, crop)
-    ref, _, _ = O.analyze(cfg, fa, fb, mode=O.FP64)
+    O, fa, fb, cfg, ch, cw, ba, bb = _oracle_inputs(wl, a, b, crop)
+    ref, _, _ = O.analyze(cfg, fa, fb, ba, bb, mode=O.FP64)
     pre, bg = preprocess_config(wl), _crop_background(wl, a, b, ch, cw)
     r = an.analyze(an.prepare(np.ascontiguousarray(a[:ch, :cw]), pre, background=bg),
                    an.prepare(np.ascontiguousarray(b[:ch, :cw]), pre, background=bg))
@@ -623,7 +639,7 @@ def main():
     dtype_code = P.api._dtype_code(a0)
     h, w = a0.shape
     # raw u16 samples on the device (held as int16 tensors: same bytes)
-    pairs_dev = [(torch.from_numpy(a.view(np.int16)).to(dev), torch.from_numpy(b.view(np.int16)).to(dev))
+    pairs_dev = [(torch.from_numpy(_torch_view(a)).to(dev), torch.from_numpy(_torch_view(b)).to(dev))
                  for a, b in pairs_host]
 
     an = P.PivAnalyzer(piv_config(wl), device=local)
@@ -706,8 +722,8 @@ def main():
     value = world * args.steps * nvec / (ms_max * 1e-3)
 
     # ---------------------------------------------------------------- timed: end to end (host buffers)
-    pin = [(torch.from_numpy(a.view(np.int16)).pin_memory().numpy().view(np.uint16),
-            torch.from_numpy(b.view(np.int16)).pin_memory().numpy().view(np.uint16)) for a, b in pairs_host[:2]]
+    pin = [(torch.from_numpy(_torch_view(a)).pin_memory().numpy().view(a.dtype),
+            torch.from_numpy(_torch_view(b)).pin_memory().numpy().view(b.dtype)) for a, b in pairs_host[:2]]
     hdx = torch.empty(nvec, dtype=torch.float32).pin_memory().numpy().reshape(g.ny, g.nx)
     hdy = torch.empty(nvec, dtype=torch.float32).pin_memory().numpy().reshape(g.ny, g.nx)
     hppr = torch.empty(nvec, dtype=torch.float32).pin_memory().numpy().reshape(g.ny, g.nx)
@@ -744,7 +760,7 @@ def main():
     # pipelined: the same calls through PivPipeline (depth 3), so one pair's uploads and downloads
     # overlap the others' kernels; host clock with the device synchronised at both ends
     depth = 3
-    pl = P.PivPipeline(an, h, w, dtype=np.uint16, cfg=pre, depth=depth)
+    pl = P.PivPipeline(an, h, w, dtype=a0.dtype, cfg=pre, depth=depth)
     pl.set_background(bg_ptr)  # one background image for the pipelined run (that of the first pair)
     outs = [tuple(torch.empty(nvec, dtype=dt).pin_memory().numpy().reshape(g.ny, g.nx)
                   for dt in (torch.float32, torch.float32, torch.float32, torch.uint8)) for _ in range(depth)]
@@ -806,7 +822,7 @@ def main():
     line = {"metric": METRIC, "value": value, "unit": "vectors/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32" if wl.get("precision", "fp32") == "fp32" else wl["precision"] + "+f32", "data": "synthetic",
-            "config": {"workload": wl["name"], "image": f"{h}x{w} u16 ({wl['bits']}-bit)", "windows": pw,
+            "config": {"workload": wl["name"], "image": f"{h}x{w} {a0.dtype.name} ({wl['bits']}-bit)", "windows": pw,
                        "overlap": wl["overlap"], "final_pass_vectors": nvec, "parallelism": f"replicas x{world}",
                        "l2": f"inputs > L2: {n_ring} shifted copies of the pair in turn, "
                              f"{n_ring * pair_bytes / 2**20:.0f} MiB of samples"
