@@ -62,7 +62,10 @@ WORKLOADS = {
         name="1920x1080 u8 particle pair, the reference's default analysis: blur 1 + local normalisation 4, "
              "96->64->64 px at 50% overlap, FP32 plain",
         h=1080, w=1920, bits=8, windows=[96, 64], overlap=0.5, final_iterations=2, ppp=0.03, dmin=2.0, dmax=4.0,
-        vmax=6.0, shear=0.005, outlier_frac=0.0, seed=12, preprocess="default"),
+        vmax=6.0, shear=0.005, outlier_frac=0.0, seed=12, preprocess="default",
+        # published: PIVKit (Metal, M5 Max) on this shape, about 200 pairs/s pipelined
+        # (docs/phase3-plan.md:479-480,561 of the reference)
+        published_pairs_per_s=200.0),
 }
 
 
@@ -819,11 +822,17 @@ def main():
             "per_pass": per_pass,
             "hbm_peak_gbs": peaks.get("hbm_gbs")}
 
+    vs_baseline = None
+    if wl.get("published_pairs_per_s"):
+        vs_baseline = value / (wl["published_pairs_per_s"] * nvec)
     line = {"metric": METRIC, "value": value, "unit": "vectors/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32" if wl.get("precision", "fp32") == "fp32" else wl["precision"] + "+f32", "data": "synthetic",
+            "vs_baseline": vs_baseline, "dtype": "f32" if wl.get("precision", "fp32") == "fp32" else wl["precision"] + "+f32", "data": "synthetic",
             "config": {"workload": wl["name"], "image": f"{h}x{w} {a0.dtype.name} ({wl['bits']}-bit)", "windows": pw,
                        "overlap": wl["overlap"], "final_pass_vectors": nvec, "parallelism": f"replicas x{world}",
+                       **({"baseline": f"published {wl['published_pairs_per_s']:.0f} pairs/s (reference's Metal port, "
+                                       f"Apple M5 Max) x {nvec} final vectors"}
+                          if wl.get("published_pairs_per_s") else {}),
                        "l2": f"inputs > L2: {n_ring} shifted copies of the pair in turn, "
                              f"{n_ring * pair_bytes / 2**20:.0f} MiB of samples"
                              + (" (+ one background image per pair)" if wl.get("background") else "")},
