@@ -151,12 +151,21 @@ __global__ void convert_f32_kernel(const float* __restrict__ raw, long long n, c
 }
 
 // ------------------------------------------------------------------------------- max |v|
+// One atomic per block (the block's warps reduce through shared memory first); launched with
+// 256 threads.
 __global__ void maxabs_kernel(const float* __restrict__ v, long long n, unsigned int* out) {
+    __shared__ float wmax[8];
     float m = 0.0f;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         m = fmaxf(m, fabsf(v[i]));
     for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));  // non-negative floats order as uints
+    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        m = threadIdx.x < (blockDim.x >> 5) ? wmax[threadIdx.x] : 0.0f;
+        for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (threadIdx.x == 0) atomicMax(out, __float_as_uint(m));  // non-negative floats order as uints
+    }
 }
 
 // ------------------------------------------------------------------------------- integral tables
@@ -266,7 +275,7 @@ __global__ void integral_cols_kernel(int H, int W, long long* sum, long long* su
 }
 
 // ------------------------------------------------------------------------------- blur
-constexpr int BT_X = 32, BT_Y = 16;
+constexpr int BT_X = 32, BT_Y = 32;
 
 __global__ void blur_kernel(const float* __restrict__ src, int H, int W, const BlurKernel k, float* __restrict__ out) {
     extern __shared__ float sm[];
@@ -302,7 +311,8 @@ __global__ void blur_kernel(const float* __restrict__ src, int H, int W, const B
 }
 
 // ------------------------------------------------------------------------------- normalize
-constexpr int NT_X = 32, NT_Y = 8;
+constexpr int NT_X = 32, NT_Y = 32;
+constexpr int NT_RUN = 4;  // output rows per thread in the column pass (256 threads = 32 columns x 8 runs)
 
 __global__ void normalize_kernel(const float* __restrict__ src, int H, int W, int r, float eps,
                                  const unsigned int* maxbits, float* __restrict__ out) {
@@ -338,21 +348,30 @@ __global__ void normalize_kernel(const float* __restrict__ src, int H, int W, in
         h2[i] = b;
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < NT_X * NT_Y; i += blockDim.x) {
-        const int ty = i / NT_X, tx = i % NT_X;
-        const int gx = gx0 + tx, gy = gy0 + ty;
-        if (gx >= W || gy >= H) continue;
+    // Column pass: each thread slides a (2r+1)-row window down NT_RUN output rows of one column
+    // (the sums are exact integers, so sliding gives the same totals as summing afresh).
+    for (int i = threadIdx.x; i < NT_X * (NT_Y / NT_RUN); i += blockDim.x) {
+        const int tx = i % NT_X, ty0 = (i / NT_X) * NT_RUN;
+        const int gx = gx0 + tx;
         long long a = 0, b = 0;
         for (int j = 0; j <= 2 * r; ++j) {
-            a += h1[(ty + j) * NT_X + tx];
-            b += h2[(ty + j) * NT_X + tx];
+            a += h1[(ty0 + j) * NT_X + tx];
+            b += h2[(ty0 + j) * NT_X + tx];
         }
-        const int x0 = max(gx - r, 0), x1 = min(gx + r + 1, W);
-        const int y0 = max(gy - r, 0), y1 = min(gy + r + 1, H);
-        float mean, sd;
-        fix_stats(a, b, fs, (float)((x1 - x0) * (y1 - y0)), &mean, &sd);
-        const float v = src[(size_t)gy * W + gx];
-        out[(size_t)gy * W + gx] = __fdiv_rn(__fsub_rn(v, mean), __fadd_rn(sd, eps));
+        for (int k = 0; k < NT_RUN; ++k) {
+            const int ty = ty0 + k, gy = gy0 + ty;
+            if (k > 0) {
+                a += h1[(ty + 2 * r) * NT_X + tx] - h1[(ty - 1) * NT_X + tx];
+                b += h2[(ty + 2 * r) * NT_X + tx] - h2[(ty - 1) * NT_X + tx];
+            }
+            if (gx >= W || gy >= H) continue;
+            const int x0 = max(gx - r, 0), x1 = min(gx + r + 1, W);
+            const int y0 = max(gy - r, 0), y1 = min(gy + r + 1, H);
+            float mean, sd;
+            fix_stats(a, b, fs, (float)((x1 - x0) * (y1 - y0)), &mean, &sd);
+            const float v = src[(size_t)gy * W + gx];
+            out[(size_t)gy * W + gx] = __fdiv_rn(__fsub_rn(v, mean), __fadd_rn(sd, eps));
+        }
     }
 }
 
