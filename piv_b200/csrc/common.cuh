@@ -143,6 +143,19 @@ __device__ __forceinline__ void fix_stats(long long sum1, long long sum2, const 
     *std_out = dd_to_float(dd_sqrt(var));
 }
 
+// The same statistics in native f64, the reference's own arithmetic (IntegralImage::stats,
+// preprocess.rs:114-125: mean = s/n, var = sq/n - mean^2, both f64, then sqrt and the casts to
+// f32), applied to the exact sums.
+__device__ __forceinline__ void fix_stats_f64(long long sum1, long long sum2, const FixScale& fs, float count,
+                                              float* mean_out, float* std_out) {
+    const double n = (double)count;
+    const double mean = __ddiv_rn(scalbn((double)sum1, -fs.s1), n);
+    const double ex2 = __ddiv_rn(scalbn((double)sum2, -fs.s2), n);
+    const double var = __dsub_rn(ex2, __dmul_rn(mean, mean));
+    *mean_out = __double2float_rn(mean);
+    *std_out = __double2float_rn(var > 0.0 ? __dsqrt_rn(var) : 0.0);
+}
+
 // Rust f32::clamp (NaN passes through).
 __device__ __forceinline__ float rclamp(float x, float lo, float hi) {
     if (x < lo) return lo;

@@ -368,7 +368,7 @@ __global__ void normalize_kernel(const float* __restrict__ src, int H, int W, in
             const int x0 = max(gx - r, 0), x1 = min(gx + r + 1, W);
             const int y0 = max(gy - r, 0), y1 = min(gy + r + 1, H);
             float mean, sd;
-            fix_stats(a, b, fs, (float)((x1 - x0) * (y1 - y0)), &mean, &sd);
+            fix_stats_f64(a, b, fs, (float)((x1 - x0) * (y1 - y0)), &mean, &sd);
             const float v = src[(size_t)gy * W + gx];
             out[(size_t)gy * W + gx] = __fdiv_rn(__fsub_rn(v, mean), __fadd_rn(sd, eps));
         }
