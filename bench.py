@@ -525,8 +525,9 @@ def accuracy_vs_fp64(wl, a, b, an, crop=1024):
 
 
 def run_profile_case(args, wl):
-    """An untimed run for profilers: one pair of the workload, analysed --steps times through the
-    host C ABI with the default launch variants (inputs cached under /tmp between processes)."""
+    """An untimed run for profilers: one pair of the workload, prepared with the workload's
+    preprocessing and analysed --steps times through the host C ABI with the default launch
+    variants (inputs cached under /tmp between processes)."""
     import piv_b200 as P
     w = dict(wl)
     if args.profile_case != "all":
@@ -539,7 +540,8 @@ def run_profile_case(args, wl):
         a, b = make_inputs(wl)
         np.savez(cache, a=a, b=b)
     an = P.PivAnalyzer(piv_config(w), device=0)
-    fa, fb = an.prepare(a, P.RAW), an.prepare(b, P.RAW)
+    pre, bg = preprocess_config(wl), _crop_background(wl, a, b, a.shape[0], a.shape[1])
+    fa, fb = an.prepare(a, pre, background=bg), an.prepare(b, pre, background=bg)
     for _ in range(max(args.steps, 1)):
         r = an.analyze(fa, fb)
     print(json.dumps({"profile_case": w["windows"], "vectors": int(r.field.dx.size), "summary": r.summary.as_dict(),
