@@ -224,6 +224,10 @@ void* piv_batch_stream(PivBatch* batch);
  * The stream must stay valid while the batch runs on it; piv_batch_destroy itself needs no
  * stream (it waits for the device). */
 int32_t piv_batch_set_stream(PivBatch* batch, void* stream);
+/* Background image (DEVICE, height*width f32) subtracted from every frame of the batch, as
+ * piv_frame_prepare's `background` (preprocess.rs:138-145); NULL = none. The next run records
+ * the batch's graph again. The image must stay valid while the batch uses it. */
+int32_t piv_batch_set_background(PivBatch* batch, const float* background_dev);
 int32_t piv_batch_sync(PivBatch* batch);
 /* Device output slabs: dx, dy, peak ratio (f32) and flags (u8), pairs*nx*ny each; 8 uint64
  * summary counters per pair; nx*ny is piv_output_grid's. */

@@ -26,7 +26,7 @@ EXPORTS = [
     "piv_batch_create", "piv_batch_destroy", "piv_batch_input_device", "piv_batch_input_bytes", "piv_batch_run",
     "piv_batch_sync", "piv_batch_outputs_device", "piv_batch_run_host", "piv_batch_kernels", "piv_batch_stream",
     "piv_batch_submit_host", "piv_batch_wait_host", "piv_batch_set_stream", "piv_pipeline_set_background",
-    "piv_tc_wait_probe",
+    "piv_tc_wait_probe", "piv_batch_set_background",
     "piv_pipeline_create", "piv_pipeline_destroy", "piv_pipeline_submit", "piv_pipeline_wait",
     "piv_place_windows", "piv_correlate_origins", "piv_place_windows_deform", "piv_correlate_deform",
     "piv_validate_field", "piv_flow_stats_device", "piv_temporal_smooth_device", "piv_spatial_smooth_device",
@@ -157,6 +157,7 @@ def load():
         "piv_batch_kernels": ([vp], i64),
         "piv_batch_stream": ([vp], vp),
         "piv_batch_set_stream": ([vp, vp], i32),
+        "piv_batch_set_background": ([vp, vp], i32),
         "piv_place_windows": ([vp, i64, i64, P(PivGridC), P(PivGridC), vp, vp, vp], i32),
         "piv_correlate_origins": ([vp, vp, vp, i64, vp, i64, vp, vp, vp, vp], i32),
         "piv_place_windows_deform": ([vp, i64, i64, P(PivGridC), P(PivGridC), vp, vp, vp, vp], i32),

@@ -552,6 +552,11 @@ class PivBatch:
         """The batch's CUDA stream handle (for torch.cuda.ExternalStream)."""
         return int(_lib.load().piv_batch_stream(self._h))
 
+    def set_background(self, background_ptr: Optional[int]):
+        """Device background image (height*width f32) subtracted from every frame of the batch;
+        None for none. It must stay alive while the batch uses it."""
+        _check(_lib.load().piv_batch_set_background(self._h, ctypes.c_void_p(background_ptr) if background_ptr else None))
+
     def set_stream(self, stream):
         """Run this batch's kernels on `stream` (a cudaStream_t handle; None: its own stream).
         Batches sharing a stream replay one after another while their host copies overlap."""

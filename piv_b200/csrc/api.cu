@@ -173,6 +173,7 @@ struct PivBatch {
     PivPreprocessC pre{};
     size_t frame_bytes = 0;
     void* raw = nullptr;
+    const float* background = nullptr;  // device image subtracted from every frame (caller-owned)
     std::vector<PivFrame*> frames;
     int64_t cells = 0;
     void* out = nullptr;
@@ -1316,7 +1317,7 @@ int batch_record(PivBatch* bt) {
     const int nf = (int)bt->frames.size();
     for (int i = 0; i < nf; ++i) {
         int st = prepare_common(an, bt->frames[i], (const char*)bt->raw + (size_t)i * bt->frame_bytes, bt->dtype, &bt->pre,
-                                nullptr);
+                                bt->background);
         if (st) return st;
     }
     std::vector<const PivFrame*> fa(bt->K), fb(bt->K);
@@ -1654,6 +1655,20 @@ int32_t piv_batch_run(PivBatch* bt) {
 }
 
 void* piv_batch_stream(PivBatch* bt) { return bt ? (void*)bt->an->cur : nullptr; }
+
+int32_t piv_batch_set_background(PivBatch* bt, const float* background_dev) {
+    if (!bt) return fail(PIV_ERR_ARGUMENT, "null batch");
+    if (bt->pending) return fail(PIV_ERR_ARGUMENT, "the batch has a submission that has not been collected");
+    if (background_dev == bt->background) return PIV_OK;
+    CUDA_TRY(cudaSetDevice(bt->an->device));
+    CUDA_TRY(cudaDeviceSynchronize());  // a replay may still read the old pointer
+    if (bt->exec) cudaGraphExecDestroy(bt->exec);
+    if (bt->graph) cudaGraphDestroy(bt->graph);
+    bt->exec = nullptr;  // the next run records the batch again with the new image
+    bt->graph = nullptr;
+    bt->background = background_dev;
+    return PIV_OK;
+}
 
 int32_t piv_batch_set_stream(PivBatch* bt, void* stream) {
     if (!bt) return fail(PIV_ERR_ARGUMENT, "null batch");
