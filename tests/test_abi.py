@@ -76,3 +76,24 @@ def test_rejects_bad_config():
     with pytest.raises(P.UnsupportedError):
         P.PivAnalyzer.check_config(P.PivConfig(windows=[40]))
     P.PivAnalyzer.check_config(P.PivConfig())
+
+
+def test_header_is_plain_c():
+    """The boundary is a C ABI: the header compiles as strict C99 (and as C++) with no warnings."""
+    import os
+    import shutil
+    import subprocess
+    import tempfile
+    cc = shutil.which("gcc")
+    if cc is None:
+        import pytest
+        pytest.skip("no C compiler")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    with tempfile.TemporaryDirectory() as d:
+        src = os.path.join(d, "h.c")
+        with open(src, "w") as f:
+            f.write('#include "piv_b200.h"\nint main(void) { return PIV_OK; }\n')
+        for cmd in ([cc, "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-fsyntax-only"],
+                    [shutil.which("g++") or "g++", "-std=c++17", "-Wall", "-Werror", "-fsyntax-only", "-x", "c++"]):
+            r = subprocess.run(cmd + ["-I", os.path.join(root, "include"), src], capture_output=True, text=True)
+            assert r.returncode == 0, r.stderr
