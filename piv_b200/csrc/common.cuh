@@ -107,11 +107,23 @@ __device__ __forceinline__ float dd_to_float(dfloat x) { return __fadd_rn(x.hi, 
 // ---------------------------------------------------------------------------------------------
 struct FixScale {
     int s1, s2;
+    // 2^s1 and 2^s2 as floats when 0 <= s <= 127: multiplying a finite float by 2^s with s >= 0
+    // is exact up to overflow, where it rounds to +-inf as scalbnf does, so the product equals
+    // scalbnf(v, s) bit for bit. Outside that range the quantisers fall back to scalbnf.
+    float m1, m2;
+    bool fast1, fast2;
+    // 2^-s1 and 2^-s2 as doubles (s1 lies in [-128, 210], s2 in [-256, 358], so both are normal
+    // doubles, and an int64 sum times either stays normal): the product is exact and equals
+    // scalbn(sum, -s).
+    double d1, d2;
 };
+
+__device__ __forceinline__ float pow2f(int s) { return __int_as_float((s + 127) << 23); }
+__device__ __forceinline__ double pow2d(int s) { return __longlong_as_double((long long)(s + 1023) << 52); }
 
 // Largest exponent e with 2^e >= maxabs, then scales that keep count * 2^(e+s) <= 2^62.
 __device__ __forceinline__ FixScale fix_scale(float maxabs, long long count) {
-    FixScale fs{0, 0};
+    FixScale fs{0, 0, 1.0f, 1.0f, true, true, 1.0, 1.0};
     if (!(maxabs > 0.0f) || !isfinite(maxabs)) return fs;
     int e;
     float m = frexpf(maxabs, &e);  // maxabs = m * 2^e, m in [0.5, 1)
@@ -120,15 +132,22 @@ __device__ __forceinline__ FixScale fix_scale(float maxabs, long long count) {
     while ((1ll << lc) < count && lc < 62) ++lc;
     fs.s1 = 62 - lc - e;
     fs.s2 = 62 - lc - 2 * e;
+    fs.fast1 = fs.s1 >= 0 && fs.s1 <= 127;
+    fs.fast2 = fs.s2 >= 0 && fs.s2 <= 127;
+    fs.m1 = fs.fast1 ? pow2f(fs.s1) : 1.0f;
+    fs.m2 = fs.fast2 ? pow2f(fs.s2) : 1.0f;
+    fs.d1 = pow2d(-fs.s1);
+    fs.d2 = pow2d(-fs.s2);
     return fs;
 }
 
 __device__ __forceinline__ long long fix_q1(float v, const FixScale& fs) {
-    return __float2ll_rn(scalbnf(v, fs.s1));
+    return __float2ll_rn(fs.fast1 ? __fmul_rn(v, fs.m1) : scalbnf(v, fs.s1));
 }
 
 __device__ __forceinline__ long long fix_q2(float v, const FixScale& fs) {
     dfloat sq = dd_two_prod(v, v);
+    if (fs.fast2) return __float2ll_rn(__fmul_rn(sq.hi, fs.m2)) + __float2ll_rn(__fmul_rn(sq.lo, fs.m2));
     return __float2ll_rn(scalbnf(sq.hi, fs.s2)) + __float2ll_rn(scalbnf(sq.lo, fs.s2));
 }
 
@@ -149,8 +168,8 @@ __device__ __forceinline__ void fix_stats(long long sum1, long long sum2, const 
 __device__ __forceinline__ void fix_stats_f64(long long sum1, long long sum2, const FixScale& fs, float count,
                                               float* mean_out, float* std_out) {
     const double n = (double)count;
-    const double mean = __ddiv_rn(scalbn((double)sum1, -fs.s1), n);
-    const double ex2 = __ddiv_rn(scalbn((double)sum2, -fs.s2), n);
+    const double mean = __ddiv_rn(__dmul_rn((double)sum1, fs.d1), n);
+    const double ex2 = __ddiv_rn(__dmul_rn((double)sum2, fs.d2), n);
     const double var = __dsub_rn(ex2, __dmul_rn(mean, mean));
     *mean_out = __double2float_rn(mean);
     *std_out = __double2float_rn(var > 0.0 ? __dsqrt_rn(var) : 0.0);

@@ -324,8 +324,11 @@ __global__ void normalize_kernel(const float* __restrict__ src, int H, int W, in
     long long* h2 = h1 + TH * NT_X;      // TH x NT_X
     const FixScale fs = fix_scale(__uint_as_float(*maxbits), (long long)(2 * r + 1) * (2 * r + 1));
     const int gx0 = blockIdx.x * NT_X, gy0 = blockIdx.y * NT_Y;
+    // i / TW as a multiply-high by ceil(2^32 / TW): exact while i * TW < 2^32, which the tile's
+    // shared-memory size guarantees by far.
+    const unsigned int tw_magic = 0xffffffffu / (unsigned int)TW + 1u;
     for (int i = threadIdx.x; i < TH * TW; i += blockDim.x) {
-        const int ty = i / TW, tx = i % TW;
+        const int ty = (int)__umulhi((unsigned int)i, tw_magic), tx = i - ty * TW;
         const int gy = gy0 + ty - r, gx = gx0 + tx - r;
         long long a = 0, b = 0;
         if (gy >= 0 && gy < H && gx >= 0 && gx < W) {
@@ -339,13 +342,23 @@ __global__ void normalize_kernel(const float* __restrict__ src, int H, int W, in
     __syncthreads();
     for (int i = threadIdx.x; i < TH * NT_X; i += blockDim.x) {
         const int ty = i / NT_X, tx = i % NT_X;
-        long long a = 0, b = 0;
-        for (int j = 0; j <= 2 * r; ++j) {
-            a += q1[ty * TW + tx + j];
-            b += q2[ty * TW + tx + j];
+        const long long* p1 = q1 + ty * TW + tx;
+        const long long* p2 = q2 + ty * TW + tx;
+        // Two accumulators per table shorten the add chains; integer sums are exact in any order.
+        long long a0 = p1[0], b0 = p2[0], a1 = 0, b1 = 0;
+        int j = 1;
+        for (; j + 1 <= 2 * r; j += 2) {
+            a0 += p1[j];
+            a1 += p1[j + 1];
+            b0 += p2[j];
+            b1 += p2[j + 1];
         }
-        h1[i] = a;
-        h2[i] = b;
+        if (j <= 2 * r) {
+            a0 += p1[j];
+            b0 += p2[j];
+        }
+        h1[i] = a0 + a1;
+        h2[i] = b0 + b1;
     }
     __syncthreads();
     // Column pass: each thread slides a (2r+1)-row window down NT_RUN output rows of one column
