@@ -97,22 +97,53 @@ __device__ __forceinline__ float div_code(float x, float d, float r) {
     return __fmaf_rn(__fmaf_rn(-q0, d, x), r, q0);
 }
 
+// The background-subtracted intensity of one sample (preprocess.rs:144-151): an integer code
+// clipped to the percentile code, divided as above, then the background subtracted and clamped
+// at zero. `begin()` reads the clip code on the device once per thread.
+template <typename CodeT>
+struct CodeSamples {
+    const CodeT* raw;
+    const float* bg;  // nullable
+    const unsigned int* clip;  // nullable; clip[2] is the clip code
+    unsigned int cl;
+    float d, r;
+    __device__ __forceinline__ void begin() {
+        cl = clip ? clip[2] : 0xffffffffu;
+        d = CodeDivisor<CodeT>::d;
+        r = __frcp_rn(d);
+    }
+    __device__ __forceinline__ float value(unsigned int c, float b) const {
+        if (c > cl) c = cl;
+        float v = div_code((float)c, d, r);
+        if (bg) v = fmaxf(__fsub_rn(v, b), 0.0f);
+        return v;
+    }
+    __device__ __forceinline__ float operator()(size_t i) const { return value(raw[i], bg ? bg[i] : 0.0f); }
+};
+
+// f32 samples, background-subtracted and clamped at zero when a background is given.
+struct FloatSamples {
+    const float* raw;
+    const float* bg;  // nullable
+    __device__ __forceinline__ void begin() {}
+    __device__ __forceinline__ float operator()(size_t i) const {
+        float v = raw[i];
+        if (bg) v = fmaxf(__fsub_rn(v, bg[i]), 0.0f);
+        return v;
+    }
+};
+
 // Streams codes 16 bytes per load (8 u16 or 16 u8) when the buffers are 16-byte aligned; the
 // rest of the frame (or an unaligned one) one code at a time.
 template <typename CodeT>
 __global__ void convert_kernel(const CodeT* __restrict__ raw, long long n, const float* __restrict__ bg,
                                const unsigned int* clip, float* __restrict__ out) {
     constexpr int V = 16 / (int)sizeof(CodeT);
-    const unsigned int cl = clip ? clip[2] : 0xffffffffu;
-    const float d = CodeDivisor<CodeT>::d, r = __frcp_rn(d);
+    CodeSamples<CodeT> src{raw, bg, clip, 0u, 0.0f, 0.0f};
+    src.begin();
     const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long stride = (long long)gridDim.x * blockDim.x;
-    auto value = [&](unsigned int c, float b) {
-        if (c > cl) c = cl;
-        float v = div_code((float)c, d, r);
-        if (bg) v = fmaxf(__fsub_rn(v, b), 0.0f);
-        return v;
-    };
+    auto value = [&](unsigned int c, float b) { return src.value(c, b); };
     long long head = 0;
     const bool aligned = (reinterpret_cast<uintptr_t>(raw) | reinterpret_cast<uintptr_t>(out) |
                           reinterpret_cast<uintptr_t>(bg)) % 16 == 0;
@@ -143,21 +174,18 @@ __global__ void convert_kernel(const CodeT* __restrict__ raw, long long n, const
 
 __global__ void convert_f32_kernel(const float* __restrict__ raw, long long n, const float* __restrict__ bg,
                                    float* __restrict__ out) {
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        float v = raw[i];
-        if (bg) v = fmaxf(__fsub_rn(v, bg[i]), 0.0f);
-        out[i] = v;
-    }
+    const FloatSamples src{raw, bg};
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] = src((size_t)i);
 }
 
 // ------------------------------------------------------------------------------- max |v|
 // One atomic per block (the block's warps reduce through shared memory first); launched with
 // 256 threads.
-__global__ void maxabs_kernel(const float* __restrict__ v, long long n, unsigned int* out) {
+// Folds each thread's running max |v| into *out: one atomic per block of <= 256 threads. Every
+// thread of the block calls it.
+__device__ __forceinline__ void block_max_to(float m, unsigned int* out) {
     __shared__ float wmax[8];
-    float m = 0.0f;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        m = fmaxf(m, fabsf(v[i]));
     for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
     if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = m;
     __syncthreads();
@@ -166,6 +194,13 @@ __global__ void maxabs_kernel(const float* __restrict__ v, long long n, unsigned
         for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
         if (threadIdx.x == 0) atomicMax(out, __float_as_uint(m));  // non-negative floats order as uints
     }
+}
+
+__global__ void maxabs_kernel(const float* __restrict__ v, long long n, unsigned int* out) {
+    float m = 0.0f;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        m = fmaxf(m, fabsf(v[i]));
+    block_max_to(m, out);
 }
 
 // ------------------------------------------------------------------------------- integral tables
@@ -277,8 +312,16 @@ __global__ void integral_cols_kernel(int H, int W, long long* sum, long long* su
 // ------------------------------------------------------------------------------- blur
 constexpr int BT_X = 32, BT_Y = 32;
 
-__global__ void blur_kernel(const float* __restrict__ src, int H, int W, const BlurKernel k, float* __restrict__ out) {
+// The tile load reads samples through `Src`: the previous stage's f32 image, or (when nothing
+// else needs the background-subtracted image) the raw frame decoded on the fly, which saves the
+// conversion kernel and its H x W f32 round trip. With a non-null `maxout` the kernel also folds
+// max |output| into *maxout for the local normalisation's fixed-point scale (launched with 256
+// threads).
+template <typename Src>
+__global__ void blur_kernel(Src src, int H, int W, const BlurKernel k, float* __restrict__ out,
+                            unsigned int* maxout) {
     extern __shared__ float sm[];
+    src.begin();
     const int R = k.radius;
     const int TW = BT_X + 2 * R, TH = BT_Y + 2 * R;
     float* tin = sm;             // TH x TW
@@ -288,7 +331,7 @@ __global__ void blur_kernel(const float* __restrict__ src, int H, int W, const B
         const int ty = i / TW, tx = i % TW;
         const int gy = min(max(gy0 + ty - R, 0), H - 1);
         const int gx = min(max(gx0 + tx - R, 0), W - 1);
-        tin[i] = src[(size_t)gy * W + gx];
+        tin[i] = src((size_t)gy * W + gx);
     }
     __syncthreads();
     // Row pass over every tile row (vertical halo included): sum in kernel order from -0.0.
@@ -300,6 +343,7 @@ __global__ void blur_kernel(const float* __restrict__ src, int H, int W, const B
     }
     __syncthreads();
     // Column pass: out starts at 0.0 and accumulates kernel terms in order (preprocess.rs:186-193).
+    float m = 0.0f;
     for (int i = threadIdx.x; i < BT_X * BT_Y; i += blockDim.x) {
         const int ty = i / BT_X, tx = i % BT_X;
         const int gx = gx0 + tx, gy = gy0 + ty;
@@ -307,7 +351,9 @@ __global__ void blur_kernel(const float* __restrict__ src, int H, int W, const B
         float o = 0.0f;
         for (int j = 0; j <= 2 * R; ++j) o = __fadd_rn(o, __fmul_rn(k.w[j], trow[(ty + j) * BT_X + tx]));
         out[(size_t)gy * W + gx] = o;
+        m = fmaxf(m, fabsf(o));
     }
+    if (maxout) block_max_to(m, maxout);
 }
 
 // ------------------------------------------------------------------------------- normalize
@@ -389,6 +435,17 @@ __global__ void normalize_kernel(const float* __restrict__ src, int H, int W, in
 }
 
 // ------------------------------------------------------------------------------- drivers
+// Opts the blur instantiation that will run (raw_type -1: the f32 image of an earlier stage)
+// into more than 48 KB of dynamic shared memory when its tile needs it.
+static cudaError_t set_blur_smem(size_t sm, int raw_type) {
+    if (sm <= 48 * 1024) return cudaSuccess;
+    const int v = (int)sm;
+    const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    if (raw_type == RAW_U8) return cudaFuncSetAttribute(blur_kernel<CodeSamples<uint8_t>>, a, v);
+    if (raw_type == RAW_U16) return cudaFuncSetAttribute(blur_kernel<CodeSamples<uint16_t>>, a, v);
+    return cudaFuncSetAttribute(blur_kernel<FloatSamples>, a, v);
+}
+
 static int grid_for(long long n) {
     long long b = (n + 255) / 256;
     if (b > 148 * 16) b = 148 * 16;
@@ -453,9 +510,11 @@ cudaError_t launch_prepare(const PrepParams& p, cudaStream_t s, int* launches) {
     }
     const bool blur = p.smooth_sigma > 0.0f;
     const bool norm = p.normalize_radius > 0;
-    // base goes straight to `image` when no further stage follows.
+    // base goes straight to `image` when no further stage follows. When the blur follows and no
+    // integral tables are wanted, the blur decodes the raw samples itself and base is not written.
     float* base = p.base;
-    switch (p.raw_type) {
+    const bool fused = blur && !p.build_stats;
+    if (!fused) switch (p.raw_type) {
         case RAW_U8:
             convert_kernel<uint8_t><<<grid_for(n), 256, 0, s>>>((const uint8_t*)p.raw, n, p.background, clip, base);
             break;
@@ -466,7 +525,7 @@ cudaError_t launch_prepare(const PrepParams& p, cudaStream_t s, int* launches) {
             convert_f32_kernel<<<grid_for(n), 256, 0, s>>>((const float*)p.raw, n, p.background, base);
             break;
     }
-    nl += 1;
+    if (!fused) nl += 1;
     if (p.build_stats) {
         e = launch_stats(base, p.H, p.W, p.sum, p.sumsq, p.scales, p.maxbits, s, &nl);
         if (e != cudaSuccess) return e;
@@ -477,22 +536,38 @@ cudaError_t launch_prepare(const PrepParams& p, cudaStream_t s, int* launches) {
         if (k.radius > (kMaxBlurTaps - 1) / 2) return cudaErrorInvalidValue;
         const int R = k.radius;
         const size_t sm = sizeof(float) * ((size_t)(BT_Y + 2 * R) * (BT_X + 2 * R) + (size_t)(BT_Y + 2 * R) * BT_X);
-        if (sm > 48 * 1024) {
-            e = cudaFuncSetAttribute(blur_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        float* dst = norm ? p.tmp : p.image;
+        unsigned int* mx = norm ? p.maxbits + 1 : nullptr;
+        if (norm) {
+            e = cudaMemsetAsync(mx, 0, sizeof(unsigned int), s);
             if (e != cudaSuccess) return e;
         }
-        float* dst = norm ? p.tmp : p.image;
         dim3 grid((p.W + BT_X - 1) / BT_X, (p.H + BT_Y - 1) / BT_Y);
-        blur_kernel<<<grid, 256, sm, s>>>(cur, p.H, p.W, k, dst);
+        e = set_blur_smem(sm, fused ? p.raw_type : -1);
+        if (e != cudaSuccess) return e;
+        if (!fused) {
+            blur_kernel<<<grid, 256, sm, s>>>(FloatSamples{cur, nullptr}, p.H, p.W, k, dst, mx);
+        } else if (p.raw_type == RAW_U8) {
+            blur_kernel<<<grid, 256, sm, s>>>(CodeSamples<uint8_t>{(const uint8_t*)p.raw, p.background, clip, 0u, 0.0f, 0.0f},
+                                              p.H, p.W, k, dst, mx);
+        } else if (p.raw_type == RAW_U16) {
+            blur_kernel<<<grid, 256, sm, s>>>(CodeSamples<uint16_t>{(const uint16_t*)p.raw, p.background, clip, 0u, 0.0f, 0.0f},
+                                              p.H, p.W, k, dst, mx);
+        } else {
+            blur_kernel<<<grid, 256, sm, s>>>(FloatSamples{(const float*)p.raw, p.background}, p.H, p.W, k, dst, mx);
+        }
         nl += 1;
         cur = dst;
     }
     if (norm) {
         const int r = p.normalize_radius;
         if (r > kMaxNormRadius) return cudaErrorInvalidValue;
-        e = cudaMemsetAsync(p.maxbits + 1, 0, sizeof(unsigned int), s);
-        if (e != cudaSuccess) return e;
-        maxabs_kernel<<<grid_for(n), 256, 0, s>>>(cur, n, p.maxbits + 1);
+        if (!blur) {
+            e = cudaMemsetAsync(p.maxbits + 1, 0, sizeof(unsigned int), s);
+            if (e != cudaSuccess) return e;
+            maxabs_kernel<<<grid_for(n), 256, 0, s>>>(cur, n, p.maxbits + 1);
+            nl += 1;
+        }
         const size_t sm = sizeof(long long) * (2 * (size_t)(NT_Y + 2 * r) * (NT_X + 2 * r) + 2 * (size_t)(NT_Y + 2 * r) * NT_X);
         if (sm > 48 * 1024) {
             e = cudaFuncSetAttribute(normalize_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -500,7 +575,7 @@ cudaError_t launch_prepare(const PrepParams& p, cudaStream_t s, int* launches) {
         }
         dim3 grid((p.W + NT_X - 1) / NT_X, (p.H + NT_Y - 1) / NT_Y);
         normalize_kernel<<<grid, 256, sm, s>>>(cur, p.H, p.W, r, p.normalize_eps, p.maxbits + 1, p.image);
-        nl += 2;
+        nl += 1;
         cur = p.image;
     }
     if (cur != p.image) {
