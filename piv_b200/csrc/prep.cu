@@ -317,18 +317,22 @@ constexpr int BT_X = 32, BT_Y = 32;
 // conversion kernel and its H x W f32 round trip. With a non-null `maxout` the kernel also folds
 // max |output| into *maxout for the local normalisation's fixed-point scale (launched with 256
 // threads).
-template <typename Src>
+// RC > 0 fixes the radius at compile time (the taps unroll; the summation order is unchanged);
+// RC = 0 takes it from k.
+template <typename Src, int RC>
 __global__ void blur_kernel(Src src, int H, int W, const BlurKernel k, float* __restrict__ out,
                             unsigned int* maxout) {
     extern __shared__ float sm[];
     src.begin();
-    const int R = k.radius;
+    const int R = RC > 0 ? RC : k.radius;
     const int TW = BT_X + 2 * R, TH = BT_Y + 2 * R;
     float* tin = sm;             // TH x TW
     float* trow = sm + TH * TW;  // TH x BT_X
     const int gx0 = blockIdx.x * BT_X, gy0 = blockIdx.y * BT_Y;
+    // i / TW as a multiply-high by ceil(2^32 / TW), exact for i * TW < 2^32.
+    const unsigned int tw_magic = 0xffffffffu / (unsigned int)TW + 1u;
     for (int i = threadIdx.x; i < TH * TW; i += blockDim.x) {
-        const int ty = i / TW, tx = i % TW;
+        const int ty = (int)__umulhi((unsigned int)i, tw_magic), tx = i - ty * TW;
         const int gy = min(max(gy0 + ty - R, 0), H - 1);
         const int gx = min(max(gx0 + tx - R, 0), W - 1);
         tin[i] = src((size_t)gy * W + gx);
@@ -338,6 +342,7 @@ __global__ void blur_kernel(Src src, int H, int W, const BlurKernel k, float* __
     for (int i = threadIdx.x; i < TH * BT_X; i += blockDim.x) {
         const int ty = i / BT_X, tx = i % BT_X;
         float s = -0.0f;
+#pragma unroll
         for (int j = 0; j <= 2 * R; ++j) s = __fadd_rn(s, __fmul_rn(k.w[j], tin[ty * TW + tx + j]));
         trow[i] = s;
     }
@@ -349,6 +354,7 @@ __global__ void blur_kernel(Src src, int H, int W, const BlurKernel k, float* __
         const int gx = gx0 + tx, gy = gy0 + ty;
         if (gx >= W || gy >= H) continue;
         float o = 0.0f;
+#pragma unroll
         for (int j = 0; j <= 2 * R; ++j) o = __fadd_rn(o, __fmul_rn(k.w[j], trow[(ty + j) * BT_X + tx]));
         out[(size_t)gy * W + gx] = o;
         m = fmaxf(m, fabsf(o));
@@ -360,9 +366,12 @@ __global__ void blur_kernel(Src src, int H, int W, const BlurKernel k, float* __
 constexpr int NT_X = 32, NT_Y = 32;
 constexpr int NT_RUN = 4;  // output rows per thread in the column pass (256 threads = 32 columns x 8 runs)
 
-__global__ void normalize_kernel(const float* __restrict__ src, int H, int W, int r, float eps,
+// RC > 0 fixes the radius at compile time; RC = 0 takes it from r_arg.
+template <int RC>
+__global__ void normalize_kernel(const float* __restrict__ src, int H, int W, int r_arg, float eps,
                                  const unsigned int* maxbits, float* __restrict__ out) {
     extern __shared__ long long smq[];
+    const int r = RC > 0 ? RC : r_arg;
     const int TW = NT_X + 2 * r, TH = NT_Y + 2 * r;
     long long* q1 = smq;                 // TH x TW
     long long* q2 = q1 + TH * TW;        // TH x TW
@@ -393,6 +402,7 @@ __global__ void normalize_kernel(const float* __restrict__ src, int H, int W, in
         // Two accumulators per table shorten the add chains; integer sums are exact in any order.
         long long a0 = p1[0], b0 = p2[0], a1 = 0, b1 = 0;
         int j = 1;
+#pragma unroll
         for (; j + 1 <= 2 * r; j += 2) {
             a0 += p1[j];
             a1 += p1[j + 1];
@@ -413,6 +423,7 @@ __global__ void normalize_kernel(const float* __restrict__ src, int H, int W, in
         const int tx = i % NT_X, ty0 = (i / NT_X) * NT_RUN;
         const int gx = gx0 + tx;
         long long a = 0, b = 0;
+#pragma unroll
         for (int j = 0; j <= 2 * r; ++j) {
             a += h1[(ty0 + j) * NT_X + tx];
             b += h2[(ty0 + j) * NT_X + tx];
@@ -435,15 +446,22 @@ __global__ void normalize_kernel(const float* __restrict__ src, int H, int W, in
 }
 
 // ------------------------------------------------------------------------------- drivers
-// Opts the blur instantiation that will run (raw_type -1: the f32 image of an earlier stage)
-// into more than 48 KB of dynamic shared memory when its tile needs it.
-static cudaError_t set_blur_smem(size_t sm, int raw_type) {
-    if (sm <= 48 * 1024) return cudaSuccess;
-    const int v = (int)sm;
-    const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
-    if (raw_type == RAW_U8) return cudaFuncSetAttribute(blur_kernel<CodeSamples<uint8_t>>, a, v);
-    if (raw_type == RAW_U16) return cudaFuncSetAttribute(blur_kernel<CodeSamples<uint16_t>>, a, v);
-    return cudaFuncSetAttribute(blur_kernel<FloatSamples>, a, v);
+// Launches the blur through sample source `src`: the radius-3 instantiation (sigma 1, the
+// default) or the general one, which is opted into more than 48 KB of dynamic shared memory when
+// its tile needs it.
+template <typename Src>
+static cudaError_t run_blur(dim3 grid, size_t sm, cudaStream_t s, const Src& src, int H, int W, const BlurKernel& k,
+                            float* dst, unsigned int* mx) {
+    if (k.radius == 3) {
+        blur_kernel<Src, 3><<<grid, 256, sm, s>>>(src, H, W, k, dst, mx);
+        return cudaSuccess;
+    }
+    if (sm > 48 * 1024) {
+        const cudaError_t e = cudaFuncSetAttribute(blur_kernel<Src, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e != cudaSuccess) return e;
+    }
+    blur_kernel<Src, 0><<<grid, 256, sm, s>>>(src, H, W, k, dst, mx);
+    return cudaSuccess;
 }
 
 static int grid_for(long long n) {
@@ -543,19 +561,18 @@ cudaError_t launch_prepare(const PrepParams& p, cudaStream_t s, int* launches) {
             if (e != cudaSuccess) return e;
         }
         dim3 grid((p.W + BT_X - 1) / BT_X, (p.H + BT_Y - 1) / BT_Y);
-        e = set_blur_smem(sm, fused ? p.raw_type : -1);
-        if (e != cudaSuccess) return e;
         if (!fused) {
-            blur_kernel<<<grid, 256, sm, s>>>(FloatSamples{cur, nullptr}, p.H, p.W, k, dst, mx);
+            e = run_blur(grid, sm, s, FloatSamples{cur, nullptr}, p.H, p.W, k, dst, mx);
         } else if (p.raw_type == RAW_U8) {
-            blur_kernel<<<grid, 256, sm, s>>>(CodeSamples<uint8_t>{(const uint8_t*)p.raw, p.background, clip, 0u, 0.0f, 0.0f},
-                                              p.H, p.W, k, dst, mx);
+            e = run_blur(grid, sm, s, CodeSamples<uint8_t>{(const uint8_t*)p.raw, p.background, clip, 0u, 0.0f, 0.0f},
+                         p.H, p.W, k, dst, mx);
         } else if (p.raw_type == RAW_U16) {
-            blur_kernel<<<grid, 256, sm, s>>>(CodeSamples<uint16_t>{(const uint16_t*)p.raw, p.background, clip, 0u, 0.0f, 0.0f},
-                                              p.H, p.W, k, dst, mx);
+            e = run_blur(grid, sm, s, CodeSamples<uint16_t>{(const uint16_t*)p.raw, p.background, clip, 0u, 0.0f, 0.0f},
+                         p.H, p.W, k, dst, mx);
         } else {
-            blur_kernel<<<grid, 256, sm, s>>>(FloatSamples{(const float*)p.raw, p.background}, p.H, p.W, k, dst, mx);
+            e = run_blur(grid, sm, s, FloatSamples{(const float*)p.raw, p.background}, p.H, p.W, k, dst, mx);
         }
+        if (e != cudaSuccess) return e;
         nl += 1;
         cur = dst;
     }
@@ -569,12 +586,16 @@ cudaError_t launch_prepare(const PrepParams& p, cudaStream_t s, int* launches) {
             nl += 1;
         }
         const size_t sm = sizeof(long long) * (2 * (size_t)(NT_Y + 2 * r) * (NT_X + 2 * r) + 2 * (size_t)(NT_Y + 2 * r) * NT_X);
-        if (sm > 48 * 1024) {
-            e = cudaFuncSetAttribute(normalize_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-            if (e != cudaSuccess) return e;
-        }
         dim3 grid((p.W + NT_X - 1) / NT_X, (p.H + NT_Y - 1) / NT_Y);
-        normalize_kernel<<<grid, 256, sm, s>>>(cur, p.H, p.W, r, p.normalize_eps, p.maxbits + 1, p.image);
+        if (r == 4) {  // the default radius: 46 KB of tile, under the 48 KB default
+            normalize_kernel<4><<<grid, 256, sm, s>>>(cur, p.H, p.W, r, p.normalize_eps, p.maxbits + 1, p.image);
+        } else {
+            if (sm > 48 * 1024) {
+                e = cudaFuncSetAttribute(normalize_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+                if (e != cudaSuccess) return e;
+            }
+            normalize_kernel<0><<<grid, 256, sm, s>>>(cur, p.H, p.W, r, p.normalize_eps, p.maxbits + 1, p.image);
+        }
         nl += 1;
         cur = p.image;
     }
