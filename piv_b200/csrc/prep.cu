@@ -10,8 +10,9 @@
 //
 // The blur repeats the reference's f32 operations in order (no FMA), so it is bit-exact given
 // the same kernel weights. The normalization's box statistics are exact integer sums turned into
-// f32 mean/std through double-float arithmetic (see common.cuh), matching the reference's f64
-// integral image to within a rounding-boundary case.
+// f32 mean/std by the reference's own f64 arithmetic (fix_stats_f64 in common.cuh). These sums
+// are exact where the reference's f64 integral image can round, so a result can differ from the
+// reference's in a rounding-boundary case.
 //
 // Percentile clip (an addition, parity unpinned against the reference, pinned against the
 // oracle): the clip code is the smallest code c with #(codes <= c) >= ceil(p/100 * H*W); codes
@@ -365,6 +366,8 @@ __global__ void blur_kernel(Src src, int H, int W, const BlurKernel k, float* __
 // ------------------------------------------------------------------------------- normalize
 constexpr int NT_X = 32, NT_Y = 32;
 constexpr int NT_RUN = 4;  // output rows per thread in the column pass (256 threads = 32 columns x 8 runs)
+constexpr int NT_XRUN = 4;  // outputs per thread in the row pass
+constexpr int NT_HW = NT_X + 1;  // row stride of the row-pass sums (odd, in 8-byte words)
 
 // RC > 0 fixes the radius at compile time; RC = 0 takes it from r_arg.
 template <int RC>
@@ -373,10 +376,13 @@ __global__ void normalize_kernel(const float* __restrict__ src, int H, int W, in
     extern __shared__ long long smq[];
     const int r = RC > 0 ? RC : r_arg;
     const int TW = NT_X + 2 * r, TH = NT_Y + 2 * r;
-    long long* q1 = smq;                 // TH x TW
-    long long* q2 = q1 + TH * TW;        // TH x TW
-    long long* h1 = q2 + TH * TW;        // TH x NT_X
-    long long* h2 = h1 + TH * NT_X;      // TH x NT_X
+    // Row strides in 8-byte words are odd (QW, NT_HW), so 16 lanes on 16 consecutive rows of one
+    // column hit 16 different bank pairs.
+    const int QW = TW | 1;
+    long long* q1 = smq;                 // TH x QW
+    long long* q2 = q1 + TH * QW;        // TH x QW
+    long long* h1 = q2 + TH * QW;        // TH x NT_HW
+    long long* h2 = h1 + TH * NT_HW;     // TH x NT_HW
     const FixScale fs = fix_scale(__uint_as_float(*maxbits), (long long)(2 * r + 1) * (2 * r + 1));
     const int gx0 = blockIdx.x * NT_X, gy0 = blockIdx.y * NT_Y;
     // i / TW as a multiply-high by ceil(2^32 / TW): exact while i * TW < 2^32, which the tile's
@@ -391,15 +397,21 @@ __global__ void normalize_kernel(const float* __restrict__ src, int H, int W, in
             a = fix_q1(f, fs);
             b = fix_q2(f, fs);
         }
-        q1[i] = a;
-        q2[i] = b;
+        q1[ty * QW + tx] = a;
+        q2[ty * QW + tx] = b;
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < TH * NT_X; i += blockDim.x) {
-        const int ty = i / NT_X, tx = i % NT_X;
-        const long long* p1 = q1 + ty * TW + tx;
-        const long long* p2 = q2 + ty * TW + tx;
-        // Two accumulators per table shorten the add chains; integer sums are exact in any order.
+    // Row pass: each thread slides a (2r+1)-tap window along NT_XRUN outputs of one tile row;
+    // consecutive threads take consecutive rows. The sums are exact integers, so sliding gives
+    // the same totals as summing afresh.
+    const unsigned int th_magic = 0xffffffffu / (unsigned int)TH + 1u;
+    for (int i = threadIdx.x; i < TH * (NT_X / NT_XRUN); i += blockDim.x) {
+        const int run = (int)__umulhi((unsigned int)i, th_magic), row = i - run * TH;
+        const long long* p1 = q1 + row * QW + run * NT_XRUN;
+        const long long* p2 = q2 + row * QW + run * NT_XRUN;
+        long long* o1 = h1 + row * NT_HW + run * NT_XRUN;
+        long long* o2 = h2 + row * NT_HW + run * NT_XRUN;
+        // Two accumulators per table shorten the first sum's add chains.
         long long a0 = p1[0], b0 = p2[0], a1 = 0, b1 = 0;
         int j = 1;
 #pragma unroll
@@ -413,8 +425,16 @@ __global__ void normalize_kernel(const float* __restrict__ src, int H, int W, in
             a0 += p1[j];
             b0 += p2[j];
         }
-        h1[i] = a0 + a1;
-        h2[i] = b0 + b1;
+        long long a = a0 + a1, b = b0 + b1;
+        o1[0] = a;
+        o2[0] = b;
+#pragma unroll
+        for (int k = 1; k < NT_XRUN; ++k) {
+            a += p1[k + 2 * r] - p1[k - 1];
+            b += p2[k + 2 * r] - p2[k - 1];
+            o1[k] = a;
+            o2[k] = b;
+        }
     }
     __syncthreads();
     // Column pass: each thread slides a (2r+1)-row window down NT_RUN output rows of one column
@@ -425,14 +445,14 @@ __global__ void normalize_kernel(const float* __restrict__ src, int H, int W, in
         long long a = 0, b = 0;
 #pragma unroll
         for (int j = 0; j <= 2 * r; ++j) {
-            a += h1[(ty0 + j) * NT_X + tx];
-            b += h2[(ty0 + j) * NT_X + tx];
+            a += h1[(ty0 + j) * NT_HW + tx];
+            b += h2[(ty0 + j) * NT_HW + tx];
         }
         for (int k = 0; k < NT_RUN; ++k) {
             const int ty = ty0 + k, gy = gy0 + ty;
             if (k > 0) {
-                a += h1[(ty + 2 * r) * NT_X + tx] - h1[(ty - 1) * NT_X + tx];
-                b += h2[(ty + 2 * r) * NT_X + tx] - h2[(ty - 1) * NT_X + tx];
+                a += h1[(ty + 2 * r) * NT_HW + tx] - h1[(ty - 1) * NT_HW + tx];
+                b += h2[(ty + 2 * r) * NT_HW + tx] - h2[(ty - 1) * NT_HW + tx];
             }
             if (gx >= W || gy >= H) continue;
             const int x0 = max(gx - r, 0), x1 = min(gx + r + 1, W);
@@ -585,9 +605,9 @@ cudaError_t launch_prepare(const PrepParams& p, cudaStream_t s, int* launches) {
             maxabs_kernel<<<grid_for(n), 256, 0, s>>>(cur, n, p.maxbits + 1);
             nl += 1;
         }
-        const size_t sm = sizeof(long long) * (2 * (size_t)(NT_Y + 2 * r) * (NT_X + 2 * r) + 2 * (size_t)(NT_Y + 2 * r) * NT_X);
+        const size_t sm = sizeof(long long) * (2 * (size_t)(NT_Y + 2 * r) * ((NT_X + 2 * r) | 1) + 2 * (size_t)(NT_Y + 2 * r) * NT_HW);
         dim3 grid((p.W + NT_X - 1) / NT_X, (p.H + NT_Y - 1) / NT_Y);
-        if (r == 4) {  // the default radius: 46 KB of tile, under the 48 KB default
+        if (r == 4) {  // the default radius: 46.3 KB of tile, under the 48 KB default
             normalize_kernel<4><<<grid, 256, sm, s>>>(cur, p.H, p.W, r, p.normalize_eps, p.maxbits + 1, p.image);
         } else {
             if (sm > 48 * 1024) {
