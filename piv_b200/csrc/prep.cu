@@ -312,6 +312,7 @@ __global__ void integral_cols_kernel(int H, int W, long long* sum, long long* su
 
 // ------------------------------------------------------------------------------- blur
 constexpr int BT_X = 32, BT_Y = 32;
+constexpr int kBlurThreads = 256;  // the blur's launch width; its loops stride by it
 
 // The tile load reads samples through `Src`: the previous stage's f32 image, or (when nothing
 // else needs the background-subtracted image) the raw frame decoded on the fly, which saves the
@@ -332,7 +333,8 @@ __global__ void blur_kernel(Src src, int H, int W, const BlurKernel k, float* __
     const int gx0 = blockIdx.x * BT_X, gy0 = blockIdx.y * BT_Y;
     // i / TW as a multiply-high by ceil(2^32 / TW), exact for i * TW < 2^32.
     const unsigned int tw_magic = 0xffffffffu / (unsigned int)TW + 1u;
-    for (int i = threadIdx.x; i < TH * TW; i += blockDim.x) {
+#pragma unroll 2
+    for (int i = threadIdx.x; i < TH * TW; i += kBlurThreads) {
         const int ty = (int)__umulhi((unsigned int)i, tw_magic), tx = i - ty * TW;
         const int gy = min(max(gy0 + ty - R, 0), H - 1);
         const int gx = min(max(gx0 + tx - R, 0), W - 1);
@@ -340,7 +342,8 @@ __global__ void blur_kernel(Src src, int H, int W, const BlurKernel k, float* __
     }
     __syncthreads();
     // Row pass over every tile row (vertical halo included): sum in kernel order from -0.0.
-    for (int i = threadIdx.x; i < TH * BT_X; i += blockDim.x) {
+#pragma unroll
+    for (int i = threadIdx.x; i < TH * BT_X; i += kBlurThreads) {
         const int ty = i / BT_X, tx = i % BT_X;
         float s = -0.0f;
 #pragma unroll
@@ -350,7 +353,8 @@ __global__ void blur_kernel(Src src, int H, int W, const BlurKernel k, float* __
     __syncthreads();
     // Column pass: out starts at 0.0 and accumulates kernel terms in order (preprocess.rs:186-193).
     float m = 0.0f;
-    for (int i = threadIdx.x; i < BT_X * BT_Y; i += blockDim.x) {
+#pragma unroll
+    for (int i = threadIdx.x; i < BT_X * BT_Y; i += kBlurThreads) {
         const int ty = i / BT_X, tx = i % BT_X;
         const int gx = gx0 + tx, gy = gy0 + ty;
         if (gx >= W || gy >= H) continue;
@@ -368,6 +372,7 @@ constexpr int NT_X = 32, NT_Y = 32;
 constexpr int NT_RUN = 4;  // output rows per thread in the column pass (256 threads = 32 columns x 8 runs)
 constexpr int NT_XRUN = 4;  // outputs per thread in the row pass
 constexpr int NT_HW = NT_X + 1;  // row stride of the row-pass sums (odd, in 8-byte words)
+constexpr int kNormThreads = 256;  // the launch width; the loops stride by it
 
 // RC > 0 fixes the radius at compile time; RC = 0 takes it from r_arg.
 template <int RC>
@@ -388,7 +393,8 @@ __global__ void normalize_kernel(const float* __restrict__ src, int H, int W, in
     // i / TW as a multiply-high by ceil(2^32 / TW): exact while i * TW < 2^32, which the tile's
     // shared-memory size guarantees by far.
     const unsigned int tw_magic = 0xffffffffu / (unsigned int)TW + 1u;
-    for (int i = threadIdx.x; i < TH * TW; i += blockDim.x) {
+#pragma unroll 2
+    for (int i = threadIdx.x; i < TH * TW; i += kNormThreads) {
         const int ty = (int)__umulhi((unsigned int)i, tw_magic), tx = i - ty * TW;
         const int gy = gy0 + ty - r, gx = gx0 + tx - r;
         long long a = 0, b = 0;
@@ -405,7 +411,7 @@ __global__ void normalize_kernel(const float* __restrict__ src, int H, int W, in
     // consecutive threads take consecutive rows. The sums are exact integers, so sliding gives
     // the same totals as summing afresh.
     const unsigned int th_magic = 0xffffffffu / (unsigned int)TH + 1u;
-    for (int i = threadIdx.x; i < TH * (NT_X / NT_XRUN); i += blockDim.x) {
+    for (int i = threadIdx.x; i < TH * (NT_X / NT_XRUN); i += kNormThreads) {
         const int run = (int)__umulhi((unsigned int)i, th_magic), row = i - run * TH;
         const long long* p1 = q1 + row * QW + run * NT_XRUN;
         const long long* p2 = q2 + row * QW + run * NT_XRUN;
@@ -439,7 +445,7 @@ __global__ void normalize_kernel(const float* __restrict__ src, int H, int W, in
     __syncthreads();
     // Column pass: each thread slides a (2r+1)-row window down NT_RUN output rows of one column
     // (the sums are exact integers, so sliding gives the same totals as summing afresh).
-    for (int i = threadIdx.x; i < NT_X * (NT_Y / NT_RUN); i += blockDim.x) {
+    for (int i = threadIdx.x; i < NT_X * (NT_Y / NT_RUN); i += kNormThreads) {
         const int tx = i % NT_X, ty0 = (i / NT_X) * NT_RUN;
         const int gx = gx0 + tx;
         long long a = 0, b = 0;
@@ -473,14 +479,14 @@ template <typename Src>
 static cudaError_t run_blur(dim3 grid, size_t sm, cudaStream_t s, const Src& src, int H, int W, const BlurKernel& k,
                             float* dst, unsigned int* mx) {
     if (k.radius == 3) {
-        blur_kernel<Src, 3><<<grid, 256, sm, s>>>(src, H, W, k, dst, mx);
+        blur_kernel<Src, 3><<<grid, kBlurThreads, sm, s>>>(src, H, W, k, dst, mx);
         return cudaSuccess;
     }
     if (sm > 48 * 1024) {
         const cudaError_t e = cudaFuncSetAttribute(blur_kernel<Src, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
     }
-    blur_kernel<Src, 0><<<grid, 256, sm, s>>>(src, H, W, k, dst, mx);
+    blur_kernel<Src, 0><<<grid, kBlurThreads, sm, s>>>(src, H, W, k, dst, mx);
     return cudaSuccess;
 }
 
@@ -608,13 +614,13 @@ cudaError_t launch_prepare(const PrepParams& p, cudaStream_t s, int* launches) {
         const size_t sm = sizeof(long long) * (2 * (size_t)(NT_Y + 2 * r) * ((NT_X + 2 * r) | 1) + 2 * (size_t)(NT_Y + 2 * r) * NT_HW);
         dim3 grid((p.W + NT_X - 1) / NT_X, (p.H + NT_Y - 1) / NT_Y);
         if (r == 4) {  // the default radius: 46.3 KB of tile, under the 48 KB default
-            normalize_kernel<4><<<grid, 256, sm, s>>>(cur, p.H, p.W, r, p.normalize_eps, p.maxbits + 1, p.image);
+            normalize_kernel<4><<<grid, kNormThreads, sm, s>>>(cur, p.H, p.W, r, p.normalize_eps, p.maxbits + 1, p.image);
         } else {
             if (sm > 48 * 1024) {
                 e = cudaFuncSetAttribute(normalize_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
                 if (e != cudaSuccess) return e;
             }
-            normalize_kernel<0><<<grid, 256, sm, s>>>(cur, p.H, p.W, r, p.normalize_eps, p.maxbits + 1, p.image);
+            normalize_kernel<0><<<grid, kNormThreads, sm, s>>>(cur, p.H, p.W, r, p.normalize_eps, p.maxbits + 1, p.image);
         }
         nl += 1;
         cur = p.image;
