@@ -252,8 +252,9 @@ int64_t piv_batch_kernels(const PivBatch* batch);
 /* Pipelined pairs (no counterpart in the reference, which analyses pairs one after another,
  * analyze.rs:441): pairs of HOST frames are submitted without waiting; `depth` slots, each with
  * its own prepared frames and workspace, let the uploads and downloads of one pair overlap the
- * kernels of the others. Uploads, kernels and downloads go on three streams shared by the slots,
- * so the kernels of successive pairs run in submission order. Each result equals piv_analyze of
+ * kernels of the others. Uploads, frame preparation, analysis and downloads go on four streams
+ * shared by the slots: the preparation of a pair overlaps the analysis of the one before it, and
+ * the analyses of successive pairs run in submission order. Each result equals piv_analyze of
  * that pair. Host buffers should be
  * pinned (cudaHostAlloc) for the copies to be asynchronous, and must stay valid (outputs
  * untouched) until piv_pipeline_wait returns for that ticket. Submitting blocks only when the

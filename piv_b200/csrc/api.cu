@@ -1457,11 +1457,15 @@ struct PivPipeline {
         PivFrame* fb = nullptr;
         unsigned long long* sums = nullptr;  // pinned: 5 counters of the slot's last pair
         cudaEvent_t uploaded = nullptr;       // on the upload stream
+        cudaEvent_t prepared = nullptr;       // on the preparation stream
         cudaEvent_t computed = nullptr;       // on the compute stream
         cudaEvent_t done = nullptr;           // on the download stream
         uint64_t ticket = 0;  // 0: idle
     };
-    cudaStream_t up = nullptr, comp = nullptr, down = nullptr;
+    // Preparation has its own stream so that a pair's frames are prepared while the previous pair
+    // is analysed (the slots' frames and workspaces are separate, and a slot is reused only after
+    // its previous pair has been waited for).
+    cudaStream_t up = nullptr, prep = nullptr, comp = nullptr, down = nullptr;
     const float* background = nullptr;  // device image subtracted from every frame (caller-owned)
     int device = 0;
     int64_t H = 0, W = 0;
@@ -1507,6 +1511,7 @@ int32_t piv_pipeline_create(const PivAnalyzer* parent, int64_t height, int64_t w
     pl->slots.resize((size_t)depth);
     {
         cudaError_t e = cudaStreamCreateWithFlags(&pl->up, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&pl->prep, cudaStreamNonBlocking);
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&pl->comp, cudaStreamNonBlocking);
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&pl->down, cudaStreamNonBlocking);
         if (e != cudaSuccess) {
@@ -1519,6 +1524,7 @@ int32_t piv_pipeline_create(const PivAnalyzer* parent, int64_t height, int64_t w
         s.an = clone_config(parent);
         s.an->cur = pl->comp;
         cudaError_t e = cudaEventCreateWithFlags(&s.uploaded, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.prepared, cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.computed, cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.sums, 8 * sizeof(unsigned long long), cudaHostAllocDefault);
@@ -1539,17 +1545,17 @@ int32_t piv_pipeline_create(const PivAnalyzer* parent, int64_t height, int64_t w
 void piv_pipeline_destroy(PivPipeline* pl) {
     if (!pl) return;
     cudaSetDevice(pl->device);
-    for (cudaStream_t st : {pl->up, pl->comp, pl->down})
+    for (cudaStream_t st : {pl->up, pl->prep, pl->comp, pl->down})
         if (st) cudaStreamSynchronize(st);
     for (auto& s : pl->slots) {
         if (s.fa) piv_frame_destroy(s.fa);
         if (s.fb) piv_frame_destroy(s.fb);
-        for (cudaEvent_t ev : {s.uploaded, s.computed, s.done})
+        for (cudaEvent_t ev : {s.uploaded, s.prepared, s.computed, s.done})
             if (ev) cudaEventDestroy(ev);
         if (s.sums) cudaFreeHost(s.sums);
         piv_analyzer_destroy(s.an);
     }
-    for (cudaStream_t st : {pl->up, pl->comp, pl->down})
+    for (cudaStream_t st : {pl->up, pl->prep, pl->comp, pl->down})
         if (st) cudaStreamDestroy(st);
     delete pl;
 }
@@ -1567,10 +1573,15 @@ int32_t piv_pipeline_submit(PivPipeline* pl, const void* frame_a, const void* fr
     CUDA_TRY(cudaMemcpyAsync(s.fa->d_raw, frame_a, raw_bytes, cudaMemcpyHostToDevice, pl->up));
     CUDA_TRY(cudaMemcpyAsync(s.fb->d_raw, frame_b, raw_bytes, cudaMemcpyHostToDevice, pl->up));
     CUDA_TRY(cudaEventRecord(s.uploaded, pl->up));
-    CUDA_TRY(cudaStreamWaitEvent(pl->comp, s.uploaded, 0));
+    CUDA_TRY(cudaStreamWaitEvent(pl->prep, s.uploaded, 0));
+    s.an->cur = pl->prep;
     int st = prepare_common(s.an, s.fa, s.fa->d_raw, pl->dtype, &pl->pre, pl->background);
     if (!st) st = prepare_common(s.an, s.fb, s.fb->d_raw, pl->dtype, &pl->pre, pl->background);
-    if (!st) st = run_passes(s.an, s.fa, s.fb);
+    s.an->cur = pl->comp;
+    if (st) return st;
+    CUDA_TRY(cudaEventRecord(s.prepared, pl->prep));
+    CUDA_TRY(cudaStreamWaitEvent(pl->comp, s.prepared, 0));
+    st = run_passes(s.an, s.fa, s.fb);
     if (st) return st;
     CUDA_TRY(cudaEventRecord(s.computed, pl->comp));
     CUDA_TRY(cudaStreamWaitEvent(pl->down, s.computed, 0));
