@@ -651,6 +651,18 @@ def main():
     stream = torch.cuda.Stream(device=dev)
     an.set_stream(stream.cuda_stream)
     fa, fb = an.frame(h, w), an.frame(h, w)
+    # Two slots, each an analyzer (workspace and pass graph) with its own frames: the frames of
+    # step i+1 are prepared on prep_stream while step i is analysed on `stream`, as PivPipeline
+    # does for host frames. Analyses stay in order on one stream.
+    an2 = P.PivAnalyzer(piv_config(wl), device=local)
+    an2.set_stream(stream.cuda_stream)
+    fa2, fb2 = an2.frame(h, w), an2.frame(h, w)
+    slots = [(an, fa, fb), (an2, fa2, fb2)]
+    prep_stream = torch.cuda.Stream(device=dev)
+    prepared = [torch.cuda.Event() for _ in slots]
+    analysed = [torch.cuda.Event() for _ in slots]
+    for ev in analysed:
+        ev.record(stream)
     g = an.output_grid(h, w)
     nvec = len(g)
     out_dx = torch.empty(nvec, device=dev, dtype=torch.float32)
@@ -680,15 +692,27 @@ def main():
     def step(i):
         k = i % n_ring
         ta, tb = pairs_dev[k]
-        fa.prepare_device(ta.data_ptr(), dtype_code, pre, bg_ptrs[k])
-        fb.prepare_device(tb.data_ptr(), dtype_code, pre, bg_ptrs[k])
-        an.analyze_device(fa, fb, out_dx.data_ptr(), out_dy.data_ptr(), out_ppr.data_ptr(), out_fl.data_ptr(),
-                          out_sum.data_ptr())
+        s_an, s_fa, s_fb = slots[i % 2]
+        # the slot's frames are free once its previous pair has been analysed
+        prep_stream.wait_event(analysed[i % 2])
+        s_an.set_stream(prep_stream.cuda_stream)
+        s_fa.prepare_device(ta.data_ptr(), dtype_code, pre, bg_ptrs[k])
+        s_fb.prepare_device(tb.data_ptr(), dtype_code, pre, bg_ptrs[k])
+        prepared[i % 2].record(prep_stream)
+        stream.wait_event(prepared[i % 2])
+        s_an.set_stream(stream.cuda_stream)
+        s_an.analyze_device(s_fa, s_fb, out_dx.data_ptr(), out_dy.data_ptr(), out_ppr.data_ptr(), out_fl.data_ptr(),
+                            out_sum.data_ptr())
+        analysed[i % 2].record(stream)
 
-    # launch-geometry autotuning on the first pair (results are identical across variants)
-    fa.prepare_device(pairs_dev[0][0].data_ptr(), dtype_code, pre, bg_ptr)
-    fb.prepare_device(pairs_dev[0][1].data_ptr(), dtype_code, pre, bg_ptr)
-    tuned = an.autotune(fa, fb) if not args.no_autotune else {}
+    # launch-geometry autotuning of both slots on the first pair (results are identical across
+    # variants)
+    tuned = {}
+    for s_an, s_fa, s_fb in slots:
+        s_fa.prepare_device(pairs_dev[0][0].data_ptr(), dtype_code, pre, bg_ptr)
+        s_fb.prepare_device(pairs_dev[0][1].data_ptr(), dtype_code, pre, bg_ptr)
+        t = s_an.autotune(s_fa, s_fb) if not args.no_autotune else {}
+        tuned = tuned or t
     for i in range(args.warmup):
         step(i)
     stream.synchronize()
@@ -702,28 +726,31 @@ def main():
     sampler = ClockSampler(gpu_uuid if gpu_uuid.startswith("GPU-") else f"GPU-{gpu_uuid}")
     sampler.start()
     time.sleep(0.3)
-    l0 = an.launches()
+    l0 = an.launches() + an2.launches()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
+    prep_stream.wait_event(e0)
     for i in range(args.steps):
         step(i)
     e1.record(stream)
     e1.synchronize()
     torch.cuda.synchronize()
-    launches = an.launches() - l0
+    launches = an.launches() + an2.launches() - l0
     clocks = sampler.stop()
     ms = e0.elapsed_time(e1)
     ms_max = ranks.max(ms)
     # the same steps again with CUDA events around every correlation launch (eager launches):
     # per-pass kernel times for the roofline
-    an.set_profiling(True)
-    for p in range(npass):
-        an.profile(p)  # reset
+    for s_an, _, _ in slots:
+        s_an.set_profiling(True)
+        for p in range(npass):
+            s_an.profile(p)  # reset
     for i in range(args.steps):
         step(i)
-    stream.synchronize()
-    corr = [an.profile(p) for p in range(npass)]
-    an.set_profiling(False)
+    torch.cuda.synchronize()
+    corr = [tuple(map(sum, zip(an.profile(p), an2.profile(p)))) for p in range(npass)]
+    for s_an, _, _ in slots:
+        s_an.set_profiling(False)
     value = world * args.steps * nvec / (ms_max * 1e-3)
 
     # ---------------------------------------------------------------- timed: end to end (host buffers)
@@ -869,6 +896,8 @@ def main():
                        **({"baseline": f"published {wl['published_pairs_per_s']:.0f} pairs/s (reference's Metal port, "
                                        f"Apple M5 Max) x {nvec} final vectors"}
                           if wl.get("published_pairs_per_s") else {}),
+                       "schedule": "two analyzer slots: the frames of pair i+1 are prepared on a second stream "
+                                   "while pair i is analysed; analyses in order on one stream",
                        "l2": f"inputs > L2: {n_ring} shifted copies of the pair in turn, "
                              f"{n_ring * pair_bytes / 2**20:.0f} MiB of samples"
                              + (" (+ one background image per pair)" if wl.get("background") else "")},
@@ -888,6 +917,7 @@ def main():
         line["accuracy"] = accuracy_vs_fp64(wl, a0, b0, an)
     if rank == 0:
         print(json.dumps(line), flush=True)
+    an2.close()
     an.close()
     ranks.close()
     return 0
