@@ -75,19 +75,59 @@ def alg_flops(n):
     return 7.5 * n * n * math.log2(n * n) + 6 * n * (n // 2 + 1) + 2 * n * n
 
 
-def make_inputs(wl, seed_offset=0):
+def product_grid(h, w, window, overlap):
+    """Grid::new (grid.rs:20-44) through the library: (nx, ny, step, x0, y0)."""
+    import piv_b200 as P
+    g = P.Grid.new(h, w, window, overlap)
+    return g.nx, g.ny, g.step, g.x0, g.y0
+
+
+def oracle_grid(h, w, window, overlap):
+    """Grid::new through the oracle, for the reference arm, which loads nothing of the product."""
+    from oracle import oracle as O
+    g = O.grid(h, w, window, overlap)
+    return g.nx, g.ny, g.step, g.x0, g.y0
+
+
+def make_inputs(wl, seed_offset=0, grid=product_grid):
+    """The workload's synthetic u8/u16 pair (numpy only); `grid` places the outlier clusters on
+    the final pass's cells."""
     from piv_b200 import synthetic as S
     h, w = wl["h"], wl["w"]
     field = S.vortex_shear_field(h, w, vmax=wl["vmax"], core=wl.get("core"), shear=wl["shear"])
     cells = None
     if wl["outlier_frac"] > 0:
-        import piv_b200 as P
-        g = P.Grid.new(h, w, wl["windows"][-1], wl["overlap"])
+        nx, ny, step, x0, y0 = grid(h, w, wl["windows"][-1], wl["overlap"])
         rng = np.random.default_rng(wl["seed"] + seed_offset)
-        k = rng.choice(len(g), int(round(wl["outlier_frac"] * len(g))), replace=False)
-        cells = np.stack([g.x0 + (k % g.nx) * g.step, g.y0 + (k // g.nx) * g.step], 1)
+        k = rng.choice(nx * ny, int(round(wl["outlier_frac"] * nx * ny)), replace=False)
+        cells = np.stack([x0 + (k % nx) * step, y0 + (k // nx) * step], 1)
     return S.baseline_pair(h, w, wl["seed"] + seed_offset, field, ppp=wl["ppp"], dmin=wl["dmin"], dmax=wl["dmax"],
                            bits=wl["bits"], outlier_cells=cells, outlier_window=wl["windows"][-1])
+
+
+def input_ring(a0, b0):
+    """A ring of shifted copies of the pair holding at least 256 MiB of samples, taken in turn by
+    the steps, so that a step's inputs come from HBM rather than from the 126 MB L2."""
+    pair_bytes = a0.nbytes + b0.nbytes
+    n_ring = max(2, -(-(256 << 20) // pair_bytes))
+    return [(a0, b0)] + [(np.ascontiguousarray(np.roll(a0, (37 * k, 53 * k), (0, 1))),
+                          np.ascontiguousarray(np.roll(b0, (37 * k, 53 * k), (0, 1)))) for k in range(1, n_ring)]
+
+
+def workload_config(wl, ring, nvec, world):
+    """The `config` object both arms print for a frame-pair workload."""
+    a0 = ring[0][0]
+    h, w = a0.shape
+    pair_bytes = a0.nbytes + ring[0][1].nbytes
+    cfg = {"workload": wl["name"], "image": f"{h}x{w} {a0.dtype.name} ({wl['bits']}-bit)", "windows": pass_windows(wl),
+           "overlap": wl["overlap"], "final_pass_vectors": nvec, "parallelism": f"replicas x{world}",
+           "inputs": f"{len(ring)} shifted copies of the pair taken in turn, {len(ring) * pair_bytes / 2**20:.0f} MiB "
+                     f"of samples" + (" (+ one background image per pair)" if wl.get("background") else ""),
+           "l2": "inputs > L2: a step's samples are not resident in the 126 MB L2 when it starts"}
+    if wl.get("published_pairs_per_s"):
+        cfg["baseline"] = (f"published {wl['published_pairs_per_s']:.0f} pairs/s (reference's Metal port, Apple M5 "
+                           f"Max) x {nvec} final vectors")
+    return cfg
 
 
 class _DeviceBuffer:
@@ -442,27 +482,47 @@ def _crop_background(wl, a, b, ch, cw):
     return (np.minimum(a[:ch, :cw], b[:ch, :cw]).astype(np.float32) / top).astype(np.float32)
 
 
-def _oracle_inputs(wl, a, b, crop):
-    """The oracle's prepared images of a crop of the pair, with the workload's preprocessing: the
-    percentile clip of each frame's codes (a3), then decoding and the background subtraction
-    base = max(raw - background, 0) (preprocess.rs:138-145)."""
+def oracle_config(wl):
     from oracle import oracle as O
-    ch, cw = min(crop, wl["h"]), min(crop, wl["w"])
+    return O.OracleConfig(tuple(wl["windows"]), wl["overlap"], wl["final_iterations"],
+                          deform=int(bool(wl.get("deform", False))))
+
+
+def oracle_frames(wl, a, b, bg):
+    """The oracle's prepared images and signal-mask intensities of a pair, with the workload's
+    preprocessing: the percentile clip of each frame's codes (a3), decoding, the background
+    subtraction base = max(raw - background, 0) and the default blur and local normalisation where
+    the workload has them (preprocess.rs:138-158)."""
+    from oracle import oracle as O
     dec = O.u16_to_f32 if a.dtype == np.uint16 else O.u8_to_f32
-    ca, cb = np.ascontiguousarray(a[:ch, :cw]), np.ascontiguousarray(b[:ch, :cw])
+    a, b = np.ascontiguousarray(a), np.ascontiguousarray(b)
     if wl.get("clip_percentile"):
-        ca, _ = O.percentile_clip_u16(ca, wl["clip_percentile"])
-        cb, _ = O.percentile_clip_u16(cb, wl["clip_percentile"])
-    fa, fb = dec(ca), dec(cb)
-    ba, bb = fa, fb  # the signal mask's intensity (preprocess.rs:138-158: base = max(raw - bg, 0))
-    bg = _crop_background(wl, a, b, ch, cw)
+        a, _ = O.percentile_clip_u16(a, wl["clip_percentile"])
+        b, _ = O.percentile_clip_u16(b, wl["clip_percentile"])
+    fa, fb = dec(a), dec(b)
+    ba, bb = fa, fb
     blur, radius, eps = (1.0, 4, 0.02) if wl.get("preprocess") == "default" else (0.0, 0, 0.0)
     if bg is not None or radius:
         fa, ba = O.prepare(fa, blur, radius, eps, background=bg)
         fb, bb = O.prepare(fb, blur, radius, eps, background=bg)
-    cfg = O.OracleConfig(tuple(wl["windows"]), wl["overlap"], wl["final_iterations"],
-                         deform=int(bool(wl.get("deform", False))))
-    return O, fa, fb, cfg, ch, cw, ba, bb
+    return fa, fb, ba, bb
+
+
+def _oracle_inputs(wl, a, b, crop):
+    from oracle import oracle as O
+    ch, cw = min(crop, wl["h"]), min(crop, wl["w"])
+    fa, fb, ba, bb = oracle_frames(wl, a[:ch, :cw], b[:ch, :cw], _crop_background(wl, a, b, ch, cw))
+    return O, fa, fb, oracle_config(wl), ch, cw, ba, bb
+
+
+def oracle_pair(wl, a, b, bg, nthreads):
+    """One analysis of a pair by the oracle port, preparation included: the reference's
+    PreparedFrame::new + PivAnalyzer::analyze (preprocess.rs:138-158, multipass.rs:136-192).
+    Returns the number of final-pass vectors."""
+    from oracle import oracle as O
+    fa, fb, ba, bb = oracle_frames(wl, a, b, bg)
+    fin, _, _ = O.analyze(oracle_config(wl), fa, fb, ba, bb, nthreads=nthreads)
+    return int(fin["dx"].size)
 
 
 def preprocess_config(wl):
@@ -478,32 +538,35 @@ def _torch_view(x):
     return x.view(np.int16) if x.dtype == np.uint16 else x
 
 
-def cpu_baseline(wl, a, b, budget_s=12.0, crop=1024, single_s=0.0):
-    """Times the oracle port (reference operation order, OpenMP over windows) on a crop of the
-    workload with the same pass schedule; returns final-pass vectors/s and the sample used, plus a
-    single-thread figure when single_s > 0."""
-    O, fa, fb, cfg, ch, cw, ba, bb = _oracle_inputs(wl, a, b, crop)
+def cpu_baseline(wl, a, b, budget_s=10.0, crop=1024, single_s=0.0):
+    """Times the oracle port (reference operation order, OpenMP over windows, all host threads) on
+    whole pairs of the workload, preparation included, until budget_s has passed (at least one
+    pair); returns final-pass vectors/s and the sample used, plus a single-thread figure on a
+    crop x crop corner of the pair with the same schedule when single_s > 0."""
     nthreads = os.cpu_count() or 1
-    vec = final_vectors(wl, ch, cw)
+    bg = _crop_background(wl, a, b, a.shape[0], a.shape[1])
 
-    def timed(nt, budget):
+    def timed(fa, fb, fbg, nt, budget):
         t0 = time.perf_counter()
-        reps = 0
+        reps, vec = 0, 0
         while True:
-            O.analyze(cfg, fa, fb, ba, bb, nthreads=nt)
+            vec += oracle_pair(wl, fa, fb, fbg, nt)
             reps += 1
             if time.perf_counter() - t0 >= budget:
                 break
-        return reps, time.perf_counter() - t0
+        return reps, vec, time.perf_counter() - t0
 
-    reps, dt = timed(nthreads, budget_s)
-    out = {"value": vec * reps / dt, "unit": "vectors/s", "cores": nthreads, "kind": "port",
-           "sample": f"{reps} x full {len(pass_windows(wl))}-pass analysis of a {ch}x{cw} crop ({vec} final vectors), "
-                     f"oracle/piv_oracle.cpp, {nthreads} OpenMP threads, {dt:.1f} s"}
+    reps, vec, dt = timed(a, b, bg, nthreads, budget_s)
+    out = {"value": vec / dt, "unit": "vectors/s", "cores": nthreads, "kind": "port",
+           "sample": f"{reps} x the whole {a.shape[0]}x{a.shape[1]} pair, preparation and all "
+                     f"{len(pass_windows(wl))} passes ({vec // reps} final vectors), oracle/piv_oracle.cpp, "
+                     f"{nthreads} OpenMP threads, {dt:.1f} s"}
     if single_s > 0:
-        r1, d1 = timed(1, single_s)
-        out["single_thread_value"] = vec * r1 / d1
-        out["single_thread_sample"] = f"{r1} x the same analysis on 1 thread, {d1:.1f} s"
+        ch, cw = min(crop, a.shape[0]), min(crop, a.shape[1])
+        ca, cb = np.ascontiguousarray(a[:ch, :cw]), np.ascontiguousarray(b[:ch, :cw])
+        r1, v1, d1 = timed(ca, cb, _crop_background(wl, a, b, ch, cw), 1, single_s)
+        out["single_thread_value"] = v1 / d1
+        out["single_thread_sample"] = f"{r1} x the same analysis of a {ch}x{cw} corner on 1 thread, {d1:.1f} s"
     return out
 
 
@@ -549,34 +612,101 @@ def run_profile_case(args, wl):
     return 0
 
 
-REF_TOTAL_S = 150.0
+# seconds of timed steps the reference arm aims at (whole pairs when the steps fit)
+REF_TOTAL_S = 165.0
 
 
 def run_reference(args, wl):
+    """The reference's CPU algorithm (the oracle port of piv-core, all host threads) on this arm's
+    workload: the same pair, the same ring of shifted copies taken in turn, the same preparation
+    and pass schedule, one step = one pair. Nothing of the product library is loaded. Steps are
+    timed one by one on the host clock; when whole pairs would take well over REF_TOTAL_S in all,
+    every step analyses the same top band of rows of its pair instead, and the line says so."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    if wl.get("serving"):
+        return run_reference_serving(args, wl)
+    nthreads = os.cpu_count() or 1
     if wl.get("stream"):
-        a, b = make_stream(dict(wl, frames=2))
+        fr = make_stream(dict(wl, frames=2))
+        a0, b0 = fr[0], fr[1]
     else:
-        a, b = make_inputs(wl)
-    for _ in range(args.warmup):
-        pass  # the oracle has no warm-up state; warm-up steps run no work
-    base = None
-    samples = []
-    # each step is a bounded sample of the workload; the whole run stays near REF_TOTAL_S seconds
-    step_s = max(0.5, min(args.ref_step_s, REF_TOTAL_S / max(args.steps, 1)))
-    for _ in range(args.steps):
-        r = cpu_baseline(wl, a, b, budget_s=step_s, crop=args.ref_crop)
-        samples.append(r["value"])
-        base = r
-    v = float(np.median(samples))
+        a0, b0 = make_inputs(wl, grid=oracle_grid)
+    ring = input_ring(a0, b0)
+    h, w = a0.shape
+    # the background of each pair (BackgroundEstimator, preprocess.rs:47-72), estimated before the
+    # steps as the reference estimates it before its pair loop
+    bgs = [_crop_background(wl, a, b, h, w) for a, b in ring]
+    nx, ny, _, _, _ = oracle_grid(h, w, wl["windows"][-1], wl["overlap"])
+    nvec = nx * ny
+    # warm-up: the same analysis on a band of the top rows (the oracle keeps no state between
+    # calls; this starts its thread pool and touches the inputs) and a size estimate for the steps
+    band = min(h, max(256, max(wl["windows"]) * 2))
+    t_band = 0.0
+    for i in range(args.warmup):
+        a, b = ring[i % len(ring)]
+        t0 = time.perf_counter()
+        v_band = oracle_pair(wl, a[:band], b[:band], None if bgs[i % len(ring)] is None else bgs[i % len(ring)][:band],
+                             nthreads)
+        t_band = time.perf_counter() - t0
+    est_pair = t_band * nvec / max(v_band, 1)
+    rows = h
+    if args.steps * est_pair > 1.5 * REF_TOTAL_S:
+        rows = max(band, int(h * REF_TOTAL_S / (args.steps * est_pair)))
+    times, vecs = [], 0
+    for i in range(args.steps):
+        a, b = ring[i % len(ring)]
+        bg = bgs[i % len(ring)]
+        t0 = time.perf_counter()
+        vecs += oracle_pair(wl, a[:rows], b[:rows], None if bg is None else bg[:rows], nthreads)
+        times.append(time.perf_counter() - t0)
+    total = float(sum(times))
+    v = vecs / total
+    sample = (f"{args.steps} whole {h}x{w} pair{'s' if args.steps != 1 else ''}" if rows == h else
+              f"{args.steps} steps, each the top {rows} of {h} rows of its pair (whole pairs would take about "
+              f"{args.steps * est_pair:.0f} s)") + (f", preparation and all {len(pass_windows(wl))} passes, "
+                                                   f"oracle/piv_oracle.cpp (C++ restatement of piv-core), "
+                                                   f"{nthreads} OpenMP threads, {total:.1f} s timed")
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "vectors/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * final_vectors(wl) / v,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": wl["name"]},
-            "cpu_baseline": {"value": v, "unit": "vectors/s", "cores": base["cores"], "kind": "port",
-                             "sample": base["sample"]},
+            "config": workload_config(wl, ring, nvec, args.gpus),
+            "cpu_baseline": {"value": v, "unit": "vectors/s", "cores": nthreads, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": "vectors/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "step_ms": {"min": 1e3 * min(times), "median": 1e3 * float(np.median(times)), "max": 1e3 * max(times)}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_reference_serving(args, wl):
+    """The reference's CPU path on the serving mix: one request of every (size, schedule) kind in
+    turn per step (the reference has no serving form; its analysis runs one pair at a time)."""
+    from piv_b200 import synthetic as S
+    nthreads = os.cpu_count() or 1
+    reqs = []
+    for si, (h, w) in enumerate(wl["sizes"]):
+        f = (lambda X, Y: (np.float32(2.0) + 0.01 * (np.asarray(Y, np.float32) - h / 2), np.float32(1.0)))
+        a, b = S.baseline_pair(h, w, 1000 * si, f, ppp=0.05, dmin=2.0, dmax=4.0, bits=12)
+        for sched in wl["schedules"]:
+            reqs.append((dict(wl, windows=list(sched), final_iterations=1, h=h, w=w), a, b))
+    for _ in range(args.warmup):
+        pass  # the oracle keeps no state between calls
+    times, vecs = [], 0
+    for i in range(args.steps):
+        t0 = time.perf_counter()
+        for rwl, a, b in reqs:
+            vecs += oracle_pair(rwl, a, b, None, nthreads)
+        times.append(time.perf_counter() - t0)
+    total = float(sum(times))
+    v = vecs / total
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "vectors/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": wl["name"], "parallelism": f"replicas x{args.gpus}"},
+            "cpu_baseline": {"value": v, "unit": "vectors/s", "cores": nthreads, "kind": "port",
+                             "sample": f"{args.steps} x one request of each of the {len(reqs)} (size, schedule) kinds "
+                                       f"in turn, {nthreads} OpenMP threads, {total:.1f} s"},
             "e2e": {"value": v, "unit": "vectors/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -596,8 +726,6 @@ def main():
     ap.add_argument("--deform", type=int, choices=[0, 1], default=None,
                     help="window deformation from the second pass on (default: the workload's setting)")
     ap.add_argument("--duration", type=float, default=None, help="serving workload: seconds of arrivals")
-    ap.add_argument("--ref-step-s", type=float, default=3.0)
-    ap.add_argument("--ref-crop", type=int, default=1024)
     ap.add_argument("--profile-case", default=None, metavar="WINDOWS",
                     help="profiler workload: analyse the workload's pair --steps times with the given comma-separated "
                          "window schedule (or 'all'), through the host API, untimed")
@@ -637,10 +765,8 @@ def main():
     a0, b0 = make_inputs(wl, seed_offset=rank)
     # a ring of shifted copies of the pair, at least 256 MiB of samples, so that the steps read
     # their inputs from HBM rather than from the 126 MB L2
-    pair_bytes = a0.nbytes + b0.nbytes
-    n_ring = max(2, -(-(256 << 20) // pair_bytes))
-    pairs_host = [(a0, b0)] + [(np.ascontiguousarray(np.roll(a0, (37 * k, 53 * k), (0, 1))),
-                                np.ascontiguousarray(np.roll(b0, (37 * k, 53 * k), (0, 1)))) for k in range(1, n_ring)]
+    pairs_host = input_ring(a0, b0)
+    n_ring = len(pairs_host)
     dtype_code = P.api._dtype_code(a0)
     h, w = a0.shape
     # raw u16 samples on the device (held as int16 tensors: same bytes)
@@ -891,16 +1017,9 @@ def main():
     line = {"metric": METRIC, "value": value, "unit": "vectors/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": vs_baseline, "dtype": "f32" if wl.get("precision", "fp32") == "fp32" else wl["precision"] + "+f32", "data": "synthetic",
-            "config": {"workload": wl["name"], "image": f"{h}x{w} {a0.dtype.name} ({wl['bits']}-bit)", "windows": pw,
-                       "overlap": wl["overlap"], "final_pass_vectors": nvec, "parallelism": f"replicas x{world}",
-                       **({"baseline": f"published {wl['published_pairs_per_s']:.0f} pairs/s (reference's Metal port, "
-                                       f"Apple M5 Max) x {nvec} final vectors"}
-                          if wl.get("published_pairs_per_s") else {}),
-                       "schedule": "two analyzer slots: the frames of pair i+1 are prepared on a second stream "
-                                   "while pair i is analysed; analyses in order on one stream",
-                       "l2": f"inputs > L2: {n_ring} shifted copies of the pair in turn, "
-                             f"{n_ring * pair_bytes / 2**20:.0f} MiB of samples"
-                             + (" (+ one background image per pair)" if wl.get("background") else "")},
+            "config": workload_config(wl, pairs_host, nvec, world),
+            "schedule": "two analyzer slots: the frames of pair i+1 are prepared on a second stream while pair i is "
+                        "analysed; analyses in order on one stream",
             "e2e": {"value": e2e_value, "unit": "vectors/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "steps": pipe_steps,
                     "ms_per_step": ms2 / pipe_steps,

@@ -422,7 +422,10 @@ int32_t piv_tc_wait_probe(int32_t device, int32_t log2_iters, int32_t* timed_out
  * Scratch lives in a fixed device array inside the library of 2 x 2,097,152 bytes, held by every
  * GPU that loads the library until exit; fields above 2,097,152 cells are rejected
  * (PIV_ERR_UNSUPPORTED). The first call on a device looks up that array's address, so make it
- * before any stream capture. All calls share the array: calls whose work overlaps on the GPU race. */
+ * before any stream capture; the address is kept until exit, so do not call this on a device
+ * after cudaDeviceReset. All calls share the array: calls whose work overlaps on the GPU race.
+ * Outputs must not overlap any input or each other (the median test reads neighbours while
+ * others are written): such calls are rejected (PIV_ERR_ARGUMENT). */
 int32_t piv_validate_field_noalloc(int64_t ny, int64_t nx, const float* dx, const float* dy, const float* peak_ratio,
                                    const uint8_t* flags, float max_displacement, float ppr_threshold,
                                    float median_threshold, float median_eps, int32_t replace, float* out_dx,

@@ -112,18 +112,13 @@ struct FixScale {
     // scalbnf(v, s) bit for bit. Outside that range the quantisers fall back to scalbnf.
     float m1, m2;
     bool fast1, fast2;
-    // 2^-s1 and 2^-s2 as doubles (s1 lies in [-128, 210], s2 in [-256, 358], so both are normal
-    // doubles, and an int64 sum times either stays normal): the product is exact and equals
-    // scalbn(sum, -s).
-    double d1, d2;
 };
 
 __device__ __forceinline__ float pow2f(int s) { return __int_as_float((s + 127) << 23); }
-__device__ __forceinline__ double pow2d(int s) { return __longlong_as_double((long long)(s + 1023) << 52); }
 
 // Largest exponent e with 2^e >= maxabs, then scales that keep count * 2^(e+s) <= 2^62.
 __device__ __forceinline__ FixScale fix_scale(float maxabs, long long count) {
-    FixScale fs{0, 0, 1.0f, 1.0f, true, true, 1.0, 1.0};
+    FixScale fs{0, 0, 1.0f, 1.0f, true, true};
     if (!(maxabs > 0.0f) || !isfinite(maxabs)) return fs;
     int e;
     float m = frexpf(maxabs, &e);  // maxabs = m * 2^e, m in [0.5, 1)
@@ -136,8 +131,6 @@ __device__ __forceinline__ FixScale fix_scale(float maxabs, long long count) {
     fs.fast2 = fs.s2 >= 0 && fs.s2 <= 127;
     fs.m1 = fs.fast1 ? pow2f(fs.s1) : 1.0f;
     fs.m2 = fs.fast2 ? pow2f(fs.s2) : 1.0f;
-    fs.d1 = pow2d(-fs.s1);
-    fs.d2 = pow2d(-fs.s2);
     return fs;
 }
 
@@ -160,19 +153,6 @@ __device__ __forceinline__ void fix_stats(long long sum1, long long sum2, const 
     dfloat var = dd_add(ex2, dd_neg(dd_mul(mean, mean)));
     *mean_out = dd_to_float(mean);
     *std_out = dd_to_float(dd_sqrt(var));
-}
-
-// The same statistics in native f64, the reference's own arithmetic (IntegralImage::stats,
-// preprocess.rs:114-125: mean = s/n, var = sq/n - mean^2, both f64, then sqrt and the casts to
-// f32), applied to the exact sums.
-__device__ __forceinline__ void fix_stats_f64(long long sum1, long long sum2, const FixScale& fs, float count,
-                                              float* mean_out, float* std_out) {
-    const double n = (double)count;
-    const double mean = __ddiv_rn(__dmul_rn((double)sum1, fs.d1), n);
-    const double ex2 = __ddiv_rn(__dmul_rn((double)sum2, fs.d2), n);
-    const double var = __dsub_rn(ex2, __dmul_rn(mean, mean));
-    *mean_out = __double2float_rn(mean);
-    *std_out = __double2float_rn(var > 0.0 ? __dsqrt_rn(var) : 0.0);
 }
 
 // Rust f32::clamp (NaN passes through).

@@ -16,9 +16,15 @@
 // Host code cannot use the array's name as a device address (it names a host-side stand-in),
 // so the address is taken with cudaGetSymbolAddress once per device, with that device current,
 // on the first call of the entry point on that device. Make that first call before any stream
-// capture begins. Every call shares the same array, and the kernels overwrite every snapshot
-// byte they later read, so nothing needs clearing between calls; two calls whose work overlaps
-// on the GPU (different streams, or different host threads on one device) race on it.
+// capture begins. The address is kept for the life of the process, so the entry point must not
+// be used on a device after cudaDeviceReset (or any reset of its primary context). Every call
+// shares the same array, and the kernels overwrite every snapshot byte they later read, so
+// nothing needs clearing between calls; two calls whose work overlaps on the GPU (different
+// streams, or different host threads on one device) race on it.
+//
+// Outputs must not overlap inputs: the median test reads neighbours' dx/dy while other threads
+// write theirs, so in-place validation would race. Overlapping buffers are rejected.
+#include <cstdint>
 #include <cstdio>
 #include <mutex>
 #include <string>
@@ -60,6 +66,12 @@ int reject(int code, const std::string& msg) {
     return code;
 }
 
+// Whether the byte ranges [a, a + na) and [b, b + nb) share a byte.
+bool overlap(const void* a, size_t na, const void* b, size_t nb) {
+    const uintptr_t x = reinterpret_cast<uintptr_t>(a), y = reinterpret_cast<uintptr_t>(b);
+    return x < y + nb && y < x + na;
+}
+
 }  // namespace
 
 extern "C" {
@@ -71,11 +83,27 @@ int32_t piv_validate_field_noalloc(int64_t ny, int64_t nx, const float* dx, cons
     if (!dx || !dy || !peak_ratio || !flags || !out_dx || !out_dy || !out_flags)
         return reject(PIV_ERR_ARGUMENT, "piv_validate_field_noalloc: null pointer");
     if (ny <= 0 || nx <= 0) return reject(PIV_ERR_ARGUMENT, "piv_validate_field_noalloc: empty field");
-    if (ny * nx > kNoAllocMaxCells) {
-        char buf[160];
-        snprintf(buf, sizeof(buf), "piv_validate_field_noalloc: %lld cells exceed the fixed scratch of %lld cells",
-                 (long long)(ny * nx), kNoAllocMaxCells);
+    // nx > max / ny rather than ny * nx > max: the product of two huge sizes would overflow.
+    if (nx > kNoAllocMaxCells / ny) {
+        char buf[200];
+        snprintf(buf, sizeof(buf),
+                 "piv_validate_field_noalloc: a %lld x %lld field exceeds the fixed scratch of %lld cells",
+                 (long long)ny, (long long)nx, kNoAllocMaxCells);
         return reject(PIV_ERR_UNSUPPORTED, buf);
+    }
+    const size_t n = (size_t)(ny * nx), nf = n * sizeof(float);
+    const void* ins[4] = {dx, dy, peak_ratio, flags};
+    const size_t in_bytes[4] = {nf, nf, nf, n};
+    const void* outs[3] = {out_dx, out_dy, out_flags};
+    const size_t out_bytes[3] = {nf, nf, n};
+    for (int o = 0; o < 3; ++o) {
+        for (int i = 0; i < 4; ++i)
+            if (overlap(outs[o], out_bytes[o], ins[i], in_bytes[i]))
+                return reject(PIV_ERR_ARGUMENT, "piv_validate_field_noalloc: an output buffer overlaps an input "
+                                                "(in-place validation would race)");
+        for (int q = o + 1; q < 3; ++q)
+            if (overlap(outs[o], out_bytes[o], outs[q], out_bytes[q]))
+                return reject(PIV_ERR_ARGUMENT, "piv_validate_field_noalloc: output buffers overlap");
     }
     uint8_t* scratch = nullptr;
     cudaError_t e = scratch_for_current_device(&scratch);

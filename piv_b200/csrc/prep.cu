@@ -10,9 +10,10 @@
 //
 // The blur repeats the reference's f32 operations in order (no FMA), so it is bit-exact given
 // the same kernel weights. The normalization's box statistics are exact integer sums turned into
-// f32 mean/std by the reference's own f64 arithmetic (fix_stats_f64 in common.cuh). These sums
-// are exact where the reference's f64 integral image can round, so a result can differ from the
-// reference's in a rounding-boundary case.
+// f32 mean/std by the reference's steps (mean = s/n, var = sq/n - mean^2, sqrt) in double-float
+// arithmetic (fix_stats in common.cuh; no FP64 instruction). These sums are exact where the
+// reference's f64 integral image can round, and double-float carries ~48 of f64's 53 bits, so a
+// result can differ from the reference's in a rounding-boundary case.
 //
 // Percentile clip (an addition, parity unpinned against the reference, pinned against the
 // oracle): the clip code is the smallest code c with #(codes <= c) >= ceil(p/100 * H*W); codes
@@ -464,7 +465,7 @@ __global__ void normalize_kernel(const float* __restrict__ src, int H, int W, in
             const int x0 = max(gx - r, 0), x1 = min(gx + r + 1, W);
             const int y0 = max(gy - r, 0), y1 = min(gy + r + 1, H);
             float mean, sd;
-            fix_stats_f64(a, b, fs, (float)((x1 - x0) * (y1 - y0)), &mean, &sd);
+            fix_stats(a, b, fs, (float)((x1 - x0) * (y1 - y0)), &mean, &sd);
             const float v = src[(size_t)gy * W + gx];
             out[(size_t)gy * W + gx] = __fdiv_rn(__fsub_rn(v, mean), __fadd_rn(sd, eps));
         }

@@ -7,7 +7,8 @@ little-endian .f32/.u8 arrays plus meta.json. This script packs each case into o
 `prepared_a`/`prepared_b` are omitted when they equal the raw frames bit for bit (cases run with
 no preprocessing and no background), and the tests then use the frames.
 
-Usage: python tests/golden/make_golden.py [reference_root]
+Usage: python tests/golden/make_golden.py <reference_root>
+   or: PIV_REFERENCE_ROOT=<reference_root> python tests/golden/make_golden.py
 """
 import json
 import os
@@ -15,7 +16,6 @@ import sys
 
 import numpy as np
 
-DEFAULT_ROOT = "/root/reference"
 CASES_REL = "swift/Tests/PIVKitTests/Fixtures/cases"
 HERE = os.path.dirname(os.path.abspath(__file__))
 
@@ -64,7 +64,10 @@ def load_case(case_dir):
 
 
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else DEFAULT_ROOT
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PIV_REFERENCE_ROOT")
+    if not root:
+        sys.exit("usage: make_golden.py <reference_root> (or set PIV_REFERENCE_ROOT): the checkout of the reference "
+                 "whose " + CASES_REL + " holds the cases")
     cases_dir = os.path.join(root, CASES_REL)
     with open(os.path.join(cases_dir, "index.json")) as f:
         names = json.load(f)
