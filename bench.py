@@ -265,7 +265,7 @@ def run_stream(args, wl):
     return 0
 
 
-def run_serving(args, wl):
+def serving_block(wl, duration, local, ranks):
     """The serving form under a Poisson load: requests of mixed sizes and window schedules are
     submitted at their arrival times to one PivServer (continuous batching); latency is submit ->
     results in host memory. vectors/s counts the final-pass vectors of all completed requests
@@ -276,13 +276,8 @@ def run_serving(args, wl):
 
     import piv_b200 as P
     from piv_b200 import synthetic as S
-    from piv_b200.replicas import Ranks
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    ranks = Ranks(backend="nccl", device=torch.device("cuda", local))
     # replicas: every rank serves its own Poisson stream on its own GPU
     rng = np.random.default_rng(wl["seed"] + 101 * ranks.rank)
-    duration = args.duration if args.duration else wl["duration"]
     pool = {}
     for si, (h, w) in enumerate(wl["sizes"]):
         for j in range(wl["pool"]):
@@ -320,8 +315,7 @@ def run_serving(args, wl):
 
     wt = th.Thread(target=waiter)
     wt.start()
-    gpu_uuid = str(torch.cuda.get_device_properties(local).uuid)
-    sampler = ClockSampler(gpu_uuid if gpu_uuid.startswith("GPU-") else f"GPU-{gpu_uuid}")
+    sampler = _clock_sampler(torch, torch.device("cuda", local))
     sampler.start()
     s0 = sv.stats()
     ranks.barrier()
@@ -343,19 +337,36 @@ def run_serving(args, wl):
     n_all = int(ranks.sum(n))
     launches = ranks.sum(s1["kernel_launches"] - s0["kernel_launches"])
     lat_a = np.concatenate([np.asarray(x) for x in ranks.gather(lat)])
-    line = {"metric": METRIC, "value": total_vec / span, "unit": "vectors/s", "n_gpus": ranks.world, "steps": n_all,
-            "warmup": 9, "ms_per_step": 1e3 * span / max(n_all, 1), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": wl["name"], "requests": n_all, "duration_s": duration,
-                       "rate_per_s": wl["rate"] * ranks.world, "parallelism": f"replicas x{ranks.world}"},
+    return {"workload": wl["name"], "value": total_vec / span, "unit": "vectors/s", "requests": n_all,
+            "duration_s": duration, "rate_per_s": wl["rate"] * ranks.world, "span_s": span,
             "latency_ms": {"p50": float(np.percentile(lat_a, 50)), "p90": float(np.percentile(lat_a, 90)),
-                           "p99": float(np.percentile(lat_a, 99)), "max": float(lat_a.max()), "mean": float(lat_a.mean())},
+                           "p99": float(np.percentile(lat_a, 99)), "max": float(lat_a.max()),
+                           "mean": float(lat_a.mean())},
             "achieved_rate_per_s": n_all / span,
-            "e2e": {"value": total_vec / span, "unit": "vectors/s",
-                    "h2d_bytes_per_step": int(np.mean([pool[(si, pj)][0].nbytes * 2 for si, _, pj in kinds])),
-                    "d2h_bytes_per_step": int(np.mean([vec[(si, ci)] * 13 for si, ci, _ in kinds]))},
-            "gpu_launches": int(launches), "server_steps": int(s1["steps"] - s0["steps"]),
-            "clocks": clocks}
+            "h2d_bytes_per_request": int(np.mean([pool[(si, pj)][0].nbytes * 2 for si, _, pj in kinds])),
+            "d2h_bytes_per_request": int(np.mean([vec[(si, ci)] * 13 for si, ci, _ in kinds])),
+            "gpu_launches": int(launches), "server_steps": int(s1["steps"] - s0["steps"]), "clocks": clocks}
+
+
+def run_serving(args, wl):
+    """The serving workload on its own: one JSON line whose value is the served vectors/s."""
+    import torch
+
+    from piv_b200.replicas import Ranks
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    ranks = Ranks(backend="nccl", device=torch.device("cuda", local))
+    duration = args.duration if args.duration else wl["duration"]
+    r = serving_block(wl, duration, local, ranks)
+    line = {"metric": METRIC, "value": r["value"], "unit": "vectors/s", "n_gpus": ranks.world, "steps": r["requests"],
+            "warmup": 9, "ms_per_step": 1e3 * r["span_s"] / max(r["requests"], 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": wl["name"], "requests": r["requests"], "duration_s": duration,
+                       "rate_per_s": r["rate_per_s"], "parallelism": f"replicas x{ranks.world}"},
+            "latency_ms": r["latency_ms"], "achieved_rate_per_s": r["achieved_rate_per_s"],
+            "e2e": {"value": r["value"], "unit": "vectors/s", "h2d_bytes_per_step": r["h2d_bytes_per_request"],
+                    "d2h_bytes_per_step": r["d2h_bytes_per_request"]},
+            "gpu_launches": r["gpu_launches"], "server_steps": r["server_steps"], "clocks": r["clocks"]}
     if ranks.rank == 0:
         print(json.dumps(line), flush=True)
     ranks.close()
@@ -570,12 +581,17 @@ def cpu_baseline(wl, a, b, budget_s=10.0, crop=1024, single_s=0.0):
     return out
 
 
-def accuracy_vs_fp64(wl, a, b, an, crop=1024):
+def accuracy_vs_fp64(wl, a, b, an, crop=1024, cache=None):
     """The GPU's final field on a crop of the pair against the FP64 oracle's (every correlation
-    step in f64): RMS and max |d| over cells both mark valid, and the share of equal flags."""
-    import piv_b200 as P
+    step in f64): RMS and max |d| over cells both mark valid, and the share of equal flags.
+    `cache` (a dict) keeps the oracle's field for further calls on the same crop."""
     O, fa, fb, cfg, ch, cw, ba, bb = _oracle_inputs(wl, a, b, crop)
-    ref, _, _ = O.analyze(cfg, fa, fb, ba, bb, mode=O.FP64)
+    if cache is not None and "fp64" in cache:
+        ref = cache["fp64"]
+    else:
+        ref, _, _ = O.analyze(cfg, fa, fb, ba, bb, mode=O.FP64)
+        if cache is not None:
+            cache["fp64"] = ref
     pre, bg = preprocess_config(wl), _crop_background(wl, a, b, ch, cw)
     r = an.analyze(an.prepare(np.ascontiguousarray(a[:ch, :cw]), pre, background=bg),
                    an.prepare(np.ascontiguousarray(b[:ch, :cw]), pre, background=bg))
@@ -712,6 +728,213 @@ def run_reference_serving(args, wl):
     return 0
 
 
+def batched_figure(args, P, torch, wl, an, pre, pairs_host, bg_ptr, dev, ranks):
+    """The batching form: K independent pairs of the ring per CUDA-graph replay (PivBatch), inputs
+    resident on the device; K pairs of samples exceed L2, so every replay reads them from HBM.
+    One background image (that of the first pair) serves the whole batch."""
+    a0 = pairs_host[0][0]
+    h, w = a0.shape
+    nvec = len(an.output_grid(h, w))
+    K = int(wl["batch_pairs"])
+    bt = P.PivBatch(an, h, w, K, sequential=False, dtype=a0.dtype, cfg=pre)
+    bt.set_background(bg_ptr)
+    frames = np.stack([x for k in range(K) for x in pairs_host[k % len(pairs_host)]])
+    tview = _torch_view(frames.reshape(-1))
+    slab = torch.as_tensor(_DeviceBuffer(bt.input_device(), tview.size, "<i2" if a0.dtype == np.uint16 else "|u1"),
+                           device=dev)
+    slab.copy_(torch.from_numpy(tview).to(dev))
+    torch.cuda.synchronize()
+    bstream = torch.cuda.ExternalStream(bt.stream(), device=dev)
+    for _ in range(max(args.warmup, 3)):
+        bt.run()
+    bt.sync()
+    runs = max(5, args.steps // 10)
+    sampler = _clock_sampler(torch, dev)
+    sampler.start()
+    time.sleep(0.2)
+    ranks.barrier()
+    ev_start, ev_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev_start.record(bstream)
+    for _ in range(runs):
+        bt.run()
+    ev_end.record(bstream)
+    ev_end.synchronize()
+    clocks = sampler.stop()
+    bms = ranks.max(ev_start.elapsed_time(ev_end)) / runs
+    out = {"workload": wl["name"], "pairs_per_graph": K, "value": ranks.world * K * nvec / (bms * 1e-3),
+           "unit": "vectors/s", "ms_per_pair": bms / K, "runs": runs, "gpu_launches": int(bt.kernels() * runs),
+           "clocks": clocks,
+           "how": f"{K} independent pairs per CUDA-graph replay of PivBatch (preparation of all frames and every "
+                  f"pass), {frames.nbytes / 2**20:.0f} MiB of samples resident on the device"}
+    del slab
+    bt.close()
+    return out
+
+
+def _clock_sampler(torch, dev):
+    gpu_uuid = str(torch.cuda.get_device_properties(dev).uuid)
+    return ClockSampler(gpu_uuid if gpu_uuid.startswith("GPU-") else f"GPU-{gpu_uuid}")
+
+
+def device_background(P, torch, an, pairs_dev, dtype_code, h, w, dev):
+    """The background of each pair, the per-pixel minimum over its two frames
+    (BackgroundEstimator, preprocess.rs:47-72), estimated on the device before the timed steps as
+    the reference estimates it before its pair loop. Returns the device images."""
+    import ctypes
+    lib = P.load_library()
+    out = []
+    for ta, tb in pairs_dev:
+        stack = torch.stack([ta, tb])
+        bgk = torch.empty((h, w), dtype=torch.float32, device=dev)
+        torch.cuda.synchronize()
+        P.api._check(lib.piv_background_device(an._h, ctypes.c_void_p(stack.data_ptr()), dtype_code, 2, h, w, 0,
+                                               ctypes.c_void_p(bgk.data_ptr())))
+        torch.cuda.synchronize()
+        out.append(bgk)
+    return out
+
+
+def c2_batched_block(args, P, torch, dev, local, ranks):
+    """c2 as configured (1024x1024 u16 Lamb-Oseen pair, min background, 99th-percentile clip,
+    deformed 64 -> 32 -> 16 px at 50 %) in the batching form, for the default run's line."""
+    wl = dict(WORKLOADS["c2"])
+    wl["name"] += ", deformed windows"
+    a0, b0 = make_inputs(wl, seed_offset=ranks.rank)
+    ring = input_ring(a0, b0)
+    h, w = a0.shape
+    dtype_code = P.api._dtype_code(a0)
+    pairs_dev = [(torch.from_numpy(_torch_view(a)).to(dev), torch.from_numpy(_torch_view(b)).to(dev)) for a, b in ring]
+    an = P.PivAnalyzer(piv_config(wl), device=local)
+    pre = preprocess_config(wl)
+    bgs = device_background(P, torch, an, pairs_dev[:1], dtype_code, h, w, dev)
+    fa, fb = an.frame(h, w), an.frame(h, w)
+    fa.prepare_device(pairs_dev[0][0].data_ptr(), dtype_code, pre, bgs[0].data_ptr())
+    fb.prepare_device(pairs_dev[0][1].data_ptr(), dtype_code, pre, bgs[0].data_ptr())
+    tuned = an.autotune(fa, fb) if not args.no_autotune else {}
+    out = batched_figure(args, P, torch, wl, an, pre, ring, bgs[0].data_ptr(), dev, ranks)
+    out["autotuned_variants"] = tuned
+    an.close()
+    return out
+
+
+def tc_tiers_block(args, P, torch, wl, pre, pairs_dev, bg_ptrs, dtype_code, dev, local, h, w, a0, b0, ranks,
+                   fp64_cache):
+    """The split-precision tensor-core tiers on this workload, timed by the same device-resident
+    step loop as the headline, with their error against the FP64 oracle."""
+    out = {}
+    for prec in ("bf16x3", "fp16x3"):
+        wlp = dict(wl, precision=prec)
+        loop = SlotLoop(P, torch, piv_config(wlp), pre, pairs_dev, bg_ptrs, dtype_code, dev, local, h, w)
+        tuned = loop.autotune() if not args.no_autotune else {}
+        for i in range(args.warmup):
+            loop.step(i)
+        torch.cuda.synchronize()
+        steps = max(10, args.steps // 2)
+        sampler = _clock_sampler(torch, dev)
+        sampler.start()
+        time.sleep(0.2)
+        ranks.barrier()
+        l0 = loop.launches()
+        ms = ranks.max(loop.run(steps))
+        launches = loop.launches() - l0
+        clocks = sampler.stop()
+        out[prec] = {"value": ranks.world * steps * loop.nvec / (ms * 1e-3), "unit": "vectors/s",
+                     "ms_per_pair": ms / steps, "steps": steps, "gpu_launches": int(launches), "clocks": clocks,
+                     "autotuned_variants": tuned,
+                     "accuracy": accuracy_vs_fp64(wlp, a0, b0, loop.slots[0][0], cache=fp64_cache)}
+        loop.close()
+    return out
+
+
+class SlotLoop:
+    """The device-resident step loop. Two slots, each an analyzer (workspace and pass graph) with
+    its own frames: the frames of step i+1 are prepared on a preparation stream while step i is
+    analysed on the analysis stream, as PivPipeline does for host frames; analyses stay in order
+    on one stream. Step i takes pair i % len(ring) of the device-resident ring, prepares both
+    frames from its raw samples and analyses them into device buffers. Repeated calls on a slot's
+    frames replay its captured pass graph."""
+
+    def __init__(self, P, torch, cfg, pre, pairs_dev, bg_ptrs, dtype_code, dev, local, h, w):
+        self.torch = torch
+        self.pre, self.pairs_dev, self.bg_ptrs, self.dtype_code = pre, pairs_dev, bg_ptrs, dtype_code
+        self.stream = torch.cuda.Stream(device=dev)
+        self.prep_stream = torch.cuda.Stream(device=dev)
+        self.slots = []
+        for _ in range(2):
+            an = P.PivAnalyzer(cfg, device=local)
+            an.set_stream(self.stream.cuda_stream)
+            self.slots.append((an, an.frame(h, w), an.frame(h, w)))
+        self.prepared = [torch.cuda.Event() for _ in self.slots]
+        self.analysed = [torch.cuda.Event() for _ in self.slots]
+        for ev in self.analysed:
+            ev.record(self.stream)
+        self.nvec = len(self.slots[0][0].output_grid(h, w))
+        self.out = ([torch.empty(self.nvec, device=dev, dtype=torch.float32) for _ in range(3)]
+                    + [torch.empty(self.nvec, device=dev, dtype=torch.uint8),
+                       torch.empty(8, device=dev, dtype=torch.int64)])
+
+    def step(self, i):
+        k = i % len(self.pairs_dev)
+        ta, tb = self.pairs_dev[k]
+        s_an, s_fa, s_fb = self.slots[i % 2]
+        # the slot's frames are free once its previous pair has been analysed
+        self.prep_stream.wait_event(self.analysed[i % 2])
+        s_an.set_stream(self.prep_stream.cuda_stream)
+        s_fa.prepare_device(ta.data_ptr(), self.dtype_code, self.pre, self.bg_ptrs[k])
+        s_fb.prepare_device(tb.data_ptr(), self.dtype_code, self.pre, self.bg_ptrs[k])
+        self.prepared[i % 2].record(self.prep_stream)
+        self.stream.wait_event(self.prepared[i % 2])
+        s_an.set_stream(self.stream.cuda_stream)
+        s_an.analyze_device(s_fa, s_fb, *[t.data_ptr() for t in self.out])
+        self.analysed[i % 2].record(self.stream)
+
+    def autotune(self):
+        """Launch-geometry (and, for the split precisions, FP32-or-tensor-core) autotuning of both
+        slots on the first pair; results are identical across FP32 variants."""
+        tuned = {}
+        ta, tb = self.pairs_dev[0]
+        for s_an, s_fa, s_fb in self.slots:
+            s_fa.prepare_device(ta.data_ptr(), self.dtype_code, self.pre, self.bg_ptrs[0])
+            s_fb.prepare_device(tb.data_ptr(), self.dtype_code, self.pre, self.bg_ptrs[0])
+            tuned = s_an.autotune(s_fa, s_fb) or tuned
+        return tuned
+
+    def launches(self):
+        return sum(s[0].launches() for s in self.slots)
+
+    def run(self, steps):
+        """`steps` steps between two events on the analysis stream (the preparation stream waits
+        for the first); returns the elapsed milliseconds."""
+        torch = self.torch
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(self.stream)
+        self.prep_stream.wait_event(e0)
+        for i in range(steps):
+            self.step(i)
+        e1.record(self.stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    def pass_times(self, steps, npass):
+        """The same steps with CUDA events around every correlation launch (eager launches):
+        per pass, (total ms, launches) over both slots."""
+        for s_an, _, _ in self.slots:
+            s_an.set_profiling(True)
+            for p in range(npass):
+                s_an.profile(p)  # reset
+        for i in range(steps):
+            self.step(i)
+        self.torch.cuda.synchronize()
+        corr = [tuple(map(sum, zip(*(s[0].profile(p) for s in self.slots)))) for p in range(npass)]
+        for s_an, _, _ in self.slots:
+            s_an.set_profiling(False)
+        return corr
+
+    def close(self):
+        for s_an, _, _ in self.slots:
+            s_an.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -721,6 +944,10 @@ def main():
     ap.add_argument("--workload", default="c5", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="c5 at N=1: skip the tensor-core tiers, the c2 batched figure and the c4 serving run")
+    ap.add_argument("--serving-s", type=float, default=10.0,
+                    help="c5 at N=1: seconds of Poisson arrivals in the short c4 serving run")
     ap.add_argument("--precision", choices=["fp32", "bf16x3", "fp16x3"], default=None,
                     help="correlation arithmetic: FP32 FFTs, or split-BF16 tensor-core DFTs (16 and 32 px windows)")
     ap.add_argument("--deform", type=int, choices=[0, 1], default=None,
@@ -773,33 +1000,15 @@ def main():
     pairs_dev = [(torch.from_numpy(_torch_view(a)).to(dev), torch.from_numpy(_torch_view(b)).to(dev))
                  for a, b in pairs_host]
 
-    an = P.PivAnalyzer(piv_config(wl), device=local)
-    stream = torch.cuda.Stream(device=dev)
-    an.set_stream(stream.cuda_stream)
-    fa, fb = an.frame(h, w), an.frame(h, w)
-    # Two slots, each an analyzer (workspace and pass graph) with its own frames: the frames of
-    # step i+1 are prepared on prep_stream while step i is analysed on `stream`, as PivPipeline
-    # does for host frames. Analyses stay in order on one stream.
-    an2 = P.PivAnalyzer(piv_config(wl), device=local)
-    an2.set_stream(stream.cuda_stream)
-    fa2, fb2 = an2.frame(h, w), an2.frame(h, w)
-    slots = [(an, fa, fb), (an2, fa2, fb2)]
-    prep_stream = torch.cuda.Stream(device=dev)
-    prepared = [torch.cuda.Event() for _ in slots]
-    analysed = [torch.cuda.Event() for _ in slots]
-    for ev in analysed:
-        ev.record(stream)
-    g = an.output_grid(h, w)
-    nvec = len(g)
-    out_dx = torch.empty(nvec, device=dev, dtype=torch.float32)
-    out_dy = torch.empty_like(out_dx)
-    out_ppr = torch.empty_like(out_dx)
-    out_fl = torch.empty(nvec, device=dev, dtype=torch.uint8)
-    out_sum = torch.empty(8, device=dev, dtype=torch.int64)
     pre = preprocess_config(wl)
     lib = P.load_library()
     import ctypes
     bg_devs, bg_ptrs, bg_hosts = [], [None] * n_ring, [None] * n_ring
+    loop = SlotLoop(P, torch, piv_config(wl), pre, pairs_dev, bg_ptrs, dtype_code, dev, local, h, w)
+    an, fa, fb = loop.slots[0]
+    stream = loop.stream
+    g = an.output_grid(h, w)
+    nvec = len(g)
     if wl.get("background") == "min":
         # the background of each pair, the per-pixel minimum over its two frames
         # (BackgroundEstimator, preprocess.rs:47-72), estimated before the timed steps as the
@@ -807,44 +1016,20 @@ def main():
         for k, (ta, tb) in enumerate(pairs_dev):
             stack = torch.stack([ta, tb])
             bgk = torch.empty((h, w), dtype=torch.float32, device=dev)
+            torch.cuda.synchronize()
             P.api._check(lib.piv_background_device(an._h, ctypes.c_void_p(stack.data_ptr()), dtype_code, 2, h, w, 0,
                                                    ctypes.c_void_p(bgk.data_ptr())))
+            torch.cuda.synchronize()
             bg_devs.append(bgk)
             bg_ptrs[k] = bgk.data_ptr()
-        torch.cuda.synchronize()
         bg_hosts = [b.cpu().numpy() for b in bg_devs[:2]] + [None] * (n_ring - 2)
     bg_ptr = bg_ptrs[0]
-
-    def step(i):
-        k = i % n_ring
-        ta, tb = pairs_dev[k]
-        s_an, s_fa, s_fb = slots[i % 2]
-        # the slot's frames are free once its previous pair has been analysed
-        prep_stream.wait_event(analysed[i % 2])
-        s_an.set_stream(prep_stream.cuda_stream)
-        s_fa.prepare_device(ta.data_ptr(), dtype_code, pre, bg_ptrs[k])
-        s_fb.prepare_device(tb.data_ptr(), dtype_code, pre, bg_ptrs[k])
-        prepared[i % 2].record(prep_stream)
-        stream.wait_event(prepared[i % 2])
-        s_an.set_stream(stream.cuda_stream)
-        s_an.analyze_device(s_fa, s_fb, out_dx.data_ptr(), out_dy.data_ptr(), out_ppr.data_ptr(), out_fl.data_ptr(),
-                            out_sum.data_ptr())
-        analysed[i % 2].record(stream)
-
-    # launch-geometry autotuning of both slots on the first pair (results are identical across
-    # variants)
-    tuned = {}
-    for s_an, s_fa, s_fb in slots:
-        s_fa.prepare_device(pairs_dev[0][0].data_ptr(), dtype_code, pre, bg_ptr)
-        s_fb.prepare_device(pairs_dev[0][1].data_ptr(), dtype_code, pre, bg_ptr)
-        t = s_an.autotune(s_fa, s_fb) if not args.no_autotune else {}
-        tuned = tuned or t
+    tuned = loop.autotune() if not args.no_autotune else {}
     for i in range(args.warmup):
-        step(i)
+        loop.step(i)
     stream.synchronize()
 
     # ---------------------------------------------------------------- timed: device-resident
-    # (repeated calls on the same frames replay the analyzer's captured pass graph)
     npass = len(pass_windows(wl))
     ranks.barrier()
     torch.cuda.synchronize()
@@ -852,31 +1037,14 @@ def main():
     sampler = ClockSampler(gpu_uuid if gpu_uuid.startswith("GPU-") else f"GPU-{gpu_uuid}")
     sampler.start()
     time.sleep(0.3)
-    l0 = an.launches() + an2.launches()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    prep_stream.wait_event(e0)
-    for i in range(args.steps):
-        step(i)
-    e1.record(stream)
-    e1.synchronize()
+    l0 = loop.launches()
+    ms = loop.run(args.steps)
     torch.cuda.synchronize()
-    launches = an.launches() + an2.launches() - l0
+    launches = loop.launches() - l0
     clocks = sampler.stop()
-    ms = e0.elapsed_time(e1)
     ms_max = ranks.max(ms)
-    # the same steps again with CUDA events around every correlation launch (eager launches):
-    # per-pass kernel times for the roofline
-    for s_an, _, _ in slots:
-        s_an.set_profiling(True)
-        for p in range(npass):
-            s_an.profile(p)  # reset
-    for i in range(args.steps):
-        step(i)
-    torch.cuda.synchronize()
-    corr = [tuple(map(sum, zip(an.profile(p), an2.profile(p)))) for p in range(npass)]
-    for s_an, _, _ in slots:
-        s_an.set_profiling(False)
+    # per-pass kernel times for the roofline, from a second loop of the same steps
+    corr = loop.pass_times(args.steps, npass)
     value = world * args.steps * nvec / (ms_max * 1e-3)
 
     # ---------------------------------------------------------------- timed: end to end (host buffers)
@@ -951,36 +1119,7 @@ def main():
     # ---------------------------------------------------------------- batched form (optional)
     batched = None
     if wl.get("batch_pairs"):
-        # K independent pairs of the ring per CUDA-graph replay (PivBatch), inputs resident on the
-        # device; K pairs of samples exceed L2, so every replay reads them from HBM
-        K = int(wl["batch_pairs"])
-        bt = P.PivBatch(an, h, w, K, sequential=False, dtype=a0.dtype, cfg=pre)
-        bt.set_background(bg_ptr)  # one background image for the batch (that of the first pair)
-        frames = np.stack([x for k in range(K) for x in pairs_host[k % n_ring]])
-        tview = _torch_view(frames.reshape(-1))
-        slab = torch.as_tensor(_DeviceBuffer(bt.input_device(), tview.size, "<i2" if a0.dtype == np.uint16 else "|u1"),
-                               device=dev)
-        slab.copy_(torch.from_numpy(tview).to(dev))
-        torch.cuda.synchronize()
-        bstream = torch.cuda.ExternalStream(bt.stream(), device=dev)
-        for _ in range(max(args.warmup, 3)):
-            bt.run()
-        bt.sync()
-        runs = max(5, args.steps // 10)
-        ranks.barrier()
-        ev_start, ev_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        ev_start.record(bstream)
-        for _ in range(runs):
-            bt.run()
-        ev_end.record(bstream)
-        ev_end.synchronize()
-        bms = ranks.max(ev_start.elapsed_time(ev_end)) / runs
-        batched = {"pairs_per_graph": K, "value": world * K * nvec / (bms * 1e-3), "unit": "vectors/s",
-                   "ms_per_pair": bms / K, "runs": runs,
-                   "how": f"{K} independent pairs per CUDA-graph replay of PivBatch (preparation of all frames and "
-                          f"every pass), {frames.nbytes / 2**20:.0f} MiB of samples resident on the device"}
-        del slab
-        bt.close()
+        batched = batched_figure(args, P, torch, wl, an, pre, pairs_host, bg_ptr, dev, ranks)
 
     # ---------------------------------------------------------------- roofline (correlation kernels)
     pw = pass_windows(wl)
@@ -1031,13 +1170,22 @@ def main():
             "gpu_launches": int(launches), "roofline": roof, "clocks": clocks, "autotuned_variants": tuned}
     if batched:
         line["batched"] = batched
+    if world == 1 and not args.no_extras and args.workload == "c5":
+        # the forms the metric names beside the plain FP32 path: the split-precision tensor-core
+        # tiers of this workload, c2 in the batching form, and a short c4 serving run
+        fp64_cache = {}
+        line["accuracy"] = accuracy_vs_fp64(wl, a0, b0, an, cache=fp64_cache)
+        line["tc"] = tc_tiers_block(args, P, torch, wl, pre, pairs_dev, bg_ptrs, dtype_code, dev, local, h, w, a0, b0,
+                                    ranks, fp64_cache)
+        line["batched"] = c2_batched_block(args, P, torch, dev, local, ranks)
+        line["serving"] = serving_block(dict(WORKLOADS["c4"]), args.serving_s, local, ranks)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(wl, a0, b0, single_s=4.0)
-        line["accuracy"] = accuracy_vs_fp64(wl, a0, b0, an)
+        if "accuracy" not in line:
+            line["accuracy"] = accuracy_vs_fp64(wl, a0, b0, an)
     if rank == 0:
         print(json.dumps(line), flush=True)
-    an2.close()
-    an.close()
+    loop.close()
     ranks.close()
     return 0
 

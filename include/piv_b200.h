@@ -43,7 +43,9 @@ typedef enum {
     PIV_ERR_FRAME_RATE = 4,      /* PivError::FrameRate (not produced by this library) */
     PIV_ERR_CUDA = 5,            /* a CUDA runtime call failed; see piv_last_error */
     PIV_ERR_UNSUPPORTED = 6,     /* valid for the reference, not supported by this GPU path */
-    PIV_ERR_ARGUMENT = 7         /* NULL handle or malformed argument */
+    PIV_ERR_ARGUMENT = 7,        /* NULL handle or malformed argument */
+    PIV_ERR_CANCELLED = 8,       /* serving form: the request was cancelled (piv_server_cancel) */
+    PIV_ERR_TIMEOUT = 9          /* serving form: a bounded wait ran out; nothing was lost */
 } PivStatus;
 
 /* Flag bits (field.rs:6-20). */
@@ -172,6 +174,19 @@ int32_t piv_frame_prepare_device(PivAnalyzer* an, PivFrame* f, const void* raw_d
 /* Installs an already prepared image (host) and the background-subtracted intensity used by the
  * signal mask (host; NULL = the image itself), as PIVKit's makeFrame(image:stats:) does. */
 int32_t piv_frame_set_prepared(PivAnalyzer* an, PivFrame* f, const float* image, const float* base);
+/* Installs a frame prepared on the host by the reference itself: PreparedFrame's `image` (HOST,
+ * height*width f32) and its `stats: IntegralImage` tables `sum` and `sumsq` (HOST, (height+1) x
+ * (width+1) f64 each, row-major with stride width+1, as IntegralImage::new builds them,
+ * preprocess.rs:76-103, 127-135). The tables are converted on the device to this library's exact
+ * fixed-point form with integer operations only: entries finer than the table's quantum
+ * (2^-(61 - e) for entries below 2^e) round to it, and window statistics are exact differences
+ * of the entries where IntegralImage::rect rounds each f64 subtraction, so a signal-mask
+ * decision can differ only for a window whose mean or standard deviation lies on the f32
+ * rounding boundary of its threshold. PIV_ERR_ARGUMENT for a non-finite entry. Blocking. This
+ * is the compatibility path for an unchanged PivAnalyzer::analyze(&PreparedFrame,
+ * &PreparedFrame); piv_frame_prepare from raw samples is the fast path. */
+int32_t piv_frame_set_prepared_tables(PivAnalyzer* an, PivFrame* f, const float* image, const double* sum,
+                                      const double* sumsq);
 /* Copies the prepared image back to the host. */
 int32_t piv_frame_download(PivAnalyzer* an, const PivFrame* f, float* image);
 /* Device address of the prepared image (height*width f32, row-major). */
@@ -305,15 +320,44 @@ typedef struct {
 typedef struct {
     int64_t submitted, admitted, completed, failed, queued, in_flight;
     int64_t memory_in_use_bytes, steps, kernel_launches;
+    int64_t cancelled;          /* requests that ended cancelled */
+    int64_t deferred;           /* admissions put back after a failed allocation */
+    int64_t last_step_requests; /* requests advanced by the most recent step */
+    int64_t max_step_requests;  /* most requests advanced by one step */
 } PivServerStatsC;
 int32_t piv_server_create(const PivServerConfigC* cfg, PivServer** out);
 /* Finishes the admitted and queued requests, then stops the scheduler and frees the server. */
 void piv_server_destroy(PivServer* server);
-/* Queues a request; fails at once for an invalid config or a request larger than the budget. */
+/* Queues a request; fails at once, queuing nothing, for a malformed request: an invalid config
+ * (odd or too small window, overlap outside [0, 1): PIV_ERR_CONFIG, as multipass.rs:91-119), a
+ * window larger than the image (PIV_ERR_IMAGE_TOO_SMALL, as grid.rs:27-33), an unknown dtype or
+ * NULL frames (PIV_ERR_ARGUMENT), or a request larger than the budget (PIV_ERR_UNSUPPORTED). */
 int32_t piv_server_submit(PivServer* server, const PivRequestC* request, uint64_t* id);
 /* Blocks until request `id` is done; fills its summary and its latency (submit to results in
- * host memory, milliseconds). Returns the request's own status. Each id may be waited once. */
+ * host memory, milliseconds). Returns the request's own status: PIV_OK, PIV_ERR_CANCELLED, or
+ * the error that ended it (e.g. PIV_ERR_CUDA when its device memory could not be allocated
+ * while nothing else was in flight). Each id may be waited once. */
 int32_t piv_server_wait(PivServer* server, uint64_t id, PivSummaryC* summary, double* latency_ms);
+/* piv_server_wait with a bound: PIV_ERR_TIMEOUT when the request is not done within timeout_ms
+ * (it stays pending and may be waited again). */
+int32_t piv_server_wait_timeout(PivServer* server, uint64_t id, double timeout_ms, PivSummaryC* summary,
+                                double* latency_ms);
+/* Cancels request `id`. A queued request is dropped at once; an admitted one stops at the next
+ * step boundary, its memory given back once the passes already queued for it have run. Either
+ * way its wait returns PIV_ERR_CANCELLED and its outputs are not written. A request whose last
+ * pass was already launched finishes normally. PIV_ERR_ARGUMENT for an unknown id. */
+int32_t piv_server_cancel(PivServer* server, uint64_t id);
+/* Host-side fault injection: the next `count` admissions fail as an out-of-memory allocation
+ * would, without calling the allocator. With other requests in flight the admission is put back
+ * and retried after one of them finishes (stats.deferred); with none, the request fails. */
+int32_t piv_server_fail_next_allocations(PivServer* server, int32_t count);
+/* Manual stepping (testing and external pacing): with manual != 0 the scheduler admits requests
+ * and launches steps only when piv_server_advance grants them; 0 returns to free running. */
+int32_t piv_server_set_manual(PivServer* server, int32_t manual);
+/* Grants `steps` steps (admission, then one pass of every admitted request) and blocks until the
+ * scheduler has taken them (a step with nothing to launch counts), or PIV_ERR_TIMEOUT after
+ * timeout_ms (< 0: no bound). */
+int32_t piv_server_advance(PivServer* server, int32_t steps, double timeout_ms);
 int32_t piv_server_stats(PivServer* server, PivServerStatsC* stats);
 
 /* PivAnalyzer::analyze_traced (multipass.rs:142-150, PassTrace :72-81): HOST arrays holding

@@ -11,6 +11,7 @@ LIB_PATH = os.path.join(HERE, "libpivb200.so")
 
 PIV_OK, PIV_ERR_CONFIG, PIV_ERR_SHAPE_MISMATCH, PIV_ERR_IMAGE_TOO_SMALL = 0, 1, 2, 3
 PIV_ERR_FRAME_RATE, PIV_ERR_CUDA, PIV_ERR_UNSUPPORTED, PIV_ERR_ARGUMENT = 4, 5, 6, 7
+PIV_ERR_CANCELLED, PIV_ERR_TIMEOUT = 8, 9
 PIV_DTYPE_U8, PIV_DTYPE_U16, PIV_DTYPE_F32 = 0, 1, 2
 
 # Every symbol include/piv_b200.h declares.
@@ -21,7 +22,7 @@ EXPORTS = [
     "piv_analyzer_profile", "piv_analyzer_autotune", "piv_analyzer_variant", "piv_num_variants",
     "piv_analyzer_set_variant",
     "piv_frame_create", "piv_frame_destroy", "piv_frame_prepare", "piv_frame_prepare_device",
-    "piv_frame_set_prepared", "piv_frame_download", "piv_frame_image_device", "piv_background_device",
+    "piv_frame_set_prepared", "piv_frame_set_prepared_tables", "piv_frame_download", "piv_frame_image_device", "piv_background_device",
     "piv_analyze", "piv_analyze_device", "piv_analyze_traced", "piv_analyze_batch_device",
     "piv_batch_create", "piv_batch_destroy", "piv_batch_input_device", "piv_batch_input_bytes", "piv_batch_run",
     "piv_batch_sync", "piv_batch_outputs_device", "piv_batch_run_host", "piv_batch_kernels", "piv_batch_stream",
@@ -32,6 +33,8 @@ EXPORTS = [
     "piv_validate_field", "piv_flow_stats_device", "piv_temporal_smooth_device", "piv_spatial_smooth_device",
     "piv_tc_selftest", "piv_validate_field_noalloc",
     "piv_server_create", "piv_server_destroy", "piv_server_submit", "piv_server_wait", "piv_server_stats",
+    "piv_server_wait_timeout", "piv_server_cancel", "piv_server_fail_next_allocations", "piv_server_set_manual",
+    "piv_server_advance",
 ]
 
 
@@ -99,7 +102,8 @@ class PivRequestC(ctypes.Structure):
 
 class PivServerStatsC(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int64) for n in ("submitted", "admitted", "completed", "failed", "queued", "in_flight",
-                                                "memory_in_use_bytes", "steps", "kernel_launches")]
+                                                "memory_in_use_bytes", "steps", "kernel_launches", "cancelled",
+                                                "deferred", "last_step_requests", "max_step_requests")]
 
 
 _lib = None
@@ -139,6 +143,7 @@ def load():
         "piv_frame_prepare": ([vp, vp, vp, i32, P(PivPreprocessC), vp], i32),
         "piv_frame_prepare_device": ([vp, vp, vp, i32, P(PivPreprocessC), vp], i32),
         "piv_frame_set_prepared": ([vp, vp, vp, vp], i32),
+        "piv_frame_set_prepared_tables": ([vp, vp, vp, vp, vp], i32),
         "piv_frame_download": ([vp, vp, vp], i32),
         "piv_frame_image_device": ([vp], vp),
         "piv_background_device": ([vp, vp, i32, i64, i64, i64, i32, vp], i32),
@@ -182,6 +187,11 @@ def load():
         "piv_server_submit": ([vp, P(PivRequestC), P(ctypes.c_uint64)], i32),
         "piv_server_wait": ([vp, ctypes.c_uint64, P(PivSummaryC), P(ctypes.c_double)], i32),
         "piv_server_stats": ([vp, P(PivServerStatsC)], i32),
+        "piv_server_wait_timeout": ([vp, ctypes.c_uint64, ctypes.c_double, P(PivSummaryC), P(ctypes.c_double)], i32),
+        "piv_server_cancel": ([vp, ctypes.c_uint64], i32),
+        "piv_server_fail_next_allocations": ([vp, i32], i32),
+        "piv_server_set_manual": ([vp, i32], i32),
+        "piv_server_advance": ([vp, i32, ctypes.c_double], i32),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)

@@ -46,6 +46,14 @@ class UnsupportedError(PivError):
     pass
 
 
+class CancelledError(PivError):
+    """The serving form's request was cancelled (no counterpart in the reference)."""
+
+
+class TimeoutError(PivError):  # noqa: A001 - the library's status, not the builtin
+    """A bounded wait of the serving form ran out; the request is still pending."""
+
+
 def _check(status):
     if status == _lib.PIV_OK:
         return
@@ -56,6 +64,8 @@ def _check(status):
         _lib.PIV_ERR_IMAGE_TOO_SMALL: ImageTooSmallError,
         _lib.PIV_ERR_CUDA: CudaError,
         _lib.PIV_ERR_UNSUPPORTED: UnsupportedError,
+        _lib.PIV_ERR_CANCELLED: CancelledError,
+        _lib.PIV_ERR_TIMEOUT: TimeoutError,
     }.get(status, PivError)
     raise cls(msg)
 
@@ -282,6 +292,19 @@ class PreparedFrame:
         image = np.ascontiguousarray(image, dtype=np.float32)
         base = None if base is None else np.ascontiguousarray(base, dtype=np.float32)
         _check(_lib.load().piv_frame_set_prepared(self.analyzer._h, self._h, _ptr(image), _ptr(base)))
+        return self
+
+    def set_prepared_tables(self, image, sum_table, sumsq_table):
+        """The reference's own PreparedFrame (preprocess.rs:127-135): the conditioned image and
+        its IntegralImage tables ((H+1) x (W+1) f64, preprocess.rs:84-103)."""
+        image = np.ascontiguousarray(image, dtype=np.float32)
+        t1 = np.ascontiguousarray(sum_table, dtype=np.float64)
+        t2 = np.ascontiguousarray(sumsq_table, dtype=np.float64)
+        shape = (self.height + 1, self.width + 1)
+        if image.shape != (self.height, self.width) or t1.shape != shape or t2.shape != shape:
+            raise ShapeMismatchError(f"image {image.shape} and tables {t1.shape}, {t2.shape} for a "
+                                     f"{(self.height, self.width)} frame")
+        _check(_lib.load().piv_frame_set_prepared_tables(self.analyzer._h, self._h, _ptr(image), _ptr(t1), _ptr(t2)))
         return self
 
     @property
@@ -704,12 +727,39 @@ class PivServer:
         self._pending[rid.value] = (a, b, out, g, cc)
         return rid.value
 
-    def wait(self, ticket):
-        a, b, out, g, cc = self._pending.pop(ticket)
+    def wait(self, ticket, timeout_ms: Optional[float] = None):
+        """(PairResult, latency ms) of the request. With timeout_ms, raises TimeoutError if it is
+        not done by then (the ticket stays valid); raises CancelledError for a cancelled one."""
         s = _lib.PivSummaryC()
         lat = ctypes.c_double()
-        _check(_lib.load().piv_server_wait(self._h, ctypes.c_uint64(ticket), ctypes.byref(s), ctypes.byref(lat)))
+        if timeout_ms is None:
+            st = _lib.load().piv_server_wait(self._h, ctypes.c_uint64(ticket), ctypes.byref(s), ctypes.byref(lat))
+        else:
+            st = _lib.load().piv_server_wait_timeout(self._h, ctypes.c_uint64(ticket), float(timeout_ms),
+                                                     ctypes.byref(s), ctypes.byref(lat))
+            if st == _lib.PIV_ERR_TIMEOUT:
+                _check(st)
+        # the request is finished (or failed): its host buffers may go
+        a, b, out, g, cc = self._pending.pop(ticket)
+        _check(st)
         return PairResult(VectorField(g, out[0], out[1], out[2], out[3]), ValidationSummary._from_c(s)), lat.value
+
+    def cancel(self, ticket):
+        """Cancels a request: a queued one at once, an admitted one at the next step boundary.
+        Its wait then raises CancelledError; a request already finishing keeps its result."""
+        _check(_lib.load().piv_server_cancel(self._h, ctypes.c_uint64(ticket)))
+
+    def fail_next_allocations(self, count: int):
+        """Host-side fault injection: the next `count` admissions fail as out-of-memory."""
+        _check(_lib.load().piv_server_fail_next_allocations(self._h, int(count)))
+
+    def set_manual(self, manual: bool):
+        """Manual stepping: admission and steps happen only when advance() grants them."""
+        _check(_lib.load().piv_server_set_manual(self._h, int(bool(manual))))
+
+    def advance(self, steps: int = 1, timeout_ms: float = 60000.0):
+        """Grants `steps` scheduler steps and waits until they have been taken."""
+        _check(_lib.load().piv_server_advance(self._h, int(steps), float(timeout_ms)))
 
     def stats(self):
         s = _lib.PivServerStatsC()

@@ -4,6 +4,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -864,6 +865,40 @@ int32_t piv_frame_set_prepared(PivAnalyzer* an, PivFrame* f, const float* image,
     an->launches += nl;
     f->stats_valid = true;
     CUDA_TRY(cudaStreamSynchronize(an->cur));
+    return PIV_OK;
+}
+
+int32_t piv_frame_set_prepared_tables(PivAnalyzer* an, PivFrame* f, const float* image, const double* sum,
+                                      const double* sumsq) {
+    if (!an || !f || !image || !sum || !sumsq) return fail(PIV_ERR_ARGUMENT, "null argument");
+    if (!f->words) return fail(PIV_ERR_ARGUMENT, "frame has no scratch");
+    int st = use_device(an);
+    if (st) return st;
+    const size_t n = (size_t)f->H * (size_t)f->W;
+    const size_t cells = (size_t)(f->H + 1) * (size_t)(f->W + 1);
+    CUDA_TRY(cudaMemcpyAsync(f->image, image, sizeof(float) * n, cudaMemcpyHostToDevice, an->cur));
+    f->nonneg = false;  // unknown: statistics are always used
+    st = alloc_stats(f);
+    if (st) return st;
+    // the f64 tables land in the int64 tables' storage (8 bytes per entry) and are converted there
+    static_assert(sizeof(double) == sizeof(long long), "8-byte entries");
+    CUDA_TRY(cudaMemcpyAsync(f->sum, sum, sizeof(double) * cells, cudaMemcpyHostToDevice, an->cur));
+    CUDA_TRY(cudaMemcpyAsync(f->sumsq, sumsq, sizeof(double) * cells, cudaMemcpyHostToDevice, an->cur));
+    unsigned long long* maxbits2 = reinterpret_cast<unsigned long long*>(f->words);  // words[0..3]
+    unsigned int* nonfinite = f->words + 4;
+    int nl = 0;
+    CUDA_TRY(launch_tables_to_fixed(f->sum, f->sumsq, (int)f->H, (int)f->W, f->scales, maxbits2, nonfinite, an->cur,
+                                    &nl));
+    an->launches += nl;
+    unsigned int bad = 0;
+    CUDA_TRY(cudaMemcpyAsync(&bad, nonfinite, sizeof(bad), cudaMemcpyDeviceToHost, an->cur));
+    CUDA_TRY(cudaStreamSynchronize(an->cur));
+    f->base = f->image;  // the tables stand for the base image, which is not needed itself
+    if (bad) {
+        f->stats_valid = false;
+        return fail(PIV_ERR_ARGUMENT, "the integral tables hold a non-finite entry");
+    }
+    f->stats_valid = true;
     return PIV_OK;
 }
 
@@ -1825,6 +1860,7 @@ struct Request {
     cudaEvent_t done_ev = nullptr;
     bool final_launched = false;
     bool done = false;
+    std::atomic<bool> cancel{false};  // set by piv_server_cancel; read by the scheduler
     int status = PIV_OK;
     std::string error;
     Clock::time_point t_submit, t_done;
@@ -1865,23 +1901,43 @@ struct PivServer {
     PivServerStatsC stats{};
     int variant[2][129] = {};
     std::vector<cudaEvent_t> step_events;  // completion of recent steps (bounded run-ahead)
+    // Admission waits for a retirement after an allocation failed while requests were in flight.
+    bool admission_blocked = false;
+    // Host-side fault injection: the next fail_allocs admissions fail as an out-of-memory
+    // allocation would, without calling the allocator.
+    int fail_allocs = 0;
+    // Manual stepping: the scheduler admits and launches only while granted steps remain.
+    bool manual = false;
+    int64_t granted = 0, stepped = 0;
+    std::condition_variable cv_step;
 
     void loop();
-    bool admit_locked(Request* r, std::string* err);
+    int admit(Request* r, std::string* err);
     void launch_step(std::vector<Request*>& work);
+    void cancel_active();
     void retire();
 };
 
 namespace {
 
+constexpr int kAdmitOutOfMemory = -1;
+
 // Allocates the request's device memory on the server stream and queues the uploads and frame
-// preparation (preprocess.rs:138-158) for both frames.
-int admit_request(PivServer* sv, Request* r) {
+// preparation (preprocess.rs:138-158) for both frames. Returns kAdmitOutOfMemory, with nothing
+// allocated or queued, when the allocation fails for lack of memory (or an injected failure).
+int admit_request(PivServer* sv, Request* r, bool inject_failure) {
     const size_t es = dtype_size(r->dtype);
     const size_t hw = (size_t)r->H * (size_t)r->W;
     const bool chain = r->pre.smooth_sigma > 0.0f || r->pre.normalize_radius > 0;
     const bool both = r->pre.smooth_sigma > 0.0f && r->pre.normalize_radius > 0;
-    CUDA_TRY(cudaMallocAsync(&r->mem, r->bytes, sv->stream));
+    if (inject_failure) return kAdmitOutOfMemory;
+    const cudaError_t ae = cudaMallocAsync(&r->mem, r->bytes, sv->stream);
+    if (ae == cudaErrorMemoryAllocation) {
+        cudaGetLastError();  // not a sticky error: clear it and report
+        r->mem = nullptr;
+        return kAdmitOutOfMemory;
+    }
+    if (ae != cudaSuccess) return fail(PIV_ERR_CUDA, "cudaMallocAsync: %s", cudaGetErrorString(ae));
     char* p = (char*)r->mem;
     auto take = [&](size_t bytes) {
         void* q = p;
@@ -1932,13 +1988,35 @@ int admit_request(PivServer* sv, Request* r) {
 
 }  // namespace
 
-bool PivServer::admit_locked(Request* r, std::string* err) {
-    const int st = admit_request(this, r);
-    if (st) {
-        *err = g_last_error;
-        return false;
+// Called with the lock released. Returns PIV_OK, kAdmitOutOfMemory, or another status with
+// *err set.
+int PivServer::admit(Request* r, std::string* err) {
+    bool inject = false;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (fail_allocs > 0) {
+            --fail_allocs;
+            inject = true;
+        }
     }
-    return true;
+    const int st = admit_request(this, r, inject);
+    if (st && st != kAdmitOutOfMemory) *err = g_last_error;
+    return st;
+}
+
+// Requests cancelled while admitted stop at the step boundary: their completion event covers the
+// work already queued for them, after which retire() gives their memory back.
+void PivServer::cancel_active() {
+    for (Request* r : active) {
+        if (r->final_launched || !r->cancel.load()) continue;
+        r->status = PIV_ERR_CANCELLED;
+        r->error = "cancelled";
+        if (cudaEventCreateWithFlags(&r->done_ev, cudaEventDisableTiming) == cudaSuccess)
+            cudaEventRecord(r->done_ev, stream);
+        else
+            r->done_ev = nullptr;
+        r->final_launched = true;
+    }
 }
 
 // One step: the next pass of every admitted request (multipass.rs:194-259 and validate.rs:51),
@@ -2063,8 +2141,12 @@ void PivServer::retire() {
         in_use -= (int64_t)r->bytes;
         std::lock_guard<std::mutex> lk(mu);
         r->done = true;
-        if (r->status == PIV_OK) stats.completed++; else stats.failed++;
+        if (r->status == PIV_OK) stats.completed++;
+        else if (r->status == PIV_ERR_CANCELLED) stats.cancelled++;
+        else stats.failed++;
         stats.in_flight--;
+        stats.memory_in_use_bytes = in_use;
+        admission_blocked = false;
         any = true;
     }
     active.swap(keep);
@@ -2074,26 +2156,49 @@ void PivServer::retire() {
 void PivServer::loop() {
     cudaSetDevice(device);
     for (;;) {
+        bool may_step = true;
         // admission at a step boundary (FIFO while slots and memory allow)
         {
             std::unique_lock<std::mutex> lk(mu);
             if (queue.empty() && active.empty()) {
                 if (stop) break;
+                if (manual && granted > 0) {  // a granted step with nothing to do
+                    --granted;
+                    ++stepped;
+                    cv_step.notify_all();
+                }
                 cv_submit.wait_for(lk, std::chrono::milliseconds(50));
                 continue;
             }
-            while (!queue.empty() && (int)active.size() < max_in_flight &&
+            may_step = !manual || granted > 0;
+            while (may_step && !admission_blocked && !queue.empty() && (int)active.size() < max_in_flight &&
                    in_use + (int64_t)queue.front()->bytes <= budget) {
                 Request* r = queue.front();
                 queue.pop_front();
                 stats.queued--;
                 lk.unlock();
                 std::string err;
-                const bool ok = admit_locked(r, &err);
+                const int st = admit(r, &err);
                 lk.lock();
-                if (!ok) {
-                    r->status = PIV_ERR_CUDA;
-                    r->error = err;
+                if (st == kAdmitOutOfMemory && !active.empty()) {
+                    // the device is short of memory although the budget allows the request: try
+                    // again once an admitted request has finished and given its memory back
+                    queue.push_front(r);
+                    stats.queued++;
+                    stats.deferred++;
+                    admission_blocked = true;
+                    break;
+                }
+                if (st) {
+                    r->status = st == kAdmitOutOfMemory ? PIV_ERR_CUDA : st;
+                    r->error = st == kAdmitOutOfMemory
+                                   ? "device memory for the request could not be allocated (out of memory)"
+                                   : err;
+                    if (r->mem) {
+                        cudaStreamSynchronize(stream);  // queued uploads may still read host memory
+                        cudaFreeAsync(r->mem, stream);
+                        r->mem = nullptr;
+                    }
                     r->done = true;
                     r->t_done = Clock::now();
                     stats.failed++;
@@ -2107,11 +2212,23 @@ void PivServer::loop() {
             }
             stats.memory_in_use_bytes = in_use;
         }
+        cancel_active();
         std::vector<Request*> work;
-        for (Request* r : active)
-            if (r->next_pass < (int)r->passes.size() && !r->final_launched) work.push_back(r);
+        if (may_step)
+            for (Request* r : active)
+                if (r->next_pass < (int)r->passes.size() && !r->final_launched) work.push_back(r);
         if (!work.empty()) {
             launch_step(work);
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                stats.last_step_requests = (int64_t)work.size();
+                stats.max_step_requests = std::max<int64_t>(stats.max_step_requests, (int64_t)work.size());
+                if (manual) {
+                    --granted;
+                    ++stepped;
+                    cv_step.notify_all();
+                }
+            }
             // bounded run-ahead: keep at most two steps queued on the device
             cudaEvent_t ev;
             if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess) {
@@ -2124,6 +2241,16 @@ void PivServer::loop() {
                 }
             }
         } else {
+            if (may_step && manual) {
+                // a granted step with no pass to launch (everything admitted has launched its
+                // last pass): it is used up
+                std::lock_guard<std::mutex> lk(mu);
+                if (granted > 0) {
+                    --granted;
+                    ++stepped;
+                    cv_step.notify_all();
+                }
+            }
             std::this_thread::sleep_for(std::chrono::microseconds(20));
         }
         retire();
@@ -2167,6 +2294,7 @@ void piv_server_destroy(PivServer* sv) {
     {
         std::lock_guard<std::mutex> lk(sv->mu);
         sv->stop = true;
+        sv->manual = false;  // finish what is queued without waiting for granted steps
     }
     sv->cv_submit.notify_all();
     if (sv->worker.joinable()) sv->worker.join();
@@ -2244,13 +2372,22 @@ int32_t piv_server_submit(PivServer* sv, const PivRequestC* q, uint64_t* id) {
     return PIV_OK;
 }
 
-int32_t piv_server_wait(PivServer* sv, uint64_t id, PivSummaryC* summary, double* latency_ms) {
+namespace {
+
+// Waits for request `id` (forever when timeout_ms < 0); on completion fills the summary and
+// latency, forgets the request and returns its status.
+int32_t server_wait(PivServer* sv, uint64_t id, double timeout_ms, PivSummaryC* summary, double* latency_ms) {
     if (!sv) return fail(PIV_ERR_ARGUMENT, "null server");
     std::unique_lock<std::mutex> lk(sv->mu);
     auto it = sv->by_id.find(id);
     if (it == sv->by_id.end()) return fail(PIV_ERR_ARGUMENT, "unknown request %llu", (unsigned long long)id);
     Request* r = it->second;
-    sv->cv_done.wait(lk, [r] { return r->done; });
+    if (timeout_ms < 0.0) {
+        sv->cv_done.wait(lk, [r] { return r->done; });
+    } else if (!sv->cv_done.wait_for(lk, std::chrono::duration<double, std::milli>(timeout_ms),
+                                     [r] { return r->done; })) {
+        return fail(PIV_ERR_TIMEOUT, "request %llu not done within %g ms", (unsigned long long)id, timeout_ms);
+    }
     sv->by_id.erase(it);
     lk.unlock();
     const int st = r->status;
@@ -2265,6 +2402,73 @@ int32_t piv_server_wait(PivServer* sv, uint64_t id, PivSummaryC* summary, double
     if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count();
     delete r;
     return st;
+}
+
+}  // namespace
+
+int32_t piv_server_wait(PivServer* sv, uint64_t id, PivSummaryC* summary, double* latency_ms) {
+    return server_wait(sv, id, -1.0, summary, latency_ms);
+}
+
+int32_t piv_server_wait_timeout(PivServer* sv, uint64_t id, double timeout_ms, PivSummaryC* summary,
+                                double* latency_ms) {
+    if (!(timeout_ms >= 0.0)) return fail(PIV_ERR_ARGUMENT, "timeout_ms must be >= 0");
+    return server_wait(sv, id, timeout_ms, summary, latency_ms);
+}
+
+int32_t piv_server_cancel(PivServer* sv, uint64_t id) {
+    if (!sv) return fail(PIV_ERR_ARGUMENT, "null server");
+    std::lock_guard<std::mutex> lk(sv->mu);
+    auto it = sv->by_id.find(id);
+    if (it == sv->by_id.end()) return fail(PIV_ERR_ARGUMENT, "unknown request %llu", (unsigned long long)id);
+    Request* r = it->second;
+    if (r->done) return PIV_OK;  // finished already: its result stands
+    auto q = std::find(sv->queue.begin(), sv->queue.end(), r);
+    if (q != sv->queue.end()) {
+        // not admitted: nothing of it is on the device
+        sv->queue.erase(q);
+        sv->stats.queued--;
+        sv->stats.cancelled++;
+        r->status = PIV_ERR_CANCELLED;
+        r->error = "cancelled before admission";
+        r->done = true;
+        r->t_done = Clock::now();
+        sv->cv_done.notify_all();
+        return PIV_OK;
+    }
+    r->cancel.store(true);  // admitted: stops at the next step boundary
+    return PIV_OK;
+}
+
+int32_t piv_server_fail_next_allocations(PivServer* sv, int32_t count) {
+    if (!sv || count < 0) return fail(PIV_ERR_ARGUMENT, "bad argument");
+    std::lock_guard<std::mutex> lk(sv->mu);
+    sv->fail_allocs = count;
+    return PIV_OK;
+}
+
+int32_t piv_server_set_manual(PivServer* sv, int32_t manual) {
+    if (!sv) return fail(PIV_ERR_ARGUMENT, "null server");
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        sv->manual = manual != 0;
+        sv->granted = 0;
+    }
+    sv->cv_submit.notify_all();
+    return PIV_OK;
+}
+
+int32_t piv_server_advance(PivServer* sv, int32_t steps, double timeout_ms) {
+    if (!sv || steps < 0) return fail(PIV_ERR_ARGUMENT, "bad argument");
+    std::unique_lock<std::mutex> lk(sv->mu);
+    if (!sv->manual) return fail(PIV_ERR_ARGUMENT, "the server is not in manual mode");
+    const int64_t target = sv->stepped + steps;
+    sv->granted += steps;
+    sv->cv_submit.notify_all();
+    const bool ok = sv->cv_step.wait_for(lk, std::chrono::duration<double, std::milli>(timeout_ms < 0 ? 1e12 : timeout_ms),
+                                         [sv, target] { return sv->stepped >= target; });
+    if (!ok) return fail(PIV_ERR_TIMEOUT, "%d steps not taken within %g ms", steps, timeout_ms);
+    return PIV_OK;
 }
 
 int32_t piv_server_stats(PivServer* sv, PivServerStatsC* out) {

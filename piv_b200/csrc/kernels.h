@@ -184,6 +184,11 @@ struct PrepParams {
 // Runs the whole PreparedFrame::new chain; returns the number of kernels launched in *launches.
 cudaError_t launch_prepare(const PrepParams& p, cudaStream_t s, int* launches);
 // Integral tables only (used when the prepared image is supplied directly).
+// The reference's f64 IntegralImage tables, already copied into `sum` / `sumsq` (8 bytes per
+// entry, (H+1) x (W+1)), converted in place to the fixed-point tables launch_stats builds;
+// *nonfinite becomes nonzero if an entry is not finite. maxbits2: 2 device words of scratch.
+cudaError_t launch_tables_to_fixed(long long* sum, long long* sumsq, int H, int W, int* scales,
+                                   unsigned long long* maxbits2, unsigned int* nonfinite, cudaStream_t s, int* launches);
 cudaError_t launch_stats(const float* base, int H, int W, long long* sum, long long* sumsq, int* scales,
                          unsigned int* maxbits, cudaStream_t s, int* launches);
 

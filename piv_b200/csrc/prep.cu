@@ -498,6 +498,73 @@ static int grid_for(long long n) {
     return (int)b;
 }
 
+// ------------------------------------------------------------------------------- reference tables
+// IntegralImage's f64 summed-area tables (preprocess.rs:76-103), handed over by a caller that
+// prepared its frames on the host, are turned into this library's int64 fixed-point tables in
+// place (each f64 entry's 8 bytes become its int64 entry): q = round(T * 2^s), with s chosen per
+// table from its largest |entry| so that every entry and every 4-term box difference fits in
+// int64. Only integer operations on the f64 bit patterns are used (no FP64 instruction). Entries
+// whose f64 spacing is below 2^-s are rounded to the nearest multiple of 2^-s (ties to even);
+// box sums are then exact differences of these entries.
+__global__ void table_maxbits_kernel(const unsigned long long* __restrict__ t, long long n, unsigned long long* out,
+                                     unsigned int* nonfinite) {
+    unsigned long long m = 0;
+    bool bad = false;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const unsigned long long b = t[i] & 0x7fffffffffffffffull;
+        if ((b >> 52) == 0x7ffull) bad = true;
+        else m = b > m ? b : m;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long v = __shfl_xor_sync(0xffffffffu, m, o);
+        m = v > m ? v : m;
+    }
+    if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(nonfinite, 1u);
+}
+
+// Scale exponent s with max|T| * 2^s < 2^61 (headroom for the box differences).
+__device__ __forceinline__ int table_scale(unsigned long long maxbits) {
+    if (!maxbits) return 0;
+    const int e = (int)(maxbits >> 52) - 1022;  // max|T| < 2^e
+    return 61 - e;
+}
+
+__device__ __forceinline__ long long f64_bits_to_fixed(unsigned long long bits, int s) {
+    const bool neg = bits >> 63;
+    const int be = (int)((bits >> 52) & 0x7ff);
+    if (be == 0x7ff) return 0;  // non-finite: reported through the flag, never used
+    unsigned long long m = bits & 0x000fffffffffffffull;
+    int k;  // |value| = m * 2^k
+    if (be) {
+        m |= 1ull << 52;
+        k = be - 1075;
+    } else {
+        k = -1074;
+    }
+    k += s;
+    unsigned long long q;
+    if (k >= 0) {
+        q = m << k;  // the scale keeps |value| * 2^s below 2^61
+    } else if (-k >= 64) {
+        q = 0;  // below half a quantum
+    } else {
+        const int r = -k;
+        q = m >> r;
+        const unsigned long long rem = m & ((1ull << r) - 1), half = 1ull << (r - 1);
+        if (rem > half || (rem == half && (q & 1))) ++q;
+    }
+    return neg ? -(long long)q : (long long)q;
+}
+
+__global__ void table_to_fixed_kernel(unsigned long long* t, long long n, const unsigned long long* maxbits,
+                                      int* scale_out) {
+    const int s = table_scale(*maxbits);
+    if (blockIdx.x == 0 && threadIdx.x == 0) *scale_out = s;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        t[i] = (unsigned long long)f64_bits_to_fixed(t[i], s);
+}
+
 cudaError_t launch_stats(const float* base, int H, int W, long long* sum, long long* sumsq, int* scales,
                          unsigned int* maxbits, cudaStream_t s, int* launches) {
     const long long n = (long long)H * W;
@@ -524,6 +591,22 @@ static BlurKernel make_blur(float sigma) {
     for (int j = 0; j <= 2 * radius; ++j) total += k.w[j];
     for (int j = 0; j <= 2 * radius; ++j) k.w[j] /= total;
     return k;
+}
+
+cudaError_t launch_tables_to_fixed(long long* sum, long long* sumsq, int H, int W, int* scales,
+                                   unsigned long long* maxbits2, unsigned int* nonfinite, cudaStream_t s, int* launches) {
+    const long long n = (long long)(H + 1) * (W + 1);
+    cudaError_t e = cudaMemsetAsync(maxbits2, 0, 2 * sizeof(unsigned long long), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(nonfinite, 0, sizeof(unsigned int), s);
+    if (e != cudaSuccess) return e;
+    unsigned long long* t1 = reinterpret_cast<unsigned long long*>(sum);
+    unsigned long long* t2 = reinterpret_cast<unsigned long long*>(sumsq);
+    table_maxbits_kernel<<<grid_for(n), 256, 0, s>>>(t1, n, maxbits2, nonfinite);
+    table_maxbits_kernel<<<grid_for(n), 256, 0, s>>>(t2, n, maxbits2 + 1, nonfinite);
+    table_to_fixed_kernel<<<grid_for(n), 256, 0, s>>>(t1, n, maxbits2, scales);
+    table_to_fixed_kernel<<<grid_for(n), 256, 0, s>>>(t2, n, maxbits2 + 1, scales + 1);
+    if (launches) *launches += 4;
+    return cudaGetLastError();
 }
 
 cudaError_t launch_prepare(const PrepParams& p, cudaStream_t s, int* launches) {
