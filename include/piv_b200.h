@@ -295,7 +295,8 @@ int32_t piv_pipeline_set_background(PivPipeline* pipeline, const float* backgrou
  * admits them (FIFO) while the in-flight count and a device-memory budget allow, keeps each
  * request's state (prepared frames, per-pass origins and predictor fields) on the device, and
  * advances ALL admitted requests by one pass per step: one placement launch for all of them,
- * one correlation launch per window size, one validation chain. A request joins at the next
+ * one fused correlation launch for all FP32 windows of 8 to 64 px (piv_server_set_fused), one
+ * validation chain. A request joins at the next
  * step boundary and leaves when its last pass is done, so requests that arrive while others run
  * share kernel launches with them. Window pairs are independent inside a launch, so each
  * result is bit-identical to PivAnalyzer::analyze of that pair alone. */
@@ -351,6 +352,11 @@ int32_t piv_server_cancel(PivServer* server, uint64_t id);
  * would, without calling the allocator. With other requests in flight the admission is put back
  * and retried after one of them finishes (stats.deferred); with none, the request fails. */
 int32_t piv_server_fail_next_allocations(PivServer* server, int32_t count);
+/* Correlation launches per step: with fused != 0 (the default) the FP32 windows of 8, 16, 32 and
+ * 64 px of all requests, uniform or deformed, run in ONE fused launch (each CTA runs the
+ * per-size kernel body of its window size, so results are bit-identical); other sizes and the
+ * tensor-core kinds take one launch per (size, kind). fused == 0: one launch per (size, kind). */
+int32_t piv_server_set_fused(PivServer* server, int32_t fused);
 /* Manual stepping (testing and external pacing): with manual != 0 the scheduler admits requests
  * and launches steps only when piv_server_advance grants them; 0 returns to free running. */
 int32_t piv_server_set_manual(PivServer* server, int32_t manual);

@@ -753,6 +753,11 @@ class PivServer:
         """Host-side fault injection: the next `count` admissions fail as out-of-memory."""
         _check(_lib.load().piv_server_fail_next_allocations(self._h, int(count)))
 
+    def set_fused(self, fused: bool):
+        """One fused correlation launch per step for the FP32 windows of 8-64 px (default), or one
+        launch per window size and kind."""
+        _check(_lib.load().piv_server_set_fused(self._h, int(bool(fused))))
+
     def set_manual(self, manual: bool):
         """Manual stepping: admission and steps happen only when advance() grants them."""
         _check(_lib.load().piv_server_set_manual(self._h, int(bool(manual))))

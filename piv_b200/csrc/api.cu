@@ -1900,6 +1900,9 @@ struct PivServer {
     int64_t in_use = 0;
     PivServerStatsC stats{};
     int variant[2][129] = {};
+    // FP32 windows of several sizes and kinds in one fused correlation launch per step (on by
+    // default; piv_server_set_fused(0) launches per (size, kind) instead)
+    bool fused = true;
     std::vector<cudaEvent_t> step_events;  // completion of recent steps (bounded run-ahead)
     // Admission waits for a retirement after an allocation failed while requests were in flight.
     bool admission_blocked = false;
@@ -2067,8 +2070,25 @@ void PivServer::launch_step(std::vector<Request*>& work) {
     }
     int nl = 0;
     cudaError_t e = launch_place_items(pps.data(), (int)pps.size(), stream, &nl);
+    // FP32 windows of 8, 16, 32 and 64 px, uniform or deformed, of all requests: one fused
+    // launch; other sizes and the tensor-core kinds: one launch per (size, kind)
+    std::vector<CorrParams> fused_items;
+    std::vector<int> fused_kinds;
+    for (auto& kv : cps) {
+        const int fk = (kv.first.second < 2 && fused && variant[kv.first.second][kv.first.first] == 0)
+                           ? fused_kind(kv.first.first, kv.first.second == 1)
+                           : -1;
+        if (fk < 0) continue;
+        for (const CorrParams& cp : kv.second) {
+            fused_items.push_back(cp);
+            fused_kinds.push_back(fk);
+        }
+        kv.second.clear();
+    }
+    if (e == cudaSuccess && !fused_items.empty())
+        e = launch_correlate_fused(fused_items.data(), fused_kinds.data(), (int)fused_items.size(), stream, &nl);
     for (auto& kv : cps)
-        if (e == cudaSuccess)
+        if (e == cudaSuccess && !kv.second.empty())
             e = kv.first.second >= 2
                     ? launch_correlate_tc_items(kv.first.first, kv.first.second == 3 || kv.first.second == 5,
                                                 kv.second.data(), (int)kv.second.size(), stream, &nl)
@@ -2444,6 +2464,13 @@ int32_t piv_server_fail_next_allocations(PivServer* sv, int32_t count) {
     if (!sv || count < 0) return fail(PIV_ERR_ARGUMENT, "bad argument");
     std::lock_guard<std::mutex> lk(sv->mu);
     sv->fail_allocs = count;
+    return PIV_OK;
+}
+
+int32_t piv_server_set_fused(PivServer* sv, int32_t fused) {
+    if (!sv) return fail(PIV_ERR_ARGUMENT, "null server");
+    std::lock_guard<std::mutex> lk(sv->mu);
+    sv->fused = fused != 0;
     return PIV_OK;
 }
 

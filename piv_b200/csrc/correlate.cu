@@ -20,6 +20,7 @@
 //      half-width footprint, the second local maximum (a vectorised 3x3 maximum) and the 3-point
 //      Gaussian fit follow.
 // The 128 px window runs one window per group with a full complex inverse (registers).
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <cstdio>
@@ -206,15 +207,12 @@ __device__ __forceinline__ float2 cross4(float2 z, float2 m) {
     return make_float2(far * fbr + fai * fbi, far * fbi - fai * fbr);
 }
 
+// One CTA's work: G window pairs (or single windows) of one item, `block` counting the item's
+// CTAs; `sbase` is the CTA's dynamic shared memory (at least C::SMEM bytes).
 template <class C>
-__global__ void __launch_bounds__(C::THREADS, C::MINB) correlate_kernel(const __grid_constant__ CorrBatch batch) {
+__device__ __forceinline__ void correlate_body(const CorrParams& prm, int block, char* sbase) {
     constexpr int N = C::N, T = C::T, G = C::G, P = C::P, NT = C::NT, WPG = C::WPG;
-    const int item = batch_item(batch.block_start, batch.n, (int)blockIdx.x);
-    const CorrParams& prm = batch.item[item];
-    const int block = (int)blockIdx.x - batch.block_start[item];
     constexpr bool PAIR = C::PAIR;
-    extern __shared__ float4 smem_f4[];
-    char* sbase = reinterpret_cast<char*>(smem_f4);
     const int tid = threadIdx.x;
     const int g = tid / NT;
     const int gt = tid - g * NT;
@@ -528,6 +526,112 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB) correlate_kernel(const __
             }
         }
     }
+}
+
+template <class C>
+__global__ void __launch_bounds__(C::THREADS, C::MINB) correlate_kernel(const __grid_constant__ CorrBatch batch) {
+    const int item = batch_item(batch.block_start, batch.n, (int)blockIdx.x);
+    extern __shared__ float4 smem_f4[];
+    correlate_body<C>(batch.item[item], (int)blockIdx.x - batch.block_start[item], reinterpret_cast<char*>(smem_f4));
+}
+
+// ---------------------------------------------------------------------------------------------
+// Fused launch over items of different window sizes and window kinds (the serving form's step):
+// every configuration below has 256 threads per CTA and the same register cap, so one kernel
+// holds them all and each CTA runs the body of its item's configuration. Each configuration is
+// the FFT decomposition (N, T, PAIR) of that size's per-size kernel, so the results are bit
+// for bit those of the per-size launches.
+// ---------------------------------------------------------------------------------------------
+using FusedC0 = CorrCfg<8, 1, true, 32, 2, true>;
+using FusedC1 = CorrCfg<16, 1, true, 16, 2, false>;
+using FusedC2 = CorrCfg<32, 2, true, 4, 2, true>;
+using FusedC3 = CorrCfg<64, 4, true, 1, 2, true>;
+using FusedC4 = CorrCfg<8, 1, true, 32, 2, false, true>;
+using FusedC5 = CorrCfg<16, 1, true, 16, 2, false, true>;
+using FusedC6 = CorrCfg<32, 2, true, 4, 2, false, true>;
+using FusedC7 = CorrCfg<64, 4, true, 1, 2, false, true>;
+constexpr int kFusedThreads = 256;
+constexpr size_t kFusedSmem =
+    std::max({FusedC0::SMEM, FusedC1::SMEM, FusedC2::SMEM, FusedC3::SMEM, FusedC4::SMEM, FusedC5::SMEM, FusedC6::SMEM,
+              FusedC7::SMEM});
+static_assert(FusedC0::THREADS == kFusedThreads && FusedC1::THREADS == kFusedThreads &&
+                  FusedC2::THREADS == kFusedThreads && FusedC3::THREADS == kFusedThreads &&
+                  FusedC4::THREADS == kFusedThreads && FusedC5::THREADS == kFusedThreads &&
+                  FusedC6::THREADS == kFusedThreads && FusedC7::THREADS == kFusedThreads,
+              "fused configurations share the block size");
+static_assert(kFusedSmem <= 227 * 1024, "shared memory");
+
+// Configuration index of (window, deformed) in the fused kernel, or -1.
+int fused_kind(int n, bool deform) {
+    const int s = n == 8 ? 0 : n == 16 ? 1 : n == 32 ? 2 : n == 64 ? 3 : -1;
+    return s < 0 ? -1 : s + (deform ? 4 : 0);
+}
+
+static int fused_cells_per_block(int kind) {
+    switch (kind & 3) {
+        case 0: return FusedC0::G * FusedC0::WPG;
+        case 1: return FusedC1::G * FusedC1::WPG;
+        case 2: return FusedC2::G * FusedC2::WPG;
+        default: return FusedC3::G * FusedC3::WPG;
+    }
+}
+
+struct FusedBatch {
+    int n;
+    int block_start[kMaxBatch + 1];
+    int kind[kMaxBatch];
+    CorrParams item[kMaxBatch];
+};
+
+__global__ void __launch_bounds__(kFusedThreads, 2) correlate_fused_kernel(const __grid_constant__ FusedBatch b) {
+    const int item = batch_item(b.block_start, b.n, (int)blockIdx.x);
+    const CorrParams& prm = b.item[item];
+    const int block = (int)blockIdx.x - b.block_start[item];
+    extern __shared__ float4 smem_f4[];
+    char* sm = reinterpret_cast<char*>(smem_f4);
+    switch (b.kind[item]) {
+        case 0: correlate_body<FusedC0>(prm, block, sm); break;
+        case 1: correlate_body<FusedC1>(prm, block, sm); break;
+        case 2: correlate_body<FusedC2>(prm, block, sm); break;
+        case 3: correlate_body<FusedC3>(prm, block, sm); break;
+        case 4: correlate_body<FusedC4>(prm, block, sm); break;
+        case 5: correlate_body<FusedC5>(prm, block, sm); break;
+        case 6: correlate_body<FusedC6>(prm, block, sm); break;
+        default: correlate_body<FusedC7>(prm, block, sm); break;
+    }
+}
+
+cudaError_t launch_correlate_fused(const CorrParams* items, const int* kinds, int count, cudaStream_t s,
+                                   int* launches) {
+    for (int i = 0; i < count; ++i) {
+        if (kinds[i] < 0 || kinds[i] > 7) return cudaErrorInvalidValue;
+        if ((kinds[i] >= 4) != (items[i].corners != nullptr)) return cudaErrorInvalidValue;
+        if (kinds[i] >= 4 && (items[i].gnx <= 0 || items[i].gstep <= 0)) return cudaErrorInvalidValue;
+    }
+    cudaError_t e = cudaFuncSetAttribute(correlate_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kFusedSmem);
+    if (e != cudaSuccess) return e;
+    for (int off = 0; off < count; off += kMaxBatch) {
+        FusedBatch b;
+        b.n = count - off < kMaxBatch ? count - off : kMaxBatch;
+        long long total = 0;
+        for (int i = 0; i < b.n; ++i) {
+            b.item[i] = items[off + i];
+            b.kind[i] = kinds[off + i];
+            b.block_start[i] = (int)total;
+            const int per = fused_cells_per_block(b.kind[i]);
+            total += (b.item[i].ncells + per - 1) / per;
+        }
+        b.block_start[b.n] = (int)total;
+        if (total > 0x7fffffffll) return cudaErrorInvalidValue;
+        if (total > 0) {
+            correlate_fused_kernel<<<(unsigned)total, kFusedThreads, kFusedSmem, s>>>(b);
+            e = cudaGetLastError();
+            if (e != cudaSuccess) return e;
+            if (launches) ++*launches;
+        }
+    }
+    return cudaSuccess;
 }
 
 // One launch over all items of the batch: item i owns blocks [block_start[i], block_start[i+1]).

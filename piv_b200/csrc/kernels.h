@@ -61,6 +61,11 @@ cudaError_t launch_correlate_variant(int n, int v, const CorrParams& p, cudaStre
 // All items share window size n and either all have corners (deformed windows) or none; v
 // indexes the variants of that kind. Returns the number of launches issued in *launches.
 cudaError_t launch_correlate_items(int n, int v, const CorrParams* items, int count, cudaStream_t s, int* launches);
+// One launch over FP32 items of different window sizes and kinds: kinds[i] = fused_kind(window,
+// deformed) of item i (window 8, 16, 32 or 64). Results equal the per-size launches bit for bit.
+int fused_kind(int n, bool deform);
+cudaError_t launch_correlate_fused(const CorrParams* items, const int* kinds, int count, cudaStream_t s,
+                                   int* launches);
 // Split-precision (BF16 or FP16 hi/lo, three products) tensor-core correlation, window sizes 16
 // and 32; all items of a call are uniform windows or all deformed (corners set).
 // corr_tc_init_device uploads its DFT matrices and deformation ramps to the current device;
