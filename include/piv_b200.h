@@ -62,9 +62,9 @@ typedef enum { PIV_DTYPE_U8 = 0, PIV_DTYPE_U16 = 1, PIV_DTYPE_F32 = 2 } PivDtype
  * PIV_PRECISION_FP32 runs the FFTs on the FP32 cores in the reference's precision;
  * PIV_PRECISION_BF16X3 runs the 2-D DFTs as DFT-matrix products on the tensor cores with every
  * operand split into two BF16 halves and three products summed in FP32 (about 16 significant
- * bits) for window sizes 16 and 32 and uniform windows; other sizes and deformed windows keep
- * the FP32 kernel. piv_analyzer_autotune also times the tensor-core kernel and keeps the FP32
- * kernel (higher precision) for a size where it is faster. */
+ * bits) for window sizes 16, 32 and 64, uniform or deformed; other sizes keep the FP32 kernel.
+ * piv_analyzer_autotune also times the tensor-core kernel and keeps the FP32 kernel (higher
+ * precision) for a size where it is faster. */
 #define PIV_PRECISION_FP32 0
 #define PIV_PRECISION_BF16X3 1
 #define PIV_PRECISION_FP16X3 2  /* as BF16X3 with FP16 halves: about 22 significant bits */

@@ -26,10 +26,18 @@
 //   I1  inverse complex DFT along ky, each lane half of the y outputs;
 //   I2  c2r along kx (rows (w, y), K = packed kx): the correlation plane, row y per thread.
 // find_peak (correlate.rs:215-303) then runs on the plane as in the FP32 kernel.
+//
+// 64 px windows (two per tile, each on two warps) use a compact form to fit shared memory with
+// two warpgroups per CTA: the complex DFTs F2 and I1 keep only [C | S] (cos and sin blocks along
+// K) instead of the 2x2 real block matrix, and form the other output half as a second MMA chain
+// over the other K half of the operand with B negated (the instruction descriptor's negate-B
+// bit), e.g. Im F2 = Zi C^T - Zr S^T. Window reductions then cross the two warps through shared
+// memory.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "common.cuh"
@@ -43,23 +51,28 @@ namespace pivb200 {
 // them), set by corr_tc_init_device.
 __constant__ float c_ramp16[16];
 __constant__ float c_ramp32[32];
+__constant__ float c_ramp64[64];
 template <int N>
 __device__ __forceinline__ const float* c_ramp() {
     if constexpr (N == 16) return c_ramp16;
-    else return c_ramp32;
+    else if constexpr (N == 32) return c_ramp32;
+    else return c_ramp64;
 }
 
 template <int N_>
 struct TcCfg {
     static constexpr int N = N_, H2 = N / 2;
     static constexpr int WPT = 128 / N;  // windows (cells) per tile
-    static constexpr int NWG = 4;        // warpgroups per CTA, each on its own tiles
+    // 64 px: compact [C | S] DFT matrices and two warpgroups per CTA (shared memory); 16 and 32
+    // px: the 2x2 real block matrices and four warpgroups per CTA
+    static constexpr bool COMPACT = N >= 64;
+    static constexpr int NWG = COMPACT ? 2 : 4;  // warpgroups per CTA, each on its own tiles
     static constexpr int THREADS = 128 * NWG;
     // DFT matrices, B operands (rows = outputs, K-major), element offsets of hi (or lo) parts
-    static constexpr int R1_OFF = 0;                 // N x N
-    static constexpr int R2_OFF = R1_OFF + N * N;    // 2N x 2N
-    static constexpr int R3_OFF = R2_OFF + 4 * N * N;  // N x 2N
-    static constexpr int R4_OFF = R3_OFF + 2 * N * N;  // N x N
+    static constexpr int R1_OFF = 0;                                     // N x N
+    static constexpr int R2_OFF = R1_OFF + N * N;                        // 2N x 2N, compact N x 2N
+    static constexpr int R3_OFF = R2_OFF + (COMPACT ? 2 : 4) * N * N;    // N x 2N, compact N/2 x 2N
+    static constexpr int R4_OFF = R3_OFF + (COMPACT ? 1 : 2) * N * N;    // N x N
     static constexpr int RMAT = R4_OFF + N * N;
     static constexpr size_t MAT_BYTES = (size_t)RMAT * 2;
     static constexpr int ABUF = 128 * 2 * N;  // operand elements per part per warpgroup
@@ -67,11 +80,14 @@ struct TcCfg {
     static constexpr int TCOLS = (2 * N < 32) ? 32 : 2 * N;  // TMEM columns per warpgroup
     static constexpr int PLD = N + 4;  // FP32 plane row pitch (floats): 16-byte rows, 8 rows on distinct banks
     static constexpr size_t BAR_OFF = 2 * MAT_BYTES + (size_t)NWG * 2 * A_BYTES;
+    // cross-warp window reductions (64 px): per warpgroup, 4 warps x 4 floats
+    static constexpr size_t RED_OFF = (BAR_OFF + 8 * NWG + 16 + sizeof(int) * NWG * WPT * 4 + 15) / 16 * 16;
     // staged DC + i*Nyquist spectra: per warpgroup, window and frame, 2N floats
-    static constexpr size_t ZST_OFF = (BAR_OFF + 8 * NWG + 16 + sizeof(int) * NWG * WPT * 4 + 15) / 16 * 16;
+    static constexpr size_t ZST_OFF = (RED_OFF + sizeof(float) * NWG * 16 + 15) / 16 * 16;
     static constexpr size_t SMEM = ZST_OFF + sizeof(float) * NWG * WPT * 4 * N + 64;
     static_assert((size_t)128 * PLD * 4 <= 2 * A_BYTES, "plane fits in the operand buffers");
     static_assert(N % 16 == 0 && 128 % N == 0, "tile shape");
+    static_assert(SMEM <= 232448, "shared memory");
     // fixed operand factors (see the top of the file) and the plane's exact rescale
     static constexpr int LOG2N = N == 16 ? 4 : (N == 32 ? 5 : 6);
     static constexpr float CROSS_SCALE = (4 * LOG2N > 12) ? 1.0f / (float)(1 << (4 * LOG2N - 12)) : 1.0f;
@@ -129,10 +145,12 @@ __device__ __forceinline__ void store_split(uint8_t* hi, uint8_t* lo, uint32_t o
     *reinterpret_cast<uint4*>(lo + off) = l;
 }
 
-// Issues D (+)= A * B^T over `ksteps` K=16 steps for the three split products.
+// Issues D (+)= A * B^T over `ksteps` K=16 steps for the three split products; with
+// `accumulate` the chain adds to what D holds.
 __device__ __forceinline__ void mma_split(uint32_t d, uint32_t a_hi, uint32_t a_lo, uint32_t a_lbo, uint32_t b_hi,
-                                          uint32_t b_lo, uint32_t b_lbo, int ksteps, uint32_t idesc) {
-    uint32_t acc = 0;
+                                          uint32_t b_lo, uint32_t b_lbo, int ksteps, uint32_t idesc,
+                                          bool accumulate = false) {
+    uint32_t acc = accumulate ? 1u : 0u;
     const uint32_t as[3] = {a_hi, a_lo, a_hi};
     const uint32_t bs[3] = {b_hi, b_hi, b_lo};
 #pragma unroll
@@ -143,6 +161,69 @@ __device__ __forceinline__ void mma_split(uint32_t d, uint32_t a_hi, uint32_t a_
             tc::mma_f16(d, ad, bd, idesc, acc);
             acc = 1;
         }
+}
+
+// Instruction-descriptor bit that negates the B operand (kind::f16 with FP32 accumulation).
+constexpr uint32_t kNegateB = 1u << 14;
+
+// Reductions over the N lanes of one window (a tile holds 128/N windows of N consecutive rows).
+// Up to 32 lanes the window is a segment of one warp; a 64 px window spans two warps, whose
+// partials meet in shared memory (`red`: 4 warps x 4 floats of this warpgroup), combined in the
+// same order by every lane.
+template <int N>
+__device__ __forceinline__ float2 win_sum2(float2 v, float* red, int i, int wg) {
+#pragma unroll
+    for (int o = (N < 32 ? N : 32) / 2; o > 0; o >>= 1) {
+        v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+        v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+    }
+    if constexpr (N > 32) {
+        const int w = i >> 5, w0 = w & ~1;
+        if ((i & 31) == 0) {
+            red[4 * w] = v.x;
+            red[4 * w + 1] = v.y;
+        }
+        wg_sync(wg);
+        v = make_float2(red[4 * w0] + red[4 * w0 + 4], red[4 * w0 + 1] + red[4 * w0 + 5]);
+        wg_sync(wg);
+    }
+    return v;
+}
+
+template <int N>
+__device__ __forceinline__ void win_argmax(float& best, int& bi, float* red, int i, int wg) {
+#pragma unroll
+    for (int o = (N < 32 ? N : 32) / 2; o > 0; o >>= 1) {
+        const float ob = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        amax_combine(best, bi, ob, oi);
+    }
+    if constexpr (N > 32) {
+        const int w = i >> 5, w0 = w & ~1;
+        if ((i & 31) == 0) {
+            red[4 * w] = best;
+            red[4 * w + 1] = __int_as_float(bi);
+        }
+        wg_sync(wg);
+        best = red[4 * w0];
+        bi = __float_as_int(red[4 * w0 + 1]);
+        amax_combine(best, bi, red[4 * w0 + 4], __float_as_int(red[4 * w0 + 5]));
+        wg_sync(wg);
+    }
+}
+
+template <int N>
+__device__ __forceinline__ float win_max(float v, float* red, int i, int wg) {
+#pragma unroll
+    for (int o = (N < 32 ? N : 32) / 2; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if constexpr (N > 32) {
+        const int w = i >> 5, w0 = w & ~1;
+        if ((i & 31) == 0) red[4 * w] = v;
+        wg_sync(wg);
+        v = fmaxf(red[4 * w0], red[4 * w0 + 4]);
+        wg_sync(wg);
+    }
+    return v;
 }
 
 template <int N, bool F16, bool DEFORM>
@@ -163,6 +244,7 @@ __global__ void __launch_bounds__(TcCfg<N>::THREADS, 1)
     uint32_t* tbase = reinterpret_cast<uint32_t*>(smem + C::BAR_OFF + 8 * C::NWG);
     int* s_hw = reinterpret_cast<int*>(smem + C::BAR_OFF + 8 * C::NWG + 16) + wg * C::WPT * 4;
     float* zst = reinterpret_cast<float*>(smem + C::ZST_OFF) + (size_t)wg * C::WPT * 4 * N;
+    float* red = reinterpret_cast<float*>(smem + C::RED_OFF) + wg * 16;
 
     for (int j = threadIdx.x; j < (int)(2 * C::MAT_BYTES / 16); j += C::THREADS)
         reinterpret_cast<uint4*>(smem)[j] = mats[j];
@@ -235,11 +317,7 @@ __global__ void __launch_bounds__(TcCfg<N>::THREADS, 1)
                 s.x += z[p].x;
                 s.y += z[p].y;
             }
-#pragma unroll
-            for (int o = N / 2; o > 0; o >>= 1) {
-                s.x += __shfl_xor_sync(0xffffffffu, s.x, o);
-                s.y += __shfl_xor_sync(0xffffffffu, s.y, o);
-            }
+            s = win_sum2<N>(s, red, i, wg);
             constexpr float inv = 1.0f / (float)(N * N);
             const float ma = s.x * inv, mb = s.y * inv;
             e = make_float2(0.f, 0.f);
@@ -250,11 +328,7 @@ __global__ void __launch_bounds__(TcCfg<N>::THREADS, 1)
                 e.x += z[p].x * z[p].x;
                 e.y += z[p].y * z[p].y;
             }
-#pragma unroll
-            for (int o = N / 2; o > 0; o >>= 1) {
-                e.x += __shfl_xor_sync(0xffffffffu, e.x, o);
-                e.y += __shfl_xor_sync(0xffffffffu, e.y, o);
-            }
+            e = win_sum2<N>(e, red, i, wg);
         }
         ok = ok && e.x > 1e-12f && e.y > 1e-12f;
         {  // unit-variance windows (a flat or masked window is zeroed: its result is discarded)
@@ -312,9 +386,22 @@ __global__ void __launch_bounds__(TcCfg<N>::THREADS, 1)
         sync_for_mma();
         if (i == 0) {
             tc::fence_after_sync();
-            constexpr uint32_t id = tc::idesc_f16(128, 2 * N, !F16, true);
-            constexpr uint32_t lb = (2 * N / 8) * 128;
-            mma_split(tmem, ah, al, LBO_A, mh + C::R2_OFF * 2, ml + C::R2_OFF * 2, lb, 2 * N / 16, id);
+            if constexpr (C::COMPACT) {
+                // B = [C | S] (N rows, K = 2N); A = [Zr | Zi] (K = 2N), MN-major
+                constexpr uint32_t id = tc::idesc_f16(128, N, !F16, true);
+                constexpr uint32_t lb = (N / 8) * 128;
+                constexpr uint32_t akoff = (N / 8) * LBO_A, bkoff = (N / 8) * lb;  // K offset N
+                const uint32_t bh = mh + C::R2_OFF * 2, bl = ml + C::R2_OFF * 2;
+                // Re = Zr C^T + Zi S^T
+                mma_split(tmem, ah, al, LBO_A, bh, bl, lb, 2 * N / 16, id);
+                // Im = Zi C^T - Zr S^T
+                mma_split(tmem + N, ah + akoff, al + akoff, LBO_A, bh, bl, lb, N / 16, id);
+                mma_split(tmem + N, ah, al, LBO_A, bh + bkoff, bl + bkoff, lb, N / 16, id | kNegateB, true);
+            } else {
+                constexpr uint32_t id = tc::idesc_f16(128, 2 * N, !F16, true);
+                constexpr uint32_t lb = (2 * N / 8) * 128;
+                mma_split(tmem, ah, al, LBO_A, mh + C::R2_OFF * 2, ml + C::R2_OFF * 2, lb, 2 * N / 16, id);
+            }
             tc::mma_commit(bar);
         }
         mma_wait();
@@ -398,9 +485,23 @@ __global__ void __launch_bounds__(TcCfg<N>::THREADS, 1)
         sync_for_mma();
         if (i == 0) {
             tc::fence_after_sync();
-            constexpr uint32_t id = tc::idesc_f16(128, N, !F16, false);
-            constexpr uint32_t lb = (N / 8) * 128;
-            mma_split(tmem, ah, al, LBO_A, mh + C::R3_OFF * 2, ml + C::R3_OFF * 2, lb, 2 * N / 16, id);
+            if constexpr (C::COMPACT) {
+                // B = [C | S] (N/2 rows: outputs y < N/2, K = 2N); A = [Pr | Pi] (K = 2N), K-major
+                constexpr uint32_t id = tc::idesc_f16(128, H2, !F16, false);
+                constexpr uint32_t lb = (H2 / 8) * 128;
+                constexpr uint32_t akoff = (N / 8) * LBO_A, bkoff = (N / 8) * lb;  // K offset N
+                const uint32_t bh = mh + C::R3_OFF * 2, bl = ml + C::R3_OFF * 2;
+                // Re = Pr C^T - Pi S^T
+                mma_split(tmem, ah, al, LBO_A, bh, bl, lb, N / 16, id);
+                mma_split(tmem, ah + akoff, al + akoff, LBO_A, bh + bkoff, bl + bkoff, lb, N / 16, id | kNegateB, true);
+                // Im = Pr S^T + Pi C^T
+                mma_split(tmem + H2, ah, al, LBO_A, bh + bkoff, bl + bkoff, lb, N / 16, id);
+                mma_split(tmem + H2, ah + akoff, al + akoff, LBO_A, bh, bl, lb, N / 16, id, true);
+            } else {
+                constexpr uint32_t id = tc::idesc_f16(128, N, !F16, false);
+                constexpr uint32_t lb = (N / 8) * 128;
+                mma_split(tmem, ah, al, LBO_A, mh + C::R3_OFF * 2, ml + C::R3_OFF * 2, lb, 2 * N / 16, id);
+            }
             tc::mma_commit(bar);
         }
         mma_wait();
@@ -461,12 +562,7 @@ __global__ void __launch_bounds__(TcCfg<N>::THREADS, 1)
                 best = v[x];
                 bi = y * N + x;
             }
-#pragma unroll
-        for (int o = N / 2; o > 0; o >>= 1) {
-            const float ob = __shfl_xor_sync(0xffffffffu, best, o);
-            const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-            amax_combine(best, bi, ob, oi);
-        }
+        win_argmax<N>(best, bi, red, i, wg);
         if (!(best > -INFINITY)) bi = 0;
         const int by = bi / N, bx = bi % N;
         wg_sync(wg);  // plane complete
@@ -500,26 +596,27 @@ __global__ void __launch_bounds__(TcCfg<N>::THREADS, 1)
         {
             // columns outside the footprint: circular distance from bx above ex, or every column
             // when this row is already farther than ex from by
+            using Mask = std::conditional_t<(N > 32), unsigned long long, uint32_t>;
+            constexpr int MB = 8 * (int)sizeof(Mask);
             const int dy = abs(y - by), cy = min(dy, N - dy);
-            uint32_t allowed = 0xffffffffu;
+            Mask allowed = ~Mask(0);
             if (cy <= ex) {
-                uint32_t band = 0xffffffffu;  // columns bx - ex .. bx + ex (circular)
+                Mask band = ~Mask(0);  // columns bx - ex .. bx + ex (circular)
                 if (2 * ex + 1 < N) {
-                    const uint32_t run = (1u << (2 * ex + 1)) - 1u;
+                    const Mask run = (Mask(1) << (2 * ex + 1)) - Mask(1);
                     const int s0 = (bx - ex + N) % N;
-                    band = (run << s0) | (s0 ? run >> (N - s0) : 0u);
-                    if constexpr (N < 32) band &= (1u << (N & 31)) - 1u;
+                    band = (run << s0) | (s0 ? run >> (N - s0) : Mask(0));
+                    if constexpr (N < MB) band &= (Mask(1) << (N % MB)) - Mask(1);
                 }
                 allowed = ~band;
             }
 #pragma unroll
             for (int x = 0; x < N; ++x) {
                 const float h = fmaxf(fmaxf(vm[(x + N - 1) % N], vm[(x + 1) % N]), vm[x]);
-                if (v[x] == h && (allowed & (1u << x))) second = fmaxf(second, v[x]);
+                if (v[x] == h && ((allowed >> x) & Mask(1))) second = fmaxf(second, v[x]);
             }
         }
-#pragma unroll
-        for (int o = N / 2; o > 0; o >>= 1) second = fmaxf(second, __shfl_xor_sync(0xffffffffu, second, o));
+        second = win_max<N>(second, red, i, wg);
         if (q == 0 && active) {
             if (ok) {
                 const float sx = subpixel(at(by, bx - 1), best, at(by, bx + 1));
@@ -610,24 +707,35 @@ static std::vector<uint16_t> build_mats() {
             else v = -cs((long long)(n - H2) * x, N, true);
             put(C::R1_OFF, N, n, x, v);
         }
-    for (int n = 0; n < 2 * N; ++n)  // R2: forward complex DFT along y
-        for (int k = 0; k < 2 * N; ++k) {
-            const int ky = n % N, r = k % N;
-            const bool out_im = n >= N, in_im = k >= N;
-            double v;
-            if (!out_im) v = in_im ? cs((long long)ky * r, N, true) : cs((long long)ky * r, N, false);
-            else v = in_im ? cs((long long)ky * r, N, false) : -cs((long long)ky * r, N, true);
-            put(C::R2_OFF, 2 * N, n, k, v);
-        }
-    for (int n = 0; n < N; ++n)  // R3: inverse complex DFT along ky, outputs y < N/2
-        for (int k = 0; k < 2 * N; ++k) {
-            const int yy = n % H2, ky = k % N;
-            const bool out_im = n >= H2, in_im = k >= N;
-            double v;
-            if (!out_im) v = in_im ? -cs((long long)ky * yy, N, true) : cs((long long)ky * yy, N, false);
-            else v = in_im ? cs((long long)ky * yy, N, false) : cs((long long)ky * yy, N, true);
-            put(C::R3_OFF, N, n, k, v);
-        }
+    if constexpr (C::COMPACT) {
+        // [C | S] blocks: row = output (ky for F2, y < N/2 for I1), K = [cos terms | sin terms];
+        // the kernel forms the other output half with B negated (see the top of the file)
+        for (int n = 0; n < N; ++n)  // R2: forward complex DFT along y
+            for (int k = 0; k < 2 * N; ++k)
+                put(C::R2_OFF, N, n, k, cs((long long)n * (k % N), N, k >= N));
+        for (int n = 0; n < H2; ++n)  // R3: inverse complex DFT along ky, outputs y < N/2
+            for (int k = 0; k < 2 * N; ++k)
+                put(C::R3_OFF, H2, n, k, cs((long long)(k % N) * n, N, k >= N));
+    } else {
+        for (int n = 0; n < 2 * N; ++n)  // R2: forward complex DFT along y
+            for (int k = 0; k < 2 * N; ++k) {
+                const int ky = n % N, r = k % N;
+                const bool out_im = n >= N, in_im = k >= N;
+                double v;
+                if (!out_im) v = in_im ? cs((long long)ky * r, N, true) : cs((long long)ky * r, N, false);
+                else v = in_im ? cs((long long)ky * r, N, false) : -cs((long long)ky * r, N, true);
+                put(C::R2_OFF, 2 * N, n, k, v);
+            }
+        for (int n = 0; n < N; ++n)  // R3: inverse complex DFT along ky, outputs y < N/2
+            for (int k = 0; k < 2 * N; ++k) {
+                const int yy = n % H2, ky = k % N;
+                const bool out_im = n >= H2, in_im = k >= N;
+                double v;
+                if (!out_im) v = in_im ? -cs((long long)ky * yy, N, true) : cs((long long)ky * yy, N, false);
+                else v = in_im ? cs((long long)ky * yy, N, false) : cs((long long)ky * yy, N, true);
+                put(C::R3_OFF, N, n, k, v);
+            }
+    }
     for (int x = 0; x < N; ++x)  // R4: c2r along kx from the packed half spectrum
         for (int k = 0; k < N; ++k) {
             double v;
@@ -642,8 +750,9 @@ static std::vector<uint16_t> build_mats() {
 
 namespace {
 constexpr int kMaxDevices = 64;
-// DFT matrix images per device: [size 16 | size 32][BF16 | FP16]
-const uint4* g_mats[kMaxDevices][2][2] = {};
+// DFT matrix images per device: [size 16 | 32 | 64][BF16 | FP16]
+const uint4* g_mats[kMaxDevices][3][2] = {};
+int size_slot(int n) { return n == 16 ? 0 : (n == 32 ? 1 : 2); }
 unsigned int* g_err_host[kMaxDevices] = {};
 unsigned int* g_err_dev[kMaxDevices] = {};
 
@@ -664,7 +773,7 @@ cudaError_t upload(const uint4** slot) {
 }
 }  // namespace
 
-bool corr_tc_supported(int n) { return n == 16 || n == 32; }
+bool corr_tc_supported(int n) { return n == 16 || n == 32 || n == 64; }
 
 cudaError_t corr_tc_init_device() {
     int dev = 0;
@@ -675,12 +784,16 @@ cudaError_t corr_tc_init_device() {
     if (e == cudaSuccess) e = upload<16, true>(&g_mats[dev][0][1]);
     if (e == cudaSuccess) e = upload<32, false>(&g_mats[dev][1][0]);
     if (e == cudaSuccess) e = upload<32, true>(&g_mats[dev][1][1]);
+    if (e == cudaSuccess) e = upload<64, false>(&g_mats[dev][2][0]);
+    if (e == cudaSuccess) e = upload<64, true>(&g_mats[dev][2][1]);
     if (e == cudaSuccess) {
-        float r16[16], r32[32];
+        float r16[16], r32[32], r64[64];
         for (int i = 0; i < 16; ++i) r16[i] = (float)i / 15.0f;
         for (int i = 0; i < 32; ++i) r32[i] = (float)i / 31.0f;
+        for (int i = 0; i < 64; ++i) r64[i] = (float)i / 63.0f;
         e = cudaMemcpyToSymbol(c_ramp16, r16, sizeof(r16));
         if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_ramp32, r32, sizeof(r32));
+        if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_ramp64, r64, sizeof(r64));
     }
     if (e == cudaSuccess && !g_err_host[dev]) {
         e = cudaHostAlloc(reinterpret_cast<void**>(&g_err_host[dev]), sizeof(unsigned int), cudaHostAllocMapped);
@@ -734,14 +847,17 @@ cudaError_t launch_correlate_tc_items(int n, bool f16, const CorrParams* items, 
         CorrBatch b;
         b.n = count - off < kMaxBatch ? count - off : kMaxBatch;
         for (int i = 0; i < b.n; ++i) b.item[i] = items[off + i];
-        const uint4* m = g_mats[dev][n == 16 ? 0 : 1][f16 ? 1 : 0];
+        const uint4* m = g_mats[dev][size_slot(n)][f16 ? 1 : 0];
         unsigned int* err = g_err_dev[dev];
         if (n == 16) {
             if (deform) e = f16 ? launch_tc<16, true, true>(b, s, m, err) : launch_tc<16, false, true>(b, s, m, err);
             else e = f16 ? launch_tc<16, true, false>(b, s, m, err) : launch_tc<16, false, false>(b, s, m, err);
-        } else {
+        } else if (n == 32) {
             if (deform) e = f16 ? launch_tc<32, true, true>(b, s, m, err) : launch_tc<32, false, true>(b, s, m, err);
             else e = f16 ? launch_tc<32, true, false>(b, s, m, err) : launch_tc<32, false, false>(b, s, m, err);
+        } else {
+            if (deform) e = f16 ? launch_tc<64, true, true>(b, s, m, err) : launch_tc<64, false, true>(b, s, m, err);
+            else e = f16 ? launch_tc<64, true, false>(b, s, m, err) : launch_tc<64, false, false>(b, s, m, err);
         }
         if (e != cudaSuccess) return e;
         if (launches) ++*launches;

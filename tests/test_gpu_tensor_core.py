@@ -71,14 +71,14 @@ def _one_pass_errors(n, precision):
 
 
 @pytest.mark.parametrize("precision", ["bf16x3", "fp16x3"])
-@pytest.mark.parametrize("n", [32, 16])
+@pytest.mark.parametrize("n", [64, 32, 16])
 def test_one_pass_against_fp64_oracle(n, precision):
     err = _one_pass_errors(n, precision)
     assert np.sqrt(np.mean(err ** 2)) < 1e-3, np.sqrt(np.mean(err ** 2))
     assert np.quantile(err, 0.999) < 0.01
 
 
-@pytest.mark.parametrize("n", [32, 16])
+@pytest.mark.parametrize("n", [64, 32, 16])
 def test_fp16_halves_are_more_accurate_than_bf16(n):
     e16 = _one_pass_errors(n, "fp16x3")
     eb = _one_pass_errors(n, "bf16x3")
@@ -138,7 +138,7 @@ def test_deformed_windows_on_tensor_cores_within_0p01_px_of_fp64(precision):
     a, b = _pair(h, seed=6, vmax=7.0)
     cfg = dict(windows=[64, 32, 16], overlap=0.5, final_iterations=1, deform=True)
     an = P.PivAnalyzer(P.PivConfig(precision=precision, **cfg))
-    assert "tensor-core" in an.variant(32) and "tensor-core" in an.variant(16)
+    assert all("tensor-core" in an.variant(n) for n in (64, 32, 16))
     r = an.analyze(an.prepare(a, P.RAW), an.prepare(b, P.RAW))
     an32 = P.PivAnalyzer(P.PivConfig(**cfg))
     r32 = an32.analyze(an32.prepare(a, P.RAW), an32.prepare(b, P.RAW))
