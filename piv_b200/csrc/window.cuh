@@ -21,13 +21,24 @@ __device__ __forceinline__ void amax_combine(float& v, int& i, float ov, int oi)
 // Indices are clamped into the image so that no access can leave it whatever the origin.
 // ---------------------------------------------------------------------------------------------
 //
+// Where a sampler reads the image: the image in global memory through the read-only path. The
+// samplers address pixels by their clamped image coordinates through at(row, col) and step rows
+// by stride().
+struct GlobalSrc {
+    const float* img;
+    int W;
+    __device__ __forceinline__ const float* at(int row, int col) const { return img + (size_t)row * W + col; }
+    __device__ __forceinline__ int stride() const { return W; }
+    __device__ __forceinline__ static float ld(const float* p) { return __ldg(p); }
+};
+
 // Two samplers with identical results. sample_column_direct loads the four bilinear taps of
 // every pixel itself (fewest live registers). sample_column loads each pixel of the patch once
 // and trades the other taps through shuffles (fewest load instructions); it suits the window
 // sizes whose register budget allows it.
-template <int N, int T, bool IMAG>
-__device__ __forceinline__ void sample_column_direct(const float* __restrict__ img, int H, int W, float ox, float oy,
-                                                     int x, int t, float2 (&z)[N / T]) {
+template <int N, int T, bool IMAG, class Src>
+__device__ __forceinline__ void sample_column_direct(const Src& src, int H, int W, float ox, float oy, int x, int t,
+                                                     float2 (&z)[N / T]) {
     constexpr int P = N / T;
     const float fx0 = floorf(ox), fy0 = floorf(oy);
     const int x0 = min(max((int)fx0, 0), W - 1), y0 = min(max((int)fy0, 0), H - 1);
@@ -35,11 +46,12 @@ __device__ __forceinline__ void sample_column_direct(const float* __restrict__ i
     const int c0 = min(x0 + x, W - 1);
     const int dc = min(x0 + x + 1, W - 1) - c0;  // right-hand tap: next float, or the same at the border
     const int last = H - 1 - y0;                  // rows below y0 that exist (row clamp)
-    const float* base = img + (size_t)y0 * W + c0;
+    const int stride = src.stride();
+    const float* base = src.at(y0, c0);
     if (tx < 1e-4f && ty < 1e-4f) {
 #pragma unroll
         for (int p = 0; p < P; ++p) {
-            const float v = __ldg(img + (size_t)min(y0 + t + T * p, H - 1) * W + c0);
+            const float v = Src::ld(base + min(t + T * p, last) * stride);
             if (IMAG) z[p].y = v; else z[p].x = v;
         }
     } else {
@@ -56,15 +68,15 @@ __device__ __forceinline__ void sample_column_direct(const float* __restrict__ i
                 s = __fadd_rn(s, __fmul_rn(w11, br));
                 if (IMAG) z[p].y = s; else z[p].x = s;
             };
-            float top = __ldg(base);
-            float topr = dc ? __ldg(base + 1) : top;
-            if (last >= P) {  // rows y0 .. y0 + P all exist: no row clamp, the row pointer steps by W
+            float top = Src::ld(base);
+            float topr = dc ? Src::ld(base + 1) : top;
+            if (last >= P) {  // rows y0 .. y0 + P all exist: no row clamp, the row pointer steps by the pitch
                 const float* bot = base;
 #pragma unroll
                 for (int p = 0; p < P; ++p) {
-                    bot += W;
-                    const float b0 = __ldg(bot);
-                    const float b1 = dc ? __ldg(bot + 1) : b0;
+                    bot += stride;
+                    const float b0 = Src::ld(bot);
+                    const float b1 = dc ? Src::ld(bot + 1) : b0;
                     blend(p, top, topr, b0, b1);
                     top = b0;
                     topr = b1;
@@ -72,24 +84,23 @@ __device__ __forceinline__ void sample_column_direct(const float* __restrict__ i
             } else {
 #pragma unroll
                 for (int p = 0; p < P; ++p) {
-                    const float* bot = base + (size_t)min(p + 1, last) * W;
-                    const float b0 = __ldg(bot);
-                    const float b1 = dc ? __ldg(bot + 1) : b0;
+                    const float* bot = base + min(p + 1, last) * stride;
+                    const float b0 = Src::ld(bot);
+                    const float b1 = dc ? Src::ld(bot + 1) : b0;
                     blend(p, top, topr, b0, b1);
                     top = b0;
                     topr = b1;
                 }
             }
         } else {
-            const int c1 = c0 + dc;
 #pragma unroll
             for (int p = 0; p < P; ++p) {
-                const float* top = img + (size_t)min(y0 + t + T * p, H - 1) * W;
-                const float* bot = img + (size_t)min(y0 + t + T * p + 1, H - 1) * W;
-                float s = __fmul_rn(w00, __ldg(top + c0));
-                s = __fadd_rn(s, __fmul_rn(w01, __ldg(top + c1)));
-                s = __fadd_rn(s, __fmul_rn(w10, __ldg(bot + c0)));
-                s = __fadd_rn(s, __fmul_rn(w11, __ldg(bot + c1)));
+                const float* top = base + min(t + T * p, last) * stride;
+                const float* bot = base + min(t + T * p + 1, last) * stride;
+                float s = __fmul_rn(w00, Src::ld(top));
+                s = __fadd_rn(s, __fmul_rn(w01, Src::ld(top + dc)));
+                s = __fadd_rn(s, __fmul_rn(w10, Src::ld(bot)));
+                s = __fadd_rn(s, __fmul_rn(w11, Src::ld(bot + dc)));
                 if (IMAG) z[p].y = s; else z[p].x = s;
             }
         }
@@ -101,9 +112,9 @@ __device__ __forceinline__ void sample_column_direct(const float* __restrict__ i
 // a shuffle, and the row below from the lane holding that row (the next register for T = 1, the
 // next lane of the line otherwise). Lanes whose neighbour is outside their warp or beyond the
 // window load the missing value themselves.
-template <int N, int T, bool IMAG>
-__device__ __forceinline__ void sample_column(const float* __restrict__ img, int H, int W, float ox, float oy, int x,
-                                              int t, float2 (&z)[N / T]) {
+template <int N, int T, bool IMAG, class Src>
+__device__ __forceinline__ void sample_column(const Src& src, int H, int W, float ox, float oy, int x, int t,
+                                              float2 (&z)[N / T]) {
     constexpr int P = N / T;
     const int lane = threadIdx.x & 31;
     const float fx0 = floorf(ox), fy0 = floorf(oy);
@@ -112,25 +123,26 @@ __device__ __forceinline__ void sample_column(const float* __restrict__ img, int
     const int c0 = min(x0 + x, W - 1);
     const int dc = min(x0 + x + 1, W - 1) - c0;  // right-hand tap: next float, or the same at the border
     const int last = H - 1 - y0;                  // rows below y0 that exist (row clamp)
-    const float* base = img + (size_t)y0 * W + c0;
+    const int stride = src.stride();
+    const float* base = src.at(y0, c0);
     const bool integer = tx < 1e-4f && ty < 1e-4f;
     float top[P];
 #pragma unroll
-    for (int p = 0; p < P; ++p) top[p] = __ldg(base + (size_t)min(t + T * p, last) * W);
+    for (int p = 0; p < P; ++p) top[p] = Src::ld(base + min(t + T * p, last) * stride);
     // Every lane runs the shuffles below (a warp may hold windows of both kinds); an integer
     // window then keeps its copied values.
     // Row N of the patch (below the window), held by the last lane of each line.
-    const float* rowN = base + (size_t)min(N, last) * W;
-    const float extra = __ldg(rowN);
+    const float* rowN = base + min(N, last) * stride;
+    const float extra = Src::ld(rowN);
     const bool edge = lane + T >= 32 || x == N - 1;  // right neighbour not reachable by a shuffle
     float right[P];
 #pragma unroll
     for (int p = 0; p < P; ++p) {
         right[p] = __shfl_down_sync(0xffffffffu, top[p], T);
-        if (edge) right[p] = __ldg(base + (size_t)min(t + T * p, last) * W + dc);
+        if (edge) right[p] = Src::ld(base + min(t + T * p, last) * stride + dc);
     }
     float extra_r = __shfl_down_sync(0xffffffffu, extra, T);
-    if (edge) extra_r = __ldg(rowN + dc);
+    if (edge) extra_r = Src::ld(rowN + dc);
     const float ux = __fsub_rn(1.0f, tx), uy = __fsub_rn(1.0f, ty);
     const float w00 = __fmul_rn(ux, uy), w01 = __fmul_rn(tx, uy), w10 = __fmul_rn(ux, ty), w11 = __fmul_rn(tx, ty);
 #pragma unroll
