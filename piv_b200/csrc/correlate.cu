@@ -283,19 +283,6 @@ __device__ __forceinline__ void correlate_body(const CorrParams& prm, int block,
             sample_column_direct<N, T, true>(gb, prm.H, prm.W, org[1].z, org[1].w, line, t, z1);
         }
     }
-    // Cells past the end are zeroed, whatever they sampled: the second cell of a pair shares the
-    // packed inverse FFT with the first, so its values must not depend on the sampling path
-    // (uniform and deformed windows sample them at different places).
-    {
-        const bool dead0 = base_cell >= prm.ncells, dead1 = base_cell + WPG - 1 >= prm.ncells;
-#pragma unroll
-        for (int p = 0; p < P; ++p) {
-            if (dead0) z0[p] = make_float2(0.f, 0.f);
-            if constexpr (PAIR) {
-                if (dead1) z1[p] = make_float2(0.f, 0.f);
-            }
-        }
-    }
     {
         float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
