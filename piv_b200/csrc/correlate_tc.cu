@@ -88,6 +88,9 @@ struct TcCfg {
     static_assert((size_t)128 * PLD * 4 <= 2 * A_BYTES, "plane fits in the operand buffers");
     static_assert(N % 16 == 0 && 128 % N == 0, "tile shape");
     static_assert(SMEM <= 232448, "shared memory");
+    // CTAs per SM: two at 16 px (83 KB of shared memory and 128 TMEM columns each, registers
+    // capped at 64 per thread), one otherwise
+    static constexpr int CTAS_PER_SM = N == 16 ? 2 : 1;
     // fixed operand factors (see the top of the file) and the plane's exact rescale
     static constexpr int LOG2N = N == 16 ? 4 : (N == 32 ? 5 : 6);
     static constexpr float CROSS_SCALE = (4 * LOG2N > 12) ? 1.0f / (float)(1 << (4 * LOG2N - 12)) : 1.0f;
@@ -227,7 +230,7 @@ __device__ __forceinline__ float win_max(float v, float* red, int i, int wg) {
 }
 
 template <int N, bool F16, bool DEFORM>
-__global__ void __launch_bounds__(TcCfg<N>::THREADS, 1)
+__global__ void __launch_bounds__(TcCfg<N>::THREADS, TcCfg<N>::CTAS_PER_SM)
     correlate_tc_kernel(const __grid_constant__ CorrBatch batch, const uint4* __restrict__ mats, int total_tiles,
                         unsigned int* err) {
     using C = TcCfg<N>;
@@ -827,7 +830,7 @@ static cudaError_t launch_tc(CorrBatch b, cudaStream_t s, const uint4* mats, uns
     auto kern = correlate_tc_kernel<N, F16, DEFORM>;
     e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
     if (e != cudaSuccess) return e;
-    const long long ctas = std::min<long long>((total + C::NWG - 1) / C::NWG, (long long)sms);
+    const long long ctas = std::min<long long>((total + C::NWG - 1) / C::NWG, (long long)sms * C::CTAS_PER_SM);
     kern<<<(unsigned)ctas, C::THREADS, C::SMEM, s>>>(b, mats, (int)total, err);
     return cudaGetLastError();
 }
