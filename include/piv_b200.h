@@ -362,7 +362,8 @@ int32_t piv_server_set_fused(PivServer* server, int32_t fused);
 int32_t piv_server_set_manual(PivServer* server, int32_t manual);
 /* Grants `steps` steps (admission, then one pass of every admitted request) and blocks until the
  * scheduler has taken them (a step with nothing to launch counts), or PIV_ERR_TIMEOUT after
- * timeout_ms (< 0: no bound). */
+ * timeout_ms (< 0: no bound); PIV_ERR_ARGUMENT if manual stepping ends meanwhile (set_manual(0)
+ * from another thread, or destroy). */
 int32_t piv_server_advance(PivServer* server, int32_t steps, double timeout_ms);
 int32_t piv_server_stats(PivServer* server, PivServerStatsC* stats);
 

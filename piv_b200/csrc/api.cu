@@ -2317,6 +2317,7 @@ void piv_server_destroy(PivServer* sv) {
         sv->manual = false;  // finish what is queued without waiting for granted steps
     }
     sv->cv_submit.notify_all();
+    sv->cv_step.notify_all();
     if (sv->worker.joinable()) sv->worker.join();
     cudaSetDevice(sv->device);
     cudaStreamSynchronize(sv->stream);
@@ -2482,6 +2483,7 @@ int32_t piv_server_set_manual(PivServer* sv, int32_t manual) {
         sv->granted = 0;
     }
     sv->cv_submit.notify_all();
+    sv->cv_step.notify_all();  // an advance still waiting returns
     return PIV_OK;
 }
 
@@ -2493,8 +2495,10 @@ int32_t piv_server_advance(PivServer* sv, int32_t steps, double timeout_ms) {
     sv->granted += steps;
     sv->cv_submit.notify_all();
     const bool ok = sv->cv_step.wait_for(lk, std::chrono::duration<double, std::milli>(timeout_ms < 0 ? 1e12 : timeout_ms),
-                                         [sv, target] { return sv->stepped >= target; });
+                                         [sv, target] { return sv->stepped >= target || !sv->manual || sv->stop; });
     if (!ok) return fail(PIV_ERR_TIMEOUT, "%d steps not taken within %g ms", steps, timeout_ms);
+    if (sv->stepped < target)
+        return fail(PIV_ERR_ARGUMENT, "manual stepping ended (piv_server_set_manual(0) or destroy) before the steps were taken");
     return PIV_OK;
 }
 
