@@ -68,6 +68,20 @@ __device__ __forceinline__ float2 mul_mi(float2 a) {
         return make_float2(-a.y, a.x);
 }
 
+// v * w_N^j (DIR = +1) or v * conj(w_N^j) (DIR = -1). Quarter and half turns are applied as the
+// exact swap and sign changes they are; in unrolled loops j is a constant, so the choice costs
+// nothing. (The root table holds f64 values rounded to f32, so its quarter turn carries a
+// cosine of 6.1e-17 instead of 0; multiplying by it changes a result only when one component
+// exceeds the other by about 2^30, so the exact form agrees except in that last bit.)
+template <int N, int DIR>
+__device__ __forceinline__ float2 twiddle(float2 v, int j, const float2 w) {
+    if (j == 0) return v;
+    if (4 * j == N) return mul_mi<DIR>(v);
+    if (2 * j == N) return make_float2(-v.x, -v.y);
+    if (4 * j == 3 * N) return mul_mi<-DIR>(v);
+    return cmulw<DIR>(v, w);
+}
+
 template <int R, int DIR>
 __device__ __forceinline__ void butterfly(float2 (&t)[R]) {
     if constexpr (R == 2) {
@@ -110,7 +124,10 @@ __device__ __forceinline__ void dft_rec(const float2* in, float2* out) {
 #pragma unroll
             for (int q = 0; q < R; ++q) {
                 float2 v = out[q * M + k];
-                if (q > 0 && k > 0) v = cmulw<DIR>(v, croot<N>((q * k * (N / LEN)) % N));
+                if (q > 0 && k > 0) {
+                    const int j = (q * k * (N / LEN)) % N;
+                    v = twiddle<N, DIR>(v, j, croot<N>(j));
+                }
                 t[q] = v;
             }
             butterfly<R, DIR>(t);
@@ -145,19 +162,33 @@ __device__ __forceinline__ int bitrev(int t) {
 // Both are written as one signed add fma(s, x, o) (s = +1 or -1, an exact single rounding like a
 // plain add) and one complex multiply by w, with w = 1 on the lower lane (exact up to the sign of
 // a zero), so a lane issues no instructions for the other lane's formula.
+// The stage twiddle of the upper lane is w_N^((t mod h) * N/(2h)): 1 for h = 1, 1 or a quarter
+// turn for h = 2, applied exactly (twiddle()); other stages multiply.
 template <int N, int T, int P, int DIR>
 __device__ __forceinline__ void xlane_dif(float2 (&x)[P], int t, const float2* s_roots) {
 #pragma unroll
     for (int h = T / 2; h >= 1; h >>= 1) {
         const bool upper = (t & h) != 0;
         const float sg = upper ? -1.0f : 1.0f;
-        const float2 w = upper ? s_roots[(t & (h - 1)) * (N / (2 * h))] : make_float2(1.0f, 0.0f);
+        if (h <= 2) {
+            const bool quarter = h == 2 && upper && (t & 1);  // w = w_N^(N/4)
 #pragma unroll
-        for (int i = 0; i < P; ++i) {
-            float2 o;
-            o.x = __shfl_xor_sync(0xffffffffu, x[i].x, h);
-            o.y = __shfl_xor_sync(0xffffffffu, x[i].y, h);
-            x[i] = cmulw<DIR>(make_float2(fmaf(sg, x[i].x, o.x), fmaf(sg, x[i].y, o.y)), w);
+            for (int i = 0; i < P; ++i) {
+                float2 o;
+                o.x = __shfl_xor_sync(0xffffffffu, x[i].x, h);
+                o.y = __shfl_xor_sync(0xffffffffu, x[i].y, h);
+                const float2 v = make_float2(fmaf(sg, x[i].x, o.x), fmaf(sg, x[i].y, o.y));
+                x[i] = quarter ? mul_mi<DIR>(v) : v;
+            }
+        } else {
+            const float2 w = upper ? s_roots[(t & (h - 1)) * (N / (2 * h))] : make_float2(1.0f, 0.0f);
+#pragma unroll
+            for (int i = 0; i < P; ++i) {
+                float2 o;
+                o.x = __shfl_xor_sync(0xffffffffu, x[i].x, h);
+                o.y = __shfl_xor_sync(0xffffffffu, x[i].y, h);
+                x[i] = cmulw<DIR>(make_float2(fmaf(sg, x[i].x, o.x), fmaf(sg, x[i].y, o.y)), w);
+            }
         }
     }
 }
@@ -173,12 +204,19 @@ __device__ __forceinline__ void xlane_dit(float2 (&x)[P], int t, const float2* s
 #pragma unroll
     for (int h = 1; h < T; h <<= 1) {
         const bool upper = (t & h) != 0;
+        // the upper lane's twiddle: 1 for h = 1, 1 or a quarter turn for h = 2 (exact forms)
+        const bool quarter = h == 2 && upper && (t & 1);
+        auto tw = [&](float2 v, float2 w) -> float2 {
+            if (h == 1) return v;
+            if (h == 2) return quarter ? mul_mi<DIR>(v) : v;
+            return cmulw<DIR>(v, w);
+        };
         if constexpr (SIGNED) {
             const float sg = upper ? -1.0f : 1.0f;
             const float2 w = upper ? s_roots[(t & (h - 1)) * (N / (2 * h))] : make_float2(1.0f, 0.0f);
 #pragma unroll
             for (int i = 0; i < P; ++i) {
-                const float2 v = cmulw<DIR>(x[i], w);
+                const float2 v = tw(x[i], w);
                 float2 o;
                 o.x = __shfl_xor_sync(0xffffffffu, v.x, h);
                 o.y = __shfl_xor_sync(0xffffffffu, v.y, h);
@@ -188,7 +226,7 @@ __device__ __forceinline__ void xlane_dit(float2 (&x)[P], int t, const float2* s
             const float2 w = s_roots[(t & (h - 1)) * (N / (2 * h))];
 #pragma unroll
             for (int i = 0; i < P; ++i) {
-                float2 v = upper ? cmulw<DIR>(x[i], w) : x[i];
+                float2 v = upper ? tw(x[i], w) : x[i];
                 float2 o;
                 o.x = __shfl_xor_sync(0xffffffffu, v.x, h);
                 o.y = __shfl_xor_sync(0xffffffffu, v.y, h);
