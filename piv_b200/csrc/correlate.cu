@@ -64,6 +64,27 @@ struct CorrCfg {
     __host__ __device__ static constexpr int B(int ky, int kx) {
         return T == 1 ? ky * LD + kx : ky * LD + (ky / P) * Q + kx + kx / P;
     }
+    // Single windows (the N = 128 inverse through half-size stages, T2 = 2T lanes per line):
+    //   BS(ky, kx)  the spectrum, rows of N + 1 (= 1 mod 16) with each 16-column chunk rotated by
+    //               2 * (chunk index), so that both the forward stores (4 rows x T lanes) and the
+    //               half-warp reads of the inverse (2 rows x T2 lanes, and their Hermitian
+    //               partners) hit 16 distinct bank pairs;
+    //   YO(r, x)    the half-inverse rows 0..N/2, x XOR f(r) with f(r) = 8 (r odd) | (r & 6):
+    //               two adjacent rows by T2 lanes, and eight adjacent rows by two columns, each
+    //               hit 16 distinct bank pairs;
+    //   CP(y, x)    the correlation plane and its vertical 3-maxima (float), rows of N plus 4 per
+    //               block of 16 rows: a warp's 8 row blocks x 4 columns hit 32 distinct banks.
+    // CP lives in plane0 after the YO rows (CP_OFF floats), the 3-maxima in plane1.
+    __host__ __device__ static constexpr int BS(int ky, int kx) {
+        return ky * (N + 1) + ((kx & ~15) | ((kx + 2 * (kx >> 4)) & 15));
+    }
+    __host__ __device__ static constexpr int YO(int r, int x) { return r * N + (x ^ (((r & 1) << 3) | (r & 6))); }
+    __host__ __device__ static constexpr int CP(int y, int x) { return y * N + x + 4 * (y >> 4); }
+    static constexpr int CP_OFF = 2 * (N / 2 + 1) * N;
+    static_assert(PAIR || (N == 128 && BS(N - 1, N - 1) < PLANE_ELEMS &&
+                           CP_OFF + CP(N - 1, N - 1) < 2 * PLANE_ELEMS &&
+                           sizeof(float) * (size_t)(CP(N - 1, N - 1) + 1) <= PLANE1),
+                  "single-window planes");
     static constexpr size_t SMEM = (size_t)G * (PLANE0 + PLANE1) + sizeof(float2) * N + sizeof(float) * (size_t)G * NSEG * 4 +
                                    (DEFORM ? sizeof(float) * N : 0) + 64;
 };
@@ -340,158 +361,267 @@ __device__ __forceinline__ void correlate_body(const CorrParams& prm, int block,
     group_sync<C>(g);
     fft_line_interleaved<N, T, 1>(z0, t, s_roots);
     if constexpr (PAIR) fft_line_interleaved<N, T, 1>(z1, t, s_roots);
-    // ------------------------------------------------------------------ cross spectra
-#pragma unroll
-    for (int k = 0; k < P; ++k) {
-        plane0[C::B(line, k + P * rt)] = z0[k];
-        if constexpr (PAIR) plane1[C::B(line, k + P * rt)] = z1[k];
-    }
-    group_sync<C>(g);
-    {
-        const int my = (N - line) % N;
-#pragma unroll
-        for (int k = 0; k < P; ++k) {
-            const int kx = (N - (k + P * rt)) % N;
-            const float2 c0 = cross4(z0[k], plane0[C::B(my, kx)]);
-            if constexpr (PAIR) {
-                const float2 c1 = cross4(z1[k], plane1[C::B(my, kx)]);
-                z0[k] = make_float2(c0.x - c1.y, c0.y + c1.x);  // D = C0 + i*C1
-            } else {
-                z0[k] = c0;
-            }
-        }
-    }
-    group_sync<C>(g);
-
-    // ------------------------------------------------------------------ inverse 2-D FFT
-    fft_line_blocked<N, T, -1>(z0, t, s_roots);
-#pragma unroll
-    for (int k = 0; k < P; ++k) plane0[C::A(line, t + T * k)] = z0[k];
-    group_sync<C>(g);
-#pragma unroll
-    for (int q = 0; q < P; ++q) z0[q] = plane0[C::A(t + T * q, line)];
-    group_sync<C>(g);
-    fft_line_interleaved<N, T, -1>(z0, t, s_roots);
-    // Lane now holds corr[y = k + P*rt][x = line]; scale as the reference does (c *= scale).
-#pragma unroll
-    for (int k = 0; k < P; ++k) {
-        z0[k].x = z0[k].x * scale[0];
-        z0[k].y = PAIR ? z0[k].y * scale[WPG - 1] : 0.0f;
-        plane0[C::A(k + P * rt, line)] = z0[k];
-    }
-
-    // ------------------------------------------------------------------ find_peak
-    // Argmax of both planes (lowest row-major index among equal maxima). A lane's indices grow
-    // with k, so inside the lane a strictly larger value is the only one that replaces the best.
+    // ------------------------------------------------------------------ cross spectra, inverse, find_peak
+    // Argmax of the planes (lowest row-major index among equal maxima). A lane visits its cells
+    // in increasing index order, so inside the lane a strictly larger value is the only one that
+    // replaces the best.
     float2 best = make_float2(-INFINITY, -INFINITY);
     int bi0 = 0x7fffffff, bi1 = 0x7fffffff;
-#pragma unroll
-    for (int k = 0; k < P; ++k) {
-        const int idx = (k + P * rt) * N + line;
-        if (z0[k].x > best.x) {
-            best.x = z0[k].x;
-            bi0 = idx;
-        }
-        if (PAIR && z0[k].y > best.y) {
-            best.y = z0[k].y;
-            bi1 = idx;
-        }
-    }
-    group_argmax<C>(best.x, bi0, s_red, g, gt);
-    if constexpr (PAIR) group_argmax<C>(best.y, bi1, s_red, g, gt);
-    if (!(best.x > -INFINITY)) bi0 = 0;
-    if (!(best.y > -INFINITY)) bi1 = 0;
-    group_sync<C>(g);  // the scaled planes are complete in shared memory
+    float2 second = make_float2(-INFINITY, -INFINITY);
+    float* const cplane = reinterpret_cast<float*>(plane0) + C::CP_OFF;  // single windows
+    float* const vm = reinterpret_cast<float*>(plane1_raw);  // vertical 3-maxima: float2 (PAIR) or float
     auto at = [&](int ch, int y, int x) -> float {
-        const float2 v = plane0[C::A(y % N, x % N)];
-        return ch == 0 ? v.x : v.y;
+        if constexpr (PAIR) {
+            const float2 v = plane0[C::A(y % N, x % N)];
+            return ch == 0 ? v.x : v.y;
+        } else {
+            return cplane[C::CP(y % N, x % N)];
+        }
+    };
+    auto circ = [](int a, int b) {
+        const int d = abs(a - b);
+        return min(d, N - d);
     };
     // Footprint of the primary peak (correlate.rs:242-254): half-width along +-y, +-x.
-    if (gt < 4 * WPG) {
-        const int ch = gt >> 2, dir = gt & 3;
-        const int bidx = ch == 0 ? bi0 : bi1;
-        const int by = bidx / N, bx = bidx % N;
-        const int sy = dir == 0 ? 1 : (dir == 1 ? N - 1 : 0);
-        const int sx = dir == 2 ? 1 : (dir == 3 ? N - 1 : 0);
-        const float half = 0.5f * (ch == 0 ? best.x : best.y);
-        int k = 0;
-        while (k < N / 2 && at(ch, by + k * sy, bx + k * sx) > half) ++k;
-        s_hw[g][gt] = k;
-    }
-    // Vertical 3-maximum of each column, for the local-maximum test.
-    float* vm = reinterpret_cast<float*>(plane1_raw);  // float2 (PAIR) or float (single) per cell
-    {
-        float2 up, dn;  // neighbours across this lane's block boundary (rows k = -1 and P)
-        if constexpr (T == 1) {
-            up = z0[P - 1];
-            dn = z0[0];
-        } else {
-            const int lane = threadIdx.x & 31;
-            const int base = lane - t;  // first lane of this line
-            const int src_up = base + bitrev<T>((rt + T - 1) % T);
-            const int src_dn = base + bitrev<T>((rt + 1) % T);
-            up.x = __shfl_sync(0xffffffffu, z0[P - 1].x, src_up);
-            up.y = __shfl_sync(0xffffffffu, z0[P - 1].y, src_up);
-            dn.x = __shfl_sync(0xffffffffu, z0[0].x, src_dn);
-            dn.y = __shfl_sync(0xffffffffu, z0[0].y, src_dn);
+    auto footprint = [&]() {
+        if (gt < 4 * WPG) {
+            const int ch = gt >> 2, dir = gt & 3;
+            const int bidx = ch == 0 ? bi0 : bi1;
+            const int by = bidx / N, bx = bidx % N;
+            const int sy = dir == 0 ? 1 : (dir == 1 ? N - 1 : 0);
+            const int sx = dir == 2 ? 1 : (dir == 3 ? N - 1 : 0);
+            const float half = 0.5f * (ch == 0 ? best.x : best.y);
+            int k = 0;
+            while (k < N / 2 && at(ch, by + k * sy, bx + k * sx) > half) ++k;
+            s_hw[g][gt] = k;
         }
+    };
+    if constexpr (PAIR) {
+        // Both windows' spectra, then D = C0 + i*C1: one complex inverse gives both (real)
+        // correlation planes, window 0 in the real part and window 1 in the imaginary part.
 #pragma unroll
         for (int k = 0; k < P; ++k) {
-            const float2 a = k == 0 ? up : z0[k - 1];
-            const float2 b = k == P - 1 ? dn : z0[k + 1];
-            const float m0 = fmaxf(fmaxf(a.x, b.x), z0[k].x);
-            const int o = C::A(k + P * rt, line);
-            if constexpr (PAIR) {
-                reinterpret_cast<float2*>(vm)[o] = make_float2(m0, fmaxf(fmaxf(a.y, b.y), z0[k].y));
-            } else {
-                vm[o] = m0;
+            plane0[C::B(line, k + P * rt)] = z0[k];
+            plane1[C::B(line, k + P * rt)] = z1[k];
+        }
+        group_sync<C>(g);
+        {
+            const int my = (N - line) % N;
+#pragma unroll
+            for (int k = 0; k < P; ++k) {
+                const int kx = (N - (k + P * rt)) % N;
+                const float2 c0 = cross4(z0[k], plane0[C::B(my, kx)]);
+                const float2 c1 = cross4(z1[k], plane1[C::B(my, kx)]);
+                z0[k] = make_float2(c0.x - c1.y, c0.y + c1.x);  // D = C0 + i*C1
             }
         }
-    }
-    group_sync<C>(g);
-    const int hw0 = max(max(s_hw[g][0], s_hw[g][1]), max(s_hw[g][2], s_hw[g][3]));
-    const int ex0 = max((int)ceilf(1.5f * (float)hw0), 2);
-    int ex1 = 0;
-    if constexpr (PAIR) {
-        const int hw1 = max(max(s_hw[g][4], s_hw[g][5]), max(s_hw[g][6], s_hw[g][7]));
-        ex1 = max((int)ceilf(1.5f * (float)hw1), 2);
-    }
-    // Highest local maximum outside the footprint (correlate.rs:255-267): v is a local maximum
-    // when it equals the maximum of its circular 3x3 neighbourhood.
-    float2 second = make_float2(-INFINITY, -INFINITY);
-    {
-        const int xl = (line + N - 1) % N, xr = (line + 1) % N;
-        const int by0 = bi0 / N, bx0 = bi0 % N, by1 = bi1 / N, bx1 = bi1 % N;
-        auto circ = [](int a, int b) {
-            const int d = abs(a - b);
-            return min(d, N - d);
-        };
-        const int cx0 = circ(line, bx0), cx1 = circ(line, bx1);
-        // A cell is outside the footprint when max(circular row distance, column distance) > ex:
-        // one bit of a per-lane mask of eligible rows (the direct test at 128 rows, where the
-        // mask measured slower).
-        constexpr bool MASK = N < 128;
-        const unsigned el0 = MASK ? eligible_rows<N, P>(by0, ex0, cx0, rt) : 0u;
-        const unsigned el1 = MASK && PAIR ? eligible_rows<N, P>(by1, ex1, cx1, rt) : 0u;
-        auto outside = [&](int k, int y, unsigned el, int by, int cx, int ex) {
-            return MASK ? ((el >> k) & 1u) != 0u : max(circ(y, by), cx) > ex;
-        };
+        group_sync<C>(g);
+
+        fft_line_blocked<N, T, -1>(z0, t, s_roots);
+#pragma unroll
+        for (int k = 0; k < P; ++k) plane0[C::A(line, t + T * k)] = z0[k];
+        group_sync<C>(g);
+#pragma unroll
+        for (int q = 0; q < P; ++q) z0[q] = plane0[C::A(t + T * q, line)];
+        group_sync<C>(g);
+        fft_line_interleaved<N, T, -1>(z0, t, s_roots);
+        // Lane now holds corr[y = k + P*rt][x = line]; scale as the reference does (c *= scale).
 #pragma unroll
         for (int k = 0; k < P; ++k) {
-            const int y = k + P * rt;
-            if constexpr (PAIR) {
-                const float2* v2 = reinterpret_cast<const float2*>(vm);
+            z0[k].x = z0[k].x * scale[0];
+            z0[k].y = z0[k].y * scale[WPG - 1];
+            plane0[C::A(k + P * rt, line)] = z0[k];
+        }
+
+#pragma unroll
+        for (int k = 0; k < P; ++k) {
+            const int idx = (k + P * rt) * N + line;
+            if (z0[k].x > best.x) {
+                best.x = z0[k].x;
+                bi0 = idx;
+            }
+            if (z0[k].y > best.y) {
+                best.y = z0[k].y;
+                bi1 = idx;
+            }
+        }
+        group_argmax<C>(best.x, bi0, s_red, g, gt);
+        group_argmax<C>(best.y, bi1, s_red, g, gt);
+        if (!(best.x > -INFINITY)) bi0 = 0;
+        if (!(best.y > -INFINITY)) bi1 = 0;
+        group_sync<C>(g);  // the scaled planes are complete in shared memory
+        footprint();
+        // Vertical 3-maximum of each column, for the local-maximum test.
+        {
+            float2 up, dn;  // neighbours across this lane's block boundary (rows k = -1 and P)
+            if constexpr (T == 1) {
+                up = z0[P - 1];
+                dn = z0[0];
+            } else {
+                const int lane = threadIdx.x & 31;
+                const int base = lane - t;  // first lane of this line
+                const int src_up = base + bitrev<T>((rt + T - 1) % T);
+                const int src_dn = base + bitrev<T>((rt + 1) % T);
+                up.x = __shfl_sync(0xffffffffu, z0[P - 1].x, src_up);
+                up.y = __shfl_sync(0xffffffffu, z0[P - 1].y, src_up);
+                dn.x = __shfl_sync(0xffffffffu, z0[0].x, src_dn);
+                dn.y = __shfl_sync(0xffffffffu, z0[0].y, src_dn);
+            }
+#pragma unroll
+            for (int k = 0; k < P; ++k) {
+                const float2 a = k == 0 ? up : z0[k - 1];
+                const float2 b = k == P - 1 ? dn : z0[k + 1];
+                reinterpret_cast<float2*>(vm)[C::A(k + P * rt, line)] =
+                    make_float2(fmaxf(fmaxf(a.x, b.x), z0[k].x), fmaxf(fmaxf(a.y, b.y), z0[k].y));
+            }
+        }
+        group_sync<C>(g);
+        const int hw0 = max(max(s_hw[g][0], s_hw[g][1]), max(s_hw[g][2], s_hw[g][3]));
+        const int ex0 = max((int)ceilf(1.5f * (float)hw0), 2);
+        const int hw1 = max(max(s_hw[g][4], s_hw[g][5]), max(s_hw[g][6], s_hw[g][7]));
+        const int ex1 = max((int)ceilf(1.5f * (float)hw1), 2);
+        // Highest local maximum outside the footprint (correlate.rs:255-267): v is a local
+        // maximum when it equals the maximum of its circular 3x3 neighbourhood. A cell is outside
+        // the footprint when max(circular row distance, column distance) > ex: one bit of a
+        // per-lane mask of eligible rows.
+        {
+            const int xl = (line + N - 1) % N, xr = (line + 1) % N;
+            const int by0 = bi0 / N, bx0 = bi0 % N, by1 = bi1 / N, bx1 = bi1 % N;
+            const unsigned el0 = eligible_rows<N, P>(by0, ex0, circ(line, bx0), rt);
+            const unsigned el1 = eligible_rows<N, P>(by1, ex1, circ(line, bx1), rt);
+            const float2* v2 = reinterpret_cast<const float2*>(vm);
+#pragma unroll
+            for (int k = 0; k < P; ++k) {
+                const int y = k + P * rt;
                 const float2 l = v2[C::A(y, xl)], c = v2[C::A(y, line)], r = v2[C::A(y, xr)];
                 const float h0 = fmaxf(fmaxf(l.x, r.x), c.x), h1 = fmaxf(fmaxf(l.y, r.y), c.y);
-                if (z0[k].x == h0 && outside(k, y, el0, by0, cx0, ex0)) second.x = fmaxf(second.x, z0[k].x);
-                if (z0[k].y == h1 && outside(k, y, el1, by1, cx1, ex1)) second.y = fmaxf(second.y, z0[k].y);
-            } else {
-                const float h0 = fmaxf(fmaxf(vm[C::A(y, xl)], vm[C::A(y, xr)]), vm[C::A(y, line)]);
-                if (z0[k].x == h0 && outside(k, y, el0, by0, cx0, ex0)) second.x = fmaxf(second.x, z0[k].x);
+                if (z0[k].x == h0 && ((el0 >> k) & 1u)) second.x = fmaxf(second.x, z0[k].x);
+                if (z0[k].y == h1 && ((el1 >> k) & 1u)) second.y = fmaxf(second.y, z0[k].y);
             }
         }
+        second = group_max2<C>(second, s_red, g, gt);
+    } else {
+        // One window: z0 is the spectrum of a + i*b and the cross spectrum C is Hermitian
+        // (C[-k] = conj C[k], exactly so in floating point: cross4(m, z) = conj cross4(z, m)), so
+        // its inverse is real and half of a complex inverse computes it:
+        //  1. rows ky = 0..N/2 only: Y[ky][x] = sum_kx C[ky][kx] w^(kx x), where Y[-ky] = conj Y[ky]
+        //     and rows 0 and N/2 are real, so those two share one line (C[0] + i*C[N/2]);
+        //  2. columns in pairs (x, x + N/2): Z[ky] = Y[ky][x] + i*Y[ky][x + N/2] (rows above N/2
+        //     from their conjugate partners); the inverse of Z is corr[.][x] + i*corr[.][x + N/2].
+        // Each stage is N/2 lines of T2 = 2T lanes (P2 = N/T2 values each) on the same threads.
+        constexpr int T2 = 2 * T, P2 = N / T2;
+        static_assert(N == 128 && T == 4 && G == 1, "single-window layout");
+        const int line2 = gt / T2, t2 = gt - line2 * T2, rt2 = bitrev<T2>(t2);
+        const int lane = threadIdx.x & 31;
+#pragma unroll
+        for (int k = 0; k < P; ++k) plane0[C::BS(line, k + P * rt)] = z0[k];
+        group_sync<C>(g);
+        float2 y[P2];
+        {
+            const int ky = line2, my = (N - line2) % N;
+#pragma unroll
+            for (int p = 0; p < P2; ++p) {
+                const int kx = p + P2 * rt2, mkx = (N - kx) % N;
+                y[p] = cross4(plane0[C::BS(ky, kx)], plane0[C::BS(my, mkx)]);
+            }
+            if (line2 == 0) {
+#pragma unroll
+                for (int p = 0; p < P2; ++p) {
+                    const int kx = p + P2 * rt2, mkx = (N - kx) % N;
+                    const float2 c = cross4(plane0[C::BS(N / 2, kx)], plane0[C::BS(N / 2, mkx)]);
+                    y[p] = make_float2(y[p].x - c.y, y[p].y + c.x);  // C[0] + i*C[N/2]
+                }
+            }
+        }
+        fft_line_blocked<N, T2, -1>(y, t2, s_roots);  // lane holds Y[line2][t2 + T2*k]
+        group_sync<C>(g);                               // every spectrum read is done
+        if (line2 == 0) {
+#pragma unroll
+            for (int k = 0; k < P2; ++k) {
+                plane0[C::YO(0, t2 + T2 * k)] = make_float2(y[k].x, 0.0f);
+                plane0[C::YO(N / 2, t2 + T2 * k)] = make_float2(y[k].y, 0.0f);
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < P2; ++k) plane0[C::YO(line2, t2 + T2 * k)] = y[k];
+        }
+        group_sync<C>(g);
+        const int x1 = line2, x2 = line2 + N / 2;
+#pragma unroll
+        for (int q = 0; q < P2; ++q) {
+            const int ky = t2 + T2 * q;
+            if (q < P2 / 2) {  // ky < N/2
+                const float2 a = plane0[C::YO(ky, x1)], b = plane0[C::YO(ky, x2)];
+                y[q] = make_float2(a.x - b.y, a.y + b.x);
+            } else {  // ky >= N/2: Y[ky] = conj Y[N - ky]
+                const float2 a = plane0[C::YO(N - ky, x1)], b = plane0[C::YO(N - ky, x2)];
+                y[q] = make_float2(a.x + b.y, b.x - a.y);
+            }
+        }
+        fft_line_interleaved<N, T2, -1>(y, t2, s_roots);
+        // Lane now holds corr[k + P2*rt2][x1] (real part) and corr[k + P2*rt2][x2] (imaginary
+        // part); scale as the reference does (c *= scale).
+#pragma unroll
+        for (int k = 0; k < P2; ++k) {
+            y[k].x = y[k].x * scale[0];
+            y[k].y = y[k].y * scale[0];
+            cplane[C::CP(k + P2 * rt2, x1)] = y[k].x;
+            cplane[C::CP(k + P2 * rt2, x2)] = y[k].y;
+        }
+#pragma unroll
+        for (int k = 0; k < P2; ++k) {
+            const int row = (k + P2 * rt2) * N;
+            if (y[k].x > best.x) {
+                best.x = y[k].x;
+                bi0 = row + x1;
+            }
+            if (y[k].y > best.x) {
+                best.x = y[k].y;
+                bi0 = row + x2;
+            }
+        }
+        group_argmax<C>(best.x, bi0, s_red, g, gt);
+        if (!(best.x > -INFINITY)) bi0 = 0;
+        group_sync<C>(g);  // the scaled plane is complete in shared memory
+        footprint();
+        {
+            const int base = lane - t2;  // first lane of this column pair
+            const int src_up = base + bitrev<T2>((rt2 + T2 - 1) % T2);
+            const int src_dn = base + bitrev<T2>((rt2 + 1) % T2);
+            float2 up, dn;
+            up.x = __shfl_sync(0xffffffffu, y[P2 - 1].x, src_up);
+            up.y = __shfl_sync(0xffffffffu, y[P2 - 1].y, src_up);
+            dn.x = __shfl_sync(0xffffffffu, y[0].x, src_dn);
+            dn.y = __shfl_sync(0xffffffffu, y[0].y, src_dn);
+#pragma unroll
+            for (int k = 0; k < P2; ++k) {
+                const float2 a = k == 0 ? up : y[k - 1];
+                const float2 b = k == P2 - 1 ? dn : y[k + 1];
+                vm[C::CP(k + P2 * rt2, x1)] = fmaxf(fmaxf(a.x, b.x), y[k].x);
+                vm[C::CP(k + P2 * rt2, x2)] = fmaxf(fmaxf(a.y, b.y), y[k].y);
+            }
+        }
+        group_sync<C>(g);
+        const int hw0 = max(max(s_hw[g][0], s_hw[g][1]), max(s_hw[g][2], s_hw[g][3]));
+        const int ex0 = max((int)ceilf(1.5f * (float)hw0), 2);
+        // Highest local maximum outside the footprint (correlate.rs:255-267), the direct
+        // distance test.
+        {
+            const int by0 = bi0 / N, bx0 = bi0 % N;
+            const int cx1 = circ(x1, bx0), cx2 = circ(x2, bx0);
+            const int x1l = (x1 + N - 1) % N, x1r = x1 + 1, x2l = x2 - 1, x2r = (x2 + 1) % N;
+#pragma unroll
+            for (int k = 0; k < P2; ++k) {
+                const int r = k + P2 * rt2;
+                const int cy = circ(r, by0);
+                const float h1 = fmaxf(fmaxf(vm[C::CP(r, x1l)], vm[C::CP(r, x1r)]), vm[C::CP(r, x1)]);
+                const float h2 = fmaxf(fmaxf(vm[C::CP(r, x2l)], vm[C::CP(r, x2r)]), vm[C::CP(r, x2)]);
+                if (y[k].x == h1 && max(cy, cx1) > ex0) second.x = fmaxf(second.x, y[k].x);
+                if (y[k].y == h2 && max(cy, cx2) > ex0) second.x = fmaxf(second.x, y[k].y);
+            }
+        }
+        second = group_max2<C>(second, s_red, g, gt);
     }
-    second = group_max2<C>(second, s_red, g, gt);
 
     // ------------------------------------------------------------------ sub-pixel fit, output
     if (gt < WPG) {
