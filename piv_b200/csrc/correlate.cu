@@ -19,7 +19,8 @@
 //   5. the scaled planes go to shared memory; argmax (lowest row-major index on ties), the
 //      half-width footprint, the second local maximum (a vectorised 3x3 maximum) and the 3-point
 //      Gaussian fit follow.
-// The 128 px window runs one window per group with a full complex inverse (registers).
+// The 128 px window runs one window per group; its real inverse runs as half-size stages (rows
+// 0..N/2, then pairs of real columns per complex line).
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
@@ -361,146 +362,18 @@ __device__ __forceinline__ void correlate_body(const CorrParams& prm, int block,
     group_sync<C>(g);
     fft_line_interleaved<N, T, 1>(z0, t, s_roots);
     if constexpr (PAIR) fft_line_interleaved<N, T, 1>(z1, t, s_roots);
-    // ------------------------------------------------------------------ cross spectra, inverse, find_peak
-    // Argmax of the planes (lowest row-major index among equal maxima). A lane visits its cells
-    // in increasing index order, so inside the lane a strictly larger value is the only one that
-    // replaces the best.
-    float2 best = make_float2(-INFINITY, -INFINITY);
-    int bi0 = 0x7fffffff, bi1 = 0x7fffffff;
-    float2 second = make_float2(-INFINITY, -INFINITY);
-    float* const cplane = reinterpret_cast<float*>(plane0) + C::CP_OFF;  // single windows
-    float* const vm = reinterpret_cast<float*>(plane1_raw);  // vertical 3-maxima: float2 (PAIR) or float
-    auto at = [&](int ch, int y, int x) -> float {
-        if constexpr (PAIR) {
-            const float2 v = plane0[C::A(y % N, x % N)];
-            return ch == 0 ? v.x : v.y;
-        } else {
-            return cplane[C::CP(y % N, x % N)];
-        }
-    };
-    auto circ = [](int a, int b) {
-        const int d = abs(a - b);
-        return min(d, N - d);
-    };
-    // Footprint of the primary peak (correlate.rs:242-254): half-width along +-y, +-x.
-    auto footprint = [&]() {
-        if (gt < 4 * WPG) {
-            const int ch = gt >> 2, dir = gt & 3;
-            const int bidx = ch == 0 ? bi0 : bi1;
-            const int by = bidx / N, bx = bidx % N;
-            const int sy = dir == 0 ? 1 : (dir == 1 ? N - 1 : 0);
-            const int sx = dir == 2 ? 1 : (dir == 3 ? N - 1 : 0);
-            const float half = 0.5f * (ch == 0 ? best.x : best.y);
-            int k = 0;
-            while (k < N / 2 && at(ch, by + k * sy, bx + k * sx) > half) ++k;
-            s_hw[g][gt] = k;
-        }
-    };
-    if constexpr (PAIR) {
-        // Both windows' spectra, then D = C0 + i*C1: one complex inverse gives both (real)
-        // correlation planes, window 0 in the real part and window 1 in the imaginary part.
-#pragma unroll
-        for (int k = 0; k < P; ++k) {
-            plane0[C::B(line, k + P * rt)] = z0[k];
-            plane1[C::B(line, k + P * rt)] = z1[k];
-        }
-        group_sync<C>(g);
-        {
-            const int my = (N - line) % N;
-#pragma unroll
-            for (int k = 0; k < P; ++k) {
-                const int kx = (N - (k + P * rt)) % N;
-                const float2 c0 = cross4(z0[k], plane0[C::B(my, kx)]);
-                const float2 c1 = cross4(z1[k], plane1[C::B(my, kx)]);
-                z0[k] = make_float2(c0.x - c1.y, c0.y + c1.x);  // D = C0 + i*C1
-            }
-        }
-        group_sync<C>(g);
-
-        fft_line_blocked<N, T, -1>(z0, t, s_roots);
-#pragma unroll
-        for (int k = 0; k < P; ++k) plane0[C::A(line, t + T * k)] = z0[k];
-        group_sync<C>(g);
-#pragma unroll
-        for (int q = 0; q < P; ++q) z0[q] = plane0[C::A(t + T * q, line)];
-        group_sync<C>(g);
-        fft_line_interleaved<N, T, -1>(z0, t, s_roots);
-        // Lane now holds corr[y = k + P*rt][x = line]; scale as the reference does (c *= scale).
-#pragma unroll
-        for (int k = 0; k < P; ++k) {
-            z0[k].x = z0[k].x * scale[0];
-            z0[k].y = z0[k].y * scale[WPG - 1];
-            plane0[C::A(k + P * rt, line)] = z0[k];
-        }
-
-#pragma unroll
-        for (int k = 0; k < P; ++k) {
-            const int idx = (k + P * rt) * N + line;
-            if (z0[k].x > best.x) {
-                best.x = z0[k].x;
-                bi0 = idx;
-            }
-            if (z0[k].y > best.y) {
-                best.y = z0[k].y;
-                bi1 = idx;
-            }
-        }
-        group_argmax<C>(best.x, bi0, s_red, g, gt);
-        group_argmax<C>(best.y, bi1, s_red, g, gt);
-        if (!(best.x > -INFINITY)) bi0 = 0;
-        if (!(best.y > -INFINITY)) bi1 = 0;
-        group_sync<C>(g);  // the scaled planes are complete in shared memory
-        footprint();
-        // Vertical 3-maximum of each column, for the local-maximum test.
-        {
-            float2 up, dn;  // neighbours across this lane's block boundary (rows k = -1 and P)
-            if constexpr (T == 1) {
-                up = z0[P - 1];
-                dn = z0[0];
-            } else {
-                const int lane = threadIdx.x & 31;
-                const int base = lane - t;  // first lane of this line
-                const int src_up = base + bitrev<T>((rt + T - 1) % T);
-                const int src_dn = base + bitrev<T>((rt + 1) % T);
-                up.x = __shfl_sync(0xffffffffu, z0[P - 1].x, src_up);
-                up.y = __shfl_sync(0xffffffffu, z0[P - 1].y, src_up);
-                dn.x = __shfl_sync(0xffffffffu, z0[0].x, src_dn);
-                dn.y = __shfl_sync(0xffffffffu, z0[0].y, src_dn);
-            }
-#pragma unroll
-            for (int k = 0; k < P; ++k) {
-                const float2 a = k == 0 ? up : z0[k - 1];
-                const float2 b = k == P - 1 ? dn : z0[k + 1];
-                reinterpret_cast<float2*>(vm)[C::A(k + P * rt, line)] =
-                    make_float2(fmaxf(fmaxf(a.x, b.x), z0[k].x), fmaxf(fmaxf(a.y, b.y), z0[k].y));
-            }
-        }
-        group_sync<C>(g);
-        const int hw0 = max(max(s_hw[g][0], s_hw[g][1]), max(s_hw[g][2], s_hw[g][3]));
-        const int ex0 = max((int)ceilf(1.5f * (float)hw0), 2);
-        const int hw1 = max(max(s_hw[g][4], s_hw[g][5]), max(s_hw[g][6], s_hw[g][7]));
-        const int ex1 = max((int)ceilf(1.5f * (float)hw1), 2);
-        // Highest local maximum outside the footprint (correlate.rs:255-267): v is a local
-        // maximum when it equals the maximum of its circular 3x3 neighbourhood. A cell is outside
-        // the footprint when max(circular row distance, column distance) > ex: one bit of a
-        // per-lane mask of eligible rows.
-        {
-            const int xl = (line + N - 1) % N, xr = (line + 1) % N;
-            const int by0 = bi0 / N, bx0 = bi0 % N, by1 = bi1 / N, bx1 = bi1 % N;
-            const unsigned el0 = eligible_rows<N, P>(by0, ex0, circ(line, bx0), rt);
-            const unsigned el1 = eligible_rows<N, P>(by1, ex1, circ(line, bx1), rt);
-            const float2* v2 = reinterpret_cast<const float2*>(vm);
-#pragma unroll
-            for (int k = 0; k < P; ++k) {
-                const int y = k + P * rt;
-                const float2 l = v2[C::A(y, xl)], c = v2[C::A(y, line)], r = v2[C::A(y, xr)];
-                const float h0 = fmaxf(fmaxf(l.x, r.x), c.x), h1 = fmaxf(fmaxf(l.y, r.y), c.y);
-                if (z0[k].x == h0 && ((el0 >> k) & 1u)) second.x = fmaxf(second.x, z0[k].x);
-                if (z0[k].y == h1 && ((el1 >> k) & 1u)) second.y = fmaxf(second.y, z0[k].y);
-            }
-        }
-        second = group_max2<C>(second, s_red, g, gt);
-    } else {
+    if constexpr (!PAIR) {
+        // ------------------------------------------------------------------ single window
+        float2 best = make_float2(-INFINITY, -INFINITY);
+        int bi0 = 0x7fffffff;
+        float2 second = make_float2(-INFINITY, -INFINITY);
+        float* const cplane = reinterpret_cast<float*>(plane0) + C::CP_OFF;
+        float* const vm = reinterpret_cast<float*>(plane1_raw);  // vertical 3-maxima
+        auto at = [&](int y, int x) -> float { return cplane[C::CP(y % N, x % N)]; };
+        auto circ = [](int a, int b) {
+            const int d = abs(a - b);
+            return min(d, N - d);
+        };
         // One window: z0 is the spectrum of a + i*b and the cross spectrum C is Hermitian
         // (C[-k] = conj C[k], exactly so in floating point: cross4(m, z) = conj cross4(z, m)), so
         // its inverse is real and half of a complex inverse computes it:
@@ -583,7 +456,16 @@ __device__ __forceinline__ void correlate_body(const CorrParams& prm, int block,
         group_argmax<C>(best.x, bi0, s_red, g, gt);
         if (!(best.x > -INFINITY)) bi0 = 0;
         group_sync<C>(g);  // the scaled plane is complete in shared memory
-        footprint();
+        // Footprint of the primary peak (correlate.rs:242-254): half-width along +-y, +-x.
+        if (gt < 4) {
+            const int by = bi0 / N, bx = bi0 % N;
+            const int sy = gt == 0 ? 1 : (gt == 1 ? N - 1 : 0);
+            const int sx = gt == 2 ? 1 : (gt == 3 ? N - 1 : 0);
+            const float half = 0.5f * best.x;
+            int k = 0;
+            while (k < N / 2 && at(by + k * sy, bx + k * sx) > half) ++k;
+            s_hw[g][gt] = k;
+        }
         {
             const int base = lane - t2;  // first lane of this column pair
             const int src_up = base + bitrev<T2>((rt2 + T2 - 1) % T2);
@@ -621,26 +503,20 @@ __device__ __forceinline__ void correlate_body(const CorrParams& prm, int block,
             }
         }
         second = group_max2<C>(second, s_red, g, gt);
-    }
 
-    // ------------------------------------------------------------------ sub-pixel fit, output
-    if (gt < WPG) {
-        const int ch = gt;
-        const long long cell = base_cell + ch;
-        const bool okc = (ch == 0) ? ok[0] : ok[WPG - 1];
-        const float4 o = (ch == 0) ? org[0] : org[WPG - 1];
-        if (cell < prm.ncells) {
-            if (okc) {
-                const int bidx = ch == 0 ? bi0 : bi1;
-                const int by = bidx / N, bx = bidx % N;
-                const float bv = ch == 0 ? best.x : best.y;
-                const float sv = ch == 0 ? second.x : second.y;
-                const float sx = subpixel(at(ch, by, bx + N - 1), bv, at(ch, by, bx + 1));
-                const float sy = subpixel(at(ch, by + N - 1, bx), bv, at(ch, by + 1, bx));
+        // ------------------------------------------------------------------ sub-pixel fit, output
+        if (gt == 0 && base_cell < prm.ncells) {
+            const long long cell = base_cell;
+            if (ok[0]) {
+                const int by = bi0 / N, bx = bi0 % N;
+                const float bv = best.x, sv = second.x;
+                const float sx = subpixel(at(by, bx + N - 1), bv, at(by, bx + 1));
+                const float sy = subpixel(at(by + N - 1, bx), bv, at(by + 1, bx));
                 const float wx = bx >= N / 2 ? (float)bx - (float)N : (float)bx;
                 const float wy = by >= N / 2 ? (float)by - (float)N : (float)by;
                 const float pdx = __fadd_rn(wx, sx), pdy = __fadd_rn(wy, sy);
                 const float ppr = sv > 0.0f ? fminf(__fdiv_rn(bv, sv), MAX_PPR) : MAX_PPR;
+                const float4 o = org[0];
                 if constexpr (C::DEFORM) {
                     prm.raw_dx[cell] = __fadd_rn(o.x, pdx);  // D(centre) + peak
                     prm.raw_dy[cell] = __fadd_rn(o.y, pdy);
@@ -655,6 +531,174 @@ __device__ __forceinline__ void correlate_body(const CorrParams& prm, int block,
                 prm.raw_dy[cell] = NAN;
                 prm.raw_ppr[cell] = 0.0f;
                 prm.raw_flags[cell] = F_NO_SIGNAL;
+            }
+        }
+    } else {
+        // ------------------------------------------------------------------ cross spectra
+        // Both windows' spectra, then D = C0 + i*C1: one complex inverse gives both (real)
+        // correlation planes, window 0 in the real part and window 1 in the imaginary part.
+#pragma unroll
+        for (int k = 0; k < P; ++k) {
+            plane0[C::B(line, k + P * rt)] = z0[k];
+            plane1[C::B(line, k + P * rt)] = z1[k];
+        }
+        group_sync<C>(g);
+        {
+            const int my = (N - line) % N;
+#pragma unroll
+            for (int k = 0; k < P; ++k) {
+                const int kx = (N - (k + P * rt)) % N;
+                const float2 c0 = cross4(z0[k], plane0[C::B(my, kx)]);
+                const float2 c1 = cross4(z1[k], plane1[C::B(my, kx)]);
+                z0[k] = make_float2(c0.x - c1.y, c0.y + c1.x);  // D = C0 + i*C1
+            }
+        }
+        group_sync<C>(g);
+
+        // ------------------------------------------------------------------ inverse 2-D FFT
+        fft_line_blocked<N, T, -1>(z0, t, s_roots);
+#pragma unroll
+        for (int k = 0; k < P; ++k) plane0[C::A(line, t + T * k)] = z0[k];
+        group_sync<C>(g);
+#pragma unroll
+        for (int q = 0; q < P; ++q) z0[q] = plane0[C::A(t + T * q, line)];
+        group_sync<C>(g);
+        fft_line_interleaved<N, T, -1>(z0, t, s_roots);
+        // Lane now holds corr[y = k + P*rt][x = line]; scale as the reference does (c *= scale).
+#pragma unroll
+        for (int k = 0; k < P; ++k) {
+            z0[k].x = z0[k].x * scale[0];
+            z0[k].y = z0[k].y * scale[WPG - 1];
+            plane0[C::A(k + P * rt, line)] = z0[k];
+        }
+
+        // ------------------------------------------------------------------ find_peak
+        // Argmax of both planes (lowest row-major index among equal maxima). A lane's indices grow
+        // with k, so inside the lane a strictly larger value is the only one that replaces the best.
+        float2 best = make_float2(-INFINITY, -INFINITY);
+        int bi0 = 0x7fffffff, bi1 = 0x7fffffff;
+#pragma unroll
+        for (int k = 0; k < P; ++k) {
+            const int idx = (k + P * rt) * N + line;
+            if (z0[k].x > best.x) {
+                best.x = z0[k].x;
+                bi0 = idx;
+            }
+            if (z0[k].y > best.y) {
+                best.y = z0[k].y;
+                bi1 = idx;
+            }
+        }
+        group_argmax<C>(best.x, bi0, s_red, g, gt);
+        group_argmax<C>(best.y, bi1, s_red, g, gt);
+        if (!(best.x > -INFINITY)) bi0 = 0;
+        if (!(best.y > -INFINITY)) bi1 = 0;
+        group_sync<C>(g);  // the scaled planes are complete in shared memory
+        auto at = [&](int ch, int y, int x) -> float {
+            const float2 v = plane0[C::A(y % N, x % N)];
+            return ch == 0 ? v.x : v.y;
+        };
+        // Footprint of the primary peak (correlate.rs:242-254): half-width along +-y, +-x.
+        if (gt < 4 * WPG) {
+            const int ch = gt >> 2, dir = gt & 3;
+            const int bidx = ch == 0 ? bi0 : bi1;
+            const int by = bidx / N, bx = bidx % N;
+            const int sy = dir == 0 ? 1 : (dir == 1 ? N - 1 : 0);
+            const int sx = dir == 2 ? 1 : (dir == 3 ? N - 1 : 0);
+            const float half = 0.5f * (ch == 0 ? best.x : best.y);
+            int k = 0;
+            while (k < N / 2 && at(ch, by + k * sy, bx + k * sx) > half) ++k;
+            s_hw[g][gt] = k;
+        }
+        // Vertical 3-maximum of each column, for the local-maximum test.
+        float2* vm = reinterpret_cast<float2*>(plane1_raw);  // vertical 3-maxima of both planes
+        {
+            float2 up, dn;  // neighbours across this lane's block boundary (rows k = -1 and P)
+            if constexpr (T == 1) {
+                up = z0[P - 1];
+                dn = z0[0];
+            } else {
+                const int lane = threadIdx.x & 31;
+                const int base = lane - t;  // first lane of this line
+                const int src_up = base + bitrev<T>((rt + T - 1) % T);
+                const int src_dn = base + bitrev<T>((rt + 1) % T);
+                up.x = __shfl_sync(0xffffffffu, z0[P - 1].x, src_up);
+                up.y = __shfl_sync(0xffffffffu, z0[P - 1].y, src_up);
+                dn.x = __shfl_sync(0xffffffffu, z0[0].x, src_dn);
+                dn.y = __shfl_sync(0xffffffffu, z0[0].y, src_dn);
+            }
+#pragma unroll
+            for (int k = 0; k < P; ++k) {
+                const float2 a = k == 0 ? up : z0[k - 1];
+                const float2 b = k == P - 1 ? dn : z0[k + 1];
+                const float m0 = fmaxf(fmaxf(a.x, b.x), z0[k].x);
+                vm[C::A(k + P * rt, line)] = make_float2(m0, fmaxf(fmaxf(a.y, b.y), z0[k].y));
+            }
+        }
+        group_sync<C>(g);
+        const int hw0 = max(max(s_hw[g][0], s_hw[g][1]), max(s_hw[g][2], s_hw[g][3]));
+        const int ex0 = max((int)ceilf(1.5f * (float)hw0), 2);
+        const int hw1 = max(max(s_hw[g][4], s_hw[g][5]), max(s_hw[g][6], s_hw[g][7]));
+        const int ex1 = max((int)ceilf(1.5f * (float)hw1), 2);
+        // Highest local maximum outside the footprint (correlate.rs:255-267): v is a local maximum
+        // when it equals the maximum of its circular 3x3 neighbourhood.
+        float2 second = make_float2(-INFINITY, -INFINITY);
+        {
+            const int xl = (line + N - 1) % N, xr = (line + 1) % N;
+            const int by0 = bi0 / N, bx0 = bi0 % N, by1 = bi1 / N, bx1 = bi1 % N;
+            auto circ = [](int a, int b) {
+                const int d = abs(a - b);
+                return min(d, N - d);
+            };
+            const int cx0 = circ(line, bx0), cx1 = circ(line, bx1);
+            // A cell is outside the footprint when max(circular row distance, column distance) > ex:
+            // one bit of a per-lane mask of eligible rows.
+            const unsigned el0 = eligible_rows<N, P>(by0, ex0, cx0, rt);
+            const unsigned el1 = eligible_rows<N, P>(by1, ex1, cx1, rt);
+#pragma unroll
+            for (int k = 0; k < P; ++k) {
+                const int y = k + P * rt;
+                const float2 l = vm[C::A(y, xl)], c = vm[C::A(y, line)], r = vm[C::A(y, xr)];
+                const float h0 = fmaxf(fmaxf(l.x, r.x), c.x), h1 = fmaxf(fmaxf(l.y, r.y), c.y);
+                if (z0[k].x == h0 && ((el0 >> k) & 1u) != 0u) second.x = fmaxf(second.x, z0[k].x);
+                if (z0[k].y == h1 && ((el1 >> k) & 1u) != 0u) second.y = fmaxf(second.y, z0[k].y);
+            }
+        }
+        second = group_max2<C>(second, s_red, g, gt);
+
+        // ------------------------------------------------------------------ sub-pixel fit, output
+        if (gt < WPG) {
+            const int ch = gt;
+            const long long cell = base_cell + ch;
+            const bool okc = (ch == 0) ? ok[0] : ok[WPG - 1];
+            const float4 o = (ch == 0) ? org[0] : org[WPG - 1];
+            if (cell < prm.ncells) {
+                if (okc) {
+                    const int bidx = ch == 0 ? bi0 : bi1;
+                    const int by = bidx / N, bx = bidx % N;
+                    const float bv = ch == 0 ? best.x : best.y;
+                    const float sv = ch == 0 ? second.x : second.y;
+                    const float sx = subpixel(at(ch, by, bx + N - 1), bv, at(ch, by, bx + 1));
+                    const float sy = subpixel(at(ch, by + N - 1, bx), bv, at(ch, by + 1, bx));
+                    const float wx = bx >= N / 2 ? (float)bx - (float)N : (float)bx;
+                    const float wy = by >= N / 2 ? (float)by - (float)N : (float)by;
+                    const float pdx = __fadd_rn(wx, sx), pdy = __fadd_rn(wy, sy);
+                    const float ppr = sv > 0.0f ? fminf(__fdiv_rn(bv, sv), MAX_PPR) : MAX_PPR;
+                    if constexpr (C::DEFORM) {
+                        prm.raw_dx[cell] = __fadd_rn(o.x, pdx);  // D(centre) + peak
+                        prm.raw_dy[cell] = __fadd_rn(o.y, pdy);
+                    } else {
+                        prm.raw_dx[cell] = __fadd_rn(__fsub_rn(o.z, o.x), pdx);
+                        prm.raw_dy[cell] = __fadd_rn(__fsub_rn(o.w, o.y), pdy);
+                    }
+                    prm.raw_ppr[cell] = ppr;
+                    prm.raw_flags[cell] = 0;
+                } else {
+                    prm.raw_dx[cell] = NAN;
+                    prm.raw_dy[cell] = NAN;
+                    prm.raw_ppr[cell] = 0.0f;
+                    prm.raw_flags[cell] = F_NO_SIGNAL;
+                }
             }
         }
     }
