@@ -173,6 +173,44 @@ def test_matches_oracle_on_synthetic_particles():
         _stage_check(an, traces, a, b, windows)
 
 
+def test_128px_peaks_in_every_quadrant_and_at_the_wrap():
+    """The 128 px window (one window per group, its real inverse as half-size stages) against the
+    oracle on window pairs whose offsets put the correlation peak in every quadrant of the plane,
+    next to the +-N/2 wrap, on the self-conjugate row and column (ky or kx in {0, N/2} carry the
+    packed lines) and at fractional positions: peak indices exact, sub-pixel within 1e-4 px, PPR
+    within 1e-5 relative."""
+    import piv_b200 as P
+    from piv_b200 import synthetic as S
+    n = 128
+    a, _ = S.particle_pair(448, 448, 31, 0.06, 0.9, lambda x, y: (0.0, 0.0))
+    a = S.add_noise(a, 0.01, 5)
+    offsets = [(0.0, 0.0), (9.0, -13.0), (-21.0, 17.0), (40.0, 40.0), (-40.0, -40.0), (55.0, -3.0), (-3.0, 55.0),
+               (-58.0, 0.0), (0.0, -58.0), (61.0, 61.0), (-61.0, 60.0), (62.5, -0.25), (-0.75, 62.5),
+               (31.3, -47.6), (-12.2, 5.7), (64.0, 0.0), (0.0, -64.0)]
+    origins = []
+    for i, (ox, oy) in enumerate(offsets):
+        ax, ay = 80.0 + 17.0 * (i % 5), 80.0 + 23.0 * (i // 5)
+        origins.append((ax, ay, ax + ox, ay + oy))
+    origins = np.array(origins, np.float32)
+    an = P.PivAnalyzer(P.PivConfig(windows=[n]))
+    fa, fb = an.prepare(a, P.RAW), an.prepare(a, P.RAW)
+    dx, dy, ppr, fl = an.correlate_origins(fa, fb, n, origins)
+    odx, ody, oppr, ofl = O.correlate_pass(a, a, a, a, n, origins)
+    assert np.array_equal(fl, ofl)
+    assert np.all(fl == 0)
+    err = np.abs(np.r_[dx - odx, dy - ody]).max()
+    assert err < 1e-4, err
+    off = np.r_[origins[:, 2] - origins[:, 0], origins[:, 3] - origins[:, 1]]
+    assert np.array_equal(np.round(np.r_[dx, dy] - off), np.round(np.r_[odx, ody] - off))
+    assert np.abs(ppr / oppr - 1).max() < 1e-5
+    # the same frame on both sides: every vector is the zero displacement up to the sub-pixel fit,
+    # modulo N (a peak at index N/2 reads as -N/2, correlate.rs:283-290, so an offset of -64
+    # gives -128)
+    d = np.r_[dx, dy]
+    assert np.abs((d + n / 2) % n - n / 2).max() < 0.5
+    assert d[len(offsets) - 1 + len(offsets)] == pytest.approx(-128.0, abs=0.5)
+
+
 def test_autotuned_variants_give_identical_results():
     """Launch-geometry autotuning never changes results: variants differ only in geometry."""
     import piv_b200 as P
