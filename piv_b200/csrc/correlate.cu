@@ -346,8 +346,12 @@ __device__ __forceinline__ void correlate_body(const CorrParams& prm, int block,
 
     // ------------------------------------------------------------------ forward 2-D FFTs
     float2* plane1 = reinterpret_cast<float2*>(plane1_raw);
-    fft_line_interleaved<N, T, 1>(z0, t, s_roots);
-    if constexpr (PAIR) fft_line_interleaved<N, T, 1>(z1, t, s_roots);
+    if constexpr (PAIR && N == 64) {
+        fft_line_interleaved2<N, T, 1>(z0, z1, t, s_roots);  // both windows stage by stage
+    } else {
+        fft_line_interleaved<N, T, 1>(z0, t, s_roots);
+        if constexpr (PAIR) fft_line_interleaved<N, T, 1>(z1, t, s_roots);
+    }
 #pragma unroll
     for (int k = 0; k < P; ++k) {
         plane0[C::A(k + P * rt, line)] = z0[k];
@@ -360,8 +364,12 @@ __device__ __forceinline__ void correlate_body(const CorrParams& prm, int block,
         if constexpr (PAIR) z1[q] = plane1[C::A(line, t + T * q)];
     }
     group_sync<C>(g);
-    fft_line_interleaved<N, T, 1>(z0, t, s_roots);
-    if constexpr (PAIR) fft_line_interleaved<N, T, 1>(z1, t, s_roots);
+    if constexpr (PAIR && N == 64) {
+        fft_line_interleaved2<N, T, 1>(z0, z1, t, s_roots);  // both windows stage by stage
+    } else {
+        fft_line_interleaved<N, T, 1>(z0, t, s_roots);
+        if constexpr (PAIR) fft_line_interleaved<N, T, 1>(z1, t, s_roots);
+    }
     if constexpr (!PAIR) {
         // ------------------------------------------------------------------ single window
         float2 best = make_float2(-INFINITY, -INFINITY);
