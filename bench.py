@@ -294,6 +294,10 @@ def serving_block(wl, duration, local, ranks):
     vec = {(si, ci): len(P.Grid.new(wl["sizes"][si][0], wl["sizes"][si][1], cfgs[ci].windows[-1], cfgs[ci].overlap))
            for si in range(len(wl["sizes"])) for ci in range(len(cfgs))}
     sv = P.PivServer(memory_budget_bytes=wl["budget"], max_in_flight=wl["max_in_flight"], device=local)
+    # the server's pool is grown to its admission budget (within the free memory) before the
+    # arrivals start, so that no admission waits on the driver to map new memory under load
+    free = torch.cuda.mem_get_info(torch.device("cuda", local))[0]
+    held0 = sv.reserve(int(max(0, min(wl["budget"], free - (16 << 30)))))
     # warm-up: one request of every kind
     for si in range(len(wl["sizes"])):
         for ci in range(len(cfgs)):
@@ -331,6 +335,7 @@ def serving_block(wl, duration, local, ranks):
     span = time.perf_counter() - t0
     clocks = sampler.stop()
     s1 = sv.stats()
+    held1 = sv.reserve(0)
     sv.close()
     total_vec = ranks.sum(sum(vec[(si, ci)] for si, ci, _ in kinds))
     span = ranks.max(span)
@@ -345,7 +350,8 @@ def serving_block(wl, duration, local, ranks):
             "achieved_rate_per_s": n_all / span,
             "h2d_bytes_per_request": int(np.mean([pool[(si, pj)][0].nbytes * 2 for si, _, pj in kinds])),
             "d2h_bytes_per_request": int(np.mean([vec[(si, ci)] * 13 for si, ci, _ in kinds])),
-            "gpu_launches": int(launches), "server_steps": int(s1["steps"] - s0["steps"]), "clocks": clocks}
+            "gpu_launches": int(launches), "server_steps": int(s1["steps"] - s0["steps"]),
+            "pool_reserved_bytes": int(held0), "pool_grew_bytes": int(held1 - held0), "clocks": clocks}
 
 
 def run_serving(args, wl):

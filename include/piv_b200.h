@@ -366,6 +366,18 @@ int32_t piv_server_set_manual(PivServer* server, int32_t manual);
  * from another thread, or destroy). */
 int32_t piv_server_advance(PivServer* server, int32_t steps, double timeout_ms);
 int32_t piv_server_stats(PivServer* server, PivServerStatsC* stats);
+/* No counterpart in the reference (the serving form's memory). Each server allocates its
+ * requests from a memory pool of its own, which keeps freed memory for later requests. The
+ * first admissions that reach a new peak of memory in flight make the pool map more device
+ * memory, and the driver call that does so can block the scheduler for hundreds of milliseconds
+ * (measured: one 54 MB admission, 585 ms), stalling every request in flight. This call grows the
+ * pool ahead of time by `bytes` (allocated and freed again in chunks of at most 1 GiB, blocking),
+ * so later admissions up to that much memory in flight are served from memory the pool already
+ * holds. The memory stays reserved to the server until piv_server_destroy; it does not count
+ * against memory_budget_bytes. bytes == 0 only reports. *reserved_bytes (may be NULL): the
+ * memory the pool holds after the call. PIV_ERR_CUDA if the device runs out of memory part way
+ * (what was reserved stays reserved). */
+int32_t piv_server_reserve(PivServer* server, int64_t bytes, int64_t* reserved_bytes);
 
 /* PivAnalyzer::analyze_traced (multipass.rs:142-150, PassTrace :72-81): HOST arrays holding
  * every pass back to back (pass 0 cells, then pass 1 ...; piv_pass_grid gives each count):

@@ -34,7 +34,7 @@ EXPORTS = [
     "piv_tc_selftest", "piv_validate_field_noalloc",
     "piv_server_create", "piv_server_destroy", "piv_server_submit", "piv_server_wait", "piv_server_stats",
     "piv_server_wait_timeout", "piv_server_cancel", "piv_server_fail_next_allocations", "piv_server_set_manual",
-    "piv_server_advance", "piv_server_set_fused",
+    "piv_server_advance", "piv_server_set_fused", "piv_server_reserve",
 ]
 
 
@@ -193,6 +193,7 @@ def load():
         "piv_server_set_manual": ([vp, i32], i32),
         "piv_server_advance": ([vp, i32, ctypes.c_double], i32),
         "piv_server_set_fused": ([vp, i32], i32),
+        "piv_server_reserve": ([vp, i64, P(i64)], i32),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)

@@ -766,6 +766,14 @@ class PivServer:
         """Grants `steps` scheduler steps and waits until they have been taken."""
         _check(_lib.load().piv_server_advance(self._h, int(steps), float(timeout_ms)))
 
+    def reserve(self, nbytes: int) -> int:
+        """Grows the server's memory pool by nbytes ahead of time (blocking), so that admissions
+        under load are served from memory the pool already holds instead of waiting on the
+        driver to map more. Returns the bytes the pool holds afterwards (nbytes = 0: only that)."""
+        held = ctypes.c_int64()
+        _check(_lib.load().piv_server_reserve(self._h, int(nbytes), ctypes.byref(held)))
+        return int(held.value)
+
     def stats(self):
         s = _lib.PivServerStatsC()
         _check(_lib.load().piv_server_stats(self._h, ctypes.byref(s)))

@@ -1898,6 +1898,7 @@ struct PivServer {
     bool stop = false;
     std::thread worker;
     int64_t in_use = 0;
+    cudaMemPool_t pool = nullptr;  // the server's own pool: requests' memory, kept when freed
     PivServerStatsC stats{};
     int variant[2][129] = {};
     // FP32 windows of several sizes and kinds in one fused correlation launch per step (on by
@@ -1934,7 +1935,7 @@ int admit_request(PivServer* sv, Request* r, bool inject_failure) {
     const bool chain = r->pre.smooth_sigma > 0.0f || r->pre.normalize_radius > 0;
     const bool both = r->pre.smooth_sigma > 0.0f && r->pre.normalize_radius > 0;
     if (inject_failure) return kAdmitOutOfMemory;
-    const cudaError_t ae = cudaMallocAsync(&r->mem, r->bytes, sv->stream);
+    const cudaError_t ae = cudaMallocFromPoolAsync(&r->mem, r->bytes, sv->pool, sv->stream);
     if (ae == cudaErrorMemoryAllocation) {
         cudaGetLastError();  // not a sticky error: clear it and report
         r->mem = nullptr;
@@ -2290,17 +2291,29 @@ int32_t piv_server_create(const PivServerConfigC* cfg, PivServer** out) {
     CUDA_TRY(cudaSetDevice(dev));
     int st = ensure_device_init(dev);
     if (st) return st;
-    // keep freed request memory in the pool instead of returning it to the driver
-    cudaMemPool_t pool;
-    CUDA_TRY(cudaDeviceGetDefaultMemPool(&pool, dev));
+    // A pool of the server's own that keeps freed request memory instead of returning it to the
+    // driver (piv_server_reserve grows it ahead of time).
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    CUDA_TRY(cudaMemPoolCreate(&pool, &props));
     uint64_t threshold = UINT64_MAX;
-    CUDA_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
+    cudaError_t e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+    if (e != cudaSuccess) {
+        cudaMemPoolDestroy(pool);
+        return fail(PIV_ERR_CUDA, "server pool: %s", cudaGetErrorString(e));
+    }
     PivServer* sv = new PivServer();
     sv->device = dev;
+    sv->pool = pool;
     sv->budget = cfg->memory_budget_bytes;
     sv->max_in_flight = cfg->max_in_flight;
-    cudaError_t e = cudaStreamCreateWithFlags(&sv->stream, cudaStreamNonBlocking);
+    e = cudaStreamCreateWithFlags(&sv->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
+        cudaMemPoolDestroy(pool);
         delete sv;
         return fail(PIV_ERR_CUDA, "server stream: %s", cudaGetErrorString(e));
     }
@@ -2323,7 +2336,46 @@ void piv_server_destroy(PivServer* sv) {
     cudaStreamSynchronize(sv->stream);
     for (auto& kv : sv->by_id) delete kv.second;
     cudaStreamDestroy(sv->stream);
+    if (sv->pool) cudaMemPoolDestroy(sv->pool);  // every request's memory has been freed into it
     delete sv;
+}
+
+int32_t piv_server_reserve(PivServer* sv, int64_t bytes, int64_t* reserved_bytes) {
+    if (!sv) return fail(PIV_ERR_ARGUMENT, "null server");
+    if (bytes < 0) return fail(PIV_ERR_ARGUMENT, "negative reservation");
+    CUDA_TRY(cudaSetDevice(sv->device));
+    int st = PIV_OK;
+    if (bytes > 0) {
+        // Allocate the reservation in chunks on a stream of its own, free it again and wait: the
+        // pool keeps the memory (release threshold at its maximum) and serves later admissions on
+        // the server stream from it once the frees have completed.
+        constexpr int64_t kChunk = 1ll << 30;
+        cudaStream_t s = nullptr;
+        CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        std::vector<void*> chunks;
+        cudaError_t e = cudaSuccess;
+        for (int64_t left = bytes; left > 0 && e == cudaSuccess;) {
+            const int64_t n = std::min(left, kChunk);
+            void* p = nullptr;
+            e = cudaMallocFromPoolAsync(&p, (size_t)n, sv->pool, s);
+            if (e == cudaSuccess) chunks.push_back(p);
+            left -= n;
+        }
+        if (e != cudaSuccess) {
+            cudaGetLastError();  // an out-of-memory allocation is not a sticky error
+            st = fail(PIV_ERR_CUDA, "piv_server_reserve: %s after %zu chunk(s)", cudaGetErrorString(e), chunks.size());
+        }
+        for (void* p : chunks) cudaFreeAsync(p, s);
+        const cudaError_t se = cudaStreamSynchronize(s);
+        cudaStreamDestroy(s);
+        if (se != cudaSuccess && st == PIV_OK) st = fail(PIV_ERR_CUDA, "piv_server_reserve: %s", cudaGetErrorString(se));
+    }
+    if (reserved_bytes) {
+        uint64_t held = 0;
+        CUDA_TRY(cudaMemPoolGetAttribute(sv->pool, cudaMemPoolAttrReservedMemCurrent, &held));
+        *reserved_bytes = (int64_t)held;
+    }
+    return st;
 }
 
 int32_t piv_server_submit(PivServer* sv, const PivRequestC* q, uint64_t* id) {

@@ -116,3 +116,24 @@ def test_one_fused_launch_per_step_gives_the_per_size_results():
     for (cfg, (a, b)), r in zip(reqs, out[True][0]):
         an = P.PivAnalyzer(cfg)
         _same(an.analyze(an.prepare(a, P.RAW), an.prepare(b, P.RAW)), r)
+
+
+def test_reserved_pool_serves_admissions_without_growing():
+    """piv_server_reserve grows the server's own pool ahead of time: a burst of requests whose
+    memory in flight stays below the reservation is admitted without the pool mapping more
+    memory, and its results equal PivAnalyzer.analyze of each pair."""
+    import piv_b200 as P
+    sv = P.PivServer(memory_budget_bytes=1 << 30, max_in_flight=64)
+    assert sv.reserve(0) == 0
+    held = sv.reserve(256 << 20)
+    assert held >= 256 << 20
+    reqs = [(256, 256, SCHEDULES[i % 3], _pair(256, 256, 300 + i)) for i in range(12)]
+    tickets = [sv.submit(a, b, _cfg(sched)) for _, _, sched, (a, b) in reqs]
+    results = [sv.wait(t)[0] for t in tickets]
+    assert sv.reserve(0) == held, "the pool grew although the burst fitted the reservation"
+    for (h, w, sched, (a, b)), r in zip(reqs, results):
+        an = P.PivAnalyzer(_cfg(sched))
+        _same(r, an.analyze(an.prepare(a, P.RAW), an.prepare(b, P.RAW)))
+    with pytest.raises(P.PivError):
+        sv.reserve(-1)
+    sv.close()
