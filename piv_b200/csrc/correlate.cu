@@ -41,6 +41,11 @@ template <int N_, int T_, bool PAIR_, int G_, int MINB_, bool SHFL_ = false, boo
 struct CorrCfg {
     static constexpr int N = N_, T = T_, G = G_, MINB = MINB_;
     static constexpr bool PAIR = PAIR_, SHFL_SAMPLE = SHFL_, DEFORM = DEFORM_;
+    // 32 and 64 px window pairs (uniform and deformed) sample in the block layout (lane t holds
+    // rows P*rev(t) + p) and run the column pass of the forward FFT from it (bit-reversed blocks
+    // in, lane t ends with the frequency rows t + T*k); every other configuration samples
+    // interleaved rows (t + T*p).
+    static constexpr bool BLOCK = PAIR && (N_ == 32 || N_ == 64);
     static constexpr int P = N / T;
     static constexpr int NT = N * T;
     static constexpr int THREADS = G * NT;
@@ -62,6 +67,14 @@ struct CorrCfg {
     static constexpr size_t PLANE0 = sizeof(float2) * (size_t)PLANE_ELEMS;
     static constexpr size_t PLANE1 = ((PAIR ? sizeof(float2) : sizeof(float)) * (size_t)PLANE_ELEMS + 15) / 16 * 16;
     __host__ __device__ static constexpr int A(int row, int col) { return row * LD + (row / P) * Q + col; }
+    // The first transpose (column spectra -> rows): A, except for the block layout on T = 2 lanes,
+    // whose stores (rows t + 2k of eight columns per half-warp) would meet its loads' layout on
+    // shared banks; there rows of N are rotated by 2 g(row), g(row) = (row/2 mod 4) + 4 (row mod 2),
+    // so that both the stores and the loads (eight rows by columns t + 2q) of a half-warp hit 16
+    // distinct bank pairs.
+    __host__ __device__ static constexpr int AF(int row, int col) {
+        return (BLOCK && T == 2) ? row * N + ((col + 2 * (((row >> 1) & 3) + 4 * (row & 1))) & (N - 1)) : A(row, col);
+    }
     __host__ __device__ static constexpr int B(int ky, int kx) {
         return T == 1 ? ky * LD + kx : ky * LD + (ky / P) * Q + kx + kx / P;
     }
@@ -82,6 +95,7 @@ struct CorrCfg {
     __host__ __device__ static constexpr int YO(int r, int x) { return r * N + (x ^ (((r & 1) << 3) | (r & 6))); }
     __host__ __device__ static constexpr int CP(int y, int x) { return y * N + x + 4 * (y >> 4); }
     static constexpr int CP_OFF = 2 * (N / 2 + 1) * N;
+    static_assert(!(BLOCK && T == 2) || N * N <= PLANE_ELEMS, "first-transpose plane");
     static_assert(PAIR || (N == 128 && BS(N - 1, N - 1) < PLANE_ELEMS &&
                            CP_OFF + CP(N - 1, N - 1) < 2 * PLANE_ELEMS &&
                            sizeof(float) * (size_t)(CP(N - 1, N - 1) + 1) <= PLANE1),
@@ -283,11 +297,19 @@ __device__ __forceinline__ void correlate_body(const CorrParams& prm, int block,
             org[wi] = make_float4(corner_blend(k0.x, k0.z, k1.x, k1.z, 0.5f, 0.5f),
                                   corner_blend(k0.y, k0.w, k1.y, k1.w, 0.5f, 0.5f), 0.f, 0.f);
             if (wi == 0) {
-                sample_deformed<N, T>(prm.img_a, prm.img_b, prm.H, prm.W, gx, gy, k0, k1, line, t, s_ramp, z0);
+                sample_deformed<N, T, C::BLOCK>(prm.img_a, prm.img_b, prm.H, prm.W, gx, gy, k0, k1, line,
+                                                C::BLOCK ? rt : t, s_ramp, z0);
             } else if constexpr (PAIR) {
-                sample_deformed<N, T>(prm.img_a, prm.img_b, prm.H, prm.W, gx, gy, k0, k1, line, t, s_ramp, z1);
+                sample_deformed<N, T, C::BLOCK>(prm.img_a, prm.img_b, prm.H, prm.W, gx, gy, k0, k1, line,
+                                                C::BLOCK ? rt : t, s_ramp, z1);
             }
         }
+    } else if constexpr (C::BLOCK) {
+        const GlobalSrc ga{prm.img_a, prm.W}, gb{prm.img_b, prm.W};
+        sample_block<N, T, false, C::SHFL_SAMPLE>(ga, prm.H, prm.W, org[0].x, org[0].y, line, rt, z0);
+        sample_block<N, T, true, C::SHFL_SAMPLE>(gb, prm.H, prm.W, org[0].z, org[0].w, line, rt, z0);
+        sample_block<N, T, false, C::SHFL_SAMPLE>(ga, prm.H, prm.W, org[1].x, org[1].y, line, rt, z1);
+        sample_block<N, T, true, C::SHFL_SAMPLE>(gb, prm.H, prm.W, org[1].z, org[1].w, line, rt, z1);
     } else if constexpr (C::SHFL_SAMPLE) {
         const GlobalSrc ga{prm.img_a, prm.W}, gb{prm.img_b, prm.W};
         sample_column<N, T, false>(ga, prm.H, prm.W, org[0].x, org[0].y, line, t, z0);
@@ -346,22 +368,37 @@ __device__ __forceinline__ void correlate_body(const CorrParams& prm, int block,
 
     // ------------------------------------------------------------------ forward 2-D FFTs
     float2* plane1 = reinterpret_cast<float2*>(plane1_raw);
-    if constexpr (PAIR && N == 64) {
-        fft_line_interleaved2<N, T, 1>(z0, z1, t, s_roots);  // both windows stage by stage
-    } else {
-        fft_line_interleaved<N, T, 1>(z0, t, s_roots);
-        if constexpr (PAIR) fft_line_interleaved<N, T, 1>(z1, t, s_roots);
-    }
+    if constexpr (C::BLOCK) {
+        // lane t ends with the rows ky = t + T*k (64 px: both windows stage by stage)
+        if constexpr (N == 64) {
+            fft_line_blocked2<N, T, 1>(z0, z1, t, s_roots);
+        } else {
+            fft_line_blocked<N, T, 1>(z0, t, s_roots);
+            fft_line_blocked<N, T, 1>(z1, t, s_roots);
+        }
 #pragma unroll
-    for (int k = 0; k < P; ++k) {
-        plane0[C::A(k + P * rt, line)] = z0[k];
-        if constexpr (PAIR) plane1[C::A(k + P * rt, line)] = z1[k];
+        for (int k = 0; k < P; ++k) {
+            plane0[C::AF(t + T * k, line)] = z0[k];
+            plane1[C::AF(t + T * k, line)] = z1[k];
+        }
+    } else {
+        if constexpr (PAIR && N == 64) {
+            fft_line_interleaved2<N, T, 1>(z0, z1, t, s_roots);  // both windows stage by stage
+        } else {
+            fft_line_interleaved<N, T, 1>(z0, t, s_roots);
+            if constexpr (PAIR) fft_line_interleaved<N, T, 1>(z1, t, s_roots);
+        }
+#pragma unroll
+        for (int k = 0; k < P; ++k) {
+            plane0[C::A(k + P * rt, line)] = z0[k];
+            if constexpr (PAIR) plane1[C::A(k + P * rt, line)] = z1[k];
+        }
     }
     group_sync<C>(g);
 #pragma unroll
     for (int q = 0; q < P; ++q) {
-        z0[q] = plane0[C::A(line, t + T * q)];
-        if constexpr (PAIR) z1[q] = plane1[C::A(line, t + T * q)];
+        z0[q] = plane0[C::AF(line, t + T * q)];
+        if constexpr (PAIR) z1[q] = plane1[C::AF(line, t + T * q)];
     }
     group_sync<C>(g);
     if constexpr (PAIR && N == 64) {

@@ -313,4 +313,63 @@ __device__ __forceinline__ void fft_line_interleaved2(float2 (&x)[N / T], float2
     }
 }
 
+// Two bit-reversed block lines at once (the two windows of a pair), stage by stage: the same
+// operations per value as two calls of fft_line_blocked (so the same results), ordered so that
+// one line's shuffles overlap the other's arithmetic.
+template <int N, int T, int DIR>
+__device__ __forceinline__ void fft_line_blocked2(float2 (&x)[N / T], float2 (&y)[N / T], int t,
+                                                  const float2* s_roots) {
+    constexpr int P = N / T;
+    constexpr bool SIGNED = !(N == 32 || N == 64);
+    if constexpr (T > 1) {
+#pragma unroll
+        for (int h = 1; h < T; h <<= 1) {
+            const bool upper = (t & h) != 0;
+            const bool quarter = h == 2 && upper && (t & 1);
+            auto tw = [&](float2 v, float2 w) -> float2 {
+                if (h == 1) return v;
+                if (h == 2) return quarter ? mul_mi<DIR>(v) : v;
+                return cmulw<DIR>(v, w);
+            };
+            if constexpr (SIGNED) {
+                const float sg = upper ? -1.0f : 1.0f;
+                const float2 w = upper ? s_roots[(t & (h - 1)) * (N / (2 * h))] : make_float2(1.0f, 0.0f);
+#pragma unroll
+                for (int i = 0; i < P; ++i) {
+                    const float2 v = tw(x[i], w), u = tw(y[i], w);
+                    float2 o, q;
+                    o.x = __shfl_xor_sync(0xffffffffu, v.x, h);
+                    o.y = __shfl_xor_sync(0xffffffffu, v.y, h);
+                    q.x = __shfl_xor_sync(0xffffffffu, u.x, h);
+                    q.y = __shfl_xor_sync(0xffffffffu, u.y, h);
+                    x[i] = make_float2(fmaf(sg, v.x, o.x), fmaf(sg, v.y, o.y));
+                    y[i] = make_float2(fmaf(sg, u.x, q.x), fmaf(sg, u.y, q.y));
+                }
+            } else {
+                const float2 w = s_roots[(t & (h - 1)) * (N / (2 * h))];
+#pragma unroll
+                for (int i = 0; i < P; ++i) {
+                    const float2 v = upper ? tw(x[i], w) : x[i];
+                    const float2 u = upper ? tw(y[i], w) : y[i];
+                    float2 o, q;
+                    o.x = __shfl_xor_sync(0xffffffffu, v.x, h);
+                    o.y = __shfl_xor_sync(0xffffffffu, v.y, h);
+                    q.x = __shfl_xor_sync(0xffffffffu, u.x, h);
+                    q.y = __shfl_xor_sync(0xffffffffu, u.y, h);
+                    x[i] = upper ? csub(o, v) : cadd(v, o);
+                    y[i] = upper ? csub(q, u) : cadd(u, q);
+                }
+            }
+        }
+#pragma unroll
+        for (int p = 1; p < P; ++p) {
+            const float2 w = s_roots[p * t];
+            x[p] = cmulw<DIR>(x[p], w);
+            y[p] = cmulw<DIR>(y[p], w);
+        }
+    }
+    dft_reg<N, P, DIR>(x);
+    dft_reg<N, P, DIR>(y);
+}
+
 }  // namespace pivb200

@@ -172,6 +172,92 @@ __device__ __forceinline__ void sample_column(const Src& src, int H, int W, floa
     }
 }
 
+// Block layout for T > 1 lanes per column: lane (x, rt) holds column x at the P consecutive rows
+// P*rt .. P*rt + P - 1 (rt = the lane's block). The lane streams down its rows carrying the row
+// below, as the one-lane-per-column sampler does, so each sample needs one new row: two loads
+// (DIRECT), or one load and the right-hand tap from the lane of the next column (lane + T, same
+// block) by a shuffle (SHFL), where lanes whose neighbour is beyond their warp or the window load
+// it themselves. The taps, weights and summation order are those of the other samplers, so the
+// samples are the same bit for bit; only their place in the lanes differs.
+template <int N, int T, bool IMAG, bool SHFL, class Src>
+__device__ __forceinline__ void sample_block(const Src& src, int H, int W, float ox, float oy, int x, int rt,
+                                             float2 (&z)[N / T]) {
+    constexpr int P = N / T;
+    const float fx0 = floorf(ox), fy0 = floorf(oy);
+    const int x0 = min(max((int)fx0, 0), W - 1), y0 = min(max((int)fy0, 0), H - 1);
+    const float tx = __fsub_rn(ox, fx0), ty = __fsub_rn(oy, fy0);
+    const int c0 = min(x0 + x, W - 1);
+    const int dc = min(x0 + x + 1, W - 1) - c0;  // right-hand tap: next float, or the same at the border
+    const int last = H - 1 - y0;                  // rows below y0 that exist (row clamp)
+    const int stride = src.stride();
+    const int r0 = P * rt;
+    const float* base = src.at(y0, c0);
+    const bool integer = tx < 1e-4f && ty < 1e-4f;
+    const float ux = __fsub_rn(1.0f, tx), uy = __fsub_rn(1.0f, ty);
+    const float w00 = __fmul_rn(ux, uy), w01 = __fmul_rn(tx, uy), w10 = __fmul_rn(ux, ty), w11 = __fmul_rn(tx, ty);
+    auto blend = [&](float tl, float tr, float bl, float br) {
+        float s = __fmul_rn(w00, tl);
+        s = __fadd_rn(s, __fmul_rn(w01, tr));
+        s = __fadd_rn(s, __fmul_rn(w10, bl));
+        return __fadd_rn(s, __fmul_rn(w11, br));
+    };
+    if constexpr (!SHFL) {
+        if (integer) {
+#pragma unroll
+            for (int p = 0; p < P; ++p) {
+                const float v = Src::ld(base + min(r0 + p, last) * stride);
+                if (IMAG) z[p].y = v; else z[p].x = v;
+            }
+            return;
+        }
+        const float* row = base + min(r0, last) * stride;
+        float top = Src::ld(row);
+        float topr = dc ? Src::ld(row + 1) : top;
+        if (last >= r0 + P) {  // rows r0 .. r0 + P all exist: the row pointer steps by the pitch
+#pragma unroll
+            for (int p = 0; p < P; ++p) {
+                row += stride;
+                const float b0 = Src::ld(row);
+                const float b1 = dc ? Src::ld(row + 1) : b0;
+                const float s = blend(top, topr, b0, b1);
+                if (IMAG) z[p].y = s; else z[p].x = s;
+                top = b0;
+                topr = b1;
+            }
+        } else {
+#pragma unroll
+            for (int p = 0; p < P; ++p) {
+                const float* bot = base + min(r0 + p + 1, last) * stride;
+                const float b0 = Src::ld(bot);
+                const float b1 = dc ? Src::ld(bot + 1) : b0;
+                const float s = blend(top, topr, b0, b1);
+                if (IMAG) z[p].y = s; else z[p].x = s;
+                top = b0;
+                topr = b1;
+            }
+        }
+    } else {
+        // Every lane runs the shuffles (an integer window then keeps its copied values).
+        const int lane = threadIdx.x & 31;
+        const bool edge = lane + T >= 32 || x == N - 1;  // right neighbour not reachable by a shuffle
+        const float* row = base + min(r0, last) * stride;
+        float top = Src::ld(row);
+        float topr = __shfl_down_sync(0xffffffffu, top, T);
+        if (edge) topr = Src::ld(row + dc);
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+            const float* bot = base + min(r0 + p + 1, last) * stride;
+            const float b0 = Src::ld(bot);
+            float b1 = __shfl_down_sync(0xffffffffu, b0, T);
+            if (edge) b1 = Src::ld(bot + dc);
+            const float s = integer ? top : blend(top, topr, b0, b1);
+            if (IMAG) z[p].y = s; else z[p].x = s;
+            top = b0;
+            topr = b1;
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------------------------
 // Deformed windows (no counterpart in the reference, whose windows only shift): pixel (r, c) of
 // the window at base position (x0, y0) (the grid origin under the placement clamp to W - n - 1,
@@ -209,7 +295,8 @@ __device__ __forceinline__ float bilinear_clamped(const float* __restrict__ img,
     return __fadd_rn(s, __fmul_rn(__fmul_rn(tx, ty), __ldg(bot + ix1)));
 }
 
-template <int N, int T>
+// BLOCKROWS: lane (x, t) fills rows P*t + p (t then names the lane's row block) instead of t + T*p.
+template <int N, int T, bool BLOCKROWS = false>
 __device__ __forceinline__ void sample_deformed(const float* __restrict__ img_a, const float* __restrict__ img_b, int H,
                                                 int W, int x0, int y0, float4 k0, float4 k1, int x, int t,
                                                 const float* s_ramp, float2 (&z)[N / T]) {
@@ -218,7 +305,7 @@ __device__ __forceinline__ void sample_deformed(const float* __restrict__ img_a,
     const float xf = (float)(x0 + x);
 #pragma unroll
     for (int p = 0; p < P; ++p) {
-        const int r = t + T * p;
+        const int r = BLOCKROWS ? P * t + p : t + T * p;
         const float v = s_ramp[r];
         const float hx = __fmul_rn(0.5f, corner_blend(k0.x, k0.z, k1.x, k1.z, u, v));
         const float hy = __fmul_rn(0.5f, corner_blend(k0.y, k0.w, k1.y, k1.w, u, v));
