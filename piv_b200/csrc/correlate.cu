@@ -8,7 +8,8 @@
 //   1. both windows of the pair are sampled (bilinear, the reference's f32 operation order, no
 //      FMA) straight into registers, each as one complex plane z = a + i*b (frame A's window in
 //      the real part, frame B's in the imaginary part); lane (x, t) holds column x at rows
-//      t + T*p, so each load instruction reads contiguous image rows;
+//      t + T*p (32 and 64 px: the block of rows P*rev(t) + p, sampled one new row at a time), so
+//      each load instruction reads contiguous image rows;
 //   2. mean removal and energies (one group reduction of 4 sums for both windows), 2-D FFT of
 //      both planes at once: columns in registers, transpose through shared memory, rows in
 //      registers;
@@ -765,8 +766,8 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB) correlate_kernel(const __
 // ---------------------------------------------------------------------------------------------
 using FusedC0 = CorrCfg<8, 1, true, 32, 2, true>;
 using FusedC1 = CorrCfg<16, 1, true, 16, 2, false>;
-using FusedC2 = CorrCfg<32, 2, true, 4, 2, true>;
-using FusedC3 = CorrCfg<64, 4, true, 1, 2, true>;
+using FusedC2 = CorrCfg<32, 2, true, 4, 2, false>;
+using FusedC3 = CorrCfg<64, 4, true, 1, 2, false>;
 using FusedC4 = CorrCfg<8, 1, true, 32, 2, false, true>;
 using FusedC5 = CorrCfg<16, 1, true, 16, 2, false, true>;
 using FusedC6 = CorrCfg<32, 2, true, 4, 2, false, true>;
@@ -904,12 +905,12 @@ static const CorrVariant kV16[] = {PIV_V(16, 1, true, 16, 2, false), PIV_V(16, 1
                                    PIV_V(16, 1, true, 4, 8, false), PIV_V(16, 1, true, 2, 16, true)};
 static const CorrVariant kV24[] = {PIV_V(24, 2, true, 4, 2, true), PIV_V(24, 2, true, 4, 2, false),
                                    PIV_V(24, 2, true, 2, 4, true)};
-static const CorrVariant kV32[] = {PIV_V(32, 2, true, 4, 2, true), PIV_V(32, 2, true, 4, 2, false),
+static const CorrVariant kV32[] = {PIV_V(32, 2, true, 4, 2, false), PIV_V(32, 2, true, 4, 2, true),
                                    PIV_V(32, 2, true, 2, 4, true), PIV_V(32, 2, true, 2, 3, true),
                                    PIV_V(32, 2, true, 1, 8, true), PIV_V(32, 2, true, 1, 8, false)};
 static const CorrVariant kV48[] = {PIV_V(48, 4, true, 1, 2, true), PIV_V(48, 4, true, 1, 2, false),
                                    PIV_V(48, 4, true, 1, 1, true)};
-static const CorrVariant kV64[] = {PIV_V(64, 4, true, 1, 2, true), PIV_V(64, 4, true, 1, 2, false),
+static const CorrVariant kV64[] = {PIV_V(64, 4, true, 1, 2, false), PIV_V(64, 4, true, 1, 2, true),
                                    PIV_V(64, 4, true, 1, 1, true)};
 static const CorrVariant kV96[] = {PIV_V(96, 4, true, 1, 1, true), PIV_V(96, 4, true, 1, 1, false)};
 static const CorrVariant kV128[] = {PIV_V(128, 4, false, 1, 1, false), PIV_V(128, 4, false, 1, 1, true)};
