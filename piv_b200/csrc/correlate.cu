@@ -370,13 +370,8 @@ __device__ __forceinline__ void correlate_body(const CorrParams& prm, int block,
     // ------------------------------------------------------------------ forward 2-D FFTs
     float2* plane1 = reinterpret_cast<float2*>(plane1_raw);
     if constexpr (C::BLOCK) {
-        // lane t ends with the rows ky = t + T*k (64 px: both windows stage by stage)
-        if constexpr (N == 64) {
-            fft_line_blocked2<N, T, 1>(z0, z1, t, s_roots);
-        } else {
-            fft_line_blocked<N, T, 1>(z0, t, s_roots);
-            fft_line_blocked<N, T, 1>(z1, t, s_roots);
-        }
+        // lane t ends with the rows ky = t + T*k; both windows stage by stage
+        fft_line_blocked2<N, T, 1>(z0, z1, t, s_roots);
 #pragma unroll
         for (int k = 0; k < P; ++k) {
             plane0[C::AF(t + T * k, line)] = z0[k];
@@ -402,7 +397,7 @@ __device__ __forceinline__ void correlate_body(const CorrParams& prm, int block,
         if constexpr (PAIR) z1[q] = plane1[C::AF(line, t + T * q)];
     }
     group_sync<C>(g);
-    if constexpr (PAIR && N == 64) {
+    if constexpr (PAIR && (N == 64 || N == 32)) {
         fft_line_interleaved2<N, T, 1>(z0, z1, t, s_roots);  // both windows stage by stage
     } else {
         fft_line_interleaved<N, T, 1>(z0, t, s_roots);
@@ -658,8 +653,8 @@ __device__ __forceinline__ void correlate_body(const CorrParams& prm, int block,
         }
         // Vertical 3-maximum of each column, for the local-maximum test.
         float2* vm = reinterpret_cast<float2*>(plane1_raw);  // vertical 3-maxima of both planes
+        float2 up, dn;  // neighbours across this lane's block boundary (rows k = -1 and P)
         {
-            float2 up, dn;  // neighbours across this lane's block boundary (rows k = -1 and P)
             if constexpr (T == 1) {
                 up = z0[P - 1];
                 dn = z0[0];
@@ -704,7 +699,16 @@ __device__ __forceinline__ void correlate_body(const CorrParams& prm, int block,
 #pragma unroll
             for (int k = 0; k < P; ++k) {
                 const int y = k + P * rt;
-                const float2 l = vm[C::A(y, xl)], c = vm[C::A(y, line)], r = vm[C::A(y, xr)];
+                const float2 l = vm[C::A(y, xl)], r = vm[C::A(y, xr)];
+                // the lane's own vertical 3-maximum: recomputed from registers at 16 and 64 px
+                // (the same value as the one stored; measured faster there), read back otherwise
+                float2 c;
+                if constexpr (N == 16 || N == 64) {
+                    const float2 va = k == 0 ? up : z0[k - 1], vb = k == P - 1 ? dn : z0[k + 1];
+                    c = make_float2(fmaxf(fmaxf(va.x, vb.x), z0[k].x), fmaxf(fmaxf(va.y, vb.y), z0[k].y));
+                } else {
+                    c = vm[C::A(y, line)];
+                }
                 const float h0 = fmaxf(fmaxf(l.x, r.x), c.x), h1 = fmaxf(fmaxf(l.y, r.y), c.y);
                 if (z0[k].x == h0 && ((el0 >> k) & 1u) != 0u) second.x = fmaxf(second.x, z0[k].x);
                 if (z0[k].y == h1 && ((el1 >> k) & 1u) != 0u) second.y = fmaxf(second.y, z0[k].y);
