@@ -1899,6 +1899,9 @@ struct PivServer {
     std::thread worker;
     int64_t in_use = 0;
     cudaMemPool_t pool = nullptr;  // the server's own pool: requests' memory, kept when freed
+    // Copy streams: an admitted request's uploads run on `up` and its result downloads on `down`,
+    // so they overlap the kernels that other requests run on `stream`.
+    cudaStream_t up = nullptr, down = nullptr;
     PivServerStatsC stats{};
     int variant[2][129] = {};
     // FP32 windows of several sizes and kinds in one fused correlation launch per step (on by
@@ -1935,7 +1938,7 @@ int admit_request(PivServer* sv, Request* r, bool inject_failure) {
     const bool chain = r->pre.smooth_sigma > 0.0f || r->pre.normalize_radius > 0;
     const bool both = r->pre.smooth_sigma > 0.0f && r->pre.normalize_radius > 0;
     if (inject_failure) return kAdmitOutOfMemory;
-    const cudaError_t ae = cudaMallocFromPoolAsync(&r->mem, r->bytes, sv->pool, sv->stream);
+    const cudaError_t ae = cudaMallocFromPoolAsync(&r->mem, r->bytes, sv->pool, sv->up);
     if (ae == cudaErrorMemoryAllocation) {
         cudaGetLastError();  // not a sticky error: clear it and report
         r->mem = nullptr;
@@ -1983,8 +1986,15 @@ int admit_request(PivServer* sv, Request* r, bool inject_failure) {
     }
     r->d_counts = (unsigned long long*)take(8 * sizeof(unsigned long long));
     r->cfg.cur = sv->stream;
-    CUDA_TRY(cudaMemcpyAsync(r->fa.d_raw, r->host_a, es * hw, cudaMemcpyHostToDevice, sv->stream));
-    CUDA_TRY(cudaMemcpyAsync(r->fb.d_raw, r->host_b, es * hw, cudaMemcpyHostToDevice, sv->stream));
+    // allocation and uploads on the upload stream; the preparation on the server stream waits for them
+    CUDA_TRY(cudaMemcpyAsync(r->fa.d_raw, r->host_a, es * hw, cudaMemcpyHostToDevice, sv->up));
+    CUDA_TRY(cudaMemcpyAsync(r->fb.d_raw, r->host_b, es * hw, cudaMemcpyHostToDevice, sv->up));
+    cudaEvent_t uploaded = nullptr;
+    CUDA_TRY(cudaEventCreateWithFlags(&uploaded, cudaEventDisableTiming));
+    cudaError_t ue = cudaEventRecord(uploaded, sv->up);
+    if (ue == cudaSuccess) ue = cudaStreamWaitEvent(sv->stream, uploaded, 0);
+    cudaEventDestroy(uploaded);
+    CUDA_TRY(ue);
     int st = prepare_common(&r->cfg, &r->fa, r->fa.d_raw, r->dtype, &r->pre, nullptr);
     if (!st) st = prepare_common(&r->cfg, &r->fb, r->fb.d_raw, r->dtype, &r->pre, nullptr);
     return st;
@@ -2105,19 +2115,29 @@ void PivServer::launch_step(std::vector<Request*>& work) {
         }
     }
     if (e == cudaSuccess && !sums.empty()) e = launch_summary_items(sums.data(), (int)sums.size(), stream, &nl);
+    // downloads of the requests that finished in this step, on the download stream after the step
+    if (e == cudaSuccess && !sums.empty()) {
+        cudaEvent_t computed = nullptr;
+        e = cudaEventCreateWithFlags(&computed, cudaEventDisableTiming);
+        if (e == cudaSuccess) {
+            e = cudaEventRecord(computed, stream);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(down, computed, 0);
+            cudaEventDestroy(computed);
+        }
+    }
     for (Request* r : work) {
         if (r->next_pass != (int)r->passes.size() || e != cudaSuccess) continue;
         const PassBuf& last = r->passes.back();
         const size_t c = (size_t)last.cells;
-        if (r->out_dx) e = cudaMemcpyAsync(r->out_dx, last.dx, 4 * c, cudaMemcpyDeviceToHost, stream);
-        if (e == cudaSuccess && r->out_dy) e = cudaMemcpyAsync(r->out_dy, last.dy, 4 * c, cudaMemcpyDeviceToHost, stream);
+        if (r->out_dx) e = cudaMemcpyAsync(r->out_dx, last.dx, 4 * c, cudaMemcpyDeviceToHost, down);
+        if (e == cudaSuccess && r->out_dy) e = cudaMemcpyAsync(r->out_dy, last.dy, 4 * c, cudaMemcpyDeviceToHost, down);
         if (e == cudaSuccess && r->out_ppr)
-            e = cudaMemcpyAsync(r->out_ppr, last.raw_ppr, 4 * c, cudaMemcpyDeviceToHost, stream);
-        if (e == cudaSuccess && r->out_flags) e = cudaMemcpyAsync(r->out_flags, last.flags, c, cudaMemcpyDeviceToHost, stream);
+            e = cudaMemcpyAsync(r->out_ppr, last.raw_ppr, 4 * c, cudaMemcpyDeviceToHost, down);
+        if (e == cudaSuccess && r->out_flags) e = cudaMemcpyAsync(r->out_flags, last.flags, c, cudaMemcpyDeviceToHost, down);
         if (e == cudaSuccess)
-            e = cudaMemcpyAsync(r->h_counts, r->d_counts, sizeof(r->h_counts), cudaMemcpyDeviceToHost, stream);
+            e = cudaMemcpyAsync(r->h_counts, r->d_counts, sizeof(r->h_counts), cudaMemcpyDeviceToHost, down);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&r->done_ev, cudaEventDisableTiming);
-        if (e == cudaSuccess) e = cudaEventRecord(r->done_ev, stream);
+        if (e == cudaSuccess) e = cudaEventRecord(r->done_ev, down);
         r->final_launched = true;
     }
     stats.steps++;
@@ -2216,7 +2236,8 @@ void PivServer::loop() {
                                    ? "device memory for the request could not be allocated (out of memory)"
                                    : err;
                     if (r->mem) {
-                        cudaStreamSynchronize(stream);  // queued uploads may still read host memory
+                        cudaStreamSynchronize(up);  // queued uploads may still read host memory
+                        cudaStreamSynchronize(stream);
                         cudaFreeAsync(r->mem, stream);
                         r->mem = nullptr;
                     }
@@ -2312,7 +2333,11 @@ int32_t piv_server_create(const PivServerConfigC* cfg, PivServer** out) {
     sv->budget = cfg->memory_budget_bytes;
     sv->max_in_flight = cfg->max_in_flight;
     e = cudaStreamCreateWithFlags(&sv->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&sv->up, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&sv->down, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
+        for (cudaStream_t q : {sv->stream, sv->up, sv->down})
+            if (q) cudaStreamDestroy(q);
         cudaMemPoolDestroy(pool);
         delete sv;
         return fail(PIV_ERR_CUDA, "server stream: %s", cudaGetErrorString(e));
@@ -2333,9 +2358,9 @@ void piv_server_destroy(PivServer* sv) {
     sv->cv_step.notify_all();
     if (sv->worker.joinable()) sv->worker.join();
     cudaSetDevice(sv->device);
-    cudaStreamSynchronize(sv->stream);
+    for (cudaStream_t q : {sv->up, sv->stream, sv->down}) cudaStreamSynchronize(q);
     for (auto& kv : sv->by_id) delete kv.second;
-    cudaStreamDestroy(sv->stream);
+    for (cudaStream_t q : {sv->up, sv->stream, sv->down}) cudaStreamDestroy(q);
     if (sv->pool) cudaMemPoolDestroy(sv->pool);  // every request's memory has been freed into it
     delete sv;
 }
