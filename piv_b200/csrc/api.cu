@@ -1855,6 +1855,12 @@ struct Request {
     std::vector<PassBuf> passes;
     unsigned long long* d_counts = nullptr;
     unsigned long long h_counts[8] = {};
+    // Pinned staging of the downloads (the summary counts, and every output that is not in pinned
+    // host memory itself): a copy into pageable memory would block the scheduler thread until the
+    // GPU reached it. Unpacked into the caller's buffers when the request retires.
+    uint8_t* stage = nullptr;
+    int stage_class = 0;
+    size_t stage_off[4] = {};  // offsets of dx, dy, peak_ratio, flags in `stage` (0: copied directly)
     bool use_stats = false;
     int next_pass = 0;
     cudaEvent_t done_ev = nullptr;
@@ -1902,6 +1908,12 @@ struct PivServer {
     // Copy streams: an admitted request's uploads run on `up` and its result downloads on `down`,
     // so they overlap the kernels that other requests run on `stream`.
     cudaStream_t up = nullptr, down = nullptr;
+    // Pinned host blocks of 2^k bytes for the download staging, reused across requests; used by the
+    // scheduler thread only.
+    std::vector<void*> pinned_free[48];
+    std::vector<void*> pinned_all;
+    uint8_t* pinned_get(size_t bytes, int* cls);
+    void pinned_put(uint8_t* p, int cls) { pinned_free[cls].push_back(p); }
     PivServerStatsC stats{};
     int variant[2][129] = {};
     // FP32 windows of several sizes and kinds in one fused correlation launch per step (on by
@@ -2018,6 +2030,35 @@ int PivServer::admit(Request* r, std::string* err) {
     return st;
 }
 
+uint8_t* PivServer::pinned_get(size_t bytes, int* cls) {
+    int k = 16;
+    while (k < 47 && ((size_t)1 << k) < bytes) ++k;
+    *cls = k;
+    if (!pinned_free[k].empty()) {
+        uint8_t* p = (uint8_t*)pinned_free[k].back();
+        pinned_free[k].pop_back();
+        return p;
+    }
+    void* p = nullptr;
+    if (cudaHostAlloc(&p, (size_t)1 << k, cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    pinned_all.push_back(p);
+    return (uint8_t*)p;
+}
+
+namespace {
+bool is_pinned(const void* p) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+}  // namespace
+
 // Requests cancelled while admitted stop at the step boundary: their completion event covers the
 // work already queued for them, after which retire() gives their memory back.
 void PivServer::cancel_active() {
@@ -2129,13 +2170,25 @@ void PivServer::launch_step(std::vector<Request*>& work) {
         if (r->next_pass != (int)r->passes.size() || e != cudaSuccess) continue;
         const PassBuf& last = r->passes.back();
         const size_t c = (size_t)last.cells;
-        if (r->out_dx) e = cudaMemcpyAsync(r->out_dx, last.dx, 4 * c, cudaMemcpyDeviceToHost, down);
-        if (e == cudaSuccess && r->out_dy) e = cudaMemcpyAsync(r->out_dy, last.dy, 4 * c, cudaMemcpyDeviceToHost, down);
-        if (e == cudaSuccess && r->out_ppr)
-            e = cudaMemcpyAsync(r->out_ppr, last.raw_ppr, 4 * c, cudaMemcpyDeviceToHost, down);
-        if (e == cudaSuccess && r->out_flags) e = cudaMemcpyAsync(r->out_flags, last.flags, c, cudaMemcpyDeviceToHost, down);
+        void* const outs[4] = {r->out_dx, r->out_dy, r->out_ppr, r->out_flags};
+        const void* const srcs[4] = {last.dx, last.dy, last.raw_ppr, last.flags};
+        const size_t sizes[4] = {4 * c, 4 * c, 4 * c, c};
+        size_t need = 256;  // the summary counts, then each staged output 256-byte aligned
+        for (int o = 0; o < 4; ++o) {
+            r->stage_off[o] = 0;
+            if (outs[o] && !is_pinned(outs[o])) {
+                r->stage_off[o] = need;
+                need += align256(sizes[o]);
+            }
+        }
+        r->stage = pinned_get(need, &r->stage_class);
+        if (!r->stage) e = cudaErrorMemoryAllocation;
+        for (int o = 0; o < 4 && e == cudaSuccess; ++o)
+            if (outs[o])
+                e = cudaMemcpyAsync(r->stage_off[o] ? r->stage + r->stage_off[o] : outs[o], srcs[o], sizes[o],
+                                    cudaMemcpyDeviceToHost, down);
         if (e == cudaSuccess)
-            e = cudaMemcpyAsync(r->h_counts, r->d_counts, sizeof(r->h_counts), cudaMemcpyDeviceToHost, down);
+            e = cudaMemcpyAsync(r->stage, r->d_counts, sizeof(r->h_counts), cudaMemcpyDeviceToHost, down);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&r->done_ev, cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaEventRecord(r->done_ev, down);
         r->final_launched = true;
@@ -2173,6 +2226,19 @@ void PivServer::retire() {
         if (!fin) {
             keep.push_back(r);
             continue;
+        }
+        if (r->stage) {  // unpack the staged downloads (they completed with the completion event)
+            if (!r->done_ev) cudaStreamSynchronize(down);  // failed before recording: copies may be queued
+            if (r->status == PIV_OK) {
+                void* const outs[4] = {r->out_dx, r->out_dy, r->out_ppr, r->out_flags};
+                const size_t c = (size_t)r->passes.back().cells;
+                const size_t sizes[4] = {4 * c, 4 * c, 4 * c, c};
+                for (int o = 0; o < 4; ++o)
+                    if (outs[o] && r->stage_off[o]) std::memcpy(outs[o], r->stage + r->stage_off[o], sizes[o]);
+                std::memcpy(r->h_counts, r->stage, sizeof(r->h_counts));
+            }
+            pinned_put(r->stage, r->stage_class);
+            r->stage = nullptr;
         }
         r->t_done = Clock::now();
         if (r->done_ev) cudaEventDestroy(r->done_ev);
@@ -2361,6 +2427,7 @@ void piv_server_destroy(PivServer* sv) {
     for (cudaStream_t q : {sv->up, sv->stream, sv->down}) cudaStreamSynchronize(q);
     for (auto& kv : sv->by_id) delete kv.second;
     for (cudaStream_t q : {sv->up, sv->stream, sv->down}) cudaStreamDestroy(q);
+    for (void* p : sv->pinned_all) cudaFreeHost(p);
     if (sv->pool) cudaMemPoolDestroy(sv->pool);  // every request's memory has been freed into it
     delete sv;
 }
