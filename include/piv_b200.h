@@ -313,7 +313,8 @@ typedef struct {
     int64_t height, width;
     const void* frame_a;         /* HOST samples (pinned memory recommended); valid until done */
     const void* frame_b;
-    float* dx;                   /* HOST outputs of output_grid's nx*ny elements; valid until done */
+    float* dx;                   /* HOST outputs of output_grid's nx*ny elements; valid until done
+                                  * (pageable memory is staged through the server's pinned blocks) */
     float* dy;
     float* peak_ratio;
     uint8_t* flags;
