@@ -137,3 +137,29 @@ def test_reserved_pool_serves_admissions_without_growing():
     with pytest.raises(P.PivError):
         sv.reserve(-1)
     sv.close()
+
+
+def test_pinned_and_pageable_result_buffers_give_the_same_result():
+    """Results land in the caller's buffers whether those are pinned (written by the download
+    directly) or pageable (staged through the server's pinned blocks and copied out at retire)."""
+    import piv_b200 as P
+    sv = P.PivServer(memory_budget_bytes=1 << 30, max_in_flight=16)
+    reqs = [(SCHEDULES[i % 3], _pair(256, 256, 400 + i)) for i in range(6)]
+    got = []
+    for pinned in (False, True):
+        outs, tickets = [], []
+        for sched, (a, b) in reqs:
+            g = P.Grid.new(256, 256, sched[-1], 0.5)
+            shape = (g.ny, g.nx)
+            if pinned:
+                o = tuple(_pin(np.zeros(shape, t)) for t in (np.float32, np.float32, np.float32, np.uint8))
+            else:
+                o = tuple(np.zeros(shape, t) for t in (np.float32, np.float32, np.float32, np.uint8))
+            outs.append(o)
+            tickets.append(sv.submit(a, b, _cfg(sched), out=o))
+        got.append([(sv.wait(t)[0], o) for t, o in zip(tickets, outs)])
+    sv.close()
+    for (rp, op), (rq, oq) in zip(*got):
+        _same(rp, rq)
+        for x, y in zip(op, oq):
+            assert np.array_equal(np.asarray(x).view(np.uint8), np.asarray(y).view(np.uint8))
