@@ -374,8 +374,9 @@ int32_t piv_server_stats(PivServer* server, PivServerStatsC* stats);
  * (measured: one 54 MB admission, 585 ms), stalling every request in flight. This call grows the
  * pool ahead of time by `bytes` (allocated and freed again in chunks of at most 1 GiB, blocking),
  * so later admissions up to that much memory in flight are served from memory the pool already
- * holds. The memory stays reserved to the server until piv_server_destroy; it does not count
- * against memory_budget_bytes. bytes == 0 only reports. *reserved_bytes (may be NULL): the
+ * holds. With bytes > 0 it also pins the server's first host staging blocks for result downloads
+ * (8 MiB for each download size up to 1 MiB). The memory stays reserved to the server until
+ * piv_server_destroy; it does not count against memory_budget_bytes. bytes == 0 only reports. *reserved_bytes (may be NULL): the
  * memory the pool holds after the call. PIV_ERR_CUDA if the device runs out of memory part way
  * (what was reserved stays reserved). */
 int32_t piv_server_reserve(PivServer* server, int64_t bytes, int64_t* reserved_bytes);

@@ -1908,12 +1908,17 @@ struct PivServer {
     // Copy streams: an admitted request's uploads run on `up` and its result downloads on `down`,
     // so they overlap the kernels that other requests run on `stream`.
     cudaStream_t up = nullptr, down = nullptr;
-    // Pinned host blocks of 2^k bytes for the download staging, reused across requests; used by the
-    // scheduler thread only.
+    // Pinned host blocks of 2^k bytes for the download staging, reused across requests (the
+    // scheduler takes and returns them; piv_server_reserve pins the first slabs ahead of time).
+    std::mutex pinned_mu;
     std::vector<void*> pinned_free[48];
     std::vector<void*> pinned_all;
+    bool pinned_grow(int k);  // pinned_mu held
     uint8_t* pinned_get(size_t bytes, int* cls);
-    void pinned_put(uint8_t* p, int cls) { pinned_free[cls].push_back(p); }
+    void pinned_put(uint8_t* p, int cls) {
+        std::lock_guard<std::mutex> lk(pinned_mu);
+        pinned_free[cls].push_back(p);
+    }
     PivServerStatsC stats{};
     int variant[2][129] = {};
     // FP32 windows of several sizes and kinds in one fused correlation launch per step (on by
@@ -2030,22 +2035,31 @@ int PivServer::admit(Request* r, std::string* err) {
     return st;
 }
 
+// Pins a slab of at least 8 MiB and splits it into blocks of class k: a cudaHostAlloc costs far
+// more than the copies a block serves (with one allocation per block, the download setup of a
+// saturated 1 200-request run took 150-169 ms of scheduler time; with slabs 68-96 ms).
+bool PivServer::pinned_grow(int k) {
+    const size_t block = (size_t)1 << k;
+    const size_t slab = std::max(block, (size_t)8 << 20);
+    void* p = nullptr;
+    if (cudaHostAlloc(&p, slab, cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    pinned_all.push_back(p);
+    for (size_t off = 0; off + block <= slab; off += block) pinned_free[k].push_back((uint8_t*)p + off);
+    return true;
+}
+
 uint8_t* PivServer::pinned_get(size_t bytes, int* cls) {
     int k = 16;
     while (k < 47 && ((size_t)1 << k) < bytes) ++k;
     *cls = k;
-    if (!pinned_free[k].empty()) {
-        uint8_t* p = (uint8_t*)pinned_free[k].back();
-        pinned_free[k].pop_back();
-        return p;
-    }
-    void* p = nullptr;
-    if (cudaHostAlloc(&p, (size_t)1 << k, cudaHostAllocDefault) != cudaSuccess) {
-        cudaGetLastError();
-        return nullptr;
-    }
-    pinned_all.push_back(p);
-    return (uint8_t*)p;
+    std::lock_guard<std::mutex> lk(pinned_mu);
+    if (pinned_free[k].empty() && !pinned_grow(k)) return nullptr;
+    uint8_t* p = (uint8_t*)pinned_free[k].back();
+    pinned_free[k].pop_back();
+    return p;
 }
 
 namespace {
@@ -2461,6 +2475,13 @@ int32_t piv_server_reserve(PivServer* sv, int64_t bytes, int64_t* reserved_bytes
         const cudaError_t se = cudaStreamSynchronize(s);
         cudaStreamDestroy(s);
         if (se != cudaSuccess && st == PIV_OK) st = fail(PIV_ERR_CUDA, "piv_server_reserve: %s", cudaGetErrorString(se));
+    }
+    if (bytes > 0) {
+        // and one staging slab for each download size up to 1 MiB (final fields up to 80 k cells),
+        // so that the first requests do not wait for host memory to be pinned either
+        std::lock_guard<std::mutex> lk(sv->pinned_mu);
+        for (int k = 16; k <= 20; ++k)
+            if (sv->pinned_free[k].empty()) sv->pinned_grow(k);
     }
     if (reserved_bytes) {
         uint64_t held = 0;
