@@ -136,6 +136,11 @@ class MultiDeviceServer:
         finally:
             self.load[i] -= cost
 
+    def reserve(self, nbytes):
+        """Grows every device's request pool by nbytes ahead of the load (PivServer.reserve);
+        returns the bytes each pool holds afterwards, in device order."""
+        return [s.reserve(nbytes) for s in self.servers]
+
     def close(self):
         for s in self.servers:
             close = getattr(s, "close", None)

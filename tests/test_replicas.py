@@ -87,6 +87,10 @@ class _FakeServer:
         a, b = self.pending.pop(t)
         return ("done", self.device, len(a))
 
+    def reserve(self, nbytes):
+        self.held = getattr(self, "held", 0) + nbytes
+        return self.held
+
 
 class _Buf:
     def __init__(self, nbytes):
@@ -110,3 +114,9 @@ def test_least_loaded_dispatch_keeps_requests_whole():
     for t in (t2, t3, t4, t5):
         ms.wait(t)
     assert ms.load == [0, 0, 0]
+
+
+def test_reserve_reaches_every_device():
+    ms = MultiDeviceServer([0, 1], make_server=_FakeServer)
+    assert ms.reserve(1 << 20) == [1 << 20, 1 << 20]
+    assert ms.reserve(0) == [1 << 20, 1 << 20]
