@@ -1961,7 +1961,7 @@ int admit_request(PivServer* sv, Request* r, bool inject_failure) {
         r->mem = nullptr;
         return kAdmitOutOfMemory;
     }
-    if (ae != cudaSuccess) return fail(PIV_ERR_CUDA, "cudaMallocAsync: %s", cudaGetErrorString(ae));
+    if (ae != cudaSuccess) return fail(PIV_ERR_CUDA, "cudaMallocFromPoolAsync: %s", cudaGetErrorString(ae));
     char* p = (char*)r->mem;
     auto take = [&](size_t bytes) {
         void* q = p;
@@ -2196,13 +2196,15 @@ void PivServer::launch_step(std::vector<Request*>& work) {
             }
         }
         r->stage = pinned_get(need, &r->stage_class);
-        if (!r->stage) e = cudaErrorMemoryAllocation;
+        if (!r->stage)  // no pinned host memory to be had: copy directly (slower, still correct)
+            for (int o = 0; o < 4; ++o) r->stage_off[o] = 0;
         for (int o = 0; o < 4 && e == cudaSuccess; ++o)
             if (outs[o])
                 e = cudaMemcpyAsync(r->stage_off[o] ? r->stage + r->stage_off[o] : outs[o], srcs[o], sizes[o],
                                     cudaMemcpyDeviceToHost, down);
         if (e == cudaSuccess)
-            e = cudaMemcpyAsync(r->stage, r->d_counts, sizeof(r->h_counts), cudaMemcpyDeviceToHost, down);
+            e = cudaMemcpyAsync(r->stage ? (void*)r->stage : (void*)r->h_counts, r->d_counts, sizeof(r->h_counts),
+                                cudaMemcpyDeviceToHost, down);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&r->done_ev, cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaEventRecord(r->done_ev, down);
         r->final_launched = true;
